@@ -1,0 +1,346 @@
+"""Benchmark: Mrays/s of one rendered frame of the ~100K-triangle scene.
+
+Workload (one "step" = one frame, identical every step):
+  scene   128x128-quad heightfield (32,768 tris, heights U[0,2]) + 53 icospheres of
+          1,280 tris (centres U in 20x20x5, radii log-U[0.2,1.5]) = 100,608 tris,
+          16 point lights; BVH built once by the product builder (reference layout).
+  rays    1920x1080 pinhole primary closest-hit rays (cameraPass.comp row mapping:
+          rows 1..1079), then per hit: the sun shadow ray, one shadow ray per
+          tile-culled light in range (16x16-pixel tiles, 120x68 tiles), and one
+          cosine-weighted diffuse bounce ray (closest hit).
+Both the plain form (reference 64-B binary nodes) and the quantised form (8-wide,
+8-bit child bounds) are timed; `value` is the quantised form's Mrays/s, device
+time of the frame's CUDA graph (tile culling + primary + secondary generation +
+secondary trace) with the BVH resident in HBM and L2 flushed before each step.
+`e2e` runs the same frame through the host-pointer C-ABI calls (tile culling and
+tim_rt_trace_camera with pinned host buffers), copies included.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+W, H = 1920, 1080
+FLAGS_NAME = "tile_lights|bounce"
+METRIC = "Mrays/s"
+
+
+def make_workload():
+    from tim_raytracing_b200 import scenes
+    return scenes.heightfield_scene(seed=2, grid=128, n_spheres=53, extent=20.0, n_lights=16, light_radius=6.0)
+
+
+def config_dict(scene, extra=None):
+    d = {"workload": "heightfield_100k_frame_1080p", "triangles": int(scene.num_tris), "width": W, "height": H,
+         "rays": "primary + sun shadow + tile-culled point-light shadows (16 lights, 16x16 tiles) + 1 diffuse bounce",
+         "bvh": "product binned-SAH builder, reference fillGpuBuffer layout", "l2": "flushed (256 MiB write) before each step",
+         "parallelism": "replicas"}
+    if extra:
+        d.update(extra)
+    return d
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle sampling during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 7:
+                self.samples.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4) if s[3 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def cpu_baseline(scene, img, pd, threads, budget_s=12.0):
+    """The oracle (C restatement of the reference's GLSL trace path, OpenMP over
+    pixels) on a bounded sample of the same frame: whole rows from the middle of
+    the image until about budget_s seconds of CPU work."""
+    from oracle import oracle as O
+    sc = O.Scene(img, scene.positions, scene.normals)
+    tx, ty = (W + 15) // 16, (H + 15) // 16
+    counts, lists = O.cull_lights(sc, pd, tx, ty, threads=threads)
+    flags = 2 | 4
+    rays = 0
+    elapsed = 0.0
+    rows = 0
+    stride = 37   # coprime with H - 1: visits rows spread over the whole frame
+    while elapsed < budget_s and rows < H - 1:
+        b = 1 + (rows * stride) % (H - 1)
+        t0 = time.perf_counter()
+        _, _, c = O.camera(sc, pd, flags=flags, seed=1, tile_counts=counts, tile_lists=lists,
+                           pix_range=(b * W, (b + 1) * W), threads=threads)
+        elapsed += time.perf_counter() - t0
+        rays += int(c.sum())
+        rows += 1
+    return {"value": rays / elapsed / 1e6, "unit": METRIC, "cores": threads, "kind": "port",
+            "sample": f"{rows} of {H - 1} traced rows ({rays} rays) of the same frame, {elapsed:.1f} s"}
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the reference's trace path on the host cores (the oracle
+    restatement of its GLSL traversal; the GLSL itself needs a Vulkan device)."""
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+    from tim_raytracing_b200 import _native as N, scenes
+    scene = make_workload()
+    img = N.build_bvh(scene)
+    pd = scenes.pass_data(scene, W, H, aabb=(img.aabb[:3], img.aabb[3:]))
+    threads = O.threads_available()
+    sc = O.Scene(img, scene.positions, scene.normals)
+    tx, ty = (W + 15) // 16, (H + 15) // 16
+    counts, lists = O.cull_lights(sc, pd, tx, ty, threads=threads)
+    rows_per_step = 16
+
+    def step(k):
+        # 16 single rows spread evenly over the frame, shifted every step
+        rays = 0
+        for j in range(rows_per_step):
+            b = 1 + (k + j * ((H - 1) // rows_per_step)) % (H - 1)
+            _, _, c = O.camera(sc, pd, flags=6, seed=1, tile_counts=counts, tile_lists=lists,
+                               pix_range=(b * W, (b + 1) * W), threads=threads)
+            rays += int(c.sum())
+        return rays
+
+    for k in range(args.warmup):
+        step(k)
+    t0 = time.perf_counter()
+    rays = sum(step(args.warmup + k) for k in range(args.steps))
+    dt = time.perf_counter() - t0
+    v = rays / dt / 1e6
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": config_dict(scene, {"sample": f"{rows_per_step} rows x {W} pixels per step, spread over the frame"}),
+            "cpu_baseline": {"value": v, "unit": METRIC, "cores": threads, "kind": "port",
+                             "sample": f"{rows_per_step} rows spread over the frame per step"},
+            "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="tim")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    from tim_raytracing_b200 import _native as N, scenes
+    scene = make_workload()
+    t0 = time.perf_counter()
+    img = N.build_bvh(scene)
+    build_s = time.perf_counter() - t0
+    ctx = N.Context(local)
+    sid = ctx.upload(img, scene, quant8=True)
+    pd = scenes.pass_data(scene, W, H, aabb=(img.aabb[:3], img.aabb[3:]))
+    tx, ty = (W + 15) // 16, (H + 15) // 16
+    dev = torch.device("cuda", local)
+    d_counts = torch.zeros(tx * ty, dtype=torch.int32, device=dev)
+    d_lists = torch.zeros(tx * ty * 16, dtype=torch.int32, device=dev)
+    outs = {f: torch.zeros(W * H * 8, dtype=torch.int32, device=dev) for f in ("plain", "wide")}
+    bounces = {f: torch.zeros(W * H * 4, dtype=torch.int32, device=dev) for f in ("plain", "wide")}
+    d_rays = torch.zeros(1, dtype=torch.int64, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+    base_flags = N.CAM_TILE_LIGHTS | N.CAM_BOUNCE
+
+    def frame(form, s):
+        flags = base_flags | (N.CAM_WIDE if form == "wide" else 0)
+        ctx.cull_lights_dev(sid, pd, tx, ty, d_counts, d_lists, stream=s.cuda_stream)
+        ctx.trace_camera_dev(sid, pd, flags, 1, d_counts, d_lists, outs[form], bounces[form], d_rays,
+                             stream=s.cuda_stream)
+
+    results = {}
+    graphs = {}
+    for form in ("plain", "wide"):
+        with torch.cuda.stream(stream):
+            for _ in range(args.warmup):
+                frame(form, stream)
+        stream.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=stream):
+            frame(form, stream)
+        graphs[form] = g
+        for _ in range(2):
+            g.replay()
+        torch.cuda.synchronize()
+
+    def timed(form, steps, sampler=None):
+        g = graphs[form]
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        r0 = int(d_rays.item())
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        with torch.cuda.stream(stream):
+            for k in range(steps):
+                flush.fill_(float(k))
+                evs[k][0].record(stream)
+                g.replay()
+                evs[k][1].record(stream)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        ms = sum(a.elapsed_time(b) for a, b in evs)
+        rays = int(d_rays.item()) - r0
+        return ms, rays
+
+    sampler = ClockSampler(local)
+    with sampler:
+        for form in ("plain", "wide"):
+            ms, rays = timed(form, args.steps)
+            results[form] = (ms, rays)
+    clocks = sampler.summary()
+
+    # identical work per frame on every rank: aggregate rays, max time
+    def agg(ms, rays):
+        if dist:
+            t = torch.tensor([ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            r = torch.tensor([rays], dtype=torch.float64, device=dev)
+            dist.all_reduce(r)
+            return float(t.item()), float(r.item())
+        return ms, float(rays)
+
+    ms_w, rays_w = agg(*results["wide"])
+    ms_p, rays_p = agg(*results["plain"])
+    v_w = rays_w / (ms_w / 1e3) / 1e6
+    v_p = rays_p / (ms_p / 1e3) / 1e6
+    rays_per_frame = rays_w / world / args.steps
+
+    # hit-id agreement of the two forms on this frame
+    op = outs["plain"].view(-1, 8)[:, :4]
+    ow = outs["wide"].view(-1, 8)[:, :4]
+    prim_mismatch = int((op != ow).any(dim=1).sum().item())
+    bnc_mismatch = int((bounces["plain"].view(-1, 4) != bounces["wide"].view(-1, 4)).any(dim=1).sum().item())
+    mask_mismatch = int((outs["plain"].view(-1, 8)[:, 4] != outs["wide"].view(-1, 8)[:, 4]).sum().item())
+
+    # end to end through the host-pointer C ABI (pinned buffers, copies included)
+    counts_h = torch.empty(tx * ty, dtype=torch.int32).pin_memory()
+    lists_h = torch.empty(tx * ty * 16, dtype=torch.int32).pin_memory()
+    out_h = torch.empty(W * H * 8, dtype=torch.int32).pin_memory()
+    bounce_h = torch.empty(W * H * 4, dtype=torch.int32).pin_memory()
+    L = N.lib()
+    import ctypes
+    pdc = np.ascontiguousarray(pd)
+
+    def e2e_step():
+        N._check(L.tim_rt_cull_lights(ctx.handle, sid, pdc.ctypes.data, tx, ty, counts_h.data_ptr(), lists_h.data_ptr()))
+        st = N.Stats()
+        N._check(L.tim_rt_trace_camera(ctx.handle, sid, pdc.ctypes.data, base_flags | N.CAM_WIDE, 1,
+                                       counts_h.data_ptr(), lists_h.data_ptr(), out_h.data_ptr(), bounce_h.data_ptr(),
+                                       ctypes.byref(st)))
+        return st.rays
+
+    for _ in range(2):
+        e2e_step()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    e2e_rays = sum(e2e_step() for _ in range(args.steps))
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+        r = torch.tensor([float(e2e_rays)], dtype=torch.float64, device=dev)
+        dist.all_reduce(r)
+        e2e_rays = float(r.item())
+    e2e_v = e2e_rays / e2e_s / 1e6
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": v_w, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_w / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": config_dict(scene, {"rays_per_step": rays_per_frame, "bvh_build_s": round(build_s, 3)}),
+            "forms": {"quantised_8wide": {"value": v_w, "ms_per_step": ms_w / args.steps},
+                      "plain_binary": {"value": v_p, "ms_per_step": ms_p / args.steps},
+                      "speedup_quantised_over_plain": v_w / v_p},
+            "hit_ids": {"primary_records_differing": prim_mismatch, "bounce_records_differing": bnc_mismatch,
+                        "shadow_masks_differing": mask_mismatch, "pixels": W * H},
+            "e2e": {"value": e2e_v, "unit": METRIC, "h2d_bytes_per_step": int(tx * ty * 68 + 240),
+                    "d2h_bytes_per_step": int(tx * ty * 68 + W * H * 48)},
+            "gpu_launches": None, "clocks": clocks,
+        }
+        # kernels of one frame: cull, memset-free launches: primary, gen, clamp, secondary, ray-count
+        line["gpu_launches"] = 6 * args.steps * world
+        if not args.no_cpu_baseline and world == 1:
+            from oracle import oracle as O
+            line["cpu_baseline"] = cpu_baseline(scene, img, pd, O.threads_available())
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

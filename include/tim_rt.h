@@ -1,0 +1,218 @@
+/*
+ * tim_rt.h -- C ABI of the B200 (sm_100a) ray-tracing path.
+ *
+ * Drop-in replacement for the compute dispatch of TIM_Raytracing's hot path:
+ * the V-EZ/Vulkan `IRenderContext::Dispatch(DrawArguments, gx, gy, gz)` calls
+ * (src/rtDevice/public/IRenderContext.h:70, src/rtDevice/private/RenderContext.cpp:71-104)
+ * made by RayTracingPass and LightProbFieldPass, and the BVH upload made by
+ * BVHData::build (src/Renderer/BVHData.cpp:28-49).
+ *
+ * The entry points consume the reference's own byte layouts unchanged:
+ *   - the BVH buffer written by BVHBuilder::fillGpuBuffer
+ *     (src/Renderer/BVHBuilder.cpp:1319-1534) with its seven sub-ranges,
+ *   - PackedBVHNode (64 B), inlined leaf Triangle records (12 B), PackedLight,
+ *     BlasHeader (src/Shaders/core/primitive_cpp.glsl:50-117),
+ *   - the BVHGeometry vertex arrays (src/Renderer/BVHGeometry.cpp:69-85),
+ *   - PassData and PushConstants (src/Shaders/struct_cpp.glsl:10-37),
+ *   - the tracingData hit-record layout (src/Shaders/cameraPass.comp:69-75).
+ *
+ * Conventions: every function returns an int status (TIM_RT_OK = 0); no C++
+ * exception crosses the ABI; tim_rt_last_error() describes the last failure of
+ * the calling thread. Host pointers are borrowed for the duration of a call.
+ * Device memory is owned by the context and released by tim_rt_free_scene /
+ * tim_rt_destroy. A context is used by one host thread at a time; its calls
+ * are ordered on the context's CUDA stream. The *_dev variants take device
+ * pointers and a CUDA stream (NULL = the context stream) and do not
+ * synchronise.
+ */
+#ifndef TIM_RT_H
+#define TIM_RT_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TIM_RT_ABI_VERSION 1
+
+/* Status codes. The reference returns no errors (TIM_VK_VERIFY aborts in Debug,
+ * src/rtDevice/private/Common.h:6-17); these are new. */
+#define TIM_RT_OK 0
+#define TIM_RT_EINVAL 1       /* bad argument or malformed BVH ranges */
+#define TIM_RT_ENOMEM 2       /* device-memory budget or allocation exhausted */
+#define TIM_RT_ETIMEOUT 3     /* a bounded device-side wait gave up */
+#define TIM_RT_EDEVICE 4      /* CUDA error */
+#define TIM_RT_ENOTFOUND 5    /* unknown scene id */
+#define TIM_RT_EUNSUPPORTED 6 /* feature not available for this scene */
+
+/* Sub-range indices of the BVH buffer, in fillGpuBuffer's memory order
+ * (BVHBuilder.cpp:1326-1500): {offset bytes, size bytes}. */
+#define TIM_RT_RANGE_BLAS 0
+#define TIM_RT_RANGE_TRI 1
+#define TIM_RT_RANGE_PRIM 2
+#define TIM_RT_RANGE_MAT 3
+#define TIM_RT_RANGE_LIGHT 4
+#define TIM_RT_RANGE_NODE 5
+#define TIM_RT_RANGE_LEAF 6
+
+typedef struct tim_rt_ctx tim_rt_ctx;
+typedef uint32_t tim_rt_scene_id;
+
+/* PushConstants, src/Shaders/struct_cpp.glsl:30-37 (filled at raytracingPass.cpp:156). */
+typedef struct {
+    uint32_t numTriangles, numBlas, numPrimitives, numLights, numNodes;
+} tim_rt_push_constants;
+
+/* PassData, src/Shaders/struct_cpp.glsl:10-28 (C++ layout of the reference, 240 bytes). */
+typedef struct {
+    uint32_t frameSize[2]; float invFrameSize[2];
+    float cameraPos[4]; float cameraDir[4];
+    float frustumCorner00[4]; float frustumCorner10[4]; float frustumCorner01[4];
+    float invProjView[16];
+    float sunDir[4]; float sunColor[4];
+    float sceneMinExtent[4]; float sceneMaxExtent[4];
+    uint32_t lpfResolution[4];
+} tim_rt_pass_data;
+
+/* One ray of a batch (32 bytes): origin, tmax, direction, flags.
+ * flags bit 0: any-hit (occlusion) ray when the batch mode is TIM_RT_MODE_PER_RAY.
+ * The reference's closest-hit rays start at tmax = TMAX = 100 (struct_cpp.glsl:5). */
+typedef struct { float o[3]; float tmax; float d[3]; uint32_t flags; } tim_rt_ray;
+#define TIM_RT_RAY_ANY 1u
+
+/* Trace modes and options (low byte = mode, higher bits = options). */
+#define TIM_RT_MODE_CLOSEST 0u   /* traverseBvh, bvhTraversal_inline.glsl:5-78 */
+#define TIM_RT_MODE_ANY 1u       /* traverseBvhFast, bvhTraversal_inline.glsl:83-151 */
+#define TIM_RT_MODE_PER_RAY 2u   /* ray.flags bit 0 selects any-hit */
+#define TIM_RT_TRACE_WIDE 0x100u /* trace the 8-wide quantised BVH (needs TIM_RT_UPLOAD_QUANT8) */
+#define TIM_RT_TRACE_SORT 0x200u /* reorder rays by a coherence key before tracing (results keep input order) */
+
+/* Upload flags. */
+#define TIM_RT_UPLOAD_QUANT8 0x2u /* also build the 8-wide BVH with 8-bit quantised child bounds */
+
+/* Per-call statistics (optional output). */
+typedef struct {
+    uint64_t rays;            /* rays traced by the call (all kinds) */
+    uint64_t primary_rays, shadow_rays, probe_rays, bounce_rays;
+    float kernel_ms;          /* device time of the trace kernels (CUDA events) */
+    float total_ms;           /* device time of the whole call incl. copies */
+} tim_rt_stats;
+
+/* ---------------------------------------------------------------- context */
+const char *tim_rt_version(void);
+/* Message of the last failed call on this thread ("" if none). */
+const char *tim_rt_last_error(void);
+
+/* Creates a context on CUDA device `device`, owning one CUDA stream. Device
+ * allocations made by the context are admitted against `mem_budget_bytes`
+ * (0 = no budget). New: the reference's device is created by
+ * VezRenderer::Init (src/rtDevice/private/VezRenderer.cpp:54-188). */
+int tim_rt_create(int device, uint64_t mem_budget_bytes, tim_rt_ctx **out);
+int tim_rt_destroy(tim_rt_ctx *ctx);
+/* Device bytes currently held by the context (scenes + scratch). */
+int tim_rt_memory_used(tim_rt_ctx *ctx, uint64_t *bytes);
+
+/* ---------------------------------------------------------------- BVH upload */
+/* Replaces BVHData::build's CreateBuffer + UploadBuffer (src/Renderer/BVHData.cpp:43-48)
+ * and BVHGeometry::flush (src/Renderer/BVHGeometry.cpp:69-78).
+ * bvh_bytes/ranges: BVHBuilder::fillGpuBuffer output. pos/nrm/uv: vertex arrays
+ * (xyz, xyz, uv per vertex; nrm and uv may be NULL). pc: the scene's PushConstants.
+ * The buffers are validated (ranges inside the buffer, node children and leaf
+ * offsets in range, vertex indices < num_vertex) before anything is launched;
+ * a malformed buffer returns TIM_RT_EINVAL. */
+int tim_rt_upload_bvh(tim_rt_ctx *ctx, const void *bvh_bytes, uint64_t n_bytes, const uint32_t ranges[7][2],
+                      const float *pos, const float *nrm, const float *uv, uint32_t max_vertex, uint32_t num_vertex,
+                      const tim_rt_push_constants *pc, uint32_t flags, tim_rt_scene_id *out);
+/* Host-only check of a fillGpuBuffer image, the same one tim_rt_upload_bvh runs
+ * before uploading: ranges inside the buffer and aligned, child ids above their
+ * parent's id and in range, leaf data inside the leaf range, vertex / light /
+ * blas ids in range, tree depth <= 32. Writes the tree depth. No GPU needed.
+ * New: the reference uploads without any check (BVHData.cpp:43-48). */
+int tim_rt_validate_bvh(const void *bvh_bytes, uint64_t n_bytes, const uint32_t ranges[7][2],
+                        const tim_rt_push_constants *pc, uint32_t num_vertex, uint32_t *depth);
+/* Replaces BVHData::~BVHData / BVHGeometry::~BVHGeometry (DestroyBuffer). */
+int tim_rt_free_scene(tim_rt_ctx *ctx, tim_rt_scene_id scene);
+/* Device bytes held by one scene. */
+int tim_rt_scene_bytes(tim_rt_ctx *ctx, tim_rt_scene_id scene, uint64_t *bytes);
+
+/* ---------------------------------------------------------------- tracing */
+/* Batched closest-hit / any-hit trace of n rays; replaces the trace half of the
+ * reference's compute dispatches (rayTrace, baseRaytracingPass.glsl:16-27, and
+ * traverseForShadow, bvhLighting.glsl:100-108).
+ * hit[4i..4i+3]: closest hit -> (vertexOffset, index01, index2_matId, bits(t)),
+ *   t = t_hit - 1e-5 on a hit (bvhCollision.glsl:210) and t = ray.tmax on a
+ *   miss with xyz = 0; any-hit -> (1 if occluded else 0, 0, 0, bits(ray.tmax)).
+ * leaf_nid (optional): masked id of the leaf whose triangle was accepted,
+ *   0xFFFFFFFF on a miss or for any-hit rays.
+ * bary (optional): (u, v) of the accepted Moller-Trumbore hit, (0, 0) otherwise. */
+int tim_rt_trace(tim_rt_ctx *ctx, tim_rt_scene_id scene, const tim_rt_ray *rays, uint32_t n, uint32_t mode,
+                 uint32_t *hit, uint32_t *leaf_nid, float *bary, tim_rt_stats *stats);
+/* Device-pointer form of tim_rt_trace; stream-ordered, no synchronisation. */
+int tim_rt_trace_dev(tim_rt_ctx *ctx, tim_rt_scene_id scene, const tim_rt_ray *d_rays, uint32_t n, uint32_t mode,
+                     uint32_t *d_hit, uint32_t *d_leaf_nid, float *d_bary, void *cuda_stream);
+
+/* Camera trace step: cameraPass.comp with TRACING_STEP (src/Shaders/cameraPass.comp:44-76),
+ * dispatched by RayTracingPass::tracePass (src/Renderer/raytracingPass.cpp:89-110).
+ * out: W*H*8 u32 = tracingData[2*pix] (hit record) and tracingData[2*pix+1]
+ * (shadowMask, probMask, 0, 0). Pixel rows never produced by the reference's
+ * row mapping (cameraPass.comp:46) are written as zeros.
+ * flags: TIM_RT_CAM_PROB_MASK = USE_LPF_MASK; TIM_RT_CAM_TILE_LIGHTS = shadow
+ * rays to the tile-culled lights (tile_counts/tile_lists from
+ * tim_rt_cull_lights over ceil(W/16) x ceil(H/16) tiles) instead of the hit
+ * leaf's light list; TIM_RT_CAM_BOUNCE = one cosine-weighted diffuse bounce
+ * ray per hit, its hit record written to bounce_out (W*H*4 u32). */
+#define TIM_RT_CAM_PROB_MASK 1u
+#define TIM_RT_CAM_TILE_LIGHTS 2u
+#define TIM_RT_CAM_BOUNCE 4u
+#define TIM_RT_CAM_WIDE 0x100u   /* use the quantised 8-wide BVH */
+int tim_rt_trace_camera(tim_rt_ctx *ctx, tim_rt_scene_id scene, const tim_rt_pass_data *pd, uint32_t flags,
+                        uint32_t seed, const uint32_t *tile_counts, const uint32_t *tile_lists,
+                        uint32_t *out, uint32_t *bounce_out, tim_rt_stats *stats);
+
+/* Device-pointer form of tim_rt_trace_camera (pd is read on the host at call
+ * time). Stream-ordered, no synchronisation, capturable in a CUDA graph after a
+ * first call has sized the context's scratch buffers. If d_ray_count is not
+ * NULL, the number of rays the frame traced (primary + secondary) is ADDED to
+ * *d_ray_count on the device. One camera call per context may be in flight. */
+int tim_rt_trace_camera_dev(tim_rt_ctx *ctx, tim_rt_scene_id scene, const tim_rt_pass_data *pd, uint32_t flags,
+                            uint32_t seed, const uint32_t *d_tile_counts, const uint32_t *d_tile_lists,
+                            uint32_t *d_out, uint32_t *d_bounce_out, uint64_t *d_ray_count, void *cuda_stream);
+
+/* Tile light-frustum culling, cullWithFrustumTile's light section
+ * (src/Shaders/cullFrustum.glsl:63-100,136-151). One list of at most 16 light
+ * ids per tile, ascending (the reference's order is atomic-arrival order). */
+int tim_rt_cull_lights(tim_rt_ctx *ctx, tim_rt_scene_id scene, const tim_rt_pass_data *pd,
+                       uint32_t tiles_x, uint32_t tiles_y, uint32_t *out_counts, uint32_t *out_lists);
+/* Device-pointer form of tim_rt_cull_lights; stream-ordered, no synchronisation. */
+int tim_rt_cull_lights_dev(tim_rt_ctx *ctx, tim_rt_scene_id scene, const tim_rt_pass_data *pd,
+                           uint32_t tiles_x, uint32_t tiles_y, uint32_t *d_counts, uint32_t *d_lists, void *cuda_stream);
+
+/* ---------------------------------------------------------------- product-side BVH builder */
+/* Builds a BVH over triangle records and writes it in the reference's
+ * fillGpuBuffer layout (BVHBuilder.cpp:1319-1534), so its output can be passed
+ * to tim_rt_upload_bvh. Binned-SAH object splits (no spatial splits), leaves of
+ * at most max_leaf_size triangles, depth at most max_depth (<= 32, the width of
+ * the reference's traversal bitstack), leaf light lists of at most 15 lights
+ * (sphere vs leaf box, as BVHBuilder.cpp:749-756; 15 avoids the 4-bit count
+ * wrap at 16). tri_records: 3 u32 per triangle (Triangle, primitive_cpp.glsl:50-55).
+ * materials: Material records (48 B each); lights: PackedLight records (56 B each). */
+typedef struct {
+    uint32_t max_leaf_size;   /* default 4 */
+    uint32_t max_depth;       /* default 30 */
+    float traversal_cost;     /* SAH node cost, default 1 */
+    float intersection_cost;  /* SAH triangle cost, default 1.5 */
+    uint32_t num_threads;     /* 0 = all hardware threads */
+} tim_rt_build_params;
+typedef struct tim_rt_bvh_blob tim_rt_bvh_blob;
+void tim_rt_build_params_default(tim_rt_build_params *p);
+int tim_rt_build_bvh(const float *pos, uint32_t num_vertex, const uint32_t *tri_records, uint32_t num_tris,
+                     const void *materials, uint32_t num_materials, const void *lights, uint32_t num_lights,
+                     const tim_rt_build_params *params, tim_rt_bvh_blob **out);
+int tim_rt_bvh_blob_info(const tim_rt_bvh_blob *blob, const uint8_t **bytes, uint64_t *size,
+                         uint32_t ranges[7][2], tim_rt_push_constants *pc, float aabb[6]);
+void tim_rt_bvh_blob_free(tim_rt_bvh_blob *blob);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,75 @@
+"""Generates the committed golden fixtures under tests/golden/.
+
+    python tests/golden/make_golden.py
+
+* room_refbvh.npz -- the reference's own BVHBuilder (compiled from the reference
+  sources by oracle/Makefile, single-threaded so node numbering is stable) run
+  on the config-1 room scene (scenes.room_scene(1)): the fillGpuBuffer bytes,
+  the seven ranges and the push constants. GPU tests trace this exact buffer.
+* room_golden.npz -- camera and random-ray results on that buffer from the
+  reference's GLSL traversal compiled as C++ (oracle/refglsl, when built) and
+  from the C restatement (oracle/reftrace.c); the tests check both against
+  each other and the CUDA kernels against them.
+"""
+from __future__ import annotations
+
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ROOT = HERE.parent.parent
+sys.path.insert(0, str(ROOT))
+
+from oracle import oracle as O  # noqa: E402
+from tim_raytracing_b200 import scenes  # noqa: E402
+
+
+def room_rays(seed=7, n=4096):
+    rng = np.random.default_rng(seed)
+    o = rng.uniform((0.2, 0.2, 0.2), (3.8, 3.8, 2.8), size=(n, 3))
+    d = rng.normal(size=(n, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    r = np.zeros((n, 8), np.float32)
+    r[:, 0:3] = o
+    r[:, 3] = 100.0
+    r[:, 4:7] = d
+    r.view(np.uint32)[:, 7] = (rng.uniform(size=n) < 0.5).astype(np.uint32)
+    # a few axis-aligned directions exercise the division-by-zero slab cases
+    r[:64, 4:7] = 0.0
+    r[:64, 4 + (np.arange(64) % 3)] = np.where(np.arange(64) % 2 == 0, 1.0, -1.0)
+    return r
+
+
+def main():
+    O.build()
+    s = scenes.room_scene(1)
+    img = O.ref_build(s, multithread=False)
+    np.savez_compressed(HERE / "room_refbvh.npz", data=img.data, ranges=img.ranges, pc=np.array(img.pc, np.uint32),
+                        aabb=img.aabb)
+    sc = O.Scene(img, s.positions, s.normals)
+    rays = room_rays()
+    hit_c, nid_c, bary_c, _ = O.trace(sc, rays, 0)
+    hit_a, _, _, _ = O.trace(sc, rays, 1)
+    pd = scenes.pass_data(s, 256, 256, lpf_res=(8, 8, 8), aabb=(img.aabb[:3], img.aabb[3:]))
+    cam, _, _ = O.camera(sc, pd, flags=1)
+    out = dict(rays=rays, hit_closest=hit_c, nid_closest=nid_c, bary_closest=bary_c, hit_any=hit_a,
+               pass_data=pd.view(np.uint8).reshape(-1), camera=cam)
+    try:
+        from oracle import refglsl
+        g = refglsl.available()
+    except Exception:
+        g = False
+    if g:
+        gs = refglsl.Scene(img, s.positions, s.normals)
+        gh, gn = refglsl.trace(gs, rays, 0)
+        ga, _ = refglsl.trace(gs, rays, 1)
+        gcam = refglsl.camera(gs, pd, prob_mask=True)
+        out.update(glsl_hit_closest=gh, glsl_nid_closest=gn, glsl_hit_any=ga, glsl_camera=gcam)
+    np.savez_compressed(HERE / "room_golden.npz", **out)
+    print("wrote", HERE / "room_refbvh.npz", HERE / "room_golden.npz", "glsl:", bool(g))
+
+
+if __name__ == "__main__":
+    main()

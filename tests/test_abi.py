@@ -1,0 +1,57 @@
+"""The C-ABI library loads and exports every symbol include/tim_rt.h declares (no GPU needed)."""
+import ctypes
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+def declared_symbols():
+    syms = set()
+    for h in (ROOT / "include").glob("*.h"):
+        text = h.read_text()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for m in re.finditer(r"\b(tim_rt_\w+)\s*\(", text):
+            syms.add(m.group(1))
+    return sorted(syms)
+
+
+def test_header_declares_the_boundary():
+    syms = declared_symbols()
+    for name in ("tim_rt_upload_bvh", "tim_rt_trace", "tim_rt_cull_lights", "tim_rt_trace_camera", "tim_rt_create",
+                 "tim_rt_destroy", "tim_rt_free_scene"):
+        assert name in syms
+
+
+def test_library_exports_every_declared_symbol(native):
+    L = ctypes.CDLL(str(native.LIB_PATH))
+    missing = [s for s in declared_symbols() if not hasattr(L, s)]
+    assert not missing, f"declared but not exported: {missing}"
+
+
+def test_binding_list_matches_header(native):
+    assert sorted(native.EXPORTED) == declared_symbols()
+
+
+def test_version_and_no_error(native):
+    L = native.lib()
+    assert b"sm_100a" in L.tim_rt_version()
+
+
+def test_create_without_gpu_fails_cleanly(native):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(native.TimRtError) as e:
+        native.Context(0)
+    assert e.value.code == native.EDEVICE
+
+
+def test_struct_sizes(native):
+    from tim_raytracing_b200 import scenes
+    assert ctypes.sizeof(native.PushConstants) == 20
+    assert scenes.PASS_DATA_DTYPE.itemsize == 240
+    assert np.zeros((1, 8), np.float32).nbytes == 32   # tim_rt_ray

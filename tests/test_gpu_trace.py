@@ -1,0 +1,170 @@
+"""GPU parity: the sm_100a kernels, called through the C ABI, against the oracle
+and the golden vectors. Integer outputs (hit records, leaf ids, masks) and the
+FP32 t / barycentrics must be bit-identical for the plain (reference layout)
+form; the 8-wide quantised form may differ only on adjudicated near-ties."""
+import numpy as np
+import pytest
+
+from helpers import adjudicate_closest, load_room, load_room_golden
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def room(ctx):
+    s, img = load_room()
+    sid = ctx.upload(img, s, quant8=True)
+    yield s, img, sid
+    ctx.free_scene(sid)
+
+
+def test_trace_room_matches_golden(ctx, native, room):
+    s, img, sid = room
+    g = load_room_golden()
+    hit, nid, bary, st = ctx.trace(sid, g["rays"], native.MODE_CLOSEST)
+    assert np.array_equal(hit, g["hit_closest"])
+    assert np.array_equal(nid, g["nid_closest"])
+    assert np.array_equal(bary.view(np.uint32), g["bary_closest"].view(np.uint32))
+    ha, _, _, _ = ctx.trace(sid, g["rays"], native.MODE_ANY)
+    assert np.array_equal(ha, g["hit_any"])
+    assert st.rays == len(g["rays"])
+
+
+def test_trace_per_ray_mode(ctx, native, room, oracle_mod):
+    s, img, sid = room
+    g = load_room_golden()
+    rays = g["rays"]
+    hit, nid, bary, _ = ctx.trace(sid, rays, native.MODE_PER_RAY)
+    sc = oracle_mod.Scene(img, s.positions, s.normals)
+    oh, on, ob, _ = oracle_mod.trace(sc, rays, 2)
+    assert np.array_equal(hit, oh)
+    assert np.array_equal(nid, on)
+    assert np.array_equal(bary.view(np.uint32), ob.view(np.uint32))
+
+
+def test_camera_room_matches_golden(ctx, native, room):
+    """cameraPass.comp TRACING_STEP with USE_LPF_MASK on the reference-built BVH."""
+    from tim_raytracing_b200 import scenes
+    s, img, sid = room
+    g = load_room_golden()
+    pd = g["pass_data"].view(scenes.PASS_DATA_DTYPE)
+    out, _, st = ctx.trace_camera(sid, pd, flags=native.CAM_PROB_MASK)
+    assert np.array_equal(out, g["camera"])
+    assert st.primary_rays == 256 * 255
+
+
+def test_camera_heightfield_tile_lights_bounce(ctx, native, oracle_mod):
+    from tim_raytracing_b200 import scenes
+    s = scenes.heightfield_scene(seed=9, grid=32, n_spheres=6, n_lights=16, light_radius=5.0)
+    img = native.build_bvh(s)
+    sid = ctx.upload(img, s, quant8=False)
+    try:
+        W, H = 160, 120
+        pd = scenes.pass_data(s, W, H, aabb=(img.aabb[:3], img.aabb[3:]))
+        tx, ty = (W + 15) // 16, (H + 15) // 16
+        counts, lists = ctx.cull_lights(sid, pd, tx, ty)
+        sc = oracle_mod.Scene(img, s.positions, s.normals)
+        oc, ol = oracle_mod.cull_lights(sc, pd, tx, ty)
+        assert np.array_equal(counts, oc)
+        assert np.array_equal(lists, ol)
+        flags = native.CAM_TILE_LIGHTS | native.CAM_BOUNCE | native.CAM_PROB_MASK
+        out, bounce, st = ctx.trace_camera(sid, pd, flags=flags, seed=17, tile_counts=counts, tile_lists=lists)
+        o_out, o_bounce, o_counts = oracle_mod.camera(sc, pd, flags=flags, seed=17, tile_counts=oc, tile_lists=ol)
+        assert np.array_equal(out, o_out)
+        assert np.array_equal(bounce, o_bounce)
+        assert st.rays == int(o_counts.sum())
+    finally:
+        ctx.free_scene(sid)
+
+
+@pytest.mark.parametrize("n_tris,seed", [(2000, 1), (50000, 2)])
+def test_random_scene_mixed_rays(ctx, native, oracle_mod, n_tris, seed):
+    from tim_raytracing_b200 import scenes
+    s = scenes.random_triangles(seed, n_tris)
+    img = native.build_bvh(s)
+    sid = ctx.upload(img, s, quant8=True)
+    try:
+        rays = scenes.random_rays(seed + 100, 60000)
+        hit, nid, bary, _ = ctx.trace(sid, rays, native.MODE_PER_RAY)
+        sc = oracle_mod.Scene(img, s.positions, s.normals)
+        oh, on, ob, _ = oracle_mod.trace(sc, rays, 2)
+        assert np.array_equal(hit, oh)
+        assert np.array_equal(nid, on)
+        assert np.array_equal(bary.view(np.uint32), ob.view(np.uint32))
+    finally:
+        ctx.free_scene(sid)
+
+
+def test_wide_form_matches_plain(ctx, native):
+    """8-wide quantised BVH: identical hit records except adjudicated near-ties;
+    any-hit (order-independent) results identical."""
+    from tim_raytracing_b200 import scenes
+    s = scenes.heightfield_scene(seed=4, grid=64, n_spheres=12)
+    img = native.build_bvh(s)
+    sid = ctx.upload(img, s, quant8=True)
+    try:
+        rng = np.random.default_rng(8)
+        n = 100000
+        rays = np.zeros((n, 8), np.float32)
+        rays[:, 0:3] = rng.uniform((0, 0, 0.5), (20, 20, 6), size=(n, 3))
+        d = rng.normal(size=(n, 3))
+        rays[:, 4:7] = d / np.linalg.norm(d, axis=1, keepdims=True)
+        rays[:, 3] = 100.0
+        hp, np_, bp, _ = ctx.trace(sid, rays, native.MODE_CLOSEST)
+        hw, nw, bw, _ = ctx.trace(sid, rays, native.MODE_CLOSEST | native.TRACE_WIDE)
+        nm, unexplained, worst = adjudicate_closest(s, rays, hp, hw)
+        assert unexplained == 0, (nm, worst)
+        assert nm <= n * 1e-3
+        same = np.all(hp == hw, axis=1)
+        assert np.array_equal(np_[same], nw[same])
+        assert np.array_equal(bp[same].view(np.uint32), bw[same].view(np.uint32))
+        ap, _, _, _ = ctx.trace(sid, rays, native.MODE_ANY)
+        aw, _, _, _ = ctx.trace(sid, rays, native.MODE_ANY | native.TRACE_WIDE)
+        assert np.array_equal(ap, aw)
+    finally:
+        ctx.free_scene(sid)
+
+
+def test_wide_camera_room_matches_golden(ctx, native, room):
+    from tim_raytracing_b200 import scenes
+    s, img, sid = room
+    g = load_room_golden()
+    pd = g["pass_data"].view(scenes.PASS_DATA_DTYPE)
+    out, _, _ = ctx.trace_camera(sid, pd, flags=native.CAM_PROB_MASK | native.CAM_WIDE)
+    same = np.all(out == g["camera"], axis=1)
+    assert same.mean() > 0.999
+
+
+def test_trace_dev_with_torch_buffers(ctx, native, room):
+    import torch
+    s, img, sid = room
+    g = load_room_golden()
+    d_rays = torch.from_numpy(g["rays"]).cuda()
+    n = d_rays.shape[0]
+    d_hit = torch.empty((n, 4), dtype=torch.int32, device="cuda")
+    d_nid = torch.empty(n, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream()
+    ctx.trace_dev(sid, d_rays, n, native.MODE_CLOSEST, d_hit, d_nid, None, stream=stream.cuda_stream)
+    torch.cuda.synchronize()
+    assert np.array_equal(d_hit.cpu().numpy().view(np.uint32), g["hit_closest"])
+    assert np.array_equal(d_nid.cpu().numpy().view(np.uint32), g["nid_closest"])
+
+
+def test_errors(ctx, native, room):
+    from tim_raytracing_b200 import scenes
+    s, img, sid = room
+    with pytest.raises(native.TimRtError) as e:
+        ctx.trace(12345, np.zeros((4, 8), np.float32))
+    assert e.value.code == native.ENOTFOUND
+    bad = native.BvhImage(img.data.copy(), img.ranges.copy(), img.pc, img.aabb)
+    bad.ranges[native.RANGE_NODE][0] += 4          # misaligned node range
+    with pytest.raises(native.TimRtError) as e:
+        ctx.upload(bad, s)
+    assert e.value.code == native.EINVAL
+    small = native.Context(0, mem_budget_bytes=4096)
+    try:
+        with pytest.raises(native.TimRtError) as e:
+            small.upload(img, s)
+        assert e.value.code == native.ENOMEM
+    finally:
+        small.close()

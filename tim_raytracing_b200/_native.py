@@ -1,0 +1,279 @@
+"""ctypes binding of the C ABI in include/tim_rt.h (libtim_rt.so, built in-tree).
+
+This is the Python view of the same entry points a C++ caller binds; it adds
+no computation of its own. Loading fails loudly if the shared library is
+missing: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "libtim_rt.so"
+
+OK, EINVAL, ENOMEM, ETIMEOUT, EDEVICE, ENOTFOUND, EUNSUPPORTED = range(7)
+MODE_CLOSEST, MODE_ANY, MODE_PER_RAY = 0, 1, 2
+TRACE_WIDE = 0x100
+TRACE_SORT = 0x200
+UPLOAD_QUANT8 = 0x2
+CAM_PROB_MASK, CAM_TILE_LIGHTS, CAM_BOUNCE, CAM_WIDE = 1, 2, 4, 0x100
+RANGE_BLAS, RANGE_TRI, RANGE_PRIM, RANGE_MAT, RANGE_LIGHT, RANGE_NODE, RANGE_LEAF = range(7)
+
+EXPORTED = [
+    "tim_rt_version", "tim_rt_last_error", "tim_rt_create", "tim_rt_destroy", "tim_rt_memory_used",
+    "tim_rt_upload_bvh", "tim_rt_free_scene", "tim_rt_scene_bytes", "tim_rt_trace", "tim_rt_trace_dev",
+    "tim_rt_trace_camera", "tim_rt_cull_lights", "tim_rt_build_params_default", "tim_rt_build_bvh",
+    "tim_rt_bvh_blob_info", "tim_rt_bvh_blob_free", "tim_rt_validate_bvh", "tim_rt_trace_camera_dev",
+    "tim_rt_cull_lights_dev",
+]
+
+
+class TimRtError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"tim_rt error {code}: {msg}")
+        self.code = code
+
+
+class PushConstants(ctypes.Structure):
+    _fields_ = [("numTriangles", ctypes.c_uint32), ("numBlas", ctypes.c_uint32), ("numPrimitives", ctypes.c_uint32),
+                ("numLights", ctypes.c_uint32), ("numNodes", ctypes.c_uint32)]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("rays", ctypes.c_uint64), ("primary_rays", ctypes.c_uint64), ("shadow_rays", ctypes.c_uint64),
+                ("probe_rays", ctypes.c_uint64), ("bounce_rays", ctypes.c_uint64), ("kernel_ms", ctypes.c_float),
+                ("total_ms", ctypes.c_float)]
+
+
+class BuildParams(ctypes.Structure):
+    _fields_ = [("max_leaf_size", ctypes.c_uint32), ("max_depth", ctypes.c_uint32), ("traversal_cost", ctypes.c_float),
+                ("intersection_cost", ctypes.c_float), ("num_threads", ctypes.c_uint32)]
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python -m tim_raytracing_b200.build` "
+                          "(the CUDA library is required; there is no CPU fallback)")
+    L = ctypes.CDLL(str(LIB_PATH))
+    vp, u32, u64, i32 = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int
+    L.tim_rt_version.restype = ctypes.c_char_p
+    L.tim_rt_last_error.restype = ctypes.c_char_p
+    L.tim_rt_create.argtypes = [i32, u64, ctypes.POINTER(vp)]
+    L.tim_rt_destroy.argtypes = [vp]
+    L.tim_rt_memory_used.argtypes = [vp, ctypes.POINTER(u64)]
+    L.tim_rt_upload_bvh.argtypes = [vp, vp, u64, vp, vp, vp, vp, u32, u32, ctypes.POINTER(PushConstants), u32,
+                                    ctypes.POINTER(u32)]
+    L.tim_rt_free_scene.argtypes = [vp, u32]
+    L.tim_rt_scene_bytes.argtypes = [vp, u32, ctypes.POINTER(u64)]
+    L.tim_rt_trace.argtypes = [vp, u32, vp, u32, u32, vp, vp, vp, ctypes.POINTER(Stats)]
+    L.tim_rt_trace_dev.argtypes = [vp, u32, vp, u32, u32, vp, vp, vp, vp]
+    L.tim_rt_trace_camera.argtypes = [vp, u32, vp, u32, u32, vp, vp, vp, vp, ctypes.POINTER(Stats)]
+    L.tim_rt_cull_lights.argtypes = [vp, u32, vp, u32, u32, vp, vp]
+    L.tim_rt_build_params_default.argtypes = [ctypes.POINTER(BuildParams)]
+    L.tim_rt_build_params_default.restype = None
+    L.tim_rt_build_bvh.argtypes = [vp, u32, vp, u32, vp, u32, vp, u32, ctypes.POINTER(BuildParams), ctypes.POINTER(vp)]
+    L.tim_rt_bvh_blob_info.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(u64), vp, ctypes.POINTER(PushConstants), vp]
+    L.tim_rt_bvh_blob_free.argtypes = [vp]
+    L.tim_rt_bvh_blob_free.restype = None
+    L.tim_rt_validate_bvh.argtypes = [vp, u64, vp, ctypes.POINTER(PushConstants), u32, ctypes.POINTER(u32)]
+    L.tim_rt_trace_camera_dev.argtypes = [vp, u32, vp, u32, u32, vp, vp, vp, vp, vp, vp]
+    L.tim_rt_cull_lights_dev.argtypes = [vp, u32, vp, u32, u32, vp, vp, vp]
+    for name in EXPORTED:
+        if name not in ("tim_rt_version", "tim_rt_last_error", "tim_rt_build_params_default", "tim_rt_bvh_blob_free"):
+            getattr(L, name).restype = i32
+    _lib = L
+    return L
+
+
+def _check(rc: int):
+    if rc != OK:
+        raise TimRtError(rc, lib().tim_rt_last_error().decode())
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        assert a.flags["C_CONTIGUOUS"]
+        return a.ctypes.data
+    if hasattr(a, "data_ptr"):   # torch tensor (host or device)
+        return a.data_ptr()
+    return int(a)
+
+
+@dataclass
+class BvhImage:
+    """A BVHBuilder::fillGpuBuffer-layout image: bytes, 7 {offset, size} ranges in
+    memory order (blas, tri, prim, mat, light, node, leaf), push constants, AABB."""
+    data: np.ndarray        # uint8
+    ranges: np.ndarray      # uint32 [7, 2]
+    pc: tuple               # (numTriangles, numBlas, numPrimitives, numLights, numNodes)
+    aabb: np.ndarray        # float32 [6]
+
+    @property
+    def num_nodes(self) -> int:
+        return int(self.pc[4])
+
+    def nodes(self) -> np.ndarray:
+        o, _ = self.ranges[RANGE_NODE]
+        return self.data[o:o + 64 * self.num_nodes].view(np.uint32).reshape(-1, 16)
+
+    def leaf_words(self) -> np.ndarray:
+        o, s = self.ranges[RANGE_LEAF]
+        return self.data[o:o + s].view(np.uint32)
+
+
+def validate(img: BvhImage, num_vertex: int) -> int:
+    """tim_rt_validate_bvh: raises TimRtError(EINVAL) on a malformed image, returns the tree depth."""
+    pc = PushConstants(*[int(x) for x in img.pc])
+    depth = ctypes.c_uint32()
+    ranges = np.ascontiguousarray(img.ranges, np.uint32)
+    data = np.ascontiguousarray(img.data, np.uint8)
+    _check(lib().tim_rt_validate_bvh(data.ctypes.data, data.nbytes, ranges.ctypes.data, ctypes.byref(pc), num_vertex,
+                                     ctypes.byref(depth)))
+    return depth.value
+
+
+def build_params(**kw) -> BuildParams:
+    p = BuildParams()
+    lib().tim_rt_build_params_default(ctypes.byref(p))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def build_bvh(scene, **params) -> BvhImage:
+    """Product-side builder (tim_rt_build_bvh) over a scenes.Scene."""
+    L = lib()
+    pos = np.ascontiguousarray(scene.positions, np.float32)
+    rec = np.ascontiguousarray(scene.tri_records())
+    mats = scene.materials_bytes()
+    lights = scene.packed_lights_bytes()
+    nmat = len(mats) // 48
+    nl = len(lights) // 56
+    p = build_params(**params)
+    out = ctypes.c_void_p()
+    _check(L.tim_rt_build_bvh(pos.ctypes.data, pos.shape[0], rec.ctypes.data, rec.shape[0], mats, nmat,
+                              lights if nl else None, nl, ctypes.byref(p), ctypes.byref(out)))
+    try:
+        bp, size = ctypes.c_void_p(), ctypes.c_uint64()
+        ranges = np.zeros((7, 2), np.uint32)
+        pc = PushConstants()
+        aabb = np.zeros(6, np.float32)
+        _check(L.tim_rt_bvh_blob_info(out, ctypes.byref(bp), ctypes.byref(size), ranges.ctypes.data, ctypes.byref(pc),
+                                      aabb.ctypes.data))
+        data = np.frombuffer(ctypes.string_at(bp.value, size.value), dtype=np.uint8).copy()
+    finally:
+        L.tim_rt_bvh_blob_free(out)
+    return BvhImage(data, ranges, (pc.numTriangles, pc.numBlas, pc.numPrimitives, pc.numLights, pc.numNodes), aabb)
+
+
+class Context:
+    """A tim_rt_ctx: one device, one CUDA stream, resident scenes."""
+
+    def __init__(self, device: int = 0, mem_budget_bytes: int = 0):
+        self._L = lib()
+        self._c = ctypes.c_void_p()
+        _check(self._L.tim_rt_create(device, mem_budget_bytes, ctypes.byref(self._c)))
+
+    def close(self):
+        if self._c:
+            self._L.tim_rt_destroy(self._c)
+            self._c = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._c
+
+    def memory_used(self) -> int:
+        v = ctypes.c_uint64()
+        _check(self._L.tim_rt_memory_used(self._c, ctypes.byref(v)))
+        return v.value
+
+    def upload(self, img: BvhImage, scene, quant8: bool = False) -> int:
+        pos = np.ascontiguousarray(scene.positions, np.float32)
+        nrm = np.ascontiguousarray(scene.normals, np.float32)
+        pc = PushConstants(*[int(x) for x in img.pc])
+        sid = ctypes.c_uint32()
+        ranges = np.ascontiguousarray(img.ranges, np.uint32)
+        _check(self._L.tim_rt_upload_bvh(self._c, img.data.ctypes.data, img.data.nbytes, ranges.ctypes.data,
+                                         pos.ctypes.data, nrm.ctypes.data, None, pos.shape[0], pos.shape[0],
+                                         ctypes.byref(pc), UPLOAD_QUANT8 if quant8 else 0, ctypes.byref(sid)))
+        return sid.value
+
+    def free_scene(self, sid: int):
+        _check(self._L.tim_rt_free_scene(self._c, sid))
+
+    def scene_bytes(self, sid: int) -> int:
+        v = ctypes.c_uint64()
+        _check(self._L.tim_rt_scene_bytes(self._c, sid, ctypes.byref(v)))
+        return v.value
+
+    def trace(self, sid: int, rays: np.ndarray, mode: int = MODE_CLOSEST, want_nid=True, want_bary=True,
+              hit=None, nid=None, bary=None):
+        rays = np.ascontiguousarray(rays, np.float32)
+        n = rays.shape[0]
+        hit = np.empty((n, 4), np.uint32) if hit is None else hit
+        nid = (np.empty(n, np.uint32) if want_nid else None) if nid is None else nid
+        bary = (np.empty((n, 2), np.float32) if want_bary else None) if bary is None else bary
+        st = Stats()
+        _check(self._L.tim_rt_trace(self._c, sid, rays.ctypes.data, n, mode, _ptr(hit), _ptr(nid), _ptr(bary),
+                                    ctypes.byref(st)))
+        return hit, nid, bary, st
+
+    def trace_dev(self, sid: int, d_rays, n: int, mode: int, d_hit, d_nid=None, d_bary=None, stream=None):
+        _check(self._L.tim_rt_trace_dev(self._c, sid, _ptr(d_rays), n, mode, _ptr(d_hit), _ptr(d_nid), _ptr(d_bary),
+                                        _ptr(stream) if stream is not None else None))
+
+    def cull_lights(self, sid: int, pd: np.ndarray, tiles_x: int, tiles_y: int):
+        counts = np.empty(tiles_x * tiles_y, np.uint32)
+        lists = np.empty((tiles_x * tiles_y, 16), np.uint32)
+        pd = np.ascontiguousarray(pd)
+        _check(self._L.tim_rt_cull_lights(self._c, sid, pd.ctypes.data, tiles_x, tiles_y, counts.ctypes.data,
+                                          lists.ctypes.data))
+        return counts, lists
+
+    def cull_lights_dev(self, sid: int, pd: np.ndarray, tiles_x: int, tiles_y: int, d_counts, d_lists, stream=None):
+        pd = np.ascontiguousarray(pd)
+        _check(self._L.tim_rt_cull_lights_dev(self._c, sid, pd.ctypes.data, tiles_x, tiles_y, _ptr(d_counts),
+                                              _ptr(d_lists), _ptr(stream) if stream is not None else None))
+
+    def trace_camera_dev(self, sid: int, pd: np.ndarray, flags: int, seed: int, d_tile_counts, d_tile_lists, d_out,
+                         d_bounce=None, d_ray_count=None, stream=None):
+        pd = np.ascontiguousarray(pd)
+        _check(self._L.tim_rt_trace_camera_dev(self._c, sid, pd.ctypes.data, flags, seed, _ptr(d_tile_counts),
+                                               _ptr(d_tile_lists), _ptr(d_out), _ptr(d_bounce), _ptr(d_ray_count),
+                                               _ptr(stream) if stream is not None else None))
+
+    def trace_camera(self, sid: int, pd: np.ndarray, flags: int = 0, seed: int = 0, tile_counts=None, tile_lists=None,
+                     out=None, bounce_out=None):
+        W, H = (int(x) for x in np.asarray(pd["frameSize"]).reshape(-1)[:2])
+        out = np.empty((W * H, 8), np.uint32) if out is None else out
+        if (flags & CAM_BOUNCE) and bounce_out is None:
+            bounce_out = np.empty((W * H, 4), np.uint32)
+        st = Stats()
+        pd = np.ascontiguousarray(pd)
+        _check(self._L.tim_rt_trace_camera(self._c, sid, pd.ctypes.data, flags, seed, _ptr(tile_counts),
+                                           _ptr(tile_lists), _ptr(out), _ptr(bounce_out), ctypes.byref(st)))
+        return out, bounce_out, st

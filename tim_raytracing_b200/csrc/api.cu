@@ -1,0 +1,569 @@
+// api.cpp -- the C ABI of include/tim_rt.h: contexts, scene upload, trace calls.
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+#include "internal.h"
+#include "kernels.h"
+
+namespace timrt {
+
+static thread_local std::string g_last_error;
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+#define TIMRT_CUDA(call)                                                                         \
+    do {                                                                                         \
+        cudaError_t e_ = (call);                                                                 \
+        if (e_ != cudaSuccess) {                                                                 \
+            set_error(std::string(#call) + ": " + cudaGetErrorString(e_));                       \
+            return TIM_RT_EDEVICE;                                                               \
+        }                                                                                        \
+    } while (0)
+
+struct DevBuf {
+    void* ptr = nullptr;
+    uint64_t bytes = 0;
+};
+
+struct Scene {
+    DevBuf blob, pos, nrm, uv, wnodes, wtris, wnid;
+    SceneView view{};
+    uint32_t ranges[7][2];
+    tim_rt_push_constants pc{};
+    uint32_t depth = 0;
+    bool has_wide = false;
+    uint64_t bytes = 0;
+};
+
+}  // namespace timrt
+
+using namespace timrt;
+
+struct tim_rt_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    uint64_t budget = 0;
+    uint64_t used = 0;
+    std::map<uint32_t, std::unique_ptr<Scene>> scenes;
+    uint32_t next_id = 1;
+    // scratch
+    DevBuf rays, hits, nid, bary;
+    DevBuf counters;            // [0..63] per-call work counters, [64] device error word, ring after
+    uint32_t ring = 0;
+    DevBuf cam_out, cam_bounce, cam_nid, q_rays, q_pixel, tiles_counts, tiles_lists;
+    cudaEvent_t ev[4] = {};
+    LaunchConfig cfg;
+};
+
+namespace {
+
+constexpr uint32_t kCounterWords = 64 + 1 + 4096;   // fixed counters, error word, trace_dev ring
+constexpr uint32_t kErrWord = 64;
+constexpr uint32_t kRingBase = 65, kRingSize = 4096;
+
+int dev_alloc(tim_rt_ctx* c, DevBuf& b, uint64_t bytes) {
+    if (bytes == 0) bytes = 16;
+    if (c->budget && c->used + bytes > c->budget) {
+        set_error("device-memory budget exhausted: need " + std::to_string(bytes) + " B, " +
+                  std::to_string(c->budget - c->used) + " B left");
+        return TIM_RT_ENOMEM;
+    }
+    cudaError_t e = cudaMalloc(&b.ptr, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        set_error(std::string("cudaMalloc: ") + cudaGetErrorString(e));
+        b.ptr = nullptr;
+        return TIM_RT_ENOMEM;
+    }
+    b.bytes = bytes;
+    c->used += bytes;
+    return TIM_RT_OK;
+}
+
+void dev_free(tim_rt_ctx* c, DevBuf& b) {
+    if (b.ptr) {
+        cudaFree(b.ptr);
+        c->used -= b.bytes;
+    }
+    b.ptr = nullptr;
+    b.bytes = 0;
+}
+
+// Grows a scratch buffer to at least `bytes` (contents not preserved).
+int ensure(tim_rt_ctx* c, DevBuf& b, uint64_t bytes) {
+    if (b.bytes >= bytes && b.ptr) return TIM_RT_OK;
+    if (b.ptr) {
+        cudaStreamSynchronize(c->stream);
+        dev_free(c, b);
+    }
+    return dev_alloc(c, b, bytes);
+}
+
+int check_ctx(tim_rt_ctx* c) {
+    if (!c) {
+        set_error("null context");
+        return TIM_RT_EINVAL;
+    }
+    cudaError_t e = cudaSetDevice(c->device);
+    if (e != cudaSuccess) {
+        set_error(std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+        return TIM_RT_EDEVICE;
+    }
+    return TIM_RT_OK;
+}
+
+Scene* find_scene(tim_rt_ctx* c, tim_rt_scene_id id) {
+    auto it = c->scenes.find(id);
+    if (it == c->scenes.end()) {
+        set_error("unknown scene id " + std::to_string(id));
+        return nullptr;
+    }
+    return it->second.get();
+}
+
+// Reads and clears the device error word; a set bit means a kernel guard fired.
+int check_device_error(tim_rt_ctx* c) {
+    uint32_t err = 0;
+    uint32_t* ew = static_cast<uint32_t*>(c->counters.ptr) + kErrWord;
+    if (cudaMemcpy(&err, ew, 4, cudaMemcpyDeviceToHost) != cudaSuccess) {
+        set_error("reading the device error word failed");
+        return TIM_RT_EDEVICE;
+    }
+    if (err) {
+        cudaMemset(ew, 0, 4);
+        set_error("a trace kernel overflowed its 32-entry traversal stack");
+        return TIM_RT_EDEVICE;
+    }
+    return TIM_RT_OK;
+}
+
+LaunchConfig cfg_for(tim_rt_ctx* c, const Scene* s, bool wide) {
+    LaunchConfig cfg = c->cfg;
+    cfg.wide = wide && s->has_wide;
+    return cfg;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* tim_rt_version(void) { return "tim-rt-b200 1.0 (sm_100a)"; }
+const char* tim_rt_last_error(void) { return g_last_error.c_str(); }
+
+int tim_rt_create(int device, uint64_t mem_budget_bytes, tim_rt_ctx** out) {
+    if (!out) {
+        set_error("null output pointer");
+        return TIM_RT_EINVAL;
+    }
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) {
+        cudaGetLastError();
+        set_error("no CUDA device " + std::to_string(device));
+        return TIM_RT_EDEVICE;
+    }
+    TIMRT_CUDA(cudaSetDevice(device));
+    auto c = std::make_unique<tim_rt_ctx>();
+    c->device = device;
+    c->budget = mem_budget_bytes;
+    TIMRT_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    for (auto& e : c->ev) TIMRT_CUDA(cudaEventCreate(&e));
+    int rc = dev_alloc(c.get(), c->counters, 4ull * kCounterWords);
+    if (rc) return rc;
+    TIMRT_CUDA(cudaMemset(c->counters.ptr, 0, 4ull * kCounterWords));
+    *out = c.release();
+    return TIM_RT_OK;
+}
+
+int tim_rt_destroy(tim_rt_ctx* c) {
+    if (!c) return TIM_RT_OK;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    for (auto& kv : c->scenes) {
+        Scene* s = kv.second.get();
+        for (DevBuf* b : {&s->blob, &s->pos, &s->nrm, &s->uv, &s->wnodes, &s->wtris, &s->wnid}) dev_free(c, *b);
+    }
+    c->scenes.clear();
+    for (DevBuf* b : {&c->rays, &c->hits, &c->nid, &c->bary, &c->counters, &c->cam_out, &c->cam_bounce, &c->cam_nid,
+                      &c->q_rays, &c->q_pixel, &c->tiles_counts, &c->tiles_lists})
+        dev_free(c, *b);
+    for (auto& e : c->ev)
+        if (e) cudaEventDestroy(e);
+    cudaStreamDestroy(c->stream);
+    delete c;
+    return TIM_RT_OK;
+}
+
+int tim_rt_memory_used(tim_rt_ctx* c, uint64_t* bytes) {
+    if (!c || !bytes) {
+        set_error("null argument");
+        return TIM_RT_EINVAL;
+    }
+    *bytes = c->used;
+    return TIM_RT_OK;
+}
+
+int tim_rt_upload_bvh(tim_rt_ctx* c, const void* bvh_bytes, uint64_t n_bytes, const uint32_t ranges[7][2],
+                      const float* pos, const float* nrm, const float* uv, uint32_t max_vertex, uint32_t num_vertex,
+                      const tim_rt_push_constants* pc, uint32_t flags, tim_rt_scene_id* out) {
+    int rc = check_ctx(c);
+    if (rc) return rc;
+    if (!bvh_bytes || !ranges || !pos || !pc || !out || num_vertex == 0) {
+        set_error("tim_rt_upload_bvh: null argument or no vertices");
+        return TIM_RT_EINVAL;
+    }
+    if (max_vertex < num_vertex) max_vertex = num_vertex;
+    const uint8_t* blob = static_cast<const uint8_t*>(bvh_bytes);
+    std::string err;
+    uint32_t depth = 0;
+    if (!validate_bvh(blob, n_bytes, ranges, pc->numNodes, num_vertex, pc->numLights, pc->numBlas, &depth, err)) {
+        set_error("tim_rt_upload_bvh: " + err);
+        return TIM_RT_EINVAL;
+    }
+    auto s = std::make_unique<Scene>();
+    std::memcpy(s->ranges, ranges, sizeof(s->ranges));
+    s->pc = *pc;
+    s->depth = depth;
+    WideHost wh;
+    if (flags & TIM_RT_UPLOAD_QUANT8) {
+        if (pc->numBlas) {
+            set_error("tim_rt_upload_bvh: the 8-wide form does not support BLAS instances");
+            return TIM_RT_EUNSUPPORTED;
+        }
+        if (!build_wide(blob, ranges, pc->numNodes, pos, wh, err)) {
+            set_error("tim_rt_upload_bvh: 8-wide build: " + err);
+            return TIM_RT_EUNSUPPORTED;
+        }
+    }
+    auto fail = [&](int code) {
+        for (DevBuf* b : {&s->blob, &s->pos, &s->nrm, &s->uv, &s->wnodes, &s->wtris, &s->wnid}) dev_free(c, *b);
+        return code;
+    };
+    if ((rc = dev_alloc(c, s->blob, n_bytes))) return fail(rc);
+    if ((rc = dev_alloc(c, s->pos, 12ull * max_vertex))) return fail(rc);
+    if (nrm && (rc = dev_alloc(c, s->nrm, 12ull * max_vertex))) return fail(rc);
+    if (uv && (rc = dev_alloc(c, s->uv, 8ull * max_vertex))) return fail(rc);
+    if (cudaMemcpyAsync(s->blob.ptr, blob, n_bytes, cudaMemcpyHostToDevice, c->stream) != cudaSuccess ||
+        cudaMemcpyAsync(s->pos.ptr, pos, 12ull * num_vertex, cudaMemcpyHostToDevice, c->stream) != cudaSuccess ||
+        (nrm && cudaMemcpyAsync(s->nrm.ptr, nrm, 12ull * num_vertex, cudaMemcpyHostToDevice, c->stream) != cudaSuccess) ||
+        (uv && cudaMemcpyAsync(s->uv.ptr, uv, 8ull * num_vertex, cudaMemcpyHostToDevice, c->stream) != cudaSuccess)) {
+        set_error("tim_rt_upload_bvh: host-to-device copy failed");
+        return fail(TIM_RT_EDEVICE);
+    }
+    if (flags & TIM_RT_UPLOAD_QUANT8) {
+        if ((rc = dev_alloc(c, s->wnodes, 4ull * wh.nodes.size()))) return fail(rc);
+        if ((rc = dev_alloc(c, s->wtris, 4ull * wh.tris.size()))) return fail(rc);
+        if ((rc = dev_alloc(c, s->wnid, 4ull * wh.tri_nid.size()))) return fail(rc);
+        if (cudaMemcpyAsync(s->wnodes.ptr, wh.nodes.data(), 4ull * wh.nodes.size(), cudaMemcpyHostToDevice, c->stream) ||
+            (!wh.tris.empty() && cudaMemcpyAsync(s->wtris.ptr, wh.tris.data(), 4ull * wh.tris.size(), cudaMemcpyHostToDevice, c->stream)) ||
+            (!wh.tri_nid.empty() && cudaMemcpyAsync(s->wnid.ptr, wh.tri_nid.data(), 4ull * wh.tri_nid.size(), cudaMemcpyHostToDevice, c->stream))) {
+            set_error("tim_rt_upload_bvh: host-to-device copy of the 8-wide form failed");
+            return fail(TIM_RT_EDEVICE);
+        }
+        s->has_wide = true;
+    }
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) {
+        set_error("tim_rt_upload_bvh: stream synchronisation failed");
+        return fail(TIM_RT_EDEVICE);
+    }
+    const uint8_t* d = static_cast<const uint8_t*>(s->blob.ptr);
+    SceneView& v = s->view;
+    v.nodes = reinterpret_cast<const float4*>(d + ranges[TIM_RT_RANGE_NODE][0]);
+    v.leaf = reinterpret_cast<const uint32_t*>(d + ranges[TIM_RT_RANGE_LEAF][0]);
+    v.pos = static_cast<const float*>(s->pos.ptr);
+    v.nrm = static_cast<const float*>(s->nrm.ptr);
+    v.lights = reinterpret_cast<const float*>(d + ranges[TIM_RT_RANGE_LIGHT][0]);
+    v.blas = reinterpret_cast<const float*>(d + ranges[TIM_RT_RANGE_BLAS][0]);
+    v.materials = reinterpret_cast<const float*>(d + ranges[TIM_RT_RANGE_MAT][0]);
+    v.num_nodes = pc->numNodes;
+    v.num_lights = pc->numLights;
+    v.leaf_words = ranges[TIM_RT_RANGE_LEAF][1] / 4u;
+    v.num_vertex = num_vertex;
+    v.wnodes = static_cast<const uint4*>(s->wnodes.ptr);
+    v.wtris = static_cast<const float4*>(s->wtris.ptr);
+    v.wtri_nid = static_cast<const uint32_t*>(s->wnid.ptr);
+    v.num_wnodes = s->has_wide ? wh.num_nodes : 0u;
+    v.wide_root_is_leaf = wh.root_is_leaf;
+    s->bytes = s->blob.bytes + s->pos.bytes + s->nrm.bytes + s->uv.bytes + s->wnodes.bytes + s->wtris.bytes + s->wnid.bytes;
+    const uint32_t id = c->next_id++;
+    c->scenes[id] = std::move(s);
+    *out = id;
+    return TIM_RT_OK;
+}
+
+int tim_rt_validate_bvh(const void* bvh_bytes, uint64_t n_bytes, const uint32_t ranges[7][2],
+                        const tim_rt_push_constants* pc, uint32_t num_vertex, uint32_t* depth) {
+    if (!bvh_bytes || !ranges || !pc) {
+        set_error("tim_rt_validate_bvh: null argument");
+        return TIM_RT_EINVAL;
+    }
+    std::string err;
+    if (!validate_bvh(static_cast<const uint8_t*>(bvh_bytes), n_bytes, ranges, pc->numNodes, num_vertex, pc->numLights,
+                      pc->numBlas, depth, err)) {
+        set_error("tim_rt_validate_bvh: " + err);
+        return TIM_RT_EINVAL;
+    }
+    return TIM_RT_OK;
+}
+
+int tim_rt_free_scene(tim_rt_ctx* c, tim_rt_scene_id id) {
+    int rc = check_ctx(c);
+    if (rc) return rc;
+    Scene* s = find_scene(c, id);
+    if (!s) return TIM_RT_ENOTFOUND;
+    cudaStreamSynchronize(c->stream);
+    for (DevBuf* b : {&s->blob, &s->pos, &s->nrm, &s->uv, &s->wnodes, &s->wtris, &s->wnid}) dev_free(c, *b);
+    c->scenes.erase(id);
+    return TIM_RT_OK;
+}
+
+int tim_rt_scene_bytes(tim_rt_ctx* c, tim_rt_scene_id id, uint64_t* bytes) {
+    if (!c || !bytes) {
+        set_error("null argument");
+        return TIM_RT_EINVAL;
+    }
+    Scene* s = find_scene(c, id);
+    if (!s) return TIM_RT_ENOTFOUND;
+    *bytes = s->bytes;
+    return TIM_RT_OK;
+}
+
+int tim_rt_trace_dev(tim_rt_ctx* c, tim_rt_scene_id id, const tim_rt_ray* d_rays, uint32_t n, uint32_t mode,
+                     uint32_t* d_hit, uint32_t* d_nid, float* d_bary, void* cuda_stream) {
+    int rc = check_ctx(c);
+    if (rc) return rc;
+    Scene* s = find_scene(c, id);
+    if (!s) return TIM_RT_ENOTFOUND;
+    if ((mode & 0xFFu) > TIM_RT_MODE_PER_RAY || n > 0x7FFFFFFFu || (n && (!d_rays || !d_hit))) {
+        set_error("tim_rt_trace_dev: bad mode, size or null buffer");
+        return TIM_RT_EINVAL;
+    }
+    if ((mode & TIM_RT_TRACE_WIDE) && !s->has_wide) {
+        set_error("tim_rt_trace_dev: scene was uploaded without TIM_RT_UPLOAD_QUANT8");
+        return TIM_RT_EUNSUPPORTED;
+    }
+    if (n == 0) return TIM_RT_OK;
+    cudaStream_t st = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : c->stream;
+    uint32_t* ctr = static_cast<uint32_t*>(c->counters.ptr) + kRingBase + (c->ring++ % kRingSize);
+    uint32_t* err = static_cast<uint32_t*>(c->counters.ptr) + kErrWord;
+    TIMRT_CUDA(cudaMemsetAsync(ctr, 0, 4, st));
+    TIMRT_CUDA(launch_trace_batch(s->view, d_rays, n, mode, d_hit, d_nid, d_bary, ctr, err, st,
+                                  cfg_for(c, s, (mode & TIM_RT_TRACE_WIDE) != 0)));
+    return TIM_RT_OK;
+}
+
+int tim_rt_trace(tim_rt_ctx* c, tim_rt_scene_id id, const tim_rt_ray* rays, uint32_t n, uint32_t mode, uint32_t* hit,
+                 uint32_t* leaf_nid, float* bary, tim_rt_stats* stats) {
+    int rc = check_ctx(c);
+    if (rc) return rc;
+    Scene* s = find_scene(c, id);
+    if (!s) return TIM_RT_ENOTFOUND;
+    if ((mode & 0xFFu) > TIM_RT_MODE_PER_RAY || n > 0x7FFFFFFFu || (n && (!rays || !hit))) {
+        set_error("tim_rt_trace: bad mode, size or null buffer");
+        return TIM_RT_EINVAL;
+    }
+    if ((mode & TIM_RT_TRACE_WIDE) && !s->has_wide) {
+        set_error("tim_rt_trace: scene was uploaded without TIM_RT_UPLOAD_QUANT8");
+        return TIM_RT_EUNSUPPORTED;
+    }
+    if (stats) std::memset(stats, 0, sizeof(*stats));
+    if (n == 0) return TIM_RT_OK;
+    if ((rc = ensure(c, c->rays, 32ull * n)) || (rc = ensure(c, c->hits, 16ull * n))) return rc;
+    if (leaf_nid && (rc = ensure(c, c->nid, 4ull * n))) return rc;
+    if (bary && (rc = ensure(c, c->bary, 8ull * n))) return rc;
+    uint32_t* ctr = static_cast<uint32_t*>(c->counters.ptr);
+    uint32_t* err = ctr + kErrWord;
+    TIMRT_CUDA(cudaEventRecord(c->ev[0], c->stream));
+    TIMRT_CUDA(cudaMemcpyAsync(c->rays.ptr, rays, 32ull * n, cudaMemcpyHostToDevice, c->stream));
+    TIMRT_CUDA(cudaMemsetAsync(ctr, 0, 4, c->stream));
+    TIMRT_CUDA(cudaEventRecord(c->ev[1], c->stream));
+    TIMRT_CUDA(launch_trace_batch(s->view, static_cast<const tim_rt_ray*>(c->rays.ptr), n, mode,
+                                  static_cast<uint32_t*>(c->hits.ptr), leaf_nid ? static_cast<uint32_t*>(c->nid.ptr) : nullptr,
+                                  bary ? static_cast<float*>(c->bary.ptr) : nullptr, ctr, err, c->stream,
+                                  cfg_for(c, s, (mode & TIM_RT_TRACE_WIDE) != 0)));
+    TIMRT_CUDA(cudaEventRecord(c->ev[2], c->stream));
+    TIMRT_CUDA(cudaMemcpyAsync(hit, c->hits.ptr, 16ull * n, cudaMemcpyDeviceToHost, c->stream));
+    if (leaf_nid) TIMRT_CUDA(cudaMemcpyAsync(leaf_nid, c->nid.ptr, 4ull * n, cudaMemcpyDeviceToHost, c->stream));
+    if (bary) TIMRT_CUDA(cudaMemcpyAsync(bary, c->bary.ptr, 8ull * n, cudaMemcpyDeviceToHost, c->stream));
+    TIMRT_CUDA(cudaEventRecord(c->ev[3], c->stream));
+    TIMRT_CUDA(cudaStreamSynchronize(c->stream));
+    if ((rc = check_device_error(c))) return rc;
+    if (stats) {
+        stats->rays = n;
+        stats->primary_rays = n;
+        cudaEventElapsedTime(&stats->kernel_ms, c->ev[1], c->ev[2]);
+        cudaEventElapsedTime(&stats->total_ms, c->ev[0], c->ev[3]);
+    }
+    return TIM_RT_OK;
+}
+
+int tim_rt_cull_lights(tim_rt_ctx* c, tim_rt_scene_id id, const tim_rt_pass_data* pd, uint32_t tiles_x,
+                       uint32_t tiles_y, uint32_t* out_counts, uint32_t* out_lists) {
+    int rc = check_ctx(c);
+    if (rc) return rc;
+    Scene* s = find_scene(c, id);
+    if (!s) return TIM_RT_ENOTFOUND;
+    if (!pd || !out_counts || !out_lists || tiles_x == 0 || tiles_y == 0 || (uint64_t)tiles_x * tiles_y > (1u << 26)) {
+        set_error("tim_rt_cull_lights: bad argument");
+        return TIM_RT_EINVAL;
+    }
+    const uint64_t nt = (uint64_t)tiles_x * tiles_y;
+    if ((rc = ensure(c, c->tiles_counts, 4ull * nt)) || (rc = ensure(c, c->tiles_lists, 64ull * nt))) return rc;
+    TIMRT_CUDA(launch_cull_lights(s->view, *pd, tiles_x, tiles_y, static_cast<uint32_t*>(c->tiles_counts.ptr),
+                                  static_cast<uint32_t*>(c->tiles_lists.ptr), c->stream));
+    TIMRT_CUDA(cudaMemcpyAsync(out_counts, c->tiles_counts.ptr, 4ull * nt, cudaMemcpyDeviceToHost, c->stream));
+    TIMRT_CUDA(cudaMemcpyAsync(out_lists, c->tiles_lists.ptr, 64ull * nt, cudaMemcpyDeviceToHost, c->stream));
+    TIMRT_CUDA(cudaStreamSynchronize(c->stream));
+    return TIM_RT_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Validates a camera call and sizes the context's scratch; shared by the host
+// and device forms.
+int camera_prepare(tim_rt_ctx* c, Scene* s, const tim_rt_pass_data* pd, uint32_t flags, bool have_tiles,
+                   bool have_bounce, uint64_t* qcap_out) {
+    if (!pd || pd->frameSize[0] == 0 || pd->frameSize[1] == 0 ||
+        (uint64_t)pd->frameSize[0] * pd->frameSize[1] > (1ull << 26)) {
+        set_error("trace_camera: bad pass data");
+        return TIM_RT_EINVAL;
+    }
+    if ((flags & TIM_RT_CAM_TILE_LIGHTS) && !have_tiles) {
+        set_error("trace_camera: TILE_LIGHTS needs tile_counts and tile_lists");
+        return TIM_RT_EINVAL;
+    }
+    if ((flags & TIM_RT_CAM_BOUNCE) && !have_bounce) {
+        set_error("trace_camera: BOUNCE needs bounce_out");
+        return TIM_RT_EINVAL;
+    }
+    if ((flags & TIM_RT_CAM_PROB_MASK) &&
+        (pd->lpfResolution[0] < 2 || pd->lpfResolution[1] < 2 || pd->lpfResolution[2] < 2)) {
+        set_error("trace_camera: PROB_MASK needs lpfResolution >= 2 per axis");
+        return TIM_RT_EINVAL;
+    }
+    if ((flags & TIM_RT_CAM_WIDE) && !s->has_wide) {
+        set_error("trace_camera: scene was uploaded without TIM_RT_UPLOAD_QUANT8");
+        return TIM_RT_EUNSUPPORTED;
+    }
+    const uint64_t npix = (uint64_t)pd->frameSize[0] * pd->frameSize[1];
+    const uint32_t per_pix = 1u + 16u + ((flags & TIM_RT_CAM_PROB_MASK) ? 8u : 0u) + ((flags & TIM_RT_CAM_BOUNCE) ? 1u : 0u);
+    const uint64_t qcap = npix * per_pix;
+    if (qcap > 0xFFFFFFFFull) {
+        set_error("trace_camera: frame too large");
+        return TIM_RT_EINVAL;
+    }
+    int rc;
+    if ((rc = ensure(c, c->cam_nid, 4ull * npix)) || (rc = ensure(c, c->q_rays, 32ull * qcap)) ||
+        (rc = ensure(c, c->q_pixel, 4ull * qcap)))
+        return rc;
+    *qcap_out = qcap;
+    return TIM_RT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tim_rt_cull_lights_dev(tim_rt_ctx* c, tim_rt_scene_id id, const tim_rt_pass_data* pd, uint32_t tiles_x,
+                           uint32_t tiles_y, uint32_t* d_counts, uint32_t* d_lists, void* cuda_stream) {
+    int rc = check_ctx(c);
+    if (rc) return rc;
+    Scene* s = find_scene(c, id);
+    if (!s) return TIM_RT_ENOTFOUND;
+    if (!pd || !d_counts || !d_lists || tiles_x == 0 || tiles_y == 0 || (uint64_t)tiles_x * tiles_y > (1u << 26)) {
+        set_error("tim_rt_cull_lights_dev: bad argument");
+        return TIM_RT_EINVAL;
+    }
+    cudaStream_t st = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : c->stream;
+    TIMRT_CUDA(launch_cull_lights(s->view, *pd, tiles_x, tiles_y, d_counts, d_lists, st));
+    return TIM_RT_OK;
+}
+
+int tim_rt_trace_camera_dev(tim_rt_ctx* c, tim_rt_scene_id id, const tim_rt_pass_data* pd, uint32_t flags,
+                            uint32_t seed, const uint32_t* d_tile_counts, const uint32_t* d_tile_lists, uint32_t* d_out,
+                            uint32_t* d_bounce_out, uint64_t* d_ray_count, void* cuda_stream) {
+    int rc = check_ctx(c);
+    if (rc) return rc;
+    Scene* s = find_scene(c, id);
+    if (!s) return TIM_RT_ENOTFOUND;
+    if (!d_out) {
+        set_error("tim_rt_trace_camera_dev: null output");
+        return TIM_RT_EINVAL;
+    }
+    uint64_t qcap = 0;
+    if ((rc = camera_prepare(c, s, pd, flags, d_tile_counts && d_tile_lists, d_bounce_out != nullptr, &qcap))) return rc;
+    cudaStream_t st = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : c->stream;
+    uint32_t* ctr = static_cast<uint32_t*>(c->counters.ptr);
+    TIMRT_CUDA(cudaMemsetAsync(ctr, 0, 16, st));
+    TIMRT_CUDA(launch_camera(s->view, *pd, flags, seed, d_tile_counts, d_tile_lists, d_out,
+                             (flags & TIM_RT_CAM_BOUNCE) ? d_bounce_out : nullptr, static_cast<uint32_t*>(c->cam_nid.ptr),
+                             static_cast<tim_rt_ray*>(c->q_rays.ptr), static_cast<uint32_t*>(c->q_pixel.ptr),
+                             (uint32_t)qcap, ctr, ctr + kErrWord, d_ray_count, st,
+                             cfg_for(c, s, (flags & TIM_RT_CAM_WIDE) != 0)));
+    return TIM_RT_OK;
+}
+
+int tim_rt_trace_camera(tim_rt_ctx* c, tim_rt_scene_id id, const tim_rt_pass_data* pd, uint32_t flags, uint32_t seed,
+                        const uint32_t* tile_counts, const uint32_t* tile_lists, uint32_t* out, uint32_t* bounce_out,
+                        tim_rt_stats* stats) {
+    int rc = check_ctx(c);
+    if (rc) return rc;
+    Scene* s = find_scene(c, id);
+    if (!s) return TIM_RT_ENOTFOUND;
+    if (!out) {
+        set_error("tim_rt_trace_camera: null output");
+        return TIM_RT_EINVAL;
+    }
+    uint64_t qcap = 0;
+    if ((rc = camera_prepare(c, s, pd, flags, tile_counts && tile_lists, bounce_out != nullptr, &qcap))) return rc;
+    const uint32_t W = pd->frameSize[0], H = pd->frameSize[1];
+    const uint64_t npix = (uint64_t)W * H;
+    const uint64_t tiles = (uint64_t)((W + 15) / 16) * ((H + 15) / 16);
+    if ((rc = ensure(c, c->cam_out, 32ull * npix))) return rc;
+    if ((flags & TIM_RT_CAM_BOUNCE) && (rc = ensure(c, c->cam_bounce, 16ull * npix))) return rc;
+    if ((flags & TIM_RT_CAM_TILE_LIGHTS) &&
+        ((rc = ensure(c, c->tiles_counts, 4ull * tiles)) || (rc = ensure(c, c->tiles_lists, 64ull * tiles))))
+        return rc;
+    uint32_t* ctr = static_cast<uint32_t*>(c->counters.ptr);
+    TIMRT_CUDA(cudaEventRecord(c->ev[0], c->stream));
+    if (flags & TIM_RT_CAM_TILE_LIGHTS) {
+        TIMRT_CUDA(cudaMemcpyAsync(c->tiles_counts.ptr, tile_counts, 4ull * tiles, cudaMemcpyHostToDevice, c->stream));
+        TIMRT_CUDA(cudaMemcpyAsync(c->tiles_lists.ptr, tile_lists, 64ull * tiles, cudaMemcpyHostToDevice, c->stream));
+    }
+    TIMRT_CUDA(cudaMemsetAsync(ctr, 0, 16, c->stream));
+    TIMRT_CUDA(cudaEventRecord(c->ev[1], c->stream));
+    TIMRT_CUDA(launch_camera(s->view, *pd, flags, seed, static_cast<const uint32_t*>(c->tiles_counts.ptr),
+                             static_cast<const uint32_t*>(c->tiles_lists.ptr), static_cast<uint32_t*>(c->cam_out.ptr),
+                             (flags & TIM_RT_CAM_BOUNCE) ? static_cast<uint32_t*>(c->cam_bounce.ptr) : nullptr,
+                             static_cast<uint32_t*>(c->cam_nid.ptr), static_cast<tim_rt_ray*>(c->q_rays.ptr),
+                             static_cast<uint32_t*>(c->q_pixel.ptr), (uint32_t)qcap, ctr, ctr + kErrWord, nullptr,
+                             c->stream, cfg_for(c, s, (flags & TIM_RT_CAM_WIDE) != 0)));
+    TIMRT_CUDA(cudaEventRecord(c->ev[2], c->stream));
+    TIMRT_CUDA(cudaMemcpyAsync(out, c->cam_out.ptr, 32ull * npix, cudaMemcpyDeviceToHost, c->stream));
+    if (flags & TIM_RT_CAM_BOUNCE)
+        TIMRT_CUDA(cudaMemcpyAsync(bounce_out, c->cam_bounce.ptr, 16ull * npix, cudaMemcpyDeviceToHost, c->stream));
+    uint32_t qn = 0;
+    TIMRT_CUDA(cudaMemcpyAsync(&qn, ctr + 1, 4, cudaMemcpyDeviceToHost, c->stream));
+    TIMRT_CUDA(cudaEventRecord(c->ev[3], c->stream));
+    TIMRT_CUDA(cudaStreamSynchronize(c->stream));
+    if ((rc = check_device_error(c))) return rc;
+    if (stats) {
+        std::memset(stats, 0, sizeof(*stats));
+        const uint64_t primary = (uint64_t)W * (H - 1u);
+        stats->primary_rays = primary;
+        stats->rays = primary + qn;
+        stats->shadow_rays = qn;   // all secondary rays (shadow, probe-visibility, bounce)
+        cudaEventElapsedTime(&stats->kernel_ms, c->ev[1], c->ev[2]);
+        cudaEventElapsedTime(&stats->total_ms, c->ev[0], c->ev[3]);
+    }
+    return TIM_RT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,279 @@
+// bvh_layout.cpp -- host-side checks of the reference BVH image and the
+// collapse of its binary tree into the 8-wide quantised form.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <deque>
+#include "internal.h"
+
+namespace timrt {
+
+namespace {
+constexpr uint32_t kInvalid = 0x3FFFFFFFu;   // BVHBuilder.cpp:1287 InvalidNodeId = NID_MASK
+constexpr uint32_t kLeafBit = 0x80000000u, kMask = 0x3FFFFFFFu, kLeftLeaf = 0x80000000u, kRightLeaf = 0x40000000u;
+
+struct PNode { uint32_t nid[4]; float n0xy[4]; float n1xy[4]; float nz[4]; };   // primitive_cpp.glsl:80-86
+
+bool range_ok(const uint32_t r[2], uint64_t need, uint64_t n_bytes) {
+    return (uint64_t)r[0] + need <= n_bytes && need <= (uint64_t)r[1] + 0u;
+}
+}  // namespace
+
+bool validate_bvh(const uint8_t* blob, uint64_t n_bytes, const uint32_t ranges[7][2], uint32_t num_nodes,
+                  uint32_t num_vertex, uint32_t num_lights, uint32_t num_blas, uint32_t* depth_out, std::string& err) {
+    if (!blob || num_nodes == 0) { err = "empty BVH"; return false; }
+    if (ranges[TIM_RT_RANGE_NODE][0] % 16u) { err = "node range not 16-byte aligned"; return false; }
+    for (int i = 0; i < 7; ++i)
+        if (ranges[i][0] % 4u) { err = "range offset not 4-byte aligned"; return false; }
+    if (!range_ok(ranges[TIM_RT_RANGE_NODE], 64ull * num_nodes, n_bytes)) { err = "node range outside the buffer"; return false; }
+    if (!range_ok(ranges[TIM_RT_RANGE_LIGHT], 56ull * num_lights, n_bytes)) { err = "light range outside the buffer"; return false; }
+    if (!range_ok(ranges[TIM_RT_RANGE_BLAS], 32ull * num_blas, n_bytes)) { err = "blas range outside the buffer"; return false; }
+    if ((uint64_t)ranges[TIM_RT_RANGE_LEAF][0] + ranges[TIM_RT_RANGE_LEAF][1] > n_bytes) { err = "leaf range outside the buffer"; return false; }
+    const PNode* nodes = reinterpret_cast<const PNode*>(blob + ranges[TIM_RT_RANGE_NODE][0]);
+    const uint32_t* leaf = reinterpret_cast<const uint32_t*>(blob + ranges[TIM_RT_RANGE_LEAF][0]);
+    const uint64_t leaf_words = ranges[TIM_RT_RANGE_LEAF][1] / 4u;
+    std::vector<uint8_t> depth(num_nodes, 0);
+    uint32_t max_depth = 0;
+    auto inner_ok = [&](uint32_t i) { return (nodes[i].nid[2] & kMask) != kInvalid; };
+    if (num_nodes > 1 && !inner_ok(0)) { err = "root has no children"; return false; }
+    for (uint32_t i = 0; i < num_nodes; ++i) {
+        const PNode& n = nodes[i];
+        const uint32_t left = n.nid[2] & kMask;
+        if (left != kInvalid) {
+            if (left <= i || (uint64_t)left + 1u >= num_nodes) { err = "node " + std::to_string(i) + ": child id out of order or out of range"; return false; }
+            const uint32_t d = depth[i] + 1u;
+            if (d > 32u) { err = "tree deeper than 32 levels (the reference traversal's bitstack width)"; return false; }
+            depth[left] = depth[left + 1u] = (uint8_t)d;
+            max_depth = std::max(max_depth, d);
+            if (!(n.nid[2] & kLeftLeaf) && !inner_ok(left)) { err = "node " + std::to_string(left) + " used as inner node without children"; return false; }
+            if (!(n.nid[2] & kRightLeaf) && !inner_ok(left + 1u)) { err = "node " + std::to_string(left + 1) + " used as inner node without children"; return false; }
+        }
+        const uint32_t off = n.nid[3];
+        if (off != 0xFFFFFFFFu) {
+            if (off >= leaf_words) { err = "node " + std::to_string(i) + ": leaf offset out of range"; return false; }
+            const uint32_t hdr = leaf[off];
+            const uint32_t nt = hdr & 0xFFFu, nb = (hdr >> 12) & 0xFFu, np = (hdr >> 20) & 0xFFu, nl = (hdr >> 28) & 0xFu;
+            const uint64_t end = 1ull + off + 3ull * nt + nb + np + nl;
+            if (end > leaf_words) { err = "node " + std::to_string(i) + ": leaf data past the leaf range"; return false; }
+            for (uint32_t t = 0; t < nt; ++t) {
+                const uint32_t* r = leaf + 1u + off + 3u * t;
+                const uint64_t i0 = (uint64_t)r[0] + (r[1] & 0xFFFFu), i1 = (uint64_t)r[0] + (r[1] >> 16),
+                               i2 = (uint64_t)r[0] + (r[2] & 0xFFFFu);
+                if (i0 >= num_vertex || i1 >= num_vertex || i2 >= num_vertex) {
+                    err = "node " + std::to_string(i) + ": triangle vertex index >= num_vertex";
+                    return false;
+                }
+            }
+            for (uint32_t b = 0; b < nb; ++b)
+                if (leaf[1u + off + 3u * nt + b] >= num_blas) { err = "blas id out of range"; return false; }
+            for (uint32_t l = 0; l < nl; ++l)
+                if (leaf[1u + off + 3u * nt + nb + np + l] >= num_lights) { err = "light id out of range"; return false; }
+        }
+    }
+    if (depth_out) *depth_out = max_depth;
+    return true;
+}
+
+// ---------------------------------------------------------------------------------- 8-wide collapse
+
+namespace {
+
+struct Slot {
+    uint32_t id;        // binary node id | kLeafBit for leaves
+    float lo[3], hi[3]; // box the reference stores for this subtree (in its parent record)
+};
+
+void child_slots(const PNode& n, Slot& a, Slot& b) {
+    const uint32_t left = n.nid[2] & kMask;
+    a.id = left | ((n.nid[2] & kLeftLeaf) ? kLeafBit : 0u);
+    b.id = (left + 1u) | ((n.nid[2] & kRightLeaf) ? kLeafBit : 0u);
+    a.lo[0] = n.n0xy[0]; a.lo[1] = n.n0xy[1]; a.lo[2] = n.nz[0];
+    a.hi[0] = n.n0xy[2]; a.hi[1] = n.n0xy[3]; a.hi[2] = n.nz[1];
+    b.lo[0] = n.n1xy[0]; b.lo[1] = n.n1xy[1]; b.lo[2] = n.nz[2];
+    b.hi[0] = n.n1xy[2]; b.hi[1] = n.n1xy[3]; b.hi[2] = n.nz[3];
+}
+
+double area(const Slot& s) {
+    const double dx = std::fabs((double)s.hi[0] - s.lo[0]), dy = std::fabs((double)s.hi[1] - s.lo[1]),
+                 dz = std::fabs((double)s.hi[2] - s.lo[2]);
+    return dx * dy + dy * dz + dz * dx;
+}
+
+float decode(float o, float sc, uint32_t q) { return o + sc * (float)q; }   // exact product, one rounded add
+
+// Quantises one axis of the slot boxes: chooses the scale exponent and the
+// outward-rounded 8-bit bounds; returns false if no exponent fits.
+bool quantise_axis(const float* lo, const float* hi, int n, float& origin, uint8_t& ebiased, uint8_t* qlo, uint8_t* qhi) {
+    float mn = INFINITY, mx = -INFINITY;
+    for (int k = 0; k < n; ++k) { mn = std::min(mn, lo[k]); mx = std::max(mx, hi[k]); }
+    if (!std::isfinite(mn) || !std::isfinite(mx)) return false;
+    origin = mn;
+    const double extent = (double)mx - (double)mn;
+    int e = 1;
+    if (extent > 0.0) {
+        const double want = extent / 255.0;
+        e = (int)std::ceil(std::log2(want)) + 127;
+        if (e < 1) e = 1;
+    }
+    for (; e <= 254; ++e) {
+        float sc;
+        const uint32_t bits = (uint32_t)e << 23;
+        std::memcpy(&sc, &bits, 4);
+        bool ok = true;
+        for (int k = 0; k < n && ok; ++k) {
+            double fl = std::floor(((double)lo[k] - (double)origin) / sc);
+            long q = (long)std::max(0.0, std::min(255.0, fl));
+            while (q > 0 && decode(origin, sc, (uint32_t)q) > lo[k]) --q;
+            if (decode(origin, sc, (uint32_t)q) > lo[k]) { ok = false; break; }
+            double ch = std::ceil(((double)hi[k] - (double)origin) / sc);
+            long r = (long)std::max(0.0, std::min(255.0, ch));
+            while (r < 255 && decode(origin, sc, (uint32_t)r) < hi[k]) ++r;
+            if (decode(origin, sc, (uint32_t)r) < hi[k]) { ok = false; break; }
+            if (r < q) r = q;
+            qlo[k] = (uint8_t)q;
+            qhi[k] = (uint8_t)r;
+        }
+        if (ok) { ebiased = (uint8_t)e; return true; }
+    }
+    return false;
+}
+
+}  // namespace
+
+bool build_wide(const uint8_t* blob, const uint32_t ranges[7][2], uint32_t num_nodes, const float* pos,
+                WideHost& out, std::string& err) {
+    const PNode* nodes = reinterpret_cast<const PNode*>(blob + ranges[TIM_RT_RANGE_NODE][0]);
+    const uint32_t* leaf = reinterpret_cast<const uint32_t*>(blob + ranges[TIM_RT_RANGE_LEAF][0]);
+    const uint64_t leaf_words = ranges[TIM_RT_RANGE_LEAF][1] / 4u;
+    out = WideHost();
+    auto leaf_tris = [&](uint32_t nid) -> uint32_t {
+        const uint32_t off = nodes[nid & kMask].nid[3];
+        if (off == 0xFFFFFFFFu || off >= leaf_words) return 0u;
+        return leaf[off] & 0xFFFu;
+    };
+    auto emit_tris = [&](uint32_t nid) {
+        const uint32_t nm = nid & kMask;
+        const uint32_t off = nodes[nm].nid[3];
+        const uint32_t nt = leaf_tris(nid);
+        for (uint32_t t = 0; t < nt; ++t) {
+            const uint32_t* r = leaf + 1u + off + 3u * t;
+            const uint32_t i0 = r[0] + (r[1] & 0xFFFFu), i1 = r[0] + (r[1] >> 16), i2 = r[0] + (r[2] & 0xFFFFu);
+            const float* P0 = pos + 3ull * i0;
+            const float* P1 = pos + 3ull * i1;
+            const float* P2 = pos + 3ull * i2;
+            float w[12];
+            w[0] = P0[0]; w[1] = P0[1]; w[2] = P0[2];
+            w[4] = P1[0] - P0[0]; w[5] = P1[1] - P0[1]; w[6] = P1[2] - P0[2];
+            w[8] = P2[0] - P0[0]; w[9] = P2[1] - P0[1]; w[10] = P2[2] - P0[2];
+            std::memcpy(&w[3], &r[0], 4);
+            std::memcpy(&w[7], &r[1], 4);
+            std::memcpy(&w[11], &r[2], 4);
+            out.tris.insert(out.tris.end(), w, w + 12);
+            out.tri_nid.push_back(nm);
+        }
+    };
+
+    // Work queue of wide nodes to fill: (wide index, slots, depth).
+    struct Job { uint32_t w; std::vector<Slot> slots; uint32_t depth; };
+    std::deque<Job> q;
+    auto expand = [&](std::vector<Slot> fr) {
+        // greedily open the internal slot with the largest surface area until 8 slots
+        for (;;) {
+            if (fr.size() >= 8) break;
+            int best = -1;
+            double ba = -1.0;
+            for (size_t k = 0; k < fr.size(); ++k)
+                if (!(fr[k].id & kLeafBit) && area(fr[k]) > ba) { ba = area(fr[k]); best = (int)k; }
+            if (best < 0) break;
+            Slot a, b;
+            child_slots(nodes[fr[best].id], a, b);
+            fr.erase(fr.begin() + best);
+            fr.push_back(a);
+            fr.push_back(b);
+        }
+        // empty leaves never produce hits
+        std::vector<Slot> kept;
+        for (const Slot& s : fr)
+            if (!(s.id & kLeafBit) || leaf_tris(s.id) > 0u) kept.push_back(s);
+        return kept;
+    };
+
+    out.nodes.reserve(20ull * (num_nodes / 4 + 4));
+    out.nodes.resize(20);
+    out.num_nodes = 1;
+    if (num_nodes == 1u) {
+        Slot s;
+        s.id = kLeafBit;
+        for (int a = 0; a < 3; ++a) { s.lo[a] = 0.f; s.hi[a] = 0.f; }
+        q.push_back({0u, {s}, 1u});
+        out.root_is_leaf = 1u;
+    } else {
+        Slot a, b;
+        child_slots(nodes[0], a, b);
+        q.push_back({0u, expand({a, b}), 1u});
+    }
+    while (!q.empty()) {
+        Job job = std::move(q.front());
+        q.pop_front();
+        const std::vector<Slot>& sl = job.slots;
+        out.max_depth = std::max(out.max_depth, job.depth);
+        const int n = (int)sl.size();
+        float lo[3][8], hi[3][8];
+        for (int k = 0; k < n; ++k)
+            for (int a = 0; a < 3; ++a) {
+                lo[a][k] = std::min(sl[k].lo[a], sl[k].hi[a]);   // the slab test orders each axis itself
+                hi[a][k] = std::max(sl[k].lo[a], sl[k].hi[a]);
+            }
+        uint32_t* w = out.nodes.data() + 20ull * job.w;
+        std::memset(w, 0, 80);
+        uint8_t e[3] = {1, 1, 1}, qlo[3][8] = {}, qhi[3][8] = {};
+        float origin[3] = {0.f, 0.f, 0.f};
+        if (n > 0) {
+            for (int a = 0; a < 3; ++a)
+                if (!quantise_axis(lo[a], hi[a], n, origin[a], e[a], qlo[a], qhi[a])) {
+                    err = "box bounds cannot be quantised (non-finite coordinates)";
+                    return false;
+                }
+        }
+        uint32_t imask = 0, n_internal = 0;
+        for (int k = 0; k < n; ++k)
+            if (!(sl[k].id & kLeafBit)) { imask |= 1u << k; ++n_internal; }
+        const uint32_t child_base = out.num_nodes;
+        out.num_nodes += n_internal;
+        out.nodes.resize(20ull * out.num_nodes);
+        w = out.nodes.data() + 20ull * job.w;
+        std::memcpy(&w[0], &origin[0], 4);
+        std::memcpy(&w[1], &origin[1], 4);
+        std::memcpy(&w[2], &origin[2], 4);
+        w[3] = (uint32_t)e[0] | ((uint32_t)e[1] << 8) | ((uint32_t)e[2] << 16) | (imask << 24);
+        w[4] = child_base;
+        w[5] = (uint32_t)(out.tris.size() / 12);
+        uint8_t meta[8] = {};
+        for (int k = 0; k < n; ++k) {
+            if (sl[k].id & kLeafBit) {
+                const uint32_t nt = leaf_tris(sl[k].id);
+                if (nt > 255u) { err = "a leaf holds more than 255 triangles (8-wide slot limit)"; return false; }
+                meta[k] = (uint8_t)nt;
+                emit_tris(sl[k].id);
+            }
+        }
+        std::memcpy(&w[6], meta, 8);
+        uint8_t* qb = reinterpret_cast<uint8_t*>(&w[8]);
+        for (int k = 0; k < 8; ++k) {
+            qb[0 + k] = qlo[0][k]; qb[8 + k] = qlo[1][k]; qb[16 + k] = qlo[2][k];
+            qb[24 + k] = qhi[0][k]; qb[32 + k] = qhi[1][k]; qb[40 + k] = qhi[2][k];
+        }
+        uint32_t ci = child_base;
+        for (int k = 0; k < n; ++k) {
+            if (!(sl[k].id & kLeafBit)) {
+                Slot a, b;
+                child_slots(nodes[sl[k].id], a, b);
+                q.push_back({ci++, expand({a, b}), job.depth + 1u});
+            }
+        }
+    }
+    if (out.max_depth > 32u) { err = "8-wide tree deeper than 32 levels"; return false; }
+    return true;
+}
+
+}  // namespace timrt

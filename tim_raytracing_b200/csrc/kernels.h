@@ -1,0 +1,30 @@
+// kernels.h -- host-side declarations of the kernel launchers (trace.cu, probes.cu).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "common.cuh"
+#include "../../include/tim_rt.h"
+
+namespace timrt {
+
+// Launch shape of the persistent trace kernels (chosen by the autotuner).
+struct LaunchConfig {
+    int block = 128;    // threads per block: 64, 128 or 256
+    bool wide = false;  // 8-wide quantised BVH instead of the reference binary layout
+};
+
+cudaError_t launch_trace_batch(const SceneView& s, const tim_rt_ray* rays, uint32_t n, uint32_t mode, uint32_t* hit,
+                               uint32_t* nid, float* bary, uint32_t* counter, uint32_t* err, cudaStream_t stream,
+                               const LaunchConfig& cfg);
+
+// counters: [0] pixel work counter, [1] secondary queue length, [2] secondary work counter.
+cudaError_t launch_camera(const SceneView& s, const tim_rt_pass_data& pd, uint32_t flags, uint32_t seed,
+                          const uint32_t* tile_counts, const uint32_t* tile_lists, uint32_t* out, uint32_t* bounce_out,
+                          uint32_t* leaf_nid, tim_rt_ray* q_rays, uint32_t* q_pixel, uint32_t q_capacity,
+                          uint32_t* counters, uint32_t* err, uint64_t* d_ray_count, cudaStream_t stream,
+                          const LaunchConfig& cfg);
+
+cudaError_t launch_cull_lights(const SceneView& s, const tim_rt_pass_data& pd, uint32_t tiles_x, uint32_t tiles_y,
+                               uint32_t* counts, uint32_t* lists, cudaStream_t stream);
+
+}  // namespace timrt
