@@ -86,6 +86,7 @@ typedef struct { float o[3]; float tmax; float d[3]; uint32_t flags; } tim_rt_ra
 #define TIM_RT_MODE_PER_RAY 2u   /* ray.flags bit 0 selects any-hit */
 #define TIM_RT_TRACE_WIDE 0x100u /* trace the 8-wide quantised BVH (needs TIM_RT_UPLOAD_QUANT8) */
 #define TIM_RT_TRACE_SORT 0x200u /* reorder rays by a coherence key before tracing (results keep input order) */
+#define TIM_RT_TRACE_COUNT 0x400u /* run the counting kernel variant and fill the work counters of tim_rt_stats */
 
 /* Upload flags. */
 #define TIM_RT_UPLOAD_QUANT8 0x2u /* also build the 8-wide BVH with 8-bit quantised child bounds */
@@ -96,6 +97,13 @@ typedef struct {
     uint64_t primary_rays, shadow_rays, probe_rays, bounce_rays;
     float kernel_ms;          /* device time of the trace kernels (CUDA events) */
     float total_ms;           /* device time of the whole call incl. copies */
+    /* work counters, filled only with TIM_RT_TRACE_COUNT / TIM_RT_CAM_COUNT:
+     * inner-node fetches (binary: 64-B node, 8-wide: 80-B node), leaf visits,
+     * triangle tests, node-header reloads (8-wide: 32 B when a pending node is popped) */
+    uint64_t node_visits, leaf_visits, tri_tests, node_reloads;
+    /* camera calls: device time of the primary trace, the secondary-ray
+     * generation and the secondary trace kernels (CUDA events) */
+    float primary_ms, gen_ms, secondary_ms;
 } tim_rt_stats;
 
 /* ---------------------------------------------------------------- context */
@@ -165,6 +173,7 @@ int tim_rt_trace_dev(tim_rt_ctx *ctx, tim_rt_scene_id scene, const tim_rt_ray *d
 #define TIM_RT_CAM_TILE_LIGHTS 2u
 #define TIM_RT_CAM_BOUNCE 4u
 #define TIM_RT_CAM_WIDE 0x100u   /* use the quantised 8-wide BVH */
+#define TIM_RT_CAM_COUNT 0x200u  /* counting kernel variant; fills the work counters of tim_rt_stats */
 int tim_rt_trace_camera(tim_rt_ctx *ctx, tim_rt_scene_id scene, const tim_rt_pass_data *pd, uint32_t flags,
                         uint32_t seed, const uint32_t *tile_counts, const uint32_t *tile_lists,
                         uint32_t *out, uint32_t *bounce_out, tim_rt_stats *stats);

@@ -161,7 +161,7 @@ def test_errors(ctx, native, room):
     with pytest.raises(native.TimRtError) as e:
         ctx.upload(bad, s)
     assert e.value.code == native.EINVAL
-    small = native.Context(0, mem_budget_bytes=4096)
+    small = native.Context(0, mem_budget_bytes=64 * 1024)   # room for the context, not the scene
     try:
         with pytest.raises(native.TimRtError) as e:
             small.upload(img, s)

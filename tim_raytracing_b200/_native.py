@@ -18,8 +18,9 @@ OK, EINVAL, ENOMEM, ETIMEOUT, EDEVICE, ENOTFOUND, EUNSUPPORTED = range(7)
 MODE_CLOSEST, MODE_ANY, MODE_PER_RAY = 0, 1, 2
 TRACE_WIDE = 0x100
 TRACE_SORT = 0x200
+TRACE_COUNT = 0x400
 UPLOAD_QUANT8 = 0x2
-CAM_PROB_MASK, CAM_TILE_LIGHTS, CAM_BOUNCE, CAM_WIDE = 1, 2, 4, 0x100
+CAM_PROB_MASK, CAM_TILE_LIGHTS, CAM_BOUNCE, CAM_WIDE, CAM_COUNT = 1, 2, 4, 0x100, 0x200
 RANGE_BLAS, RANGE_TRI, RANGE_PRIM, RANGE_MAT, RANGE_LIGHT, RANGE_NODE, RANGE_LEAF = range(7)
 
 EXPORTED = [
@@ -45,7 +46,9 @@ class PushConstants(ctypes.Structure):
 class Stats(ctypes.Structure):
     _fields_ = [("rays", ctypes.c_uint64), ("primary_rays", ctypes.c_uint64), ("shadow_rays", ctypes.c_uint64),
                 ("probe_rays", ctypes.c_uint64), ("bounce_rays", ctypes.c_uint64), ("kernel_ms", ctypes.c_float),
-                ("total_ms", ctypes.c_float)]
+                ("total_ms", ctypes.c_float), ("node_visits", ctypes.c_uint64), ("leaf_visits", ctypes.c_uint64),
+                ("tri_tests", ctypes.c_uint64), ("node_reloads", ctypes.c_uint64), ("primary_ms", ctypes.c_float),
+                ("gen_ms", ctypes.c_float), ("secondary_ms", ctypes.c_float)]
 
 
 class BuildParams(ctypes.Structure):

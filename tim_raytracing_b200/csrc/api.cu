@@ -56,7 +56,9 @@ struct tim_rt_ctx {
     DevBuf counters;            // [0..63] per-call work counters, [64] device error word, ring after
     uint32_t ring = 0;
     DevBuf cam_out, cam_bounce, cam_nid, q_rays, q_pixel, tiles_counts, tiles_lists;
+    DevBuf dstats;              // 8 x u64 work counters of the counting kernels
     cudaEvent_t ev[4] = {};
+    cudaEvent_t pev[4] = {};   // camera phases
     LaunchConfig cfg;
 };
 
@@ -142,10 +144,21 @@ int check_device_error(tim_rt_ctx* c) {
     return TIM_RT_OK;
 }
 
-LaunchConfig cfg_for(tim_rt_ctx* c, const Scene* s, bool wide) {
+LaunchConfig cfg_for(tim_rt_ctx* c, const Scene* s, bool wide, bool count = false) {
     LaunchConfig cfg = c->cfg;
     cfg.wide = wide && s->has_wide;
+    cfg.stats = count ? static_cast<unsigned long long*>(c->dstats.ptr) : nullptr;
     return cfg;
+}
+
+// Copies the counting kernels' totals into the caller's stats (after a sync).
+void read_counts(tim_rt_ctx* c, tim_rt_stats* st) {
+    unsigned long long v[8] = {};
+    cudaMemcpy(v, c->dstats.ptr, sizeof(v), cudaMemcpyDeviceToHost);
+    st->node_visits = v[1];
+    st->leaf_visits = v[2];
+    st->tri_tests = v[3];
+    st->node_reloads = v[4];
 }
 
 }  // namespace
@@ -173,8 +186,10 @@ int tim_rt_create(int device, uint64_t mem_budget_bytes, tim_rt_ctx** out) {
     c->budget = mem_budget_bytes;
     TIMRT_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     for (auto& e : c->ev) TIMRT_CUDA(cudaEventCreate(&e));
+    for (auto& e : c->pev) TIMRT_CUDA(cudaEventCreate(&e));
     int rc = dev_alloc(c.get(), c->counters, 4ull * kCounterWords);
     if (rc) return rc;
+    if ((rc = dev_alloc(c.get(), c->dstats, 64))) return rc;
     TIMRT_CUDA(cudaMemset(c->counters.ptr, 0, 4ull * kCounterWords));
     *out = c.release();
     return TIM_RT_OK;
@@ -190,9 +205,11 @@ int tim_rt_destroy(tim_rt_ctx* c) {
     }
     c->scenes.clear();
     for (DevBuf* b : {&c->rays, &c->hits, &c->nid, &c->bary, &c->counters, &c->cam_out, &c->cam_bounce, &c->cam_nid,
-                      &c->q_rays, &c->q_pixel, &c->tiles_counts, &c->tiles_lists})
+                      &c->q_rays, &c->q_pixel, &c->tiles_counts, &c->tiles_lists, &c->dstats})
         dev_free(c, *b);
     for (auto& e : c->ev)
+        if (e) cudaEventDestroy(e);
+    for (auto& e : c->pev)
         if (e) cudaEventDestroy(e);
     cudaStreamDestroy(c->stream);
     delete c;
@@ -378,6 +395,8 @@ int tim_rt_trace(tim_rt_ctx* c, tim_rt_scene_id id, const tim_rt_ray* rays, uint
     if (bary && (rc = ensure(c, c->bary, 8ull * n))) return rc;
     uint32_t* ctr = static_cast<uint32_t*>(c->counters.ptr);
     uint32_t* err = ctr + kErrWord;
+    const bool count = (mode & TIM_RT_TRACE_COUNT) != 0;
+    if (count) TIMRT_CUDA(cudaMemsetAsync(c->dstats.ptr, 0, 64, c->stream));
     TIMRT_CUDA(cudaEventRecord(c->ev[0], c->stream));
     TIMRT_CUDA(cudaMemcpyAsync(c->rays.ptr, rays, 32ull * n, cudaMemcpyHostToDevice, c->stream));
     TIMRT_CUDA(cudaMemsetAsync(ctr, 0, 4, c->stream));
@@ -385,7 +404,7 @@ int tim_rt_trace(tim_rt_ctx* c, tim_rt_scene_id id, const tim_rt_ray* rays, uint
     TIMRT_CUDA(launch_trace_batch(s->view, static_cast<const tim_rt_ray*>(c->rays.ptr), n, mode,
                                   static_cast<uint32_t*>(c->hits.ptr), leaf_nid ? static_cast<uint32_t*>(c->nid.ptr) : nullptr,
                                   bary ? static_cast<float*>(c->bary.ptr) : nullptr, ctr, err, c->stream,
-                                  cfg_for(c, s, (mode & TIM_RT_TRACE_WIDE) != 0)));
+                                  cfg_for(c, s, (mode & TIM_RT_TRACE_WIDE) != 0, count)));
     TIMRT_CUDA(cudaEventRecord(c->ev[2], c->stream));
     TIMRT_CUDA(cudaMemcpyAsync(hit, c->hits.ptr, 16ull * n, cudaMemcpyDeviceToHost, c->stream));
     if (leaf_nid) TIMRT_CUDA(cudaMemcpyAsync(leaf_nid, c->nid.ptr, 4ull * n, cudaMemcpyDeviceToHost, c->stream));
@@ -398,6 +417,7 @@ int tim_rt_trace(tim_rt_ctx* c, tim_rt_scene_id id, const tim_rt_ray* rays, uint
         stats->primary_rays = n;
         cudaEventElapsedTime(&stats->kernel_ms, c->ev[1], c->ev[2]);
         cudaEventElapsedTime(&stats->total_ms, c->ev[0], c->ev[3]);
+        if (count) read_counts(c, stats);
     }
     return TIM_RT_OK;
 }
@@ -538,13 +558,17 @@ int tim_rt_trace_camera(tim_rt_ctx* c, tim_rt_scene_id id, const tim_rt_pass_dat
         TIMRT_CUDA(cudaMemcpyAsync(c->tiles_lists.ptr, tile_lists, 64ull * tiles, cudaMemcpyHostToDevice, c->stream));
     }
     TIMRT_CUDA(cudaMemsetAsync(ctr, 0, 16, c->stream));
+    const bool count = (flags & TIM_RT_CAM_COUNT) != 0;
+    if (count) TIMRT_CUDA(cudaMemsetAsync(c->dstats.ptr, 0, 64, c->stream));
     TIMRT_CUDA(cudaEventRecord(c->ev[1], c->stream));
+    LaunchConfig cam_cfg = cfg_for(c, s, (flags & TIM_RT_CAM_WIDE) != 0, count);
+    cam_cfg.phase_ev = c->pev;
     TIMRT_CUDA(launch_camera(s->view, *pd, flags, seed, static_cast<const uint32_t*>(c->tiles_counts.ptr),
                              static_cast<const uint32_t*>(c->tiles_lists.ptr), static_cast<uint32_t*>(c->cam_out.ptr),
                              (flags & TIM_RT_CAM_BOUNCE) ? static_cast<uint32_t*>(c->cam_bounce.ptr) : nullptr,
                              static_cast<uint32_t*>(c->cam_nid.ptr), static_cast<tim_rt_ray*>(c->q_rays.ptr),
                              static_cast<uint32_t*>(c->q_pixel.ptr), (uint32_t)qcap, ctr, ctr + kErrWord, nullptr,
-                             c->stream, cfg_for(c, s, (flags & TIM_RT_CAM_WIDE) != 0)));
+                             c->stream, cam_cfg));
     TIMRT_CUDA(cudaEventRecord(c->ev[2], c->stream));
     TIMRT_CUDA(cudaMemcpyAsync(out, c->cam_out.ptr, 32ull * npix, cudaMemcpyDeviceToHost, c->stream));
     if (flags & TIM_RT_CAM_BOUNCE)
@@ -562,6 +586,10 @@ int tim_rt_trace_camera(tim_rt_ctx* c, tim_rt_scene_id id, const tim_rt_pass_dat
         stats->shadow_rays = qn;   // all secondary rays (shadow, probe-visibility, bounce)
         cudaEventElapsedTime(&stats->kernel_ms, c->ev[1], c->ev[2]);
         cudaEventElapsedTime(&stats->total_ms, c->ev[0], c->ev[3]);
+        cudaEventElapsedTime(&stats->primary_ms, c->pev[0], c->pev[1]);
+        cudaEventElapsedTime(&stats->gen_ms, c->pev[1], c->pev[2]);
+        cudaEventElapsedTime(&stats->secondary_ms, c->pev[2], c->pev[3]);
+        if (count) read_counts(c, stats);
     }
     return TIM_RT_OK;
 }

@@ -11,6 +11,11 @@ namespace timrt {
 struct LaunchConfig {
     int block = 128;    // threads per block: 64, 128 or 256
     bool wide = false;  // 8-wide quantised BVH instead of the reference binary layout
+    // when set, a counting variant of the kernel adds per-ray work to
+    // stats[0..4] = (rays, node visits, leaf visits, triangle tests, node reloads)
+    unsigned long long* stats = nullptr;
+    // when set, the camera launcher records ev[0..3] around its three phases
+    cudaEvent_t* phase_ev = nullptr;
 };
 
 cudaError_t launch_trace_batch(const SceneView& s, const tim_rt_ray* rays, uint32_t n, uint32_t mode, uint32_t* hit,

@@ -124,9 +124,10 @@ struct SecondaryPolicy {
 
 // -------------------------------------------------------------------- persistent loop
 
-template <int BLOCK, bool WIDE, class Policy>
+template <int BLOCK, bool WIDE, bool STATS, class Policy>
 __global__ void __launch_bounds__(BLOCK) k_persistent(SceneView s, Policy P, uint32_t n_static,
-                                                      const uint32_t* n_dev, uint32_t* counter, uint32_t* err) {
+                                                      const uint32_t* n_dev, uint32_t* counter, uint32_t* err,
+                                                      unsigned long long* stats) {
     extern __shared__ uint32_t stack_mem[];   // (WIDE ? 2 : 1) * kStackSize * BLOCK words
     uint32_t* stk = stack_mem + threadIdx.x;
     const uint32_t lane = threadIdx.x & 31u;
@@ -172,6 +173,13 @@ __global__ void __launch_bounds__(BLOCK) k_persistent(SceneView s, Policy P, uin
             else plain_step<BLOCK>(s, st, stk, err);
             if (st.done) {
                 P.store(s, idx, st, tmax0);
+                if (STATS) {
+                    atomicAdd(stats + 0, 1ull);
+                    atomicAdd(stats + 1, (unsigned long long)st.c_node);
+                    atomicAdd(stats + 2, (unsigned long long)st.c_leaf);
+                    atomicAdd(stats + 3, (unsigned long long)st.c_tri);
+                    atomicAdd(stats + 4, (unsigned long long)st.c_reload);
+                }
                 active = false;
             }
         }
@@ -472,36 +480,41 @@ constexpr size_t stack_bytes() {
 
 // Grid of the persistent kernels: as many resident blocks as the occupancy
 // calculator allows on every SM (the dynamic shared memory holds the stacks).
-template <int BLOCK, bool WIDE, class Policy>
+template <int BLOCK, bool WIDE, bool STATS, class Policy>
 static int grid_for() {
     static int blocks = 0;
     if (!blocks) {
         int dev = 0, sms = 0, per = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaFuncSetAttribute(k_persistent<BLOCK, WIDE, Policy>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(k_persistent<BLOCK, WIDE, STATS, Policy>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)stack_bytes<BLOCK, WIDE>());
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_persistent<BLOCK, WIDE, Policy>, BLOCK,
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_persistent<BLOCK, WIDE, STATS, Policy>, BLOCK,
                                                       stack_bytes<BLOCK, WIDE>());
         blocks = sms * (per > 0 ? per : 1);
     }
     return blocks;
 }
 
-template <int BLOCK, bool WIDE, class Policy>
+template <int BLOCK, bool WIDE, bool STATS, class Policy>
 static void launch_block(const SceneView& s, const Policy& P, uint32_t n_static, const uint32_t* n_dev,
-                         uint32_t* counter, uint32_t* err, cudaStream_t stream) {
-    k_persistent<BLOCK, WIDE, Policy><<<grid_for<BLOCK, WIDE, Policy>(), BLOCK, stack_bytes<BLOCK, WIDE>(), stream>>>(
-        s, P, n_static, n_dev, counter, err);
+                         uint32_t* counter, uint32_t* err, unsigned long long* stats, cudaStream_t stream) {
+    k_persistent<BLOCK, WIDE, STATS, Policy>
+        <<<grid_for<BLOCK, WIDE, STATS, Policy>(), BLOCK, stack_bytes<BLOCK, WIDE>(), stream>>>(s, P, n_static, n_dev,
+                                                                                            counter, err, stats);
 }
 
 template <bool WIDE, class Policy>
 static cudaError_t launch_persistent(const SceneView& s, const Policy& P, uint32_t n_static, const uint32_t* n_dev,
-                                     uint32_t* counter, uint32_t* err, cudaStream_t stream, int block) {
-    switch (block) {
-        case 64: launch_block<64, WIDE>(s, P, n_static, n_dev, counter, err, stream); break;
-        case 256: launch_block<256, WIDE>(s, P, n_static, n_dev, counter, err, stream); break;
-        default: launch_block<128, WIDE>(s, P, n_static, n_dev, counter, err, stream); break;
+                                     uint32_t* counter, uint32_t* err, cudaStream_t stream, const LaunchConfig& cfg) {
+    if (cfg.stats) {
+        launch_block<128, WIDE, true>(s, P, n_static, n_dev, counter, err, cfg.stats, stream);
+        return cudaGetLastError();
+    }
+    switch (cfg.block) {
+        case 64: launch_block<64, WIDE, false>(s, P, n_static, n_dev, counter, err, nullptr, stream); break;
+        case 256: launch_block<256, WIDE, false>(s, P, n_static, n_dev, counter, err, nullptr, stream); break;
+        default: launch_block<128, WIDE, false>(s, P, n_static, n_dev, counter, err, nullptr, stream); break;
     }
     return cudaGetLastError();
 }
@@ -510,8 +523,8 @@ cudaError_t launch_trace_batch(const SceneView& s, const tim_rt_ray* rays, uint3
                                uint32_t* nid, float* bary, uint32_t* counter, uint32_t* err, cudaStream_t stream,
                                const LaunchConfig& cfg) {
     BatchPolicy P{rays, reinterpret_cast<uint4*>(hit), nid, reinterpret_cast<float2*>(bary), mode & 0xFFu};
-    if (cfg.wide) return launch_persistent<true>(s, P, n, nullptr, counter, err, stream, cfg.block);
-    return launch_persistent<false>(s, P, n, nullptr, counter, err, stream, cfg.block);
+    if (cfg.wide) return launch_persistent<true>(s, P, n, nullptr, counter, err, stream, cfg);
+    return launch_persistent<false>(s, P, n, nullptr, counter, err, stream, cfg);
 }
 
 cudaError_t launch_camera(const SceneView& s, const tim_rt_pass_data& pd, uint32_t flags, uint32_t seed,
@@ -523,9 +536,11 @@ cudaError_t launch_camera(const SceneView& s, const tim_rt_pass_data& pd, uint32
     const uint32_t npix = W * H;
     const uint32_t ngy16 = 16u * ((H + 15u) / 16u);
     CameraPolicy CP{pd, ngy16, reinterpret_cast<uint4*>(out), leaf_nid};
-    cudaError_t e = cfg.wide ? launch_persistent<true>(s, CP, npix, nullptr, counters + 0, err, stream, cfg.block)
-                             : launch_persistent<false>(s, CP, npix, nullptr, counters + 0, err, stream, cfg.block);
+    if (cfg.phase_ev) cudaEventRecord(cfg.phase_ev[0], stream);
+    cudaError_t e = cfg.wide ? launch_persistent<true>(s, CP, npix, nullptr, counters + 0, err, stream, cfg)
+                             : launch_persistent<false>(s, CP, npix, nullptr, counters + 0, err, stream, cfg);
     if (e != cudaSuccess) return e;
+    if (cfg.phase_ev) cudaEventRecord(cfg.phase_ev[1], stream);
     GenParams g;
     g.pd = pd;
     g.flags = flags;
@@ -544,9 +559,11 @@ cudaError_t launch_camera(const SceneView& s, const tim_rt_pass_data& pd, uint32
     k_gen_secondary<<<(npix + 255u) / 256u, 256, 0, stream>>>(s, g);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     k_clamp_count<<<1, 1, 0, stream>>>(counters + 1, q_capacity);
+    if (cfg.phase_ev) cudaEventRecord(cfg.phase_ev[2], stream);
     SecondaryPolicy SP{q_rays, q_pixel, out, reinterpret_cast<uint4*>(bounce_out)};
-    e = cfg.wide ? launch_persistent<true>(s, SP, 0u, counters + 1, counters + 2, err, stream, cfg.block)
-                 : launch_persistent<false>(s, SP, 0u, counters + 1, counters + 2, err, stream, cfg.block);
+    e = cfg.wide ? launch_persistent<true>(s, SP, 0u, counters + 1, counters + 2, err, stream, cfg)
+                 : launch_persistent<false>(s, SP, 0u, counters + 1, counters + 2, err, stream, cfg);
+    if (cfg.phase_ev) cudaEventRecord(cfg.phase_ev[3], stream);
     if (e != cudaSuccess || !d_ray_count) return e;
     k_add_ray_count<<<1, 1, 0, stream>>>(d_ray_count, (uint64_t)W * (H - 1u), counters + 1);
     return cudaGetLastError();

@@ -26,6 +26,8 @@ struct TravState {
     bool hit;         // closest: a triangle was accepted; any: occluded
     uint32_t rec0, rec1, rec2, nid;
     float u, v;
+    // work counters (dead code unless a counting kernel reads them)
+    uint32_t c_node, c_leaf, c_tri, c_reload;
     // 8-wide form only
     float ix, iy, iz;   // 1 / direction
     uint32_t order;     // remaining slots of the current wide node, nearest first
@@ -34,6 +36,7 @@ struct TravState {
 
 __device__ __forceinline__ void trav_init(TravState& st, uint32_t root) {
     st.node = root;
+    st.c_node = st.c_leaf = st.c_tri = st.c_reload = 0u;
     st.sp = 0;
     st.done = false;
     st.hit = false;
@@ -50,7 +53,9 @@ __device__ __forceinline__ void plain_leaf(const SceneView& s, TravState& st, ui
     const uint32_t hdr = leaf_header(s, off);
     const uint32_t ntri = hdr & ((1u << kTriBits) - 1u);
     const uint32_t* rec = s.leaf + off + 1u;
+    st.c_leaf++;
     for (uint32_t i = 0; i < ntri; ++i, rec += 3) {
+        st.c_tri++;
         const uint32_t r0 = __ldg(rec), r1 = __ldg(rec + 1), r2 = __ldg(rec + 2);
         const uint32_t i0 = r0 + (r1 & 0xFFFFu), i1 = r0 + (r1 >> 16), i2 = r0 + (r2 & 0xFFFFu);
         const float* P0 = s.pos + 3u * i0;
@@ -99,6 +104,7 @@ __device__ __forceinline__ void plain_step(const SceneView& s, TravState& st, ui
     uint32_t node = st.node;
     while (!(node & kNidLeafBit)) {
         const float4* np = s.nodes + 4u * node;
+        st.c_node++;
         const uint4 nid = __ldg(reinterpret_cast<const uint4*>(np));
         const float4 a = __ldg(np + 1);   // n0xy = (c0.min.x, c0.min.y, c0.max.x, c0.max.y)
         const float4 b = __ldg(np + 2);   // n1xy

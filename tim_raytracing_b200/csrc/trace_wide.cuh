@@ -66,8 +66,10 @@ __device__ __forceinline__ uint32_t wide_visit(const SceneView& s, const TravSta
         const float t0z = (lz - st.r.oz) * iz, t1z = (hz - st.r.oz) * iz;
         float nearv = fmaxf(fminf(t0x, t1x), fmaxf(fminf(t0y, t1y), fminf(t0z, t1z)));
         float farv = fminf(fmaxf(t0x, t1x), fminf(fmaxf(t0y, t1y), fmaxf(t0z, t1z)));
-        nearv = nearv - fabsf(nearv) * 3.814697265625e-06f;   // 2^-18
-        farv = farv + fabsf(farv) * 3.814697265625e-06f;
+        // widen by a relative 2^-18; a product keeps +-inf (direction component 0)
+        // infinite, where a subtraction of |x| * eps would turn inf into NaN
+        nearv = nearv * (nearv > 0.0f ? 0.999996185302734375f : 1.000003814697265625f);
+        farv = farv * (farv > 0.0f ? 1.000003814697265625f : 0.999996185302734375f);
         const float tmin = fmaxf(0.0f, nearv);
         const float tm = fminf(tcur, farv);
         const bool hit = valid && (tmin < tm);
@@ -118,7 +120,9 @@ __device__ __forceinline__ void wide_leaf(const SceneView& s, TravState& st, con
     const uint32_t first = h.tri_base + __dp4a(below_lo, 0x01010101u, __dp4a(below_hi, 0x01010101u, 0u));
     const uint32_t cnt = ((slot < 4u ? h.meta_lo : h.meta_hi) >> (8u * (slot & 3u))) & 0xFFu;
     const float4* tp = s.wtris + 3u * first;
+    st.c_leaf++;
     for (uint32_t i = 0; i < cnt; ++i, tp += 3) {
+        st.c_tri++;
         const float4 A = __ldg(tp), B = __ldg(tp + 1), C = __ldg(tp + 2);
         float u, v;
         const float t = collide_triangle_e(st.r, A.x, A.y, A.z, B.x, B.y, B.z, C.x, C.y, C.z, st.t, u, v);
@@ -151,6 +155,7 @@ __device__ __forceinline__ void wide_init(const SceneView& s, TravState& st, uin
     st.nid = 0xFFFFFFFFu;
     st.u = st.v = 0.0f;
     st.node = 0u;
+    st.c_node = st.c_leaf = st.c_tri = st.c_reload = 0u;
     if (s.num_wnodes == 0u) {
         st.done = true;
         return;
@@ -159,6 +164,7 @@ __device__ __forceinline__ void wide_init(const SceneView& s, TravState& st, uin
         wide_read_hdr(s, 0u, st.h);
         st.order = 1u << 24;
     } else {
+        st.c_node++;
         st.order = wide_visit(s, st, st.ix, st.iy, st.iz, 0u, st.h);
     }
 }
@@ -179,6 +185,7 @@ __device__ __forceinline__ void wide_step(const SceneView& s, TravState& st, uin
             st.node = stk[(2 * st.sp) * BLOCK];
             st.order = stk[(2 * st.sp + 1) * BLOCK];
             wide_read_hdr(s, st.node, st.h);
+            st.c_reload++;
             continue;
         }
         const uint32_t slot = st.order & 7u;
@@ -196,6 +203,7 @@ __device__ __forceinline__ void wide_step(const SceneView& s, TravState& st, uin
                 ++st.sp;
             }
             st.node = child;
+            st.c_node++;
             st.order = wide_visit(s, st, st.ix, st.iy, st.iz, child, st.h);
         } else {
             wide_leaf<BLOCK>(s, st, st.h, slot);
