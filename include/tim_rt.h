@@ -120,6 +120,16 @@ int tim_rt_destroy(tim_rt_ctx *ctx);
 /* Device bytes currently held by the context (scenes + scratch). */
 int tim_rt_memory_used(tim_rt_ctx *ctx, uint64_t *bytes);
 
+/* Launch shape of the persistent trace kernels (the knobs the autotuner picks). */
+typedef struct {
+    uint32_t block;        /* threads per block: 64, 128 or 256 */
+    uint32_t stack_depth;  /* traversal-stack entries per thread; 0 = the scene's tree depth (<= 32) */
+    uint32_t refill_min;   /* a warp fetches new rays once this many of its 32 lanes are idle (1..32) */
+    uint32_t reserved;
+} tim_rt_launch_config;
+int tim_rt_get_launch_config(tim_rt_ctx *ctx, tim_rt_launch_config *cfg);
+int tim_rt_set_launch_config(tim_rt_ctx *ctx, const tim_rt_launch_config *cfg);
+
 /* ---------------------------------------------------------------- BVH upload */
 /* Replaces BVHData::build's CreateBuffer + UploadBuffer (src/Renderer/BVHData.cpp:43-48)
  * and BVHGeometry::flush (src/Renderer/BVHGeometry.cpp:69-78).

@@ -28,7 +28,7 @@ EXPORTED = [
     "tim_rt_upload_bvh", "tim_rt_free_scene", "tim_rt_scene_bytes", "tim_rt_trace", "tim_rt_trace_dev",
     "tim_rt_trace_camera", "tim_rt_cull_lights", "tim_rt_build_params_default", "tim_rt_build_bvh",
     "tim_rt_bvh_blob_info", "tim_rt_bvh_blob_free", "tim_rt_validate_bvh", "tim_rt_trace_camera_dev",
-    "tim_rt_cull_lights_dev",
+    "tim_rt_cull_lights_dev", "tim_rt_get_launch_config", "tim_rt_set_launch_config",
 ]
 
 
@@ -49,6 +49,11 @@ class Stats(ctypes.Structure):
                 ("total_ms", ctypes.c_float), ("node_visits", ctypes.c_uint64), ("leaf_visits", ctypes.c_uint64),
                 ("tri_tests", ctypes.c_uint64), ("node_reloads", ctypes.c_uint64), ("primary_ms", ctypes.c_float),
                 ("gen_ms", ctypes.c_float), ("secondary_ms", ctypes.c_float)]
+
+
+class LaunchConfig(ctypes.Structure):
+    _fields_ = [("block", ctypes.c_uint32), ("stack_depth", ctypes.c_uint32), ("refill_min", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32)]
 
 
 class BuildParams(ctypes.Structure):
@@ -90,6 +95,8 @@ def lib() -> ctypes.CDLL:
     L.tim_rt_validate_bvh.argtypes = [vp, u64, vp, ctypes.POINTER(PushConstants), u32, ctypes.POINTER(u32)]
     L.tim_rt_trace_camera_dev.argtypes = [vp, u32, vp, u32, u32, vp, vp, vp, vp, vp, vp]
     L.tim_rt_cull_lights_dev.argtypes = [vp, u32, vp, u32, u32, vp, vp, vp]
+    L.tim_rt_get_launch_config.argtypes = [vp, ctypes.POINTER(LaunchConfig)]
+    L.tim_rt_set_launch_config.argtypes = [vp, ctypes.POINTER(LaunchConfig)]
     for name in EXPORTED:
         if name not in ("tim_rt_version", "tim_rt_last_error", "tim_rt_build_params_default", "tim_rt_bvh_blob_free"):
             getattr(L, name).restype = i32
@@ -208,6 +215,15 @@ class Context:
     @property
     def handle(self):
         return self._c
+
+    def launch_config(self) -> dict:
+        c = LaunchConfig()
+        _check(self._L.tim_rt_get_launch_config(self._c, ctypes.byref(c)))
+        return {"block": c.block, "stack_depth": c.stack_depth, "refill_min": c.refill_min}
+
+    def set_launch_config(self, block: int = 128, stack_depth: int = 0, refill_min: int = 1):
+        c = LaunchConfig(block, stack_depth, refill_min, 0)
+        _check(self._L.tim_rt_set_launch_config(self._c, ctypes.byref(c)))
 
     def memory_used(self) -> int:
         v = ctypes.c_uint64()

@@ -216,6 +216,30 @@ int tim_rt_destroy(tim_rt_ctx* c) {
     return TIM_RT_OK;
 }
 
+int tim_rt_get_launch_config(tim_rt_ctx* c, tim_rt_launch_config* cfg) {
+    if (!c || !cfg) {
+        set_error("null argument");
+        return TIM_RT_EINVAL;
+    }
+    cfg->block = (uint32_t)c->cfg.block;
+    cfg->stack_depth = (uint32_t)c->cfg.stack_depth;
+    cfg->refill_min = (uint32_t)c->cfg.refill_min;
+    cfg->reserved = 0;
+    return TIM_RT_OK;
+}
+
+int tim_rt_set_launch_config(tim_rt_ctx* c, const tim_rt_launch_config* cfg) {
+    if (!c || !cfg || (cfg->block != 64 && cfg->block != 128 && cfg->block != 256) || cfg->stack_depth > 32 ||
+        cfg->refill_min < 1 || cfg->refill_min > 32) {
+        set_error("tim_rt_set_launch_config: block must be 64/128/256, stack_depth <= 32, refill_min 1..32");
+        return TIM_RT_EINVAL;
+    }
+    c->cfg.block = (int)cfg->block;
+    c->cfg.stack_depth = (int)cfg->stack_depth;
+    c->cfg.refill_min = (int)cfg->refill_min;
+    return TIM_RT_OK;
+}
+
 int tim_rt_memory_used(tim_rt_ctx* c, uint64_t* bytes) {
     if (!c || !bytes) {
         set_error("null argument");
@@ -301,6 +325,8 @@ int tim_rt_upload_bvh(tim_rt_ctx* c, const void* bvh_bytes, uint64_t n_bytes, co
     v.num_lights = pc->numLights;
     v.leaf_words = ranges[TIM_RT_RANGE_LEAF][1] / 4u;
     v.num_vertex = num_vertex;
+    v.depth = depth;
+    v.wide_depth = wh.max_depth;
     v.wnodes = static_cast<const uint4*>(s->wnodes.ptr);
     v.wtris = static_cast<const float4*>(s->wtris.ptr);
     v.wtri_nid = static_cast<const uint32_t*>(s->wnid.ptr);
@@ -473,8 +499,7 @@ int camera_prepare(tim_rt_ctx* c, Scene* s, const tim_rt_pass_data* pd, uint32_t
         return TIM_RT_EUNSUPPORTED;
     }
     const uint64_t npix = (uint64_t)pd->frameSize[0] * pd->frameSize[1];
-    const uint32_t per_pix = 1u + 16u + ((flags & TIM_RT_CAM_PROB_MASK) ? 8u : 0u) + ((flags & TIM_RT_CAM_BOUNCE) ? 1u : 0u);
-    const uint64_t qcap = npix * per_pix;
+    const uint64_t qcap = npix * camera_queue_kinds();   // one segment of W*H slots per secondary-ray kind
     if (qcap > 0xFFFFFFFFull) {
         set_error("trace_camera: frame too large");
         return TIM_RT_EINVAL;
@@ -483,7 +508,7 @@ int camera_prepare(tim_rt_ctx* c, Scene* s, const tim_rt_pass_data* pd, uint32_t
     if ((rc = ensure(c, c->cam_nid, 4ull * npix)) || (rc = ensure(c, c->q_rays, 32ull * qcap)) ||
         (rc = ensure(c, c->q_pixel, 4ull * qcap)))
         return rc;
-    *qcap_out = qcap;
+    *qcap_out = npix;
     return TIM_RT_OK;
 }
 
@@ -521,7 +546,7 @@ int tim_rt_trace_camera_dev(tim_rt_ctx* c, tim_rt_scene_id id, const tim_rt_pass
     if ((rc = camera_prepare(c, s, pd, flags, d_tile_counts && d_tile_lists, d_bounce_out != nullptr, &qcap))) return rc;
     cudaStream_t st = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : c->stream;
     uint32_t* ctr = static_cast<uint32_t*>(c->counters.ptr);
-    TIMRT_CUDA(cudaMemsetAsync(ctr, 0, 16, st));
+    TIMRT_CUDA(cudaMemsetAsync(ctr, 0, 4 * kCamCounterWords, st));
     TIMRT_CUDA(launch_camera(s->view, *pd, flags, seed, d_tile_counts, d_tile_lists, d_out,
                              (flags & TIM_RT_CAM_BOUNCE) ? d_bounce_out : nullptr, static_cast<uint32_t*>(c->cam_nid.ptr),
                              static_cast<tim_rt_ray*>(c->q_rays.ptr), static_cast<uint32_t*>(c->q_pixel.ptr),
@@ -557,7 +582,7 @@ int tim_rt_trace_camera(tim_rt_ctx* c, tim_rt_scene_id id, const tim_rt_pass_dat
         TIMRT_CUDA(cudaMemcpyAsync(c->tiles_counts.ptr, tile_counts, 4ull * tiles, cudaMemcpyHostToDevice, c->stream));
         TIMRT_CUDA(cudaMemcpyAsync(c->tiles_lists.ptr, tile_lists, 64ull * tiles, cudaMemcpyHostToDevice, c->stream));
     }
-    TIMRT_CUDA(cudaMemsetAsync(ctr, 0, 16, c->stream));
+    TIMRT_CUDA(cudaMemsetAsync(ctr, 0, 4 * kCamCounterWords, c->stream));
     const bool count = (flags & TIM_RT_CAM_COUNT) != 0;
     if (count) TIMRT_CUDA(cudaMemsetAsync(c->dstats.ptr, 0, 64, c->stream));
     TIMRT_CUDA(cudaEventRecord(c->ev[1], c->stream));
@@ -574,7 +599,7 @@ int tim_rt_trace_camera(tim_rt_ctx* c, tim_rt_scene_id id, const tim_rt_pass_dat
     if (flags & TIM_RT_CAM_BOUNCE)
         TIMRT_CUDA(cudaMemcpyAsync(bounce_out, c->cam_bounce.ptr, 16ull * npix, cudaMemcpyDeviceToHost, c->stream));
     uint32_t qn = 0;
-    TIMRT_CUDA(cudaMemcpyAsync(&qn, ctr + 1, 4, cudaMemcpyDeviceToHost, c->stream));
+    TIMRT_CUDA(cudaMemcpyAsync(&qn, ctr + kCamTotalWord, 4, cudaMemcpyDeviceToHost, c->stream));
     TIMRT_CUDA(cudaEventRecord(c->ev[3], c->stream));
     TIMRT_CUDA(cudaStreamSynchronize(c->stream));
     if ((rc = check_device_error(c))) return rc;

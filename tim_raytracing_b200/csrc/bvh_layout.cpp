@@ -99,7 +99,23 @@ double area(const Slot& s) {
     return dx * dy + dy * dz + dz * dx;
 }
 
-float decode(float o, float sc, uint32_t q) { return o + sc * (float)q; }   // exact product, one rounded add
+// Plane o + sc * q compared with a float bound in real arithmetic: the kernel
+// evaluates planes in t-space, so the quantised box must contain the
+// reference box exactly, not only after rounding. Extended precision plus a
+// relative margin of 2^-60 keeps the comparison one-sided; q = 0 (the plane
+// is o itself) is compared exactly.
+bool plane_le(float o, float sc, uint32_t q, float x) {   // o + sc*q <= x
+    if (q == 0) return o <= x;
+    const long double v = (long double)o + (long double)sc * (long double)q;
+    const long double m = fabsl((long double)x) * 8.67e-19L + 1e-300L;
+    return v <= (long double)x - m;
+}
+bool plane_ge(float o, float sc, uint32_t q, float x) {   // o + sc*q >= x
+    if (q == 0) return o >= x;
+    const long double v = (long double)o + (long double)sc * (long double)q;
+    const long double m = fabsl((long double)x) * 8.67e-19L + 1e-300L;
+    return v >= (long double)x + m;
+}
 
 // Quantises one axis of the slot boxes: chooses the scale exponent and the
 // outward-rounded 8-bit bounds; returns false if no exponent fits.
@@ -115,7 +131,7 @@ bool quantise_axis(const float* lo, const float* hi, int n, float& origin, uint8
         e = (int)std::ceil(std::log2(want)) + 127;
         if (e < 1) e = 1;
     }
-    for (; e <= 254; ++e) {
+    for (; e <= 167; ++e) {   // scale <= 2^40 keeps scale / d finite in the kernel
         float sc;
         const uint32_t bits = (uint32_t)e << 23;
         std::memcpy(&sc, &bits, 4);
@@ -123,12 +139,12 @@ bool quantise_axis(const float* lo, const float* hi, int n, float& origin, uint8
         for (int k = 0; k < n && ok; ++k) {
             double fl = std::floor(((double)lo[k] - (double)origin) / sc);
             long q = (long)std::max(0.0, std::min(255.0, fl));
-            while (q > 0 && decode(origin, sc, (uint32_t)q) > lo[k]) --q;
-            if (decode(origin, sc, (uint32_t)q) > lo[k]) { ok = false; break; }
+            while (q > 0 && !plane_le(origin, sc, (uint32_t)q, lo[k])) --q;
+            if (!plane_le(origin, sc, (uint32_t)q, lo[k])) { ok = false; break; }
             double ch = std::ceil(((double)hi[k] - (double)origin) / sc);
             long r = (long)std::max(0.0, std::min(255.0, ch));
-            while (r < 255 && decode(origin, sc, (uint32_t)r) < hi[k]) ++r;
-            if (decode(origin, sc, (uint32_t)r) < hi[k]) { ok = false; break; }
+            while (r < 255 && !plane_ge(origin, sc, (uint32_t)r, hi[k])) ++r;
+            if (!plane_ge(origin, sc, (uint32_t)r, hi[k])) { ok = false; break; }
             if (r < q) r = q;
             qlo[k] = (uint8_t)q;
             qhi[k] = (uint8_t)r;

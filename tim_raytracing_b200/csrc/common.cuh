@@ -36,6 +36,8 @@ struct SceneView {
     uint32_t num_lights;
     uint32_t leaf_words;
     uint32_t num_vertex;
+    uint32_t depth;             // binary tree depth (stack entries needed)
+    uint32_t wide_depth;        // 8-wide tree depth
     // 8-wide quantised form (null when not built)
     const uint4* wnodes;        // WideNode, 5 x 16 B
     const float4* wtris;        // 3 x float4 per leaf triangle: (p0, vo) (e1, i01) (e2, i2m)

@@ -10,6 +10,9 @@ namespace timrt {
 // Launch shape of the persistent trace kernels (chosen by the autotuner).
 struct LaunchConfig {
     int block = 128;    // threads per block: 64, 128 or 256
+    int stack_depth = 0;  // traversal-stack entries per thread; 0 = the scene's tree depth
+    int refill_min = 16;  // a warp fetches new rays once this many lanes are idle (1..32)
+    int wide_order = 1;   // 8-wide slot order: 1 = full nearest-first sort, 0 = nearest first, rest by slot
     bool wide = false;  // 8-wide quantised BVH instead of the reference binary layout
     // when set, a counting variant of the kernel adds per-ray work to
     // stats[0..4] = (rays, node visits, leaf visits, triangle tests, node reloads)
@@ -22,10 +25,14 @@ cudaError_t launch_trace_batch(const SceneView& s, const tim_rt_ray* rays, uint3
                                uint32_t* nid, float* bary, uint32_t* counter, uint32_t* err, cudaStream_t stream,
                                const LaunchConfig& cfg);
 
-// counters: [0] pixel work counter, [1] secondary queue length, [2] secondary work counter.
+// Secondary rays are queued in camera_queue_kinds() segments of seg_cap = W*H slots.
+// counters: [0] pixel work, [1] secondary work, [2..27] per-kind counts,
+// [28..54] per-kind prefix ([54] = secondary rays traced).
+uint32_t camera_queue_kinds();
+constexpr uint32_t kCamCounterWords = 55, kCamTotalWord = 54;
 cudaError_t launch_camera(const SceneView& s, const tim_rt_pass_data& pd, uint32_t flags, uint32_t seed,
                           const uint32_t* tile_counts, const uint32_t* tile_lists, uint32_t* out, uint32_t* bounce_out,
-                          uint32_t* leaf_nid, tim_rt_ray* q_rays, uint32_t* q_pixel, uint32_t q_capacity,
+                          uint32_t* leaf_nid, tim_rt_ray* q_rays, uint32_t* q_pixel, uint32_t seg_cap,
                           uint32_t* counters, uint32_t* err, uint64_t* d_ray_count, cudaStream_t stream,
                           const LaunchConfig& cfg);
 

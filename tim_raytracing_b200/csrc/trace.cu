@@ -6,7 +6,12 @@
 // items from a global atomic counter (one atomicAdd per refill, issued by one
 // elected lane). A policy object turns a work item into a ray (load) and
 // writes the result (store): plain ray batches, camera pixels, secondary
-// (shadow / probe-visibility / bounce) rays, probe rays.
+// (shadow / probe-visibility / bounce) rays.
+//
+// Coherence: camera work items walk the frame in 8x4-pixel tiles (32 pixels =
+// one warp), and the secondary rays of those pixels are queued by kind -- sun,
+// tile-light slot j, probe corner i, bounce -- in one segment per kind, so a
+// warp traces 32 rays of the same kind from neighbouring pixels.
 #include <cuda_runtime.h>
 #include <cstdio>
 #include "common.cuh"
@@ -16,6 +21,22 @@
 #include "../../include/tim_rt.h"
 
 namespace timrt {
+
+// Secondary-ray kinds, one queue segment each.
+constexpr uint32_t kKindSun = 0, kKindLight0 = 1, kKindProbe0 = 17, kKindBounce = 25, kNumKinds = 26;
+
+// Work item -> pixel in 8x4 tiles (row-major tiles over the frame).
+__device__ __forceinline__ bool tile_pixel(uint32_t i, uint32_t W, uint32_t H, uint32_t& px, uint32_t& py) {
+    const uint32_t tiles_x = (W + 7u) >> 3;
+    const uint32_t tile = i >> 5, within = i & 31u;
+    px = (tile % tiles_x) * 8u + (within & 7u);
+    py = (tile / tiles_x) * 4u + (within >> 3);
+    return px < W && py < H;
+}
+
+__host__ __device__ __forceinline__ uint32_t tiled_work_items(uint32_t W, uint32_t H) {
+    return ((W + 7u) >> 3) * ((H + 3u) >> 2) * 32u;
+}
 
 // -------------------------------------------------------------------- policies
 
@@ -50,58 +71,82 @@ struct BatchPolicy {
     __device__ __forceinline__ void skip(uint32_t) const {}
 };
 
-// cameraPass.comp:44-76: one work item per output pixel.
+// cameraPass.comp:44-76 pinhole ray of invocation (gx, gy) (cameraPass.comp:50-54).
+__device__ __forceinline__ void camera_ray(const tim_rt_pass_data& pd, uint32_t gx, uint32_t gy, float& dx, float& dy,
+                                           float& dz) {
+    const float fx = (float)gx, fy = (float)gy;
+    const float swx = (pd.frustumCorner10[0] - pd.frustumCorner00[0]) * pd.invFrameSize[0];
+    const float swy = (pd.frustumCorner10[1] - pd.frustumCorner00[1]) * pd.invFrameSize[0];
+    const float swz = (pd.frustumCorner10[2] - pd.frustumCorner00[2]) * pd.invFrameSize[0];
+    const float shx = (pd.frustumCorner01[0] - pd.frustumCorner00[0]) * pd.invFrameSize[1];
+    const float shy = (pd.frustumCorner01[1] - pd.frustumCorner00[1]) * pd.invFrameSize[1];
+    const float shz = (pd.frustumCorner01[2] - pd.frustumCorner00[2]) * pd.invFrameSize[1];
+    const float tx = (pd.frustumCorner00[0] + swx * fx) + shx * fy;
+    const float ty = (pd.frustumCorner00[1] + swy * fx) + shy * fy;
+    const float tz = (pd.frustumCorner00[2] + swz * fx) + shz * fy;
+    const float vx = tx - pd.cameraPos[0], vy = ty - pd.cameraPos[1], vz = tz - pd.cameraPos[2];
+    const float len = sqrtf(dot3(vx, vy, vz, vx, vy, vz));   // normalize(v) = v / sqrt(dot(v, v))
+    dx = vx / len;
+    dy = vy / len;
+    dz = vz / len;
+}
+
+// One work item per pixel, tile order. Output row py is traced by invocation
+// gy = 16*ceil(H/16) - py (cameraPass.comp:46), so row 0 is never traced.
 struct CameraPolicy {
     tim_rt_pass_data pd;
     uint32_t ngy16;         // 16 * ceil(H / 16)
     uint4* out;             // 2 x uint4 per pixel
     uint32_t* leaf_nid;     // per pixel, for the leaf-light shadow mask
 
-    __device__ __forceinline__ bool load(const SceneView&, uint32_t pix, TravState& st) const {
-        const uint32_t W = pd.frameSize[0];
-        const uint32_t px = pix % W, py = pix / W;
-        if (py == 0u) return false;   // never produced by the reference's row mapping
-        const uint32_t gx = px, gy = ngy16 - py;
-        const float fx = (float)gx, fy = (float)gy;
-        const float swx = (pd.frustumCorner10[0] - pd.frustumCorner00[0]) * pd.invFrameSize[0];
-        const float swy = (pd.frustumCorner10[1] - pd.frustumCorner00[1]) * pd.invFrameSize[0];
-        const float swz = (pd.frustumCorner10[2] - pd.frustumCorner00[2]) * pd.invFrameSize[0];
-        const float shx = (pd.frustumCorner01[0] - pd.frustumCorner00[0]) * pd.invFrameSize[1];
-        const float shy = (pd.frustumCorner01[1] - pd.frustumCorner00[1]) * pd.invFrameSize[1];
-        const float shz = (pd.frustumCorner01[2] - pd.frustumCorner00[2]) * pd.invFrameSize[1];
-        const float tx = (pd.frustumCorner00[0] + swx * fx) + shx * fy;
-        const float ty = (pd.frustumCorner00[1] + swy * fx) + shy * fy;
-        const float tz = (pd.frustumCorner00[2] + swz * fx) + shz * fy;
-        const float vx = tx - pd.cameraPos[0], vy = ty - pd.cameraPos[1], vz = tz - pd.cameraPos[2];
-        const float len = sqrtf(dot3(vx, vy, vz, vx, vy, vz));
+    __device__ __forceinline__ bool load(const SceneView&, uint32_t i, TravState& st) const {
+        uint32_t px, py;
+        if (!tile_pixel(i, pd.frameSize[0], pd.frameSize[1], px, py) || py == 0u) return false;
+        st.slot = py * pd.frameSize[0] + px;
+        camera_ray(pd, px, ngy16 - py, st.r.dx, st.r.dy, st.r.dz);
         st.r.ox = pd.cameraPos[0]; st.r.oy = pd.cameraPos[1]; st.r.oz = pd.cameraPos[2];
-        st.r.dx = vx / len; st.r.dy = vy / len; st.r.dz = vz / len;
         st.t = kTMax;
         st.any = false;
         return true;
     }
-    __device__ __forceinline__ void store(const SceneView&, uint32_t pix, const TravState& st, float) const {
+    __device__ __forceinline__ void store(const SceneView&, uint32_t, const TravState& st, float) const {
+        const uint32_t pix = st.slot;
         out[2u * pix] = make_uint4(st.rec0, st.rec1, st.rec2, __float_as_uint(st.t));
         out[2u * pix + 1u] = make_uint4(0u, 0u, 0u, 0u);
         leaf_nid[pix] = st.hit ? st.nid : 0xFFFFFFFFu;
     }
-    __device__ __forceinline__ void skip(uint32_t pix) const {
+    __device__ __forceinline__ void skip(uint32_t i) const {
+        uint32_t px, py;
+        if (!tile_pixel(i, pd.frameSize[0], pd.frameSize[1], px, py)) return;
+        const uint32_t pix = py * pd.frameSize[0] + px;
         out[2u * pix] = make_uint4(0u, 0u, 0u, 0u);
         out[2u * pix + 1u] = make_uint4(0u, 0u, 0u, 0u);
         leaf_nid[pix] = 0xFFFFFFFFu;
     }
 };
 
-// Secondary rays generated from camera hits. ray.flags: bit 0 any-hit, bits
-// 8..15 the mask bit, bits 16..17 the kind (0 shadow mask, 1 probe mask, 2 bounce).
+// Secondary rays queued by kind: segment k holds seg_cap slots; prefix[k] is
+// the first work item of kind k and prefix[kNumKinds] the total.
+// ray.flags: bit 0 any-hit, bits 8..15 the mask bit, bits 16..17 the output
+// (0 shadow mask, 1 probe mask, 2 bounce record).
 struct SecondaryPolicy {
     const tim_rt_ray* rays;
     const uint32_t* pixel;
+    const uint32_t* prefix;
+    uint32_t seg_cap;
     uint32_t* out_words;    // tracingData as u32 words (8 per pixel)
     uint4* bounce_out;
 
     __device__ __forceinline__ bool load(const SceneView&, uint32_t i, TravState& st) const {
-        const float4* rp = reinterpret_cast<const float4*>(rays + i);
+        uint32_t lo = 0, hi = kNumKinds;   // largest k with prefix[k] <= i
+        while (hi - lo > 1u) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (__ldg(prefix + mid) <= i) lo = mid;
+            else hi = mid;
+        }
+        const uint32_t slot = lo * seg_cap + (i - __ldg(prefix + lo));
+        st.slot = slot;
+        const float4* rp = reinterpret_cast<const float4*>(rays + slot);
         const float4 a = __ldg(rp), b = __ldg(rp + 1);
         st.r.ox = a.x; st.r.oy = a.y; st.r.oz = a.z;
         st.r.dx = b.x; st.r.dy = b.y; st.r.dz = b.z;
@@ -109,10 +154,11 @@ struct SecondaryPolicy {
         st.any = (__float_as_uint(b.w) & 1u) != 0u;
         return true;
     }
-    __device__ __forceinline__ void store(const SceneView&, uint32_t i, const TravState& st, float) const {
-        const uint32_t fl = __float_as_uint(__ldg(reinterpret_cast<const float*>(rays + i) + 7));
+    __device__ __forceinline__ void store(const SceneView&, uint32_t, const TravState& st, float) const {
+        const uint32_t slot = st.slot;
+        const uint32_t fl = __float_as_uint(__ldg(reinterpret_cast<const float*>(rays + slot) + 7));
         const uint32_t kind = (fl >> 16) & 3u, bit = (fl >> 8) & 0xFFu;
-        const uint32_t p = __ldg(pixel + i);
+        const uint32_t p = __ldg(pixel + slot);
         if (kind == 2u) {
             bounce_out[p] = make_uint4(st.rec0, st.rec1, st.rec2, __float_as_uint(st.t));
         } else if (st.hit) {
@@ -124,11 +170,14 @@ struct SecondaryPolicy {
 
 // -------------------------------------------------------------------- persistent loop
 
+// sdepth: traversal-stack entries per thread (the tree depth; <= 32). The stack
+// lives in dynamic shared memory, entry k of thread t at [k * BLOCK + t]
+// (binary form) or [(2k, 2k+1) * BLOCK + t] (8-wide form).
 template <int BLOCK, bool WIDE, bool STATS, class Policy>
 __global__ void __launch_bounds__(BLOCK) k_persistent(SceneView s, Policy P, uint32_t n_static,
                                                       const uint32_t* n_dev, uint32_t* counter, uint32_t* err,
-                                                      unsigned long long* stats) {
-    extern __shared__ uint32_t stack_mem[];   // (WIDE ? 2 : 1) * kStackSize * BLOCK words
+                                                      unsigned long long* stats, int sdepth, int refill_min) {
+    extern __shared__ uint32_t stack_mem[];
     uint32_t* stk = stack_mem + threadIdx.x;
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t n = n_dev ? *n_dev : n_static;
@@ -142,7 +191,9 @@ __global__ void __launch_bounds__(BLOCK) k_persistent(SceneView s, Policy P, uin
     for (;;) {
         if (!exhausted) {
             const uint32_t need = __ballot_sync(0xFFFFFFFFu, !active);
-            if (need) {
+            // refill once at least refill_min lanes are idle (32: whole-warp
+            // batches, which keeps coherent rays of a batch in lockstep)
+            if (need && (__popc(need) >= refill_min || need == 0xFFFFFFFFu)) {
                 const int leader = __ffs(need) - 1;
                 uint32_t base = 0;
                 if ((int)lane == leader) base = atomicAdd(counter, (uint32_t)__popc(need));
@@ -169,8 +220,8 @@ __global__ void __launch_bounds__(BLOCK) k_persistent(SceneView s, Policy P, uin
             continue;
         }
         if (active) {
-            if (WIDE) wide_step<BLOCK>(s, st, stk, err);
-            else plain_step<BLOCK>(s, st, stk, err);
+            if (WIDE) wide_step<BLOCK>(s, st, stk, err, sdepth);
+            else plain_step<BLOCK>(s, st, stk, err, sdepth);
             if (st.done) {
                 P.store(s, idx, st, tmax0);
                 if (STATS) {
@@ -230,8 +281,8 @@ struct GenParams {
     uint4* bounce_out;
     tim_rt_ray* q_rays;
     uint32_t* q_pixel;
-    uint32_t* q_count;
-    uint32_t q_capacity;
+    uint32_t* q_counts;     // kNumKinds counters
+    uint32_t seg_cap;
 };
 
 __device__ __forceinline__ void lpf_position(const tim_rt_pass_data& pd, uint32_t cx, uint32_t cy, uint32_t cz,
@@ -245,53 +296,61 @@ __device__ __forceinline__ void lpf_position(const tim_rt_pass_data& pd, uint32_
     z = pd.sceneMinExtent[2] + stz * ((float)cz + 0.5f);
 }
 
+// Appends one ray of `kind` for the lanes with has == true: warp-aggregated
+// atomic on the kind's counter, lane order preserved inside the segment.
+__device__ __forceinline__ void emit(const GenParams& g, uint32_t kind, bool has, uint32_t pix, float ox, float oy,
+                                     float oz, float tmax, float dx, float dy, float dz, uint32_t flags) {
+    const uint32_t m = __ballot_sync(0xFFFFFFFFu, has);
+    if (!m) return;
+    const uint32_t lane = threadIdx.x & 31u;
+    const int leader = __ffs(m) - 1;
+    uint32_t base = 0;
+    if ((int)lane == leader) base = atomicAdd(g.q_counts + kind, (uint32_t)__popc(m));
+    base = __shfl_sync(0xFFFFFFFFu, base, leader);
+    if (has) {
+        const uint32_t off = base + __popc(m & lanemask_lt());
+        if (off < g.seg_cap) {
+            const uint64_t slot = (uint64_t)kind * g.seg_cap + off;
+            float4* rp = reinterpret_cast<float4*>(g.q_rays + slot);
+            rp[0] = make_float4(ox, oy, oz, tmax);
+            rp[1] = make_float4(dx, dy, dz, __uint_as_float(flags));
+            g.q_pixel[slot] = pix;
+        }
+    }
+}
+
 // For each camera hit, emit the rays of computeAdditionalHitData
 // (baseRaytracingPass.glsl:85-97): the sun shadow ray and one ray per light of
 // the hit leaf's list (bvhLighting.glsl:143-163) or of the pixel's tile list,
 // the 8 probe-visibility segments (bvhLighting.glsl:165-184) and the bounce.
 // Lights out of range set their bit directly (evalShadow returns true,
-// bvhLighting.glsl:121-124).
+// bvhLighting.glsl:121-124). One thread per pixel, pixels in 8x4 tiles.
 __global__ void __launch_bounds__(256) k_gen_secondary(SceneView s, GenParams g) {
-    const uint32_t W = g.pd.frameSize[0], H = g.pd.frameSize[1];
-    const uint32_t pix = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t lane = threadIdx.x & 31u;
-    tim_rt_ray local[1 + 16 + 8 + 1];
-    uint32_t nr = 0;
-    uint32_t direct_bits = 0;
-    bool valid = pix < W * H;
+    const tim_rt_pass_data& pd = g.pd;
+    const uint32_t W = pd.frameSize[0], H = pd.frameSize[1];
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t px = 0, py = 0;
+    const bool valid = i < tiled_work_items(W, H) && tile_pixel(i, W, H, px, py);
+    const uint32_t pix = py * W + px;
     uint4 rec = make_uint4(0, 0, 0, 0);
     if (valid) rec = reinterpret_cast<const uint4*>(g.out_words)[2u * pix];
     const float t = __uint_as_float(rec.w);
-    const uint32_t py = valid ? pix / W : 0u;
-    if (valid && py != 0u && t < kTMax) {
-        const uint32_t px = pix % W, gx = px, gy = g.ngy16 - py;
-        // primary ray (same arithmetic as CameraPolicy::load)
-        const tim_rt_pass_data& pd = g.pd;
-        const float fx = (float)gx, fy = (float)gy;
-        const float swx = (pd.frustumCorner10[0] - pd.frustumCorner00[0]) * pd.invFrameSize[0];
-        const float swy = (pd.frustumCorner10[1] - pd.frustumCorner00[1]) * pd.invFrameSize[0];
-        const float swz = (pd.frustumCorner10[2] - pd.frustumCorner00[2]) * pd.invFrameSize[0];
-        const float shx = (pd.frustumCorner01[0] - pd.frustumCorner00[0]) * pd.invFrameSize[1];
-        const float shy = (pd.frustumCorner01[1] - pd.frustumCorner00[1]) * pd.invFrameSize[1];
-        const float shz = (pd.frustumCorner01[2] - pd.frustumCorner00[2]) * pd.invFrameSize[1];
-        const float tx = (pd.frustumCorner00[0] + swx * fx) + shx * fy;
-        const float ty = (pd.frustumCorner00[1] + swy * fx) + shy * fy;
-        const float tz = (pd.frustumCorner00[2] + swz * fx) + shz * fy;
-        const float vx = tx - pd.cameraPos[0], vy = ty - pd.cameraPos[1], vz = tz - pd.cameraPos[2];
-        const float len = sqrtf(dot3(vx, vy, vz, vx, vy, vz));
-        const float dx = vx / len, dy = vy / len, dz = vz / len;
+    const bool hit = valid && py != 0u && t < kTMax;
+    const uint32_t gx = px, gy = g.ngy16 - py;
+    float dx = 0.f, dy = 0.f, dz = 0.f, hx = 0.f, hy = 0.f, hz = 0.f;
+    if (hit) {
+        camera_ray(pd, gx, gy, dx, dy, dz);
         // baseRaytracingPass.glsl:91 hitPos = from + dir * t
-        const float hx = pd.cameraPos[0] + dx * t, hy = pd.cameraPos[1] + dy * t, hz = pd.cameraPos[2] + dz * t;
-        // sun ray (tmax = TMAX)
-        {
-            tim_rt_ray& r = local[nr++];
-            r.o[0] = hx; r.o[1] = hy; r.o[2] = hz; r.tmax = kTMax;
-            r.d[0] = -pd.sunDir[0]; r.d[1] = -pd.sunDir[1]; r.d[2] = -pd.sunDir[2];
-            r.flags = 1u | (0u << 8) | (0u << 16);
-        }
-        // light list
-        const uint32_t* list;
-        uint32_t count;
+        hx = pd.cameraPos[0] + dx * t;
+        hy = pd.cameraPos[1] + dy * t;
+        hz = pd.cameraPos[2] + dz * t;
+    }
+    // sun ray, tmax = TMAX (bvhLighting.glsl:148-149)
+    emit(g, kKindSun, hit, pix, hx, hy, hz, kTMax, -pd.sunDir[0], -pd.sunDir[1], -pd.sunDir[2], 1u);
+    // light list of the tile or of the hit leaf
+    const uint32_t* list = nullptr;
+    uint32_t count = 0;
+    if (hit) {
         if (g.flags & TIM_RT_CAM_TILE_LIGHTS) {
             const uint32_t tile = (gy / 16u) * g.tiles_x + gx / 16u;
             list = g.tile_lists + 16u * tile;
@@ -306,26 +365,31 @@ __global__ void __launch_bounds__(256) k_gen_secondary(SceneView s, GenParams g)
             count = (hdr >> (kTriBits + kBlasBits + kPrimBits)) & ((1u << kLightBits) - 1u);
             list = s.leaf + skip + 1u + off;
         }
-        for (uint32_t i = 0; i < count; ++i) {
-            const uint32_t li = __ldg(list + i);
+    }
+    uint32_t direct_bits = 0;
+    for (uint32_t j = 0; j < 16u; ++j) {
+        bool has = false;
+        float lx = 0.f, ly = 0.f, lz = 0.f, rl = 1.f;
+        uint32_t bit = 0;
+        if (j < count) {
+            const uint32_t li = __ldg(list + j);
             const float* L = s.lights + 14u * li;
-            if (__float_as_uint(__ldg(L)) != kLightSphere) continue;   // evalShadow returns false
-            const float lx = __ldg(L + 1) - hx, ly = __ldg(L + 2) - hy, lz = __ldg(L + 3) - hz;
-            const float radius = __ldg(L + 4);
-            const float rl = sqrtf(dot3(lx, ly, lz, lx, ly, lz));
-            const uint32_t bit = li + 1u;
-            if (bit >= 32u) continue;   // the 32-bit mask has no bit for this light
-            if (rl < radius) {
-                tim_rt_ray& r = local[nr++];
-                r.o[0] = hx; r.o[1] = hy; r.o[2] = hz; r.tmax = rl;
-                r.d[0] = lx / rl; r.d[1] = ly / rl; r.d[2] = lz / rl;
-                r.flags = 1u | (bit << 8) | (0u << 16);
-            } else {
-                direct_bits |= 1u << bit;
+            bit = li + 1u;
+            if (__float_as_uint(__ldg(L)) == kLightSphere && bit < 32u) {   // evalShadow: sphere lights only
+                lx = __ldg(L + 1) - hx;
+                ly = __ldg(L + 2) - hy;
+                lz = __ldg(L + 3) - hz;
+                rl = sqrtf(dot3(lx, ly, lz, lx, ly, lz));
+                if (rl < __ldg(L + 4)) has = true;
+                else direct_bits |= 1u << bit;   // out of range counts as masked
             }
         }
-        if (g.flags & TIM_RT_CAM_PROB_MASK) {
-            // lightprobHelpers.glsl:71-77 getLightProbCoordUVW and bvhLighting.glsl:170-180
+        emit(g, kKindLight0 + j, has, pix, hx, hy, hz, rl, lx / rl, ly / rl, lz / rl, 1u | (bit << 8));
+    }
+    if (g.flags & TIM_RT_CAM_PROB_MASK) {
+        // lightprobHelpers.glsl:71-77 getLightProbCoordUVW and bvhLighting.glsl:170-180
+        uint32_t cx = 0, cy = 0, cz = 0;
+        if (hit) {
             const uint32_t* res = pd.lpfResolution;
             const float stx = (pd.sceneMaxExtent[0] - pd.sceneMinExtent[0]) / (float)res[0];
             const float sty = (pd.sceneMaxExtent[1] - pd.sceneMinExtent[1]) / (float)res[1];
@@ -337,17 +401,19 @@ __global__ void __launch_bounds__(256) k_gen_secondary(SceneView s, GenParams g)
             uy = fminf(fmaxf(uy, 0.0f), (float)res[1] - 1.0f);
             uz = fminf(fmaxf(uz, 0.0f), (float)res[2] - 1.0f);
             const uint32_t ix = (uint32_t)(int32_t)ux, iy = (uint32_t)(int32_t)uy, iz = (uint32_t)(int32_t)uz;
-            const uint32_t cx = min(ix, res[0] - 2u), cy = min(iy, res[1] - 2u), cz = min(iz, res[2] - 2u);
-            for (uint32_t i = 0; i < 8u; ++i) {
-                float qx, qy, qz;
-                lpf_position(pd, cx + (i & 1u), cy + ((i >> 1) & 1u), cz + ((i >> 2) & 1u), qx, qy, qz);
-                tim_rt_ray& r = local[nr++];
-                r.o[0] = hx; r.o[1] = hy; r.o[2] = hz; r.tmax = 1.0f;
-                r.d[0] = qx - hx; r.d[1] = qy - hy; r.d[2] = qz - hz;
-                r.flags = 1u | (i << 8) | (1u << 16);
-            }
+            cx = min(ix, res[0] - 2u);
+            cy = min(iy, res[1] - 2u);
+            cz = min(iz, res[2] - 2u);
         }
-        if (g.flags & TIM_RT_CAM_BOUNCE) {
+        for (uint32_t k = 0; k < 8u; ++k) {
+            float qx = 0.f, qy = 0.f, qz = 0.f;
+            if (hit) lpf_position(pd, cx + (k & 1u), cy + ((k >> 1) & 1u), cz + ((k >> 2) & 1u), qx, qy, qz);
+            emit(g, kKindProbe0 + k, hit, pix, hx, hy, hz, 1.0f, qx - hx, qy - hy, qz - hz, 1u | (k << 8) | (1u << 16));
+        }
+    }
+    if (g.flags & TIM_RT_CAM_BOUNCE) {
+        float bx = 0.f, by = 0.f, bz = 0.f;
+        if (hit) {
             // geometric normal of the hit triangle, facing the incoming ray
             const uint32_t i0 = rec.x + (rec.y & 0xFFFFu), i1 = rec.x + (rec.y >> 16), i2 = rec.x + (rec.z & 0xFFFFu);
             const float p0x = s.pos[3u * i0], p0y = s.pos[3u * i0 + 1], p0z = s.pos[3u * i0 + 2];
@@ -357,49 +423,30 @@ __global__ void __launch_bounds__(256) k_gen_secondary(SceneView s, GenParams g)
             const float nl = sqrtf(dot3(nx, ny, nz, nx, ny, nz));
             nx = nx / nl; ny = ny / nl; nz = nz / nl;
             if (dot3(nx, ny, nz, dx, dy, dz) > 0.0f) { nx = -nx; ny = -ny; nz = -nz; }
-            float bx, by, bz;
             bounce_dir(nx, ny, nz, pix, g.seed, bx, by, bz);
-            tim_rt_ray& r = local[nr++];
-            r.o[0] = hx; r.o[1] = hy; r.o[2] = hz; r.tmax = kTMax;
-            r.d[0] = bx; r.d[1] = by; r.d[2] = bz;
-            r.flags = 0u | (0u << 8) | (2u << 16);
         }
+        emit(g, kKindBounce, hit, pix, hx, hy, hz, kTMax, bx, by, bz, 2u << 16);
     }
     if (valid) {
         g.out_words[8u * pix + 4u] = direct_bits;
         g.out_words[8u * pix + 5u] = 0u;
         if (g.bounce_out) g.bounce_out[pix] = make_uint4(0u, 0u, 0u, 0u);
     }
-    // warp-aggregated append into the secondary queue
-    uint32_t incl = nr;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-        if ((int)lane >= o) incl += v;
-    }
-    const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
-    uint32_t base = 0;
-    if (lane == 31u && total) base = atomicAdd(g.q_count, total);
-    base = __shfl_sync(0xFFFFFFFFu, base, 31);
-    const uint32_t my = base + incl - nr;
-    for (uint32_t k = 0; k < nr; ++k) {
-        const uint32_t slot = my + k;
-        if (slot < g.q_capacity) {
-            g.q_rays[slot] = local[k];
-            g.q_pixel[slot] = pix;
-        }
-    }
 }
 
-// Clamp the queue count to its capacity (the generator sizes the queue for the
-// worst case, so this only guards the trace kernel's bounds).
-__global__ void k_clamp_count(uint32_t* q_count, uint32_t cap) {
-    if (*q_count > cap) *q_count = cap;
+// prefix[k] = first work item of kind k over the (capacity-clamped) segment counts.
+__global__ void k_kind_prefix(const uint32_t* q_counts, uint32_t* prefix, uint32_t cap) {
+    uint32_t acc = 0;
+    for (uint32_t k = 0; k < kNumKinds; ++k) {
+        prefix[k] = acc;
+        acc += min(q_counts[k], cap);
+    }
+    prefix[kNumKinds] = acc;
 }
 
 // Adds the frame's ray count (primary rays of rows 1..H-1 plus the secondary queue).
-__global__ void k_add_ray_count(uint64_t* dst, uint64_t primary, const uint32_t* q_count) {
-    *dst += primary + *q_count;
+__global__ void k_add_ray_count(uint64_t* dst, uint64_t primary, const uint32_t* total) {
+    *dst += primary + *total;
 }
 
 // -------------------------------------------------------------------- tile light culling
@@ -474,47 +521,53 @@ __global__ void __launch_bounds__(256) k_cull_lights(SceneView s, tim_rt_pass_da
 // -------------------------------------------------------------------- launchers
 
 template <int BLOCK, bool WIDE>
-constexpr size_t stack_bytes() {
-    return sizeof(uint32_t) * (WIDE ? 2 : 1) * kStackSize * BLOCK;
+constexpr size_t stack_bytes(int depth) {
+    return sizeof(uint32_t) * (WIDE ? 2 : 1) * (size_t)depth * BLOCK;
 }
 
 // Grid of the persistent kernels: as many resident blocks as the occupancy
-// calculator allows on every SM (the dynamic shared memory holds the stacks).
+// calculator allows on every SM for this stack depth (cached per depth).
 template <int BLOCK, bool WIDE, bool STATS, class Policy>
-static int grid_for() {
-    static int blocks = 0;
-    if (!blocks) {
+static int grid_for(int depth) {
+    static int blocks[kStackSize + 1] = {};
+    if (!blocks[depth]) {
         int dev = 0, sms = 0, per = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         cudaFuncSetAttribute(k_persistent<BLOCK, WIDE, STATS, Policy>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)stack_bytes<BLOCK, WIDE>());
+                             (int)stack_bytes<BLOCK, WIDE>(kStackSize));
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_persistent<BLOCK, WIDE, STATS, Policy>, BLOCK,
-                                                      stack_bytes<BLOCK, WIDE>());
-        blocks = sms * (per > 0 ? per : 1);
+                                                      stack_bytes<BLOCK, WIDE>(depth));
+        blocks[depth] = sms * (per > 0 ? per : 1);
     }
-    return blocks;
+    return blocks[depth];
 }
 
 template <int BLOCK, bool WIDE, bool STATS, class Policy>
 static void launch_block(const SceneView& s, const Policy& P, uint32_t n_static, const uint32_t* n_dev,
-                         uint32_t* counter, uint32_t* err, unsigned long long* stats, cudaStream_t stream) {
-    k_persistent<BLOCK, WIDE, STATS, Policy>
-        <<<grid_for<BLOCK, WIDE, STATS, Policy>(), BLOCK, stack_bytes<BLOCK, WIDE>(), stream>>>(s, P, n_static, n_dev,
-                                                                                            counter, err, stats);
+                         uint32_t* counter, uint32_t* err, unsigned long long* stats, int depth, int refill,
+                         cudaStream_t stream) {
+    k_persistent<BLOCK, WIDE, STATS, Policy><<<grid_for<BLOCK, WIDE, STATS, Policy>(depth), BLOCK,
+                                               stack_bytes<BLOCK, WIDE>(depth), stream>>>(s, P, n_static, n_dev,
+                                                                                          counter, err, stats, depth,
+                                                                                          refill);
 }
 
 template <bool WIDE, class Policy>
 static cudaError_t launch_persistent(const SceneView& s, const Policy& P, uint32_t n_static, const uint32_t* n_dev,
                                      uint32_t* counter, uint32_t* err, cudaStream_t stream, const LaunchConfig& cfg) {
+    int depth = WIDE ? (int)s.wide_depth : (int)s.depth;
+    if (cfg.stack_depth > depth) depth = cfg.stack_depth;
+    depth = depth < 1 ? 1 : (depth > kStackSize ? kStackSize : depth);
+    const int refill = cfg.refill_min < 1 ? 1 : (cfg.refill_min > 32 ? 32 : cfg.refill_min);
     if (cfg.stats) {
-        launch_block<128, WIDE, true>(s, P, n_static, n_dev, counter, err, cfg.stats, stream);
+        launch_block<128, WIDE, true>(s, P, n_static, n_dev, counter, err, cfg.stats, depth, refill, stream);
         return cudaGetLastError();
     }
     switch (cfg.block) {
-        case 64: launch_block<64, WIDE, false>(s, P, n_static, n_dev, counter, err, nullptr, stream); break;
-        case 256: launch_block<256, WIDE, false>(s, P, n_static, n_dev, counter, err, nullptr, stream); break;
-        default: launch_block<128, WIDE, false>(s, P, n_static, n_dev, counter, err, nullptr, stream); break;
+        case 64: launch_block<64, WIDE, false>(s, P, n_static, n_dev, counter, err, nullptr, depth, refill, stream); break;
+        case 256: launch_block<256, WIDE, false>(s, P, n_static, n_dev, counter, err, nullptr, depth, refill, stream); break;
+        default: launch_block<128, WIDE, false>(s, P, n_static, n_dev, counter, err, nullptr, depth, refill, stream); break;
     }
     return cudaGetLastError();
 }
@@ -527,18 +580,24 @@ cudaError_t launch_trace_batch(const SceneView& s, const tim_rt_ray* rays, uint3
     return launch_persistent<false>(s, P, n, nullptr, counter, err, stream, cfg);
 }
 
+uint32_t camera_queue_segment(uint32_t W, uint32_t H) { return W * H; }
+uint32_t camera_queue_kinds() { return kNumKinds; }
+
 cudaError_t launch_camera(const SceneView& s, const tim_rt_pass_data& pd, uint32_t flags, uint32_t seed,
                           const uint32_t* tile_counts, const uint32_t* tile_lists, uint32_t* out, uint32_t* bounce_out,
-                          uint32_t* leaf_nid, tim_rt_ray* q_rays, uint32_t* q_pixel, uint32_t q_capacity,
+                          uint32_t* leaf_nid, tim_rt_ray* q_rays, uint32_t* q_pixel, uint32_t seg_cap,
                           uint32_t* counters, uint32_t* err, uint64_t* d_ray_count, cudaStream_t stream,
                           const LaunchConfig& cfg) {
     const uint32_t W = pd.frameSize[0], H = pd.frameSize[1];
-    const uint32_t npix = W * H;
+    const uint32_t items = tiled_work_items(W, H);
     const uint32_t ngy16 = 16u * ((H + 15u) / 16u);
+    // counters: [0] pixel work, [1] secondary work, [2..27] kind counts, [28..54] kind prefix
+    uint32_t* q_counts = counters + 2;
+    uint32_t* prefix = counters + 2 + kNumKinds;
     CameraPolicy CP{pd, ngy16, reinterpret_cast<uint4*>(out), leaf_nid};
     if (cfg.phase_ev) cudaEventRecord(cfg.phase_ev[0], stream);
-    cudaError_t e = cfg.wide ? launch_persistent<true>(s, CP, npix, nullptr, counters + 0, err, stream, cfg)
-                             : launch_persistent<false>(s, CP, npix, nullptr, counters + 0, err, stream, cfg);
+    cudaError_t e = cfg.wide ? launch_persistent<true>(s, CP, items, nullptr, counters + 0, err, stream, cfg)
+                             : launch_persistent<false>(s, CP, items, nullptr, counters + 0, err, stream, cfg);
     if (e != cudaSuccess) return e;
     if (cfg.phase_ev) cudaEventRecord(cfg.phase_ev[1], stream);
     GenParams g;
@@ -554,18 +613,18 @@ cudaError_t launch_camera(const SceneView& s, const tim_rt_pass_data& pd, uint32
     g.bounce_out = reinterpret_cast<uint4*>(bounce_out);
     g.q_rays = q_rays;
     g.q_pixel = q_pixel;
-    g.q_count = counters + 1;
-    g.q_capacity = q_capacity;
-    k_gen_secondary<<<(npix + 255u) / 256u, 256, 0, stream>>>(s, g);
+    g.q_counts = q_counts;
+    g.seg_cap = seg_cap;
+    k_gen_secondary<<<(items + 255u) / 256u, 256, 0, stream>>>(s, g);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    k_clamp_count<<<1, 1, 0, stream>>>(counters + 1, q_capacity);
+    k_kind_prefix<<<1, 1, 0, stream>>>(q_counts, prefix, seg_cap);
     if (cfg.phase_ev) cudaEventRecord(cfg.phase_ev[2], stream);
-    SecondaryPolicy SP{q_rays, q_pixel, out, reinterpret_cast<uint4*>(bounce_out)};
-    e = cfg.wide ? launch_persistent<true>(s, SP, 0u, counters + 1, counters + 2, err, stream, cfg)
-                 : launch_persistent<false>(s, SP, 0u, counters + 1, counters + 2, err, stream, cfg);
+    SecondaryPolicy SP{q_rays, q_pixel, prefix, seg_cap, out, reinterpret_cast<uint4*>(bounce_out)};
+    e = cfg.wide ? launch_persistent<true>(s, SP, 0u, prefix + kNumKinds, counters + 1, err, stream, cfg)
+                 : launch_persistent<false>(s, SP, 0u, prefix + kNumKinds, counters + 1, err, stream, cfg);
     if (cfg.phase_ev) cudaEventRecord(cfg.phase_ev[3], stream);
     if (e != cudaSuccess || !d_ray_count) return e;
-    k_add_ray_count<<<1, 1, 0, stream>>>(d_ray_count, (uint64_t)W * (H - 1u), counters + 1);
+    k_add_ray_count<<<1, 1, 0, stream>>>(d_ray_count, (uint64_t)W * (H - 1u), prefix + kNumKinds);
     return cudaGetLastError();
 }
 

@@ -28,6 +28,7 @@ struct TravState {
     float u, v;
     // work counters (dead code unless a counting kernel reads them)
     uint32_t c_node, c_leaf, c_tri, c_reload;
+    uint32_t slot;      // policy scratch (pixel or queue slot of the ray)
     // 8-wide form only
     float ix, iy, iz;   // 1 / direction
     uint32_t order;     // remaining slots of the current wide node, nearest first
@@ -100,7 +101,8 @@ __device__ __forceinline__ void plain_leaf(const SceneView& s, TravState& st, ui
 // One traversal step: descend to the next leaf (or exhaust the stack), test it,
 // and pop the next pending subtree. Returns with st.done set when the ray ends.
 template <int BLOCK>
-__device__ __forceinline__ void plain_step(const SceneView& s, TravState& st, uint32_t* stk, uint32_t* err) {
+__device__ __forceinline__ void plain_step(const SceneView& s, TravState& st, uint32_t* stk, uint32_t* err,
+                                           int sdepth) {
     uint32_t node = st.node;
     while (!(node & kNidLeafBit)) {
         const float4* np = s.nodes + 4u * node;
@@ -126,7 +128,7 @@ __device__ __forceinline__ void plain_step(const SceneView& s, TravState& st, ui
         }
         if (d0 >= 0.0f && d1 >= 0.0f) {
             const bool first1 = d1 < d0;
-            if (st.sp >= kStackSize) {   // unreachable for validated trees (depth <= 32)
+            if (st.sp >= sdepth) {   // unreachable: the stack holds the tree depth
                 atomicOr(err, 1u);
                 st.done = true;
                 return;

@@ -1,42 +1,54 @@
 // trace_wide.cuh -- traversal of the 8-wide BVH with 8-bit quantised child bounds.
 //
-// Node layout (80 B = 5 x 16 B, built by wide_build.cpp from the reference's
-// binary tree):
-//   w0..w2  origin (float) of the quantisation grid
-//   w3      ex | ey << 8 | ez << 16 | imask << 24   (scale per axis = 2^(e-127);
+// Node layout (80 B = 5 x 16 B, built by bvh_layout.cpp from the reference's
+// binary tree; the compressed wide-node idea follows Ylitie, Karras & Laine,
+// "Efficient Incoherent Ray Traversal on GPUs Through Compressed Wide BVHs",
+// HPG 2017, with a layout of our own):
+//   w0..w2  origin o (float) of the quantisation grid
+//   w3      ex | ey << 8 | ez << 16 | imask << 24   (scale per axis s = 2^(e-127);
 //           imask bit k: slot k is an internal wide node)
 //   w4      index of the first internal child node (internal children are contiguous)
 //   w5      first triangle (in the leaf-triangle array) of this node's leaf slots
 //   w6,w7   meta byte per slot: triangle count of a leaf slot (0 = empty / internal)
 //   w8..w19 qlo_x[8] qlo_y[8] qlo_z[8] qhi_x[8] qhi_y[8] qhi_z[8]
-// Slot k's box decodes to lo = origin + scale * qlo, hi = origin + scale * qhi
-// (an exact product and one rounded add); the builder chooses qlo / qhi so the
-// decoded float box contains the box the reference stores for that subtree.
+// Slot k spans [o + s*qlo, o + s*qhi] per axis (real arithmetic); the builder
+// rounds outward so this box contains the box the reference stores for the
+// subtree.
 //
 // Leaf triangles are stored as 3 x float4: (p0, vertexOffset) (p1-p0, index01)
 // (p2-p0, index2_matId) -- the edges are the same rounded differences
 // CollideTriangle computes, so the triangle test stays bit-identical.
 //
-// Box test: the reference's slab test divides by the direction; here it
-// multiplies by 1/d and then widens near/far by a relative 2^-18, which covers
-// the (<= 2^-21 relative) difference between the two forms. Together with the
-// outward-rounded bounds, a child whose reference box test passes always
-// passes here: the quantised traversal never loses a hit the binary one finds.
+// Box test, and why it never rejects a child the reference accepts. Per node
+// and axis the kernel forms A = RN(RN(o - r) * inv) and B = s * inv (exact: s is
+// a power of two), with inv = RN(1/d), and evaluates every plane as one fused
+// multiply-add t = RN(q * B + A). Against the exact distance T = (o + s*q - r)/d
+// the error is below 3u|A| + 2u|T| (u = 2^-24). The |A| part is absorbed by
+// moving A itself by |A| * 2^-18 (outward: down for near planes, up for far
+// planes), the |T| part by scaling the final near / far by (1 -+ 2^-18). Near
+// and far planes are picked from the sign of inv, which for d != 0 equals the
+// min / max of the two slab distances. A zero direction component is replaced
+// by +-2^-80 for this test only: the slab then holds every t the reference's
+// test (which divides by zero) accepts, and all values stay finite.
+// So tmin_here <= tmin_reference and tmax_here >= tmax_reference for every
+// child: the quantised traversal visits a superset of the binary traversal's
+// leaves and never loses a hit.
 #pragma once
 #include "common.cuh"
 #include "trace_plain.cuh"
 
 namespace timrt {
 
-__device__ __forceinline__ float wdecode(float o, float sc, uint32_t word, uint32_t k) {
-    const uint32_t q = (word >> (8u * k)) & 0xFFu;
-    return o + sc * (float)q;
+constexpr float kWiden = 3.814697265625e-06f;   // 2^-18
+
+// Byte k of `word` as a float (0x4B0000qq is 2^23 + q exactly).
+__device__ __forceinline__ float wbyte(uint32_t word, uint32_t k) {
+    return __uint_as_float(__byte_perm(word, 0x4B000000u, 0x7650u | k)) - 8388608.0f;
 }
 
 // Tests the 8 slots of wide node `ni` and returns the hit slots ordered by
 // entry distance: bits 0..23 = slots (3 bits each, nearest first), bits 24..27 = count.
-__device__ __forceinline__ uint32_t wide_visit(const SceneView& s, const TravState& st, float ix, float iy, float iz,
-                                               uint32_t ni, WideHdr& h) {
+__device__ __forceinline__ uint32_t wide_visit(const SceneView& s, const TravState& st, uint32_t ni, WideHdr& h) {
     const uint4* np = s.wnodes + 5u * ni;
     const uint4 U0 = __ldg(np), U1 = __ldg(np + 1), U2 = __ldg(np + 2), U3 = __ldg(np + 3), U4 = __ldg(np + 4);
     h.imask = U0.w >> 24;
@@ -44,10 +56,22 @@ __device__ __forceinline__ uint32_t wide_visit(const SceneView& s, const TravSta
     h.tri_base = U1.y;
     h.meta_lo = U1.z;
     h.meta_hi = U1.w;
-    const float ox = __uint_as_float(U0.x), oy = __uint_as_float(U0.y), oz = __uint_as_float(U0.z);
-    const float sx = __uint_as_float((U0.w & 0xFFu) << 23);
-    const float sy = __uint_as_float(((U0.w >> 8) & 0xFFu) << 23);
-    const float sz = __uint_as_float(((U0.w >> 16) & 0xFFu) << 23);
+    const float ix = st.ix, iy = st.iy, iz = st.iz;
+    // per-axis plane coefficients: t = q * B + A
+    const float Bx = __uint_as_float((U0.w & 0xFFu) << 23) * ix;
+    const float By = __uint_as_float(((U0.w >> 8) & 0xFFu) << 23) * iy;
+    const float Bz = __uint_as_float(((U0.w >> 16) & 0xFFu) << 23) * iz;
+    const float Ax = (__uint_as_float(U0.x) - st.r.ox) * ix;
+    const float Ay = (__uint_as_float(U0.y) - st.r.oy) * iy;
+    const float Az = (__uint_as_float(U0.z) - st.r.oz) * iz;
+    const float Anx = __fmaf_rn(-fabsf(Ax), kWiden, Ax), Afx = __fmaf_rn(fabsf(Ax), kWiden, Ax);
+    const float Any = __fmaf_rn(-fabsf(Ay), kWiden, Ay), Afy = __fmaf_rn(fabsf(Ay), kWiden, Ay);
+    const float Anz = __fmaf_rn(-fabsf(Az), kWiden, Az), Afz = __fmaf_rn(fabsf(Az), kWiden, Az);
+    // near / far plane words from the direction's sign
+    const bool negx = __float_as_uint(ix) >> 31, negy = __float_as_uint(iy) >> 31, negz = __float_as_uint(iz) >> 31;
+    const uint32_t nx0 = negx ? U3.z : U2.x, nx1 = negx ? U3.w : U2.y, fx0 = negx ? U2.x : U3.z, fx1 = negx ? U2.y : U3.w;
+    const uint32_t ny0 = negy ? U4.x : U2.z, ny1 = negy ? U4.y : U2.w, fy0 = negy ? U2.z : U4.x, fy1 = negy ? U2.w : U4.y;
+    const uint32_t nz0 = negz ? U4.z : U3.x, nz1 = negz ? U4.w : U3.y, fz0 = negz ? U3.x : U4.z, fz1 = negz ? U3.y : U4.w;
     const float tcur = st.t;
     uint32_t key[8];
 #pragma unroll
@@ -55,23 +79,16 @@ __device__ __forceinline__ uint32_t wide_visit(const SceneView& s, const TravSta
         const uint32_t wsel = k < 4u ? 0u : 1u, kk = k & 3u;
         const uint32_t meta = ((wsel ? h.meta_hi : h.meta_lo) >> (8u * kk)) & 0xFFu;
         const bool valid = ((h.imask >> k) & 1u) || meta != 0u;
-        const float lx = wdecode(ox, sx, wsel ? U2.y : U2.x, kk);
-        const float ly = wdecode(oy, sy, wsel ? U2.w : U2.z, kk);
-        const float lz = wdecode(oz, sz, wsel ? U3.y : U3.x, kk);
-        const float hx = wdecode(ox, sx, wsel ? U3.w : U3.z, kk);
-        const float hy = wdecode(oy, sy, wsel ? U4.y : U4.x, kk);
-        const float hz = wdecode(oz, sz, wsel ? U4.w : U4.z, kk);
-        const float t0x = (lx - st.r.ox) * ix, t1x = (hx - st.r.ox) * ix;
-        const float t0y = (ly - st.r.oy) * iy, t1y = (hy - st.r.oy) * iy;
-        const float t0z = (lz - st.r.oz) * iz, t1z = (hz - st.r.oz) * iz;
-        float nearv = fmaxf(fminf(t0x, t1x), fmaxf(fminf(t0y, t1y), fminf(t0z, t1z)));
-        float farv = fminf(fmaxf(t0x, t1x), fminf(fmaxf(t0y, t1y), fmaxf(t0z, t1z)));
-        // widen by a relative 2^-18; a product keeps +-inf (direction component 0)
-        // infinite, where a subtraction of |x| * eps would turn inf into NaN
-        nearv = nearv * (nearv > 0.0f ? 0.999996185302734375f : 1.000003814697265625f);
-        farv = farv * (farv > 0.0f ? 1.000003814697265625f : 0.999996185302734375f);
-        const float tmin = fmaxf(0.0f, nearv);
-        const float tm = fminf(tcur, farv);
+        const float tnx = __fmaf_rn(wbyte(wsel ? nx1 : nx0, kk), Bx, Anx);
+        const float tny = __fmaf_rn(wbyte(wsel ? ny1 : ny0, kk), By, Any);
+        const float tnz = __fmaf_rn(wbyte(wsel ? nz1 : nz0, kk), Bz, Anz);
+        const float tfx = __fmaf_rn(wbyte(wsel ? fx1 : fx0, kk), Bx, Afx);
+        const float tfy = __fmaf_rn(wbyte(wsel ? fy1 : fy0, kk), By, Afy);
+        const float tfz = __fmaf_rn(wbyte(wsel ? fz1 : fz0, kk), Bz, Afz);
+        const float nearv = fmaxf(tnx, fmaxf(tny, tnz));
+        const float farv = fminf(tfx, fminf(tfy, tfz));
+        const float tmin = fmaxf(0.0f, __fmaf_rn(-fabsf(nearv), kWiden, nearv));
+        const float tm = fminf(tcur, __fmaf_rn(fabsf(farv), kWiden, farv));
         const bool hit = valid && (tmin < tm);
         // non-negative floats order like their bit patterns; the low 3 bits carry the slot
         key[k] = hit ? ((__float_as_uint(tmin) & ~7u) | k) : 0xFFFFFFFFu;
@@ -113,6 +130,8 @@ __device__ __forceinline__ void wide_read_hdr(const SceneView& s, uint32_t ni, W
     h.meta_hi = U1.w;
 }
 
+// Tests the triangles of leaf slot `slot` in their stored order (bvh_collide /
+// bvh_collide_fast semantics, bvhCollision.glsl:177-284).
 template <int BLOCK>
 __device__ __forceinline__ void wide_leaf(const SceneView& s, TravState& st, const WideHdr& h, uint32_t slot) {
     const uint32_t below_lo = slot >= 4u ? h.meta_lo : (slot == 0u ? 0u : (h.meta_lo & ((1u << (8u * slot)) - 1u)));
@@ -144,10 +163,13 @@ __device__ __forceinline__ void wide_leaf(const SceneView& s, TravState& st, con
     }
 }
 
+// 1 / d for the quantised box test; a zero component becomes +-2^-80 (see above).
+__device__ __forceinline__ float wide_inv(float d) { return 1.0f / (d == 0.0f ? copysignf(8.271806125530277e-25f, d) : d); }
+
 __device__ __forceinline__ void wide_init(const SceneView& s, TravState& st, uint32_t*) {
-    st.ix = 1.0f / st.r.dx;
-    st.iy = 1.0f / st.r.dy;
-    st.iz = 1.0f / st.r.dz;
+    st.ix = wide_inv(st.r.dx);
+    st.iy = wide_inv(st.r.dy);
+    st.iz = wide_inv(st.r.dz);
     st.sp = 0;
     st.done = false;
     st.hit = false;
@@ -165,7 +187,7 @@ __device__ __forceinline__ void wide_init(const SceneView& s, TravState& st, uin
         st.order = 1u << 24;
     } else {
         st.c_node++;
-        st.order = wide_visit(s, st, st.ix, st.iy, st.iz, 0u, st.h);
+        st.order = wide_visit(s, st, 0u, st.h);
     }
 }
 
@@ -173,7 +195,8 @@ __device__ __forceinline__ void wide_init(const SceneView& s, TravState& st, uin
 // of the current node is pushed as one (node, order) entry), until one leaf
 // slot has been tested or the traversal ends.
 template <int BLOCK>
-__device__ __forceinline__ void wide_step(const SceneView& s, TravState& st, uint32_t* stk, uint32_t* err) {
+__device__ __forceinline__ void wide_step(const SceneView& s, TravState& st, uint32_t* stk, uint32_t* err,
+                                          int sdepth) {
     for (;;) {
         const uint32_t cnt = st.order >> 24;
         if (cnt == 0u) {
@@ -193,7 +216,7 @@ __device__ __forceinline__ void wide_step(const SceneView& s, TravState& st, uin
         if ((st.h.imask >> slot) & 1u) {
             const uint32_t child = st.h.child_base + __popc(st.h.imask & ((1u << slot) - 1u));
             if ((st.order >> 24) != 0u) {
-                if (st.sp >= kStackSize) {   // unreachable: wide depth <= binary depth <= 32
+                if (st.sp >= sdepth) {   // unreachable: the stack holds the 8-wide tree depth
                     atomicOr(err, 1u);
                     st.done = true;
                     return;
@@ -204,7 +227,7 @@ __device__ __forceinline__ void wide_step(const SceneView& s, TravState& st, uin
             }
             st.node = child;
             st.c_node++;
-            st.order = wide_visit(s, st, st.ix, st.iy, st.iz, child, st.h);
+            st.order = wide_visit(s, st, child, st.h);
         } else {
             wide_leaf<BLOCK>(s, st, st.h, slot);
             return;
