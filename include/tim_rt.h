@@ -197,6 +197,30 @@ int tim_rt_trace_camera_dev(tim_rt_ctx *ctx, tim_rt_scene_id scene, const tim_rt
                             uint32_t seed, const uint32_t *d_tile_counts, const uint32_t *d_tile_lists,
                             uint32_t *d_out, uint32_t *d_bounce_out, uint64_t *d_ray_count, void *cuda_stream);
 
+/* Camera trace that allocates nothing. It has no counterpart in the reference.
+ * For callers that may not allocate device memory while they trace (a fixed
+ * device budget owned by their engine, a CUDA graph being captured around the
+ * call, or a frame loop that cannot take cudaMalloc's synchronisation): the
+ * caller passes its own device copies of the BVH buffer (fillGpuBuffer image),
+ * the vertex positions, the tile lists and the outputs; the scratch (counters,
+ * hit-leaf ids, secondary-ray queue) is a static device array inside the
+ * library, which holds it on every GPU that loads it until the process exits
+ * (3.85 MB). Frames are limited to TIM_RT_NOALLOC_MAX_PIXELS pixels; larger
+ * ones return TIM_RT_EINVAL. Same results as tim_rt_trace_camera_dev on the
+ * binary form (flags PROB_MASK, TILE_LIGHTS, BOUNCE only). tree_depth is the
+ * depth tim_rt_validate_bvh reports (0 = 32); the buffer must have passed that
+ * check, since this call reads device memory it cannot validate. The first call
+ * on a device looks up the scratch address (cudaGetSymbolAddress) and should
+ * come before any stream capture. All calls share the one scratch array:
+ * calls whose kernels overlap on the GPU (different streams, no ordering) race.
+ * Stream-ordered, no synchronisation. */
+#define TIM_RT_NOALLOC_MAX_PIXELS 4096u
+int tim_rt_trace_camera_noalloc(const void *d_bvh, const uint32_t ranges[7][2], const tim_rt_push_constants *pc,
+                                const float *d_pos, uint32_t num_vertex, uint32_t tree_depth,
+                                const tim_rt_pass_data *pd, uint32_t flags, uint32_t seed,
+                                const uint32_t *d_tile_counts, const uint32_t *d_tile_lists,
+                                uint32_t *d_out, uint32_t *d_bounce_out, void *cuda_stream);
+
 /* Tile light-frustum culling, cullWithFrustumTile's light section
  * (src/Shaders/cullFrustum.glsl:63-100,136-151). One list of at most 16 light
  * ids per tile, ascending (the reference's order is atomic-arrival order). */

@@ -28,7 +28,7 @@ EXPORTED = [
     "tim_rt_upload_bvh", "tim_rt_free_scene", "tim_rt_scene_bytes", "tim_rt_trace", "tim_rt_trace_dev",
     "tim_rt_trace_camera", "tim_rt_cull_lights", "tim_rt_build_params_default", "tim_rt_build_bvh",
     "tim_rt_bvh_blob_info", "tim_rt_bvh_blob_free", "tim_rt_validate_bvh", "tim_rt_trace_camera_dev",
-    "tim_rt_cull_lights_dev", "tim_rt_get_launch_config", "tim_rt_set_launch_config",
+    "tim_rt_cull_lights_dev", "tim_rt_get_launch_config", "tim_rt_set_launch_config", "tim_rt_trace_camera_noalloc",
 ]
 
 
@@ -96,6 +96,8 @@ def lib() -> ctypes.CDLL:
     L.tim_rt_trace_camera_dev.argtypes = [vp, u32, vp, u32, u32, vp, vp, vp, vp, vp, vp]
     L.tim_rt_cull_lights_dev.argtypes = [vp, u32, vp, u32, u32, vp, vp, vp]
     L.tim_rt_get_launch_config.argtypes = [vp, ctypes.POINTER(LaunchConfig)]
+    L.tim_rt_trace_camera_noalloc.argtypes = [vp, vp, ctypes.POINTER(PushConstants), vp, u32, u32, vp, u32, u32, vp,
+                                              vp, vp, vp, vp]
     L.tim_rt_set_launch_config.argtypes = [vp, ctypes.POINTER(LaunchConfig)]
     for name in EXPORTED:
         if name not in ("tim_rt_version", "tim_rt_last_error", "tim_rt_build_params_default", "tim_rt_bvh_blob_free"):
