@@ -104,6 +104,9 @@ typedef struct {
     /* camera calls: device time of the primary trace, the secondary-ray
      * generation and the secondary trace kernels (CUDA events) */
     float primary_ms, gen_ms, secondary_ms;
+    /* camera calls with TIM_RT_CAM_COUNT: the secondary-trace kernel's share of the counters */
+    uint64_t secondary_rays_counted, secondary_node_visits, secondary_leaf_visits, secondary_tri_tests,
+        secondary_node_reloads;
 } tim_rt_stats;
 
 /* ---------------------------------------------------------------- context */
@@ -129,6 +132,11 @@ typedef struct {
 } tim_rt_launch_config;
 int tim_rt_get_launch_config(tim_rt_ctx *ctx, tim_rt_launch_config *cfg);
 int tim_rt_set_launch_config(tim_rt_ctx *ctx, const tim_rt_launch_config *cfg);
+
+/* Measures L2 read bandwidth (GB/s) on `device` by reading a `bytes`-sized
+ * buffer (1..64 MiB, i.e. L2-resident) `passes` times. A measurement utility for
+ * roofline reporting; no counterpart in the reference. */
+int tim_rt_measure_l2_bandwidth(int device, uint64_t bytes, int passes, float *gbs);
 
 /* ---------------------------------------------------------------- BVH upload */
 /* Replaces BVHData::build's CreateBuffer + UploadBuffer (src/Renderer/BVHData.cpp:43-48)

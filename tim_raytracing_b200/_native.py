@@ -29,6 +29,7 @@ EXPORTED = [
     "tim_rt_trace_camera", "tim_rt_cull_lights", "tim_rt_build_params_default", "tim_rt_build_bvh",
     "tim_rt_bvh_blob_info", "tim_rt_bvh_blob_free", "tim_rt_validate_bvh", "tim_rt_trace_camera_dev",
     "tim_rt_cull_lights_dev", "tim_rt_get_launch_config", "tim_rt_set_launch_config", "tim_rt_trace_camera_noalloc",
+    "tim_rt_measure_l2_bandwidth",
 ]
 
 
@@ -48,7 +49,9 @@ class Stats(ctypes.Structure):
                 ("probe_rays", ctypes.c_uint64), ("bounce_rays", ctypes.c_uint64), ("kernel_ms", ctypes.c_float),
                 ("total_ms", ctypes.c_float), ("node_visits", ctypes.c_uint64), ("leaf_visits", ctypes.c_uint64),
                 ("tri_tests", ctypes.c_uint64), ("node_reloads", ctypes.c_uint64), ("primary_ms", ctypes.c_float),
-                ("gen_ms", ctypes.c_float), ("secondary_ms", ctypes.c_float)]
+                ("gen_ms", ctypes.c_float), ("secondary_ms", ctypes.c_float), ("secondary_rays_counted", ctypes.c_uint64),
+                ("secondary_node_visits", ctypes.c_uint64), ("secondary_leaf_visits", ctypes.c_uint64),
+                ("secondary_tri_tests", ctypes.c_uint64), ("secondary_node_reloads", ctypes.c_uint64)]
 
 
 class LaunchConfig(ctypes.Structure):
@@ -96,6 +99,7 @@ def lib() -> ctypes.CDLL:
     L.tim_rt_trace_camera_dev.argtypes = [vp, u32, vp, u32, u32, vp, vp, vp, vp, vp, vp]
     L.tim_rt_cull_lights_dev.argtypes = [vp, u32, vp, u32, u32, vp, vp, vp]
     L.tim_rt_get_launch_config.argtypes = [vp, ctypes.POINTER(LaunchConfig)]
+    L.tim_rt_measure_l2_bandwidth.argtypes = [i32, u64, i32, ctypes.POINTER(ctypes.c_float)]
     L.tim_rt_trace_camera_noalloc.argtypes = [vp, vp, ctypes.POINTER(PushConstants), vp, u32, u32, vp, u32, u32, vp,
                                               vp, vp, vp, vp]
     L.tim_rt_set_launch_config.argtypes = [vp, ctypes.POINTER(LaunchConfig)]
@@ -153,6 +157,12 @@ def validate(img: BvhImage, num_vertex: int) -> int:
     _check(lib().tim_rt_validate_bvh(data.ctypes.data, data.nbytes, ranges.ctypes.data, ctypes.byref(pc), num_vertex,
                                      ctypes.byref(depth)))
     return depth.value
+
+
+def measure_l2_gbs(device: int = 0, nbytes: int = 32 << 20, passes: int = 50) -> float:
+    v = ctypes.c_float()
+    _check(lib().tim_rt_measure_l2_bandwidth(device, nbytes, passes, ctypes.byref(v)))
+    return float(v.value)
 
 
 def build_params(**kw) -> BuildParams:

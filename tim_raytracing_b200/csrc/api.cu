@@ -153,12 +153,17 @@ LaunchConfig cfg_for(tim_rt_ctx* c, const Scene* s, bool wide, bool count = fals
 
 // Copies the counting kernels' totals into the caller's stats (after a sync).
 void read_counts(tim_rt_ctx* c, tim_rt_stats* st) {
-    unsigned long long v[8] = {};
+    unsigned long long v[16] = {};
     cudaMemcpy(v, c->dstats.ptr, sizeof(v), cudaMemcpyDeviceToHost);
-    st->node_visits = v[1];
-    st->leaf_visits = v[2];
-    st->tri_tests = v[3];
-    st->node_reloads = v[4];
+    st->node_visits = v[1] + v[9];
+    st->leaf_visits = v[2] + v[10];
+    st->tri_tests = v[3] + v[11];
+    st->node_reloads = v[4] + v[12];
+    st->secondary_rays_counted = v[8];
+    st->secondary_node_visits = v[9];
+    st->secondary_leaf_visits = v[10];
+    st->secondary_tri_tests = v[11];
+    st->secondary_node_reloads = v[12];
 }
 
 }  // namespace
@@ -189,7 +194,7 @@ int tim_rt_create(int device, uint64_t mem_budget_bytes, tim_rt_ctx** out) {
     for (auto& e : c->pev) TIMRT_CUDA(cudaEventCreate(&e));
     int rc = dev_alloc(c.get(), c->counters, 4ull * kCounterWords);
     if (rc) return rc;
-    if ((rc = dev_alloc(c.get(), c->dstats, 64))) return rc;
+    if ((rc = dev_alloc(c.get(), c->dstats, 128))) return rc;
     TIMRT_CUDA(cudaMemset(c->counters.ptr, 0, 4ull * kCounterWords));
     *out = c.release();
     return TIM_RT_OK;
@@ -422,7 +427,7 @@ int tim_rt_trace(tim_rt_ctx* c, tim_rt_scene_id id, const tim_rt_ray* rays, uint
     uint32_t* ctr = static_cast<uint32_t*>(c->counters.ptr);
     uint32_t* err = ctr + kErrWord;
     const bool count = (mode & TIM_RT_TRACE_COUNT) != 0;
-    if (count) TIMRT_CUDA(cudaMemsetAsync(c->dstats.ptr, 0, 64, c->stream));
+    if (count) TIMRT_CUDA(cudaMemsetAsync(c->dstats.ptr, 0, 128, c->stream));
     TIMRT_CUDA(cudaEventRecord(c->ev[0], c->stream));
     TIMRT_CUDA(cudaMemcpyAsync(c->rays.ptr, rays, 32ull * n, cudaMemcpyHostToDevice, c->stream));
     TIMRT_CUDA(cudaMemsetAsync(ctr, 0, 4, c->stream));
@@ -584,7 +589,7 @@ int tim_rt_trace_camera(tim_rt_ctx* c, tim_rt_scene_id id, const tim_rt_pass_dat
     }
     TIMRT_CUDA(cudaMemsetAsync(ctr, 0, 4 * kCamCounterWords, c->stream));
     const bool count = (flags & TIM_RT_CAM_COUNT) != 0;
-    if (count) TIMRT_CUDA(cudaMemsetAsync(c->dstats.ptr, 0, 64, c->stream));
+    if (count) TIMRT_CUDA(cudaMemsetAsync(c->dstats.ptr, 0, 128, c->stream));
     TIMRT_CUDA(cudaEventRecord(c->ev[1], c->stream));
     LaunchConfig cam_cfg = cfg_for(c, s, (flags & TIM_RT_CAM_WIDE) != 0, count);
     cam_cfg.phase_ev = c->pev;

@@ -620,8 +620,10 @@ cudaError_t launch_camera(const SceneView& s, const tim_rt_pass_data& pd, uint32
     k_kind_prefix<<<1, 1, 0, stream>>>(q_counts, prefix, seg_cap);
     if (cfg.phase_ev) cudaEventRecord(cfg.phase_ev[2], stream);
     SecondaryPolicy SP{q_rays, q_pixel, prefix, seg_cap, out, reinterpret_cast<uint4*>(bounce_out)};
-    e = cfg.wide ? launch_persistent<true>(s, SP, 0u, prefix + kNumKinds, counters + 1, err, stream, cfg)
-                 : launch_persistent<false>(s, SP, 0u, prefix + kNumKinds, counters + 1, err, stream, cfg);
+    LaunchConfig cfg2 = cfg;   // the secondary kernel counts into stats[8..12]
+    if (cfg.stats) cfg2.stats = cfg.stats + 8;
+    e = cfg.wide ? launch_persistent<true>(s, SP, 0u, prefix + kNumKinds, counters + 1, err, stream, cfg2)
+                 : launch_persistent<false>(s, SP, 0u, prefix + kNumKinds, counters + 1, err, stream, cfg2);
     if (cfg.phase_ev) cudaEventRecord(cfg.phase_ev[3], stream);
     if (e != cudaSuccess || !d_ray_count) return e;
     k_add_ray_count<<<1, 1, 0, stream>>>(d_ray_count, (uint64_t)W * (H - 1u), prefix + kNumKinds);
