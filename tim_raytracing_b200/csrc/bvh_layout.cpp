@@ -117,6 +117,48 @@ bool plane_ge(float o, float sc, uint32_t q, float x) {   // o + sc*q >= x
     return v >= (long double)x + m;
 }
 
+// Places up to 8 children in the 8 slots by their direction from the node
+// centre: slot bit a set means "on the + side of axis a". The (child, slot)
+// pair that best matches is taken first (greedy; Ylitie et al. 2017 use an
+// auction for the same assignment). A ray then visits its hit slots in the
+// order slot XOR octant(ray), which is roughly front to back, with no sort.
+// A single-leaf root keeps its leaf in slot 0.
+void assign_octant_slots(const std::vector<Slot>& fr, bool single_leaf_root, int slot_child[8]) {
+    for (int k = 0; k < 8; ++k) slot_child[k] = -1;
+    const int n = (int)fr.size();
+    if (single_leaf_root || n == 0) {
+        for (int i = 0; i < n && i < 8; ++i) slot_child[i] = i;
+        return;
+    }
+    double c[3];
+    double cen[8][3];
+    for (int a = 0; a < 3; ++a) {
+        double mn = INFINITY, mx = -INFINITY;
+        for (int i = 0; i < n; ++i) {
+            mn = std::min(mn, (double)std::min(fr[i].lo[a], fr[i].hi[a]));
+            mx = std::max(mx, (double)std::max(fr[i].lo[a], fr[i].hi[a]));
+            cen[i][a] = 0.5 * ((double)fr[i].lo[a] + (double)fr[i].hi[a]);
+        }
+        c[a] = 0.5 * (mn + mx);
+    }
+    bool child_done[8] = {};
+    for (int step = 0; step < n; ++step) {
+        double best = INFINITY;
+        int bi = -1, bs = -1;
+        for (int i = 0; i < n; ++i) {
+            if (child_done[i]) continue;
+            for (int s = 0; s < 8; ++s) {
+                if (slot_child[s] >= 0) continue;
+                double cost = 0.0;
+                for (int a = 0; a < 3; ++a) cost -= (cen[i][a] - c[a]) * (((s >> a) & 1) ? 1.0 : -1.0);
+                if (cost < best) { best = cost; bi = i; bs = s; }
+            }
+        }
+        slot_child[bs] = bi;
+        child_done[bi] = true;
+    }
+}
+
 // Quantises one axis of the slot boxes: chooses the scale exponent and the
 // outward-rounded 8-bit bounds; returns false if no exponent fits.
 bool quantise_axis(const float* lo, const float* hi, int n, float& origin, uint8_t& ebiased, uint8_t* qlo, uint8_t* qhi) {
@@ -231,29 +273,42 @@ bool build_wide(const uint8_t* blob, const uint32_t ranges[7][2], uint32_t num_n
     while (!q.empty()) {
         Job job = std::move(q.front());
         q.pop_front();
-        const std::vector<Slot>& sl = job.slots;
         out.max_depth = std::max(out.max_depth, job.depth);
-        const int n = (int)sl.size();
+        // slot k of the node holds child slot_child[k] (-1 = empty)
+        const std::vector<Slot>& fr = job.slots;
+        int slot_child[8];
+        assign_octant_slots(fr, out.root_is_leaf != 0, slot_child);
+        const int nf = (int)fr.size();
         float lo[3][8], hi[3][8];
-        for (int k = 0; k < n; ++k)
+        for (int i = 0; i < nf; ++i)
             for (int a = 0; a < 3; ++a) {
-                lo[a][k] = std::min(sl[k].lo[a], sl[k].hi[a]);   // the slab test orders each axis itself
-                hi[a][k] = std::max(sl[k].lo[a], sl[k].hi[a]);
+                lo[a][i] = std::min(fr[i].lo[a], fr[i].hi[a]);   // the slab test orders each axis itself
+                hi[a][i] = std::max(fr[i].lo[a], fr[i].hi[a]);
             }
         uint32_t* w = out.nodes.data() + 20ull * job.w;
         std::memset(w, 0, 80);
-        uint8_t e[3] = {1, 1, 1}, qlo[3][8] = {}, qhi[3][8] = {};
+        uint8_t e[3] = {1, 1, 1}, cq_lo[3][8] = {}, cq_hi[3][8] = {}, qlo[3][8] = {}, qhi[3][8] = {};
         float origin[3] = {0.f, 0.f, 0.f};
-        if (n > 0) {
+        if (nf > 0) {
             for (int a = 0; a < 3; ++a)
-                if (!quantise_axis(lo[a], hi[a], n, origin[a], e[a], qlo[a], qhi[a])) {
+                if (!quantise_axis(lo[a], hi[a], nf, origin[a], e[a], cq_lo[a], cq_hi[a])) {
                     err = "box bounds cannot be quantised (non-finite coordinates)";
                     return false;
                 }
         }
+        Slot sl[8];
+        bool used[8] = {};
+        for (int k = 0; k < 8; ++k) {
+            const int i = slot_child[k];
+            if (i < 0) continue;
+            used[k] = true;
+            sl[k] = fr[i];
+            for (int a = 0; a < 3; ++a) { qlo[a][k] = cq_lo[a][i]; qhi[a][k] = cq_hi[a][i]; }
+        }
+        const int n = 8;
         uint32_t imask = 0, n_internal = 0;
         for (int k = 0; k < n; ++k)
-            if (!(sl[k].id & kLeafBit)) { imask |= 1u << k; ++n_internal; }
+            if (used[k] && !(sl[k].id & kLeafBit)) { imask |= 1u << k; ++n_internal; }
         const uint32_t child_base = out.num_nodes;
         out.num_nodes += n_internal;
         out.nodes.resize(20ull * out.num_nodes);
@@ -266,7 +321,7 @@ bool build_wide(const uint8_t* blob, const uint32_t ranges[7][2], uint32_t num_n
         w[5] = (uint32_t)(out.tris.size() / 12);
         uint8_t meta[8] = {};
         for (int k = 0; k < n; ++k) {
-            if (sl[k].id & kLeafBit) {
+            if (used[k] && (sl[k].id & kLeafBit)) {
                 const uint32_t nt = leaf_tris(sl[k].id);
                 if (nt > 255u) { err = "a leaf holds more than 255 triangles (8-wide slot limit)"; return false; }
                 meta[k] = (uint8_t)nt;
@@ -281,7 +336,7 @@ bool build_wide(const uint8_t* blob, const uint32_t ranges[7][2], uint32_t num_n
         }
         uint32_t ci = child_base;
         for (int k = 0; k < n; ++k) {
-            if (!(sl[k].id & kLeafBit)) {
+            if (used[k] && !(sl[k].id & kLeafBit)) {
                 Slot a, b;
                 child_slots(nodes[sl[k].id], a, b);
                 q.push_back({ci++, expand({a, b}), job.depth + 1u});
@@ -289,6 +344,7 @@ bool build_wide(const uint8_t* blob, const uint32_t ranges[7][2], uint32_t num_n
         }
     }
     if (out.max_depth > 32u) { err = "8-wide tree deeper than 32 levels"; return false; }
+    if (out.num_nodes >= (1u << 24)) { err = "more than 2^24 8-wide nodes"; return false; }
     return true;
 }
 

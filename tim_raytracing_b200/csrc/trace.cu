@@ -522,7 +522,7 @@ __global__ void __launch_bounds__(256) k_cull_lights(SceneView s, tim_rt_pass_da
 
 template <int BLOCK, bool WIDE>
 constexpr size_t stack_bytes(int depth) {
-    return sizeof(uint32_t) * (WIDE ? 2 : 1) * (size_t)depth * BLOCK;
+    return sizeof(uint32_t) * (size_t)depth * BLOCK;   // one word per entry in both forms
 }
 
 // Grid of the persistent kernels: as many resident blocks as the occupancy

@@ -31,7 +31,9 @@ struct TravState {
     uint32_t slot;      // policy scratch (pixel or queue slot of the ray)
     // 8-wide form only
     float ix, iy, iz;   // 1 / direction
-    uint32_t order;     // remaining slots of the current wide node, nearest first
+    uint32_t order;     // rank mask of the current wide node's hit slots still to visit
+    uint32_t oct;       // ray octant: bit a set when the direction's component a is negative
+    uint32_t first;     // rank of the nearest hit slot still to visit first (8 = none)
     WideHdr h;          // header of the current wide node
 };
 

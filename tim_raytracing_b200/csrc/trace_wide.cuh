@@ -46,9 +46,13 @@ __device__ __forceinline__ float wbyte(uint32_t word, uint32_t k) {
     return __uint_as_float(__byte_perm(word, 0x4B000000u, 0x7650u | k)) - 8388608.0f;
 }
 
-// Tests the 8 slots of wide node `ni` and returns the hit slots ordered by
-// entry distance: bits 0..23 = slots (3 bits each, nearest first), bits 24..27 = count.
-__device__ __forceinline__ uint32_t wide_visit(const SceneView& s, const TravState& st, uint32_t ni, WideHdr& h) {
+// Tests the 8 slots of wide node `ni` and returns the hit slots as a rank mask:
+// bit r set = slot r ^ octant(ray) was hit. Visiting ranks in increasing order is
+// roughly front to back because the builder placed each child in the slot of its
+// direction from the node centre (bit a = + side of axis a) and the octant bit a
+// is set for rays going towards -a.
+__device__ __forceinline__ uint32_t wide_visit(const SceneView& s, const TravState& st, uint32_t ni, WideHdr& h,
+                                               uint32_t& first) {
     const uint4* np = s.wnodes + 5u * ni;
     const uint4 U0 = __ldg(np), U1 = __ldg(np + 1), U2 = __ldg(np + 2), U3 = __ldg(np + 3), U4 = __ldg(np + 4);
     h.imask = U0.w >> 24;
@@ -73,7 +77,7 @@ __device__ __forceinline__ uint32_t wide_visit(const SceneView& s, const TravSta
     const uint32_t ny0 = negy ? U4.x : U2.z, ny1 = negy ? U4.y : U2.w, fy0 = negy ? U2.z : U4.x, fy1 = negy ? U2.w : U4.y;
     const uint32_t nz0 = negz ? U4.z : U3.x, nz1 = negz ? U4.w : U3.y, fz0 = negz ? U3.x : U4.z, fz1 = negz ? U3.y : U4.w;
     const float tcur = st.t;
-    uint32_t key[8];
+    uint32_t mask = 0, nearest = 0xFFFFFFFFu;
 #pragma unroll
     for (uint32_t k = 0; k < 8u; ++k) {
         const uint32_t wsel = k < 4u ? 0u : 1u, kk = k & 3u;
@@ -90,34 +94,13 @@ __device__ __forceinline__ uint32_t wide_visit(const SceneView& s, const TravSta
         const float tmin = fmaxf(0.0f, __fmaf_rn(-fabsf(nearv), kWiden, nearv));
         const float tm = fminf(tcur, __fmaf_rn(fabsf(farv), kWiden, farv));
         const bool hit = valid && (tmin < tm);
-        // non-negative floats order like their bit patterns; the low 3 bits carry the slot
-        key[k] = hit ? ((__float_as_uint(tmin) & ~7u) | k) : 0xFFFFFFFFu;
+        // slot k is visited at rank k ^ octant: children were placed by direction
+        mask |= (hit ? 1u : 0u) << (k ^ st.oct);
+        // the nearest hit slot goes first (non-negative floats order like their bits)
+        nearest = min(nearest, hit ? ((__float_as_uint(tmin) & ~7u) | (k ^ st.oct)) : 0xFFFFFFFFu);
     }
-    // sorting network for 8 keys (Batcher odd-even merge, 19 compare-exchanges)
-#define TIMRT_CX(a, b)                               \
-    {                                                \
-        const uint32_t lo_ = min(key[a], key[b]);    \
-        const uint32_t hi_ = max(key[a], key[b]);    \
-        key[a] = lo_;                                \
-        key[b] = hi_;                                \
-    }
-    TIMRT_CX(0, 1) TIMRT_CX(2, 3) TIMRT_CX(4, 5) TIMRT_CX(6, 7)
-    TIMRT_CX(0, 2) TIMRT_CX(1, 3) TIMRT_CX(4, 6) TIMRT_CX(5, 7)
-    TIMRT_CX(1, 2) TIMRT_CX(5, 6) TIMRT_CX(0, 4) TIMRT_CX(3, 7)
-    TIMRT_CX(1, 5) TIMRT_CX(2, 6)
-    TIMRT_CX(1, 4) TIMRT_CX(3, 6)
-    TIMRT_CX(2, 4) TIMRT_CX(3, 5)
-    TIMRT_CX(3, 4)
-#undef TIMRT_CX
-    uint32_t order = 0, cnt = 0;
-#pragma unroll
-    for (uint32_t k = 0; k < 8u; ++k) {
-        if (key[k] != 0xFFFFFFFFu) {
-            order |= (key[k] & 7u) << (3u * cnt);
-            ++cnt;
-        }
-    }
-    return order | (cnt << 24);
+    first = nearest & 7u;
+    return mask;
 }
 
 __device__ __forceinline__ void wide_read_hdr(const SceneView& s, uint32_t ni, WideHdr& h) {
@@ -170,6 +153,7 @@ __device__ __forceinline__ void wide_init(const SceneView& s, TravState& st, uin
     st.ix = wide_inv(st.r.dx);
     st.iy = wide_inv(st.r.dy);
     st.iz = wide_inv(st.r.dz);
+    st.oct = (__float_as_uint(st.ix) >> 31) | ((__float_as_uint(st.iy) >> 31) << 1) | ((__float_as_uint(st.iz) >> 31) << 2);
     st.sp = 0;
     st.done = false;
     st.hit = false;
@@ -184,50 +168,58 @@ __device__ __forceinline__ void wide_init(const SceneView& s, TravState& st, uin
     }
     if (s.wide_root_is_leaf) {   // the reference intersects a single-leaf tree without a box test
         wide_read_hdr(s, 0u, st.h);
-        st.order = 1u << 24;
+        st.order = 1u << st.oct;   // slot 0
+        st.first = 8u;
     } else {
         st.c_node++;
-        st.order = wide_visit(s, st, 0u, st.h);
+        st.order = wide_visit(s, st, 0u, st.h, st.first);
     }
 }
 
-// One step: walk slots nearest-first, descending into internal slots (the rest
-// of the current node is pushed as one (node, order) entry), until one leaf
-// slot has been tested or the traversal ends.
+// One step: walk hit slots in rank order, descending into internal slots (the
+// rest of the current node is pushed as one (node << 8 | rank mask) entry),
+// until one leaf slot has been tested or the traversal ends.
 template <int BLOCK>
 __device__ __forceinline__ void wide_step(const SceneView& s, TravState& st, uint32_t* stk, uint32_t* err,
                                           int sdepth) {
     for (;;) {
-        const uint32_t cnt = st.order >> 24;
-        if (cnt == 0u) {
+        if (st.order == 0u) {
             if (st.sp == 0) {
                 st.done = true;
                 return;
             }
             --st.sp;
-            st.node = stk[(2 * st.sp) * BLOCK];
-            st.order = stk[(2 * st.sp + 1) * BLOCK];
+            const uint32_t e = stk[st.sp * BLOCK];
+            st.node = e >> 8;
+            st.order = e & 0xFFu;
+            st.first = 8u;
             wide_read_hdr(s, st.node, st.h);
             st.c_reload++;
             continue;
         }
-        const uint32_t slot = st.order & 7u;
-        st.order = ((st.order & 0xFFFFFFu) >> 3) | ((cnt - 1u) << 24);
+        uint32_t r;
+        if (st.first < 8u) {   // the nearest hit slot of a freshly visited node
+            r = st.first;
+            st.first = 8u;
+        } else {
+            r = (uint32_t)(__ffs(st.order) - 1);
+        }
+        st.order &= ~(1u << r);
+        const uint32_t slot = r ^ st.oct;
         if ((st.h.imask >> slot) & 1u) {
             const uint32_t child = st.h.child_base + __popc(st.h.imask & ((1u << slot) - 1u));
-            if ((st.order >> 24) != 0u) {
+            if (st.order != 0u) {
                 if (st.sp >= sdepth) {   // unreachable: the stack holds the 8-wide tree depth
                     atomicOr(err, 1u);
                     st.done = true;
                     return;
                 }
-                stk[(2 * st.sp) * BLOCK] = st.node;
-                stk[(2 * st.sp + 1) * BLOCK] = st.order;
+                stk[st.sp * BLOCK] = (st.node << 8) | st.order;   // fewer than 2^24 nodes (checked at build)
                 ++st.sp;
             }
             st.node = child;
             st.c_node++;
-            st.order = wide_visit(s, st, child, st.h);
+            st.order = wide_visit(s, st, child, st.h, st.first);
         } else {
             wide_leaf<BLOCK>(s, st, st.h, slot);
             return;
