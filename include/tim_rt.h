@@ -238,6 +238,47 @@ int tim_rt_cull_lights(tim_rt_ctx *ctx, tim_rt_scene_id scene, const tim_rt_pass
 int tim_rt_cull_lights_dev(tim_rt_ctx *ctx, tim_rt_scene_id scene, const tim_rt_pass_data *pd,
                            uint32_t tiles_x, uint32_t tiles_y, uint32_t *d_counts, uint32_t *d_lists, void *cuda_stream);
 
+/* ---------------------------------------------------------------- light-probe field */
+/* Probe field update: genLightProbField.comp (trace step and lighting step,
+ * src/Shaders/genLightProbField.comp:41-81) followed by updateLightProbField.comp
+ * (src/Shaders/updateLightProbField.comp:33-64), dispatched by
+ * LightProbFieldPass::traceLightProbField / updateLightProbField
+ * (src/Renderer/lightProbFieldPass.cpp:81-149).
+ *   - probe p (tiled 4x4x4 order, lightprobHelpers.glsl:33-61) sits at
+ *     aabbMin + (aabbMax - aabbMin) / resolution * (coord + 0.5); resolution must
+ *     be divisible by 4 on every axis;
+ *   - ray r of probe p goes along dirs[r].xyz (the caller's directions, e.g.
+ *     LightProbFieldPass::sampleRays or an octahedral grid), closest hit, then the
+ *     sun (direction -sunDir, not normalised, as lightProbFieldPass.cpp:29 passes it)
+ *     and leaf-light shadow mask; the probe-visibility mask is 0;
+ *   - lit value: computeLighting with NO_LPF (bvhLighting.glsl:42-85) with texColor 1,
+ *     the sky colour 0.3 * (200, 220, 255) / 255 on a miss (baseRaytracingPass.glsl:81);
+ *   - SH9: sum_r L_r * sh_basis[r][j] * 4*pi/num_dirs, new = prev * (1 - h) + sh * h
+ *     (GLSL mix), where prev is read from and new written to sh9_fp16: 7 RGBA16F
+ *     3-D images [7][res_z][res_y][res_x][4] in the channel layout of storeSH9
+ *     (lightprob/storeSH_inline.glsl:6-18);
+ *   - octa (TIM_RT_PROBE_OCTA): dirs form a side x side octahedral grid in row-major
+ *     order (side^2 = num_dirs, side a multiple of 8); texel (i*8/side, j*8/side)
+ *     of probe p holds the mean radiance of its rays, FP32 [probes][64][3]. Not in
+ *     the reference.
+ * Outputs of probes [probe_begin, probe_end) only; all optional except sh9_fp16.
+ * trace_out: [probes][num_dirs][8] u32 tracingData; irradiance: [probes][num_dirs][3];
+ * sh9_fp32: the new SH9 before FP16 rounding, [probes][9][3]. */
+typedef struct {
+    float aabbMin[4]; float aabbMax[4];
+    uint32_t resolution[4];
+    float sunDir[4]; float sunColor[4];
+    float hysteresis;          /* 0.03 in the reference */
+    uint32_t num_dirs;
+    uint32_t flags;            /* TIM_RT_PROBE_* */
+    uint32_t reserved;
+} tim_rt_probe_desc;
+#define TIM_RT_PROBE_OCTA 1u
+#define TIM_RT_PROBE_WIDE 0x100u
+int tim_rt_update_probes(tim_rt_ctx *ctx, tim_rt_scene_id scene, const tim_rt_probe_desc *desc, const float *dirs,
+                         const float *sh_basis, uint32_t probe_begin, uint32_t probe_end, uint32_t *trace_out,
+                         float *irradiance, uint16_t *sh9_fp16, float *sh9_fp32, float *octa, tim_rt_stats *stats);
+
 /* ---------------------------------------------------------------- product-side BVH builder */
 /* Builds a BVH over triangle records and writes it in the reference's
  * fillGpuBuffer layout (BVHBuilder.cpp:1319-1534), so its output can be passed

@@ -408,6 +408,7 @@ static uint32_t shadow_mask_leaf(const orc_scene *s, v3 pos, uint32_t hit_nid, v
     const uint32_t *ld = leaf_data(s);
     for (uint32_t i = 0; i < nl; ++i) {
         uint32_t li = ld[base + i];
+        if (li + 1u >= 32u) continue;   /* the 32-bit mask has no bit for this light */
         mask |= eval_shadow(s, li, pos, st, traced) ? light_bit(li) : 0u;
     }
     return mask;
@@ -421,6 +422,7 @@ static uint32_t shadow_mask_tile(const orc_scene *s, v3 pos, const uint32_t *lis
     mask |= trace_shadow(s, pos, neg(sunDir), TMAX, st) ? 1u : 0u;
     for (uint32_t i = 0; i < count; ++i) {
         uint32_t li = list[i];
+        if (li + 1u >= 32u) continue;   /* the 32-bit mask has no bit for this light */
         mask |= eval_shadow(s, li, pos, st, traced) ? light_bit(li) : 0u;
     }
     return mask;
@@ -668,7 +670,7 @@ static v3 interp_normal(const orc_scene *s, const uint32_t *rec, v3 pos) {
 /* bvhLighting.glsl:42-85 computeLighting with NO_LPF (genLightProbField.comp:5), and
  * baseRaytracingPass.glsl:67-82 for the miss colour. */
 static v3 probe_lit(const orc_scene *s, const orc_probe_desc *pd, const ray_t *r, float t, const uint32_t *rec, uint32_t mask) {
-    if (!(t < TMAX)) return muls(mk(200.0f, 220.0f, 255.0f), 0.3f / 255.0f);
+    if (!(t < TMAX)) return divs(muls(mk(200.0f, 220.0f, 255.0f), 0.3f), 255.0f);   /* 0.3 * vec3(...) / 255 */
     v3 pos = add(r->from, muls(r->dir, t));
     v3 N = interp_normal(s, rec, pos);
     const material *m = material_at(s, (rec[2] & 0xFFFF0000u) >> 16);

@@ -29,8 +29,29 @@ EXPORTED = [
     "tim_rt_trace_camera", "tim_rt_cull_lights", "tim_rt_build_params_default", "tim_rt_build_bvh",
     "tim_rt_bvh_blob_info", "tim_rt_bvh_blob_free", "tim_rt_validate_bvh", "tim_rt_trace_camera_dev",
     "tim_rt_cull_lights_dev", "tim_rt_get_launch_config", "tim_rt_set_launch_config", "tim_rt_trace_camera_noalloc",
-    "tim_rt_measure_l2_bandwidth",
+    "tim_rt_measure_l2_bandwidth", "tim_rt_update_probes",
 ]
+PROBE_OCTA, PROBE_WIDE = 1, 0x100
+
+
+class ProbeDesc(ctypes.Structure):
+    _fields_ = [("aabbMin", ctypes.c_float * 4), ("aabbMax", ctypes.c_float * 4), ("resolution", ctypes.c_uint32 * 4),
+                ("sunDir", ctypes.c_float * 4), ("sunColor", ctypes.c_float * 4), ("hysteresis", ctypes.c_float),
+                ("num_dirs", ctypes.c_uint32), ("flags", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+
+def probe_desc(aabb_min, aabb_max, res, sun_dir, sun_color, num_dirs, hysteresis=0.03, flags=0) -> ProbeDesc:
+    d = ProbeDesc()
+    for i in range(3):
+        d.aabbMin[i] = float(aabb_min[i])
+        d.aabbMax[i] = float(aabb_max[i])
+        d.resolution[i] = int(res[i])
+        d.sunDir[i] = float(sun_dir[i])
+        d.sunColor[i] = float(sun_color[i])
+    d.hysteresis = hysteresis
+    d.num_dirs = num_dirs
+    d.flags = flags
+    return d
 
 
 class TimRtError(RuntimeError):
@@ -100,6 +121,8 @@ def lib() -> ctypes.CDLL:
     L.tim_rt_cull_lights_dev.argtypes = [vp, u32, vp, u32, u32, vp, vp, vp]
     L.tim_rt_get_launch_config.argtypes = [vp, ctypes.POINTER(LaunchConfig)]
     L.tim_rt_measure_l2_bandwidth.argtypes = [i32, u64, i32, ctypes.POINTER(ctypes.c_float)]
+    L.tim_rt_update_probes.argtypes = [vp, u32, ctypes.POINTER(ProbeDesc), vp, vp, u32, u32, vp, vp, vp, vp, vp,
+                                       ctypes.POINTER(Stats)]
     L.tim_rt_trace_camera_noalloc.argtypes = [vp, vp, ctypes.POINTER(PushConstants), vp, u32, u32, vp, u32, u32, vp,
                                               vp, vp, vp, vp]
     L.tim_rt_set_launch_config.argtypes = [vp, ctypes.POINTER(LaunchConfig)]
@@ -296,6 +319,28 @@ class Context:
         _check(self._L.tim_rt_trace_camera_dev(self._c, sid, pd.ctypes.data, flags, seed, _ptr(d_tile_counts),
                                                _ptr(d_tile_lists), _ptr(d_out), _ptr(d_bounce), _ptr(d_ray_count),
                                                _ptr(stream) if stream is not None else None))
+
+    def update_probes(self, sid: int, desc: ProbeDesc, dirs: np.ndarray, sh_basis: np.ndarray, sh16: np.ndarray,
+                      probe_begin: int = 0, probe_end: int = None, want_trace=False, want_irr=False, want_sh32=False,
+                      want_octa=False):
+        """tim_rt_update_probes. sh16 (uint16 [7, rz, ry, rx, 4]) is updated in place."""
+        res = [int(desc.resolution[i]) for i in range(3)]
+        total = res[0] * res[1] * res[2]
+        probe_end = total if probe_end is None else probe_end
+        np_ = probe_end - probe_begin
+        nd = int(desc.num_dirs)
+        assert sh16.dtype == np.uint16 and sh16.size == 7 * total * 4 and sh16.flags["C_CONTIGUOUS"]
+        dirs = np.ascontiguousarray(dirs, np.float32)
+        basis = np.ascontiguousarray(sh_basis, np.float32)
+        tr = np.empty((np_, nd, 8), np.uint32) if want_trace else None
+        irr = np.empty((np_, nd, 3), np.float32) if want_irr else None
+        s32 = np.empty((np_, 9, 3), np.float32) if want_sh32 else None
+        octa = np.empty((np_, 64, 3), np.float32) if want_octa else None
+        st = Stats()
+        _check(self._L.tim_rt_update_probes(self._c, sid, ctypes.byref(desc), dirs.ctypes.data, basis.ctypes.data,
+                                            probe_begin, probe_end, _ptr(tr), _ptr(irr), sh16.ctypes.data, _ptr(s32),
+                                            _ptr(octa), ctypes.byref(st)))
+        return tr, irr, s32, octa, st
 
     def trace_camera(self, sid: int, pd: np.ndarray, flags: int = 0, seed: int = 0, tile_counts=None, tile_lists=None,
                      out=None, bounce_out=None):

@@ -57,6 +57,7 @@ struct tim_rt_ctx {
     uint32_t ring = 0;
     DevBuf cam_out, cam_bounce, cam_nid, q_rays, q_pixel, tiles_counts, tiles_lists;
     DevBuf dstats;              // 8 x u64 work counters of the counting kernels
+    DevBuf p_dirs, p_basis, p_out, p_nid, p_irr, p_sh16, p_sh32, p_octa;   // light-probe update
     cudaEvent_t ev[4] = {};
     cudaEvent_t pev[4] = {};   // camera phases
     LaunchConfig cfg;
@@ -210,7 +211,8 @@ int tim_rt_destroy(tim_rt_ctx* c) {
     }
     c->scenes.clear();
     for (DevBuf* b : {&c->rays, &c->hits, &c->nid, &c->bary, &c->counters, &c->cam_out, &c->cam_bounce, &c->cam_nid,
-                      &c->q_rays, &c->q_pixel, &c->tiles_counts, &c->tiles_lists, &c->dstats})
+                      &c->q_rays, &c->q_pixel, &c->tiles_counts, &c->tiles_lists, &c->dstats, &c->p_dirs, &c->p_basis,
+                      &c->p_out, &c->p_nid, &c->p_irr, &c->p_sh16, &c->p_sh32, &c->p_octa})
         dev_free(c, *b);
     for (auto& e : c->ev)
         if (e) cudaEventDestroy(e);
@@ -557,6 +559,111 @@ int tim_rt_trace_camera_dev(tim_rt_ctx* c, tim_rt_scene_id id, const tim_rt_pass
                              static_cast<tim_rt_ray*>(c->q_rays.ptr), static_cast<uint32_t*>(c->q_pixel.ptr),
                              (uint32_t)qcap, ctr, ctr + kErrWord, d_ray_count, st,
                              cfg_for(c, s, (flags & TIM_RT_CAM_WIDE) != 0)));
+    return TIM_RT_OK;
+}
+
+int tim_rt_update_probes(tim_rt_ctx* c, tim_rt_scene_id id, const tim_rt_probe_desc* desc, const float* dirs,
+                         const float* sh_basis, uint32_t probe_begin, uint32_t probe_end, uint32_t* trace_out,
+                         float* irradiance, uint16_t* sh9_fp16, float* sh9_fp32, float* octa, tim_rt_stats* stats) {
+    int rc = check_ctx(c);
+    if (rc) return rc;
+    Scene* s = find_scene(c, id);
+    if (!s) return TIM_RT_ENOTFOUND;
+    if (!desc || !dirs || !sh_basis || !sh9_fp16 || desc->num_dirs == 0 || desc->num_dirs > 4096) {
+        set_error("tim_rt_update_probes: null argument or num_dirs outside 1..4096");
+        return TIM_RT_EINVAL;
+    }
+    const uint32_t* res = desc->resolution;
+    if (res[0] == 0 || res[1] == 0 || res[2] == 0 || res[0] % 4u || res[1] % 4u || res[2] % 4u) {
+        set_error("tim_rt_update_probes: the probe resolution must be a positive multiple of 4 per axis "
+                  "(4x4x4 probe tiles, lightprobHelpers.glsl:16-61)");
+        return TIM_RT_EINVAL;
+    }
+    const uint64_t total = (uint64_t)res[0] * res[1] * res[2];
+    if (probe_begin >= probe_end || probe_end > total || total > (1u << 24)) {
+        set_error("tim_rt_update_probes: bad probe range");
+        return TIM_RT_EINVAL;
+    }
+    const uint32_t nd = desc->num_dirs, np = probe_end - probe_begin;
+    const uint64_t n = (uint64_t)np * nd;
+    if (n * camera_queue_kinds() > 0xFFFFFFFFull) {
+        set_error("tim_rt_update_probes: too many probe rays in one call");
+        return TIM_RT_EINVAL;
+    }
+    uint32_t side = 0;
+    if (desc->flags & TIM_RT_PROBE_OCTA) {
+        while ((uint64_t)side * side < nd) ++side;
+        if ((uint64_t)side * side != nd || side % 8u) {
+            set_error("tim_rt_update_probes: OCTA needs num_dirs = side^2 with side a multiple of 8");
+            return TIM_RT_EINVAL;
+        }
+    }
+    if ((desc->flags & TIM_RT_PROBE_WIDE) && !s->has_wide) {
+        set_error("tim_rt_update_probes: scene was uploaded without TIM_RT_UPLOAD_QUANT8");
+        return TIM_RT_EUNSUPPORTED;
+    }
+    if (!s->nrm.ptr) {
+        set_error("tim_rt_update_probes: the lit value needs vertex normals (upload with nrm)");
+        return TIM_RT_EINVAL;
+    }
+    if ((rc = ensure(c, c->p_dirs, 16ull * nd)) || (rc = ensure(c, c->p_basis, 36ull * nd)) ||
+        (rc = ensure(c, c->p_out, 32ull * n)) || (rc = ensure(c, c->p_nid, 4ull * n)) ||
+        (rc = ensure(c, c->p_irr, 12ull * n)) || (rc = ensure(c, c->p_sh16, 56ull * total)) ||
+        (rc = ensure(c, c->q_rays, 32ull * n * camera_queue_kinds())) ||
+        (rc = ensure(c, c->q_pixel, 4ull * n * camera_queue_kinds())))
+        return rc;
+    if (sh9_fp32 && (rc = ensure(c, c->p_sh32, 108ull * np))) return rc;
+    if (octa && side && (rc = ensure(c, c->p_octa, 768ull * np))) return rc;
+    ProbeArgs d{};
+    for (int a = 0; a < 3; ++a) {
+        d.mn[a] = desc->aabbMin[a];
+        d.mx[a] = desc->aabbMax[a];
+        d.res[a] = res[a];
+        d.sun[a] = desc->sunDir[a];
+        d.sunc[a] = desc->sunColor[a];
+    }
+    d.hyst = desc->hysteresis;
+    d.nd = nd;
+    d.p0 = probe_begin;
+    d.np = np;
+    d.dirs = static_cast<const float4*>(c->p_dirs.ptr);
+    d.basis = static_cast<const float*>(c->p_basis.ptr);
+    uint32_t* ctr = static_cast<uint32_t*>(c->counters.ptr);
+    TIMRT_CUDA(cudaEventRecord(c->ev[0], c->stream));
+    TIMRT_CUDA(cudaMemcpyAsync(c->p_dirs.ptr, dirs, 16ull * nd, cudaMemcpyHostToDevice, c->stream));
+    TIMRT_CUDA(cudaMemcpyAsync(c->p_basis.ptr, sh_basis, 36ull * nd, cudaMemcpyHostToDevice, c->stream));
+    TIMRT_CUDA(cudaMemcpyAsync(c->p_sh16.ptr, sh9_fp16, 56ull * total, cudaMemcpyHostToDevice, c->stream));
+    TIMRT_CUDA(cudaMemsetAsync(ctr, 0, 4 * kCamCounterWords, c->stream));
+    TIMRT_CUDA(cudaEventRecord(c->ev[1], c->stream));
+    LaunchConfig cfg = cfg_for(c, s, (desc->flags & TIM_RT_PROBE_WIDE) != 0);
+    cfg.phase_ev = c->pev;
+    TIMRT_CUDA(launch_probes(s->view, d, static_cast<uint32_t*>(c->p_out.ptr), static_cast<uint32_t*>(c->p_nid.ptr),
+                             static_cast<tim_rt_ray*>(c->q_rays.ptr), static_cast<uint32_t*>(c->q_pixel.ptr), ctr,
+                             ctr + kErrWord, static_cast<float*>(c->p_irr.ptr), static_cast<uint16_t*>(c->p_sh16.ptr),
+                             sh9_fp32 ? static_cast<float*>(c->p_sh32.ptr) : nullptr,
+                             (octa && side) ? static_cast<float*>(c->p_octa.ptr) : nullptr, side, c->stream, cfg));
+    TIMRT_CUDA(cudaEventRecord(c->ev[2], c->stream));
+    TIMRT_CUDA(cudaMemcpyAsync(sh9_fp16, c->p_sh16.ptr, 56ull * total, cudaMemcpyDeviceToHost, c->stream));
+    if (trace_out) TIMRT_CUDA(cudaMemcpyAsync(trace_out, c->p_out.ptr, 32ull * n, cudaMemcpyDeviceToHost, c->stream));
+    if (irradiance) TIMRT_CUDA(cudaMemcpyAsync(irradiance, c->p_irr.ptr, 12ull * n, cudaMemcpyDeviceToHost, c->stream));
+    if (sh9_fp32) TIMRT_CUDA(cudaMemcpyAsync(sh9_fp32, c->p_sh32.ptr, 108ull * np, cudaMemcpyDeviceToHost, c->stream));
+    if (octa && side) TIMRT_CUDA(cudaMemcpyAsync(octa, c->p_octa.ptr, 768ull * np, cudaMemcpyDeviceToHost, c->stream));
+    uint32_t qn = 0;
+    TIMRT_CUDA(cudaMemcpyAsync(&qn, ctr + kCamTotalWord, 4, cudaMemcpyDeviceToHost, c->stream));
+    TIMRT_CUDA(cudaEventRecord(c->ev[3], c->stream));
+    TIMRT_CUDA(cudaStreamSynchronize(c->stream));
+    if ((rc = check_device_error(c))) return rc;
+    if (stats) {
+        std::memset(stats, 0, sizeof(*stats));
+        stats->primary_rays = n;
+        stats->shadow_rays = qn;
+        stats->rays = n + qn;
+        cudaEventElapsedTime(&stats->kernel_ms, c->ev[1], c->ev[2]);
+        cudaEventElapsedTime(&stats->total_ms, c->ev[0], c->ev[3]);
+        cudaEventElapsedTime(&stats->primary_ms, c->pev[0], c->pev[1]);
+        cudaEventElapsedTime(&stats->gen_ms, c->pev[1], c->pev[2]);
+        cudaEventElapsedTime(&stats->secondary_ms, c->pev[2], c->pev[3]);
+    }
     return TIM_RT_OK;
 }
 

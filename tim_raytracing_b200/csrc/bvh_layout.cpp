@@ -300,7 +300,10 @@ bool build_wide(const uint8_t* blob, const uint32_t ranges[7][2], uint32_t num_n
         bool used[8] = {};
         for (int k = 0; k < 8; ++k) {
             const int i = slot_child[k];
-            if (i < 0) continue;
+            if (i < 0) {   // empty slot: an inverted box, which the kernel's slab test rejects
+                for (int a = 0; a < 3; ++a) { qlo[a][k] = 255; qhi[a][k] = 0; }
+                continue;
+            }
             used[k] = true;
             sl[k] = fr[i];
             for (int a = 0; a < 3; ++a) { qlo[a][k] = cq_lo[a][i]; qhi[a][k] = cq_hi[a][i]; }

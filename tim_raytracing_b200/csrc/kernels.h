@@ -36,6 +36,24 @@ cudaError_t launch_camera(const SceneView& s, const tim_rt_pass_data& pd, uint32
                           uint32_t* counters, uint32_t* err, uint64_t* d_ray_count, cudaStream_t stream,
                           const LaunchConfig& cfg);
 
+// Light-probe update of probes [p0, p0 + np), nd directions each.
+struct ProbeArgs {
+    float mn[3], mx[3];
+    uint32_t res[3];
+    float sun[3], sunc[3];
+    float hyst;
+    uint32_t nd, p0, np;
+    const float4* dirs;     // nd
+    const float* basis;     // nd x 9
+};
+// out: np*nd*8 u32 trace records; leaf_nid: np*nd; the queue holds
+// camera_queue_kinds() segments of np*nd slots; irr: np*nd*3; sh16: the whole
+// field's 7 RGBA16F images (read and written for the updated probes); sh32 and
+// octa optional; side: octahedral grid side (0 = no octahedral texels).
+cudaError_t launch_probes(const SceneView& s, const ProbeArgs& d, uint32_t* out, uint32_t* leaf_nid, tim_rt_ray* q_rays,
+                          uint32_t* q_pixel, uint32_t* counters, uint32_t* err, float* irr, uint16_t* sh16, float* sh32,
+                          float* octa, uint32_t side, cudaStream_t stream, const LaunchConfig& cfg);
+
 cudaError_t launch_cull_lights(const SceneView& s, const tim_rt_pass_data& pd, uint32_t tiles_x, uint32_t tiles_y,
                                uint32_t* counts, uint32_t* lists, cudaStream_t stream);
 

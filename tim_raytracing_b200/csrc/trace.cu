@@ -12,6 +12,7 @@
 // one warp), and the secondary rays of those pixels are queued by kind -- sun,
 // tile-light slot j, probe corner i, bounce -- in one segment per kind, so a
 // warp traces 32 rays of the same kind from neighbouring pixels.
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <cstdio>
 #include "common.cuh"
@@ -635,6 +636,343 @@ cudaError_t launch_cull_lights(const SceneView& s, const tim_rt_pass_data& pd, u
     const uint32_t warps = tiles_x * tiles_y;
     const uint32_t blocks = (warps * 32u + 255u) / 256u;
     k_cull_lights<<<blocks, 256, 0, stream>>>(s, pd, tiles_x, tiles_y, counts, lists);
+    return cudaGetLastError();
+}
+
+// -------------------------------------------------------------------- light-probe field
+
+// lightprobHelpers.glsl:33-61 getLightProbCoord (LP_TILE_RES = 4)
+__device__ __forceinline__ void probe_coord(uint32_t index, const uint32_t* res, uint32_t& x, uint32_t& y, uint32_t& z) {
+    const uint32_t trx = res[0] / 4u, try_ = res[1] / 4u;
+    uint32_t tile = index / 64u;
+    const uint32_t in = index % 64u;
+    z = tile / (trx * try_);
+    tile = tile % (trx * try_);
+    y = tile / trx;
+    x = tile % trx;
+    x = x * 4u + in % 4u;
+    y = y * 4u + (in / 4u) % 4u;
+    z = z * 4u + (in / 16u) % 4u;
+}
+
+// lightprobHelpers.glsl:63-69 getLightProbPosition
+__device__ __forceinline__ void probe_position(const ProbeArgs& d, uint32_t p, float& x, float& y, float& z) {
+    uint32_t cx, cy, cz;
+    probe_coord(p, d.res, cx, cy, cz);
+    const float stx = (d.mx[0] - d.mn[0]) / (float)d.res[0];
+    const float sty = (d.mx[1] - d.mn[1]) / (float)d.res[1];
+    const float stz = (d.mx[2] - d.mn[2]) / (float)d.res[2];
+    x = d.mn[0] + stx * ((float)cx + 0.5f);
+    y = d.mn[1] + sty * ((float)cy + 0.5f);
+    z = d.mn[2] + stz * ((float)cz + 0.5f);
+}
+
+// Work item i of the probe trace: direction-major (r = i / np) so that a warp
+// traces one direction from 32 neighbouring probes; results are stored
+// probe-major (sample = probe * nd + r) as genLightProbField.comp:47 indexes them.
+__device__ __forceinline__ uint32_t probe_sample(const ProbeArgs& d, uint32_t i, uint32_t& pl, uint32_t& r) {
+    r = i / d.np;
+    pl = i % d.np;
+    return pl * d.nd + r;
+}
+
+struct ProbePolicy {
+    ProbeArgs d;
+    uint4* out;          // 2 x uint4 per sample (tracingData layout)
+    uint32_t* leaf_nid;
+
+    __device__ __forceinline__ bool load(const SceneView&, uint32_t i, TravState& st) const {
+        uint32_t pl, r;
+        st.slot = probe_sample(d, i, pl, r);
+        probe_position(d, d.p0 + pl, st.r.ox, st.r.oy, st.r.oz);
+        const float4 dir = __ldg(d.dirs + r);
+        st.r.dx = dir.x; st.r.dy = dir.y; st.r.dz = dir.z;
+        st.t = kTMax;
+        st.any = false;
+        return true;
+    }
+    __device__ __forceinline__ void store(const SceneView&, uint32_t, const TravState& st, float) const {
+        out[2u * st.slot] = make_uint4(st.rec0, st.rec1, st.rec2, __float_as_uint(st.t));
+        out[2u * st.slot + 1u] = make_uint4(0u, 0u, 0u, 0u);
+        leaf_nid[st.slot] = st.hit ? st.nid : 0xFFFFFFFFu;
+    }
+    __device__ __forceinline__ void skip(uint32_t) const {}
+};
+
+// Shadow rays of the probe hits: the sun (tmax = TMAX) and the hit leaf's lights
+// (computeAdditionalHitData / computeShadowMask, baseRaytracingPass.glsl:85-97,
+// bvhLighting.glsl:143-163); the probe mask stays 0 (no USE_LPF_MASK).
+__global__ void __launch_bounds__(256) k_probe_gen(SceneView s, ProbeArgs d, GenParams g, const uint32_t* leaf_nid) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i < d.np * d.nd;
+    uint32_t pl = 0, r = 0, sample = 0;
+    if (valid) sample = probe_sample(d, i, pl, r);
+    uint4 rec = make_uint4(0, 0, 0, 0);
+    if (valid) rec = reinterpret_cast<const uint4*>(g.out_words)[2u * sample];
+    const float t = __uint_as_float(rec.w);
+    const bool hit = valid && t < kTMax;
+    float hx = 0.f, hy = 0.f, hz = 0.f;
+    if (hit) {
+        float ox, oy, oz;
+        probe_position(d, d.p0 + pl, ox, oy, oz);
+        const float4 dir = __ldg(d.dirs + r);
+        hx = ox + dir.x * t;
+        hy = oy + dir.y * t;
+        hz = oz + dir.z * t;
+    }
+    emit(g, kKindSun, hit, sample, hx, hy, hz, kTMax, -d.sun[0], -d.sun[1], -d.sun[2], 1u);
+    const uint32_t* list = nullptr;
+    uint32_t count = 0;
+    if (hit) {
+        const uint32_t nid = leaf_nid[sample];
+        const uint32_t off = __ldg(reinterpret_cast<const uint32_t*>(s.nodes + 4u * nid) + 3);
+        const uint32_t hdr = leaf_header(s, off);
+        uint32_t skip = 3u * (hdr & ((1u << kTriBits) - 1u));
+        skip += (hdr >> kTriBits) & ((1u << kBlasBits) - 1u);
+        skip += (hdr >> (kTriBits + kBlasBits)) & ((1u << kPrimBits) - 1u);
+        count = (hdr >> (kTriBits + kBlasBits + kPrimBits)) & ((1u << kLightBits) - 1u);
+        list = s.leaf + skip + 1u + off;
+    }
+    uint32_t direct_bits = 0;
+    for (uint32_t j = 0; j < 15u; ++j) {
+        bool has = false;
+        float lx = 0.f, ly = 0.f, lz = 0.f, rl = 1.f;
+        uint32_t bit = 0;
+        if (j < count) {
+            const uint32_t li = __ldg(list + j);
+            const float* L = s.lights + 14u * li;
+            bit = li + 1u;
+            if (__float_as_uint(__ldg(L)) == kLightSphere && bit < 32u) {
+                lx = __ldg(L + 1) - hx;
+                ly = __ldg(L + 2) - hy;
+                lz = __ldg(L + 3) - hz;
+                rl = sqrtf(dot3(lx, ly, lz, lx, ly, lz));
+                if (rl < __ldg(L + 4)) has = true;
+                else direct_bits |= 1u << bit;
+            }
+        }
+        emit(g, kKindLight0 + j, has, sample, hx, hy, hz, rl, lx / rl, ly / rl, lz / rl, 1u | (bit << 8));
+    }
+    if (valid) {
+        g.out_words[8u * sample + 4u] = direct_bits;
+        g.out_words[8u * sample + 5u] = 0u;
+    }
+}
+
+// core/lighting.glsl:16-20 computeAttenuation
+__device__ __forceinline__ float attenuation(float dist, float radius) {
+    const float att = (radius * radius + 1.0f) / (255.0f * dist * dist);
+    return fminf(fmaxf(att - (1.0f / 255.0f), 0.0f), 1.0f);
+}
+
+// core/lighting.glsl:22-57 computeLighting (texColor = 1, no shadow ray on the fly)
+// and 137-182 computePbrLighting; m = the Material record (12 words).
+__device__ void compute_lighting(const float* m, float lcx, float lcy, float lcz, float px, float py, float pz,
+                                 float Lx, float Ly, float Lz, float Nx, float Ny, float Nz, float ex, float ey,
+                                 float ez, float att, float& ox, float& oy, float& oz) {
+    const uint32_t type = __float_as_uint(__ldg(m));
+    const float cr = __ldg(m + 4), cg = __ldg(m + 5), cb = __ldg(m + 6);
+    if (type == 1u) { ox = cr; oy = cg; oz = cb; return; }            // Material_Emissive
+    if (type == 4u) { ox = oy = oz = 0.0f; return; }                  // Material_Transparent
+    float rx = 0.f, ry = 0.f, rz = 0.f;
+    const float dotL = fminf(fmaxf(dot3(Nx, Ny, Nz, Lx, Ly, Lz), 0.0f), 1.0f);
+    if (type == 5u) {                                                 // Material_PBR
+        const float metal = __ldg(m + 8);
+        float vx = ex - px, vy = ey - py, vz = ez - pz;
+        const float vl = sqrtf(dot3(vx, vy, vz, vx, vy, vz));
+        vx = vx / vl; vy = vy / vl; vz = vz / vl;
+        float hx = vx + Lx, hy = vy + Ly, hz = vz + Lz;
+        const float hl = sqrtf(dot3(hx, hy, hz, hx, hy, hz));
+        hx = hx / hl; hy = hy / hl; hz = hz / hl;
+        const float NoV = fabsf(dot3(Nx, Ny, Nz, vx, vy, vz)) + 1e-5f;
+        const float NoL = fminf(fmaxf(dot3(Nx, Ny, Nz, Lx, Ly, Lz), 0.0f), 1.0f);
+        const float NoH = fminf(fmaxf(dot3(Nx, Ny, Nz, hx, hy, hz), 0.0f), 1.0f);
+        const float LoH = fminf(fmaxf(dot3(Lx, Ly, Lz, hx, hy, hz), 0.0f), 1.0f);
+        const float rough = 0.02f * 0.02f;
+        const float a2 = rough * rough;
+        const float f = (NoH * a2 - NoH) * NoH + 1.0f;
+        const float D = a2 / (3.141592f * f * f);
+        const float f0x = 0.04f * (1.0f - metal) + cr * metal, f0y = 0.04f * (1.0f - metal) + cg * metal,
+                    f0z = 0.04f * (1.0f - metal) + cb * metal;
+        const float p5 = powf(1.0f - LoH, 5.0f);
+        const float Fx = f0x + (1.0f - f0x) * p5, Fy = f0y + (1.0f - f0y) * p5, Fz = f0z + (1.0f - f0z) * p5;
+        const float GGXL = NoV * sqrtf((-NoL * a2 + NoL) * NoL + a2);
+        const float GGXV = NoL * sqrtf((-NoV * a2 + NoV) * NoV + a2);
+        const float V = 0.5f / (GGXV + GGXL);
+        const float DV = D * V;
+        const float dx = cr * (1.0f - metal) / 3.141592f, dy = cg * (1.0f - metal) / 3.141592f,
+                    dz = cb * (1.0f - metal) / 3.141592f;
+        rx = ((dx + Fx * DV) * lcx) * NoL;
+        ry = ((dy + Fy * DV) * lcy) * NoL;
+        rz = ((dz + Fz * DV) * lcz) * NoL;
+    } else if (type == 2u) {                                          // Material_Lambert
+        rx = (lcx * dotL) * cr;
+        ry = (lcy * dotL) * cg;
+        rz = (lcz * dotL) * cb;
+    }
+    ox = rx * att;
+    oy = ry * att;
+    oz = rz * att;
+}
+
+// Lit value of one probe ray: bvhLighting.glsl:42-85 computeLighting with NO_LPF
+// (genLightProbField.comp:5), normal from baseRaytracingPass.glsl:38-64, sky
+// colour on a miss (baseRaytracingPass.glsl:81).
+__global__ void __launch_bounds__(256) k_probe_light(SceneView s, ProbeArgs d, const uint32_t* out_words, float* irr) {
+    const uint32_t sample = blockIdx.x * blockDim.x + threadIdx.x;
+    if (sample >= d.np * d.nd) return;
+    const uint32_t pl = sample / d.nd, r = sample % d.nd;
+    const uint4 rec = reinterpret_cast<const uint4*>(out_words)[2u * sample];
+    const uint32_t mask = out_words[8u * sample + 4u];
+    const float t = __uint_as_float(rec.w);
+    float lx = 0.f, ly = 0.f, lz = 0.f;
+    if (!(t < kTMax)) {
+        lx = (0.3f * 200.0f) / 255.0f;
+        ly = (0.3f * 220.0f) / 255.0f;
+        lz = (0.3f * 255.0f) / 255.0f;
+    } else {
+        float ox, oy, oz;
+        probe_position(d, d.p0 + pl, ox, oy, oz);
+        const float4 dir = __ldg(d.dirs + r);
+        const float px = ox + dir.x * t, py = oy + dir.y * t, pz = oz + dir.z * t;
+        const uint32_t i0 = rec.x + (rec.y & 0xFFFFu), i1 = rec.x + (rec.y >> 16), i2 = rec.x + (rec.z & 0xFFFFu);
+        const float* P = s.pos;
+        const float v0x = P[3 * i1] - P[3 * i0], v0y = P[3 * i1 + 1] - P[3 * i0 + 1], v0z = P[3 * i1 + 2] - P[3 * i0 + 2];
+        const float v1x = P[3 * i2] - P[3 * i0], v1y = P[3 * i2 + 1] - P[3 * i0 + 1], v1z = P[3 * i2 + 2] - P[3 * i0 + 2];
+        const float v2x = px - P[3 * i0], v2y = py - P[3 * i0 + 1], v2z = pz - P[3 * i0 + 2];
+        const float d00 = dot3(v0x, v0y, v0z, v0x, v0y, v0z), d01 = dot3(v0x, v0y, v0z, v1x, v1y, v1z);
+        const float d11 = dot3(v1x, v1y, v1z, v1x, v1y, v1z);
+        const float d20 = dot3(v2x, v2y, v2z, v0x, v0y, v0z), d21 = dot3(v2x, v2y, v2z, v1x, v1y, v1z);
+        const float denom = d00 * d11 - d01 * d01;
+        const float v = (d11 * d20 - d01 * d21) / denom;
+        const float w = (d00 * d21 - d01 * d20) / denom;
+        const float u = 1.0f - v - w;
+        const float* Nn = s.nrm;
+        const float Nx = (Nn[3 * i0] * u + Nn[3 * i1] * v) + Nn[3 * i2] * w;
+        const float Ny = (Nn[3 * i0 + 1] * u + Nn[3 * i1 + 1] * v) + Nn[3 * i2 + 1] * w;
+        const float Nz = (Nn[3 * i0 + 2] * u + Nn[3 * i1 + 2] * v) + Nn[3 * i2 + 2] * w;
+        const float* m = s.materials + 12u * (rec.z >> 16);
+        for (uint32_t li = 0; li < s.num_lights && li < 31u; ++li) {
+            if (mask & (1u << (li + 1u))) continue;
+            const float* L = s.lights + 14u * li;
+            if (__float_as_uint(__ldg(L)) != kLightSphere) continue;
+            const float ax = __ldg(L + 1) - px, ay = __ldg(L + 2) - py, az = __ldg(L + 3) - pz;
+            float dd = sqrtf(dot3(ax, ay, az, ax, ay, az));
+            if (dd < __ldg(L + 4)) {
+                const float Lx = ax / dd, Ly = ay / dd, Lz = az / dd;
+                dd = fmaxf(0.01f, dd - __ldg(L + 8));
+                float cx, cy, cz;
+                compute_lighting(m, __ldg(L + 5), __ldg(L + 6), __ldg(L + 7), px, py, pz, Lx, Ly, Lz, Nx, Ny, Nz, ox,
+                                 oy, oz, attenuation(dd, __ldg(L + 4)), cx, cy, cz);
+                lx = lx + cx; ly = ly + cy; lz = lz + cz;
+            }
+        }
+        if ((mask & 1u) == 0u) {
+            float cx, cy, cz;
+            compute_lighting(m, d.sunc[0], d.sunc[1], d.sunc[2], px, py, pz, -d.sun[0], -d.sun[1], -d.sun[2], Nx, Ny,
+                             Nz, ox, oy, oz, 1.0f, cx, cy, cz);
+            lx = lx + cx; ly = ly + cy; lz = lz + cz;
+        }
+    }
+    irr[3u * sample] = lx;
+    irr[3u * sample + 1u] = ly;
+    irr[3u * sample + 2u] = lz;
+}
+
+// updateLightProbField.comp:33-64: one thread per probe, rays summed in order
+// (j-th SH coefficient, r,g,b), x 4*pi/N, GLSL mix with the previous FP16 value,
+// stored back as FP16 in storeSH9's channel layout; plus the octahedral texels.
+__global__ void __launch_bounds__(128) k_probe_accum(ProbeArgs d, const float* irr, uint16_t* sh16, float* sh32,
+                                                     float* octa, uint32_t side) {
+    const uint32_t pl = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pl >= d.np) return;
+    const uint32_t nd = d.nd;
+    float acc[27];
+#pragma unroll
+    for (int q = 0; q < 27; ++q) acc[q] = 0.0f;
+    const float* L = irr + 3ull * pl * nd;
+    for (uint32_t r = 0; r < nd; ++r) {
+        const float Lr = L[3 * r], Lg = L[3 * r + 1], Lb = L[3 * r + 2];
+        const float* w = d.basis + 9u * r;
+#pragma unroll
+        for (int j = 0; j < 9; ++j) {
+            const float wj = __ldg(w + j);
+            acc[3 * j] = acc[3 * j] + Lr * wj;
+            acc[3 * j + 1] = acc[3 * j + 1] + Lg * wj;
+            acc[3 * j + 2] = acc[3 * j + 2] + Lb * wj;
+        }
+    }
+    const float norm = (4.0f * 3.14159265358979323846f) / (float)nd;
+    uint32_t cx, cy, cz;
+    probe_coord(d.p0 + pl, d.res, cx, cy, cz);
+    const uint64_t texel = ((uint64_t)cz * d.res[1] + cy) * d.res[0] + cx;
+    const uint64_t img = (uint64_t)d.res[0] * d.res[1] * d.res[2];
+    const float a = d.hyst;
+#pragma unroll
+    for (int j = 0; j < 9; ++j) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const uint32_t image = j == 0 ? 0u : (j <= 4 ? 1u + 2u * c : 2u + 2u * c);
+            const uint32_t ch = j == 0 ? (uint32_t)c : (j <= 4 ? (uint32_t)(j - 1) : (uint32_t)(j - 5));
+            uint16_t* h = sh16 + 4ull * (image * img + texel) + ch;
+            const float prev = __half2float(__ushort_as_half(*h));
+            const float nw = prev * (1.0f - a) + (acc[3 * j + c] * norm) * a;
+            *h = __half_as_ushort(__float2half_rn(nw));
+            if (sh32) sh32[27ull * pl + 3 * j + c] = nw;
+        }
+    }
+    sh16[4ull * texel + 3] = 0;   // image 0 alpha (storeSH9 writes 0)
+    if (octa) {
+        const uint32_t per = (side / 8u) * (side / 8u);
+        const float inv = 1.0f / (float)per;
+        float* o = octa + 192ull * pl;
+        for (uint32_t q = 0; q < 64u; ++q) {
+            const uint32_t tx = q % 8u, ty = q / 8u, step = side / 8u;
+            float sr = 0.f, sg = 0.f, sb = 0.f;
+            for (uint32_t jj = ty * step; jj < (ty + 1u) * step; ++jj)
+                for (uint32_t ii = tx * step; ii < (tx + 1u) * step; ++ii) {
+                    const uint32_t k = jj * side + ii;
+                    sr = sr + L[3 * k]; sg = sg + L[3 * k + 1]; sb = sb + L[3 * k + 2];
+                }
+            o[3 * q] = sr * inv;
+            o[3 * q + 1] = sg * inv;
+            o[3 * q + 2] = sb * inv;
+        }
+    }
+}
+
+cudaError_t launch_probes(const SceneView& s, const ProbeArgs& d, uint32_t* out, uint32_t* leaf_nid, tim_rt_ray* q_rays,
+                          uint32_t* q_pixel, uint32_t* counters, uint32_t* err, float* irr, uint16_t* sh16, float* sh32,
+                          float* octa, uint32_t side, cudaStream_t stream, const LaunchConfig& cfg) {
+    const uint32_t n = d.np * d.nd;
+    uint32_t* q_counts = counters + 2;
+    uint32_t* prefix = counters + 2 + kNumKinds;
+    ProbePolicy PP{d, reinterpret_cast<uint4*>(out), leaf_nid};
+    if (cfg.phase_ev) cudaEventRecord(cfg.phase_ev[0], stream);
+    cudaError_t e = cfg.wide ? launch_persistent<true>(s, PP, n, nullptr, counters + 0, err, stream, cfg)
+                             : launch_persistent<false>(s, PP, n, nullptr, counters + 0, err, stream, cfg);
+    if (e != cudaSuccess) return e;
+    if (cfg.phase_ev) cudaEventRecord(cfg.phase_ev[1], stream);
+    GenParams g{};
+    g.out_words = out;
+    g.q_rays = q_rays;
+    g.q_pixel = q_pixel;
+    g.q_counts = q_counts;
+    g.seg_cap = n;
+    k_probe_gen<<<(n + 255u) / 256u, 256, 0, stream>>>(s, d, g, leaf_nid);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    k_kind_prefix<<<1, 1, 0, stream>>>(q_counts, prefix, n);
+    if (cfg.phase_ev) cudaEventRecord(cfg.phase_ev[2], stream);
+    SecondaryPolicy SP{q_rays, q_pixel, prefix, n, out, nullptr};
+    LaunchConfig cfg2 = cfg;
+    if (cfg.stats) cfg2.stats = cfg.stats + 8;
+    e = cfg.wide ? launch_persistent<true>(s, SP, 0u, prefix + kNumKinds, counters + 1, err, stream, cfg2)
+                 : launch_persistent<false>(s, SP, 0u, prefix + kNumKinds, counters + 1, err, stream, cfg2);
+    if (cfg.phase_ev) cudaEventRecord(cfg.phase_ev[3], stream);
+    if (e != cudaSuccess) return e;
+    k_probe_light<<<(n + 255u) / 256u, 256, 0, stream>>>(s, d, out, irr);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    k_probe_accum<<<(d.np + 127u) / 128u, 128, 0, stream>>>(d, irr, sh16, sh32, octa, side);
     return cudaGetLastError();
 }
 

@@ -81,8 +81,8 @@ __device__ __forceinline__ uint32_t wide_visit(const SceneView& s, const TravSta
 #pragma unroll
     for (uint32_t k = 0; k < 8u; ++k) {
         const uint32_t wsel = k < 4u ? 0u : 1u, kk = k & 3u;
-        const uint32_t meta = ((wsel ? h.meta_hi : h.meta_lo) >> (8u * kk)) & 0xFFu;
-        const bool valid = ((h.imask >> k) & 1u) || meta != 0u;
+        // empty slots carry the inverted box qlo = 255, qhi = 0 and fail this test by
+        // themselves (if rounding ever lets one through, it is a leaf of 0 triangles)
         const float tnx = __fmaf_rn(wbyte(wsel ? nx1 : nx0, kk), Bx, Anx);
         const float tny = __fmaf_rn(wbyte(wsel ? ny1 : ny0, kk), By, Any);
         const float tnz = __fmaf_rn(wbyte(wsel ? nz1 : nz0, kk), Bz, Anz);
@@ -93,7 +93,7 @@ __device__ __forceinline__ uint32_t wide_visit(const SceneView& s, const TravSta
         const float farv = fminf(tfx, fminf(tfy, tfz));
         const float tmin = fmaxf(0.0f, __fmaf_rn(-fabsf(nearv), kWiden, nearv));
         const float tm = fminf(tcur, __fmaf_rn(fabsf(farv), kWiden, farv));
-        const bool hit = valid && (tmin < tm);
+        const bool hit = tmin < tm;
         // slot k is visited at rank k ^ octant: children were placed by direction
         mask |= (hit ? 1u : 0u) << (k ^ st.oct);
         // the nearest hit slot goes first (non-negative floats order like their bits)
