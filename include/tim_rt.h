@@ -128,8 +128,11 @@ typedef struct {
     uint32_t block;        /* threads per block: 64, 128 or 256 */
     uint32_t stack_depth;  /* traversal-stack entries per thread; 0 = the scene's tree depth (<= 32) */
     uint32_t refill_min;   /* a warp fetches new rays once this many of its 32 lanes are idle (1..32) */
-    uint32_t reserved;
+    uint32_t ray_sort;     /* batched traces: TIM_RT_SORT_* coherence key the rays are reordered by */
 } tim_rt_launch_config;
+#define TIM_RT_SORT_NONE 0u     /* trace in input order */
+#define TIM_RT_SORT_OCTANT 1u   /* group each job's rays by direction octant (stable) */
+#define TIM_RT_SORT_MORTON 2u   /* octant, then 30-bit Morton code of the origin in the scene's bounds */
 int tim_rt_get_launch_config(tim_rt_ctx *ctx, tim_rt_launch_config *cfg);
 int tim_rt_set_launch_config(tim_rt_ctx *ctx, const tim_rt_launch_config *cfg);
 
@@ -176,6 +179,125 @@ int tim_rt_trace(tim_rt_ctx *ctx, tim_rt_scene_id scene, const tim_rt_ray *rays,
 /* Device-pointer form of tim_rt_trace; stream-ordered, no synchronisation. */
 int tim_rt_trace_dev(tim_rt_ctx *ctx, tim_rt_scene_id scene, const tim_rt_ray *d_rays, uint32_t n, uint32_t mode,
                      uint32_t *d_hit, uint32_t *d_leaf_nid, float *d_bary, void *cuda_stream);
+
+/* ---------------------------------------------------------------- batched multi-scene trace */
+/* Not in the reference, which dispatches one scene per compute pass. A batch is
+ * a device-resident table of jobs, each a ray buffer traced against one resident
+ * scene; tim_rt_batch_launch traces all of them in ONE persistent kernel launch
+ * whose warps take rays from any job (a lane loads its job's scene when it
+ * fetches a ray), so scenes of very uneven size share the GPU without a tail of
+ * small launches. Each job's outputs are exactly those of tim_rt_trace_dev on the
+ * same scene, rays and mode (same layouts), whatever the launch configuration and
+ * ray-sort key. The launch issues only memsets and kernels on the given stream
+ * (no host<->device copies, no allocation once the sort scratch exists), so it
+ * can be captured in a CUDA graph and replayed; the job table is fixed at create
+ * time but the ray buffers' contents may change between launches. Scenes used by
+ * a live batch cannot be freed (TIM_RT_EINVAL). Launches of one batch must not
+ * overlap on the GPU (they share the batch's work counter). */
+typedef struct {
+    tim_rt_scene_id scene;
+    uint32_t mode;             /* TIM_RT_MODE_CLOSEST / ANY / PER_RAY */
+    uint32_t n;                /* rays */
+    uint32_t reserved;
+    const tim_rt_ray *d_rays;  /* device, 32 B per ray, 16-byte aligned */
+    uint32_t *d_hit;           /* device, 4 u32 per ray */
+    uint32_t *d_leaf_nid;      /* device, optional */
+    float *d_bary;             /* device, optional, 2 floats per ray */
+} tim_rt_job;
+typedef struct tim_rt_batch tim_rt_batch;
+#define TIM_RT_BATCH_WIDE 0x100u   /* trace the 8-wide quantised BVHs (all scenes need TIM_RT_UPLOAD_QUANT8) */
+int tim_rt_batch_create(tim_rt_ctx *ctx, const tim_rt_job *jobs, uint32_t num_jobs, uint32_t flags,
+                        tim_rt_batch **out);
+/* Traces every job of the batch with the context's launch configuration. The
+ * first launch with a ray-sort key allocates the batch's sort scratch (24 B per
+ * ray plus the radix sort's temporary storage): make it before capturing. */
+int tim_rt_batch_launch(tim_rt_ctx *ctx, tim_rt_batch *batch, void *cuda_stream);
+/* Rays in the batch and its device bytes (job table + sort scratch). */
+int tim_rt_batch_info(tim_rt_ctx *ctx, const tim_rt_batch *batch, uint64_t *rays, uint64_t *bytes);
+int tim_rt_batch_destroy(tim_rt_ctx *ctx, tim_rt_batch *batch);
+
+/* Autotuner (not in the reference, whose launch shape is fixed at 16x16 tiles).
+ * Times the batch's launch under candidate launch configurations (threads per
+ * block, refill threshold, stack depth, ray-sort key and, with TIM_RT_TUNE_WIDTH,
+ * node width) by coordinate descent, each candidate the median of `reps` timed
+ * launches (CUDA events on the context's stream, after one warm-up launch), and
+ * installs the fastest as the context's launch configuration (node width: the
+ * batch's). Synchronous. Results do not depend on the configuration, except that
+ * the two node widths may resolve exact near-ties of t differently, which is why
+ * width is only tried when asked for. */
+typedef struct {
+    tim_rt_launch_config best;
+    uint32_t wide;          /* node width of the fastest configuration: 1 = 8-wide */
+    uint32_t tried;         /* configurations timed */
+    float best_ms;          /* median device time of one launch, best configuration */
+    float start_ms;         /* the same for the configuration in force before tuning */
+} tim_rt_tune_result;
+#define TIM_RT_TUNE_WIDTH 1u
+int tim_rt_autotune_batch(tim_rt_ctx *ctx, tim_rt_batch *batch, uint32_t flags, uint32_t reps,
+                          tim_rt_tune_result *result);
+
+/* ---------------------------------------------------------------- serving loop */
+/* Not in the reference (a single-user renderer). A server owns a worker thread
+ * that traces requests from any number of submitting threads against the
+ * context's resident scenes, with continuous batching:
+ *   - admission: a request is admitted once its device staging (rays, hit
+ *     records and the optional outputs it asks for) fits in the server's device
+ *     arena of memory_budget_bytes (FIFO; a request larger than the whole arena
+ *     is refused at submit with TIM_RT_ENOMEM); its rays are then copied to the
+ *     device on an upload stream;
+ *   - steps: each step is one batched multi-scene launch (the kernel of
+ *     tim_rt_batch_launch) over chunks of the admitted requests, at most
+ *     max_rays_per_step rays: first an equal share for every admitted request,
+ *     then the unused capacity in admission order, so small requests finish in
+ *     their first step while large ones span several; up to max_inflight_steps
+ *     steps are queued on the GPU, and requests that arrive meanwhile join the
+ *     next step;
+ *   - completion: when a request's last chunk has been traced its results are
+ *     copied to the caller's host buffers on a download stream and the request
+ *     completes; its latency is measured from submit to the end of that copy.
+ * Each request's outputs are exactly those of tim_rt_trace on the same scene,
+ * rays and mode (closest / any / per-ray), whatever else is in flight. Host
+ * buffers should be pinned (cudaHostAlloc / cudaHostRegister) for the copies to
+ * overlap; they must stay valid until the request completes. Scenes with pending
+ * requests cannot be freed. While a server runs, the context may be used from
+ * other threads only through tim_rt_server_* calls, which are thread-safe. */
+typedef struct tim_rt_server tim_rt_server;
+typedef struct {
+    uint64_t memory_budget_bytes;  /* device arena for admitted requests; 0 = 1 GiB */
+    uint32_t max_rays_per_step;    /* 0 = 4M */
+    uint32_t max_inflight_steps;   /* 1..8; 0 = 2 */
+    uint32_t max_jobs_per_step;    /* request chunks per step; 0 = 256 */
+    uint32_t flags;                /* TIM_RT_BATCH_WIDE: trace the 8-wide BVHs */
+} tim_rt_server_params;
+typedef struct {
+    tim_rt_scene_id scene;
+    uint32_t mode;             /* TIM_RT_MODE_CLOSEST / ANY / PER_RAY */
+    uint32_t n;                /* rays, >= 1 */
+    uint32_t reserved;
+    const tim_rt_ray *rays;    /* host */
+    uint32_t *hit;             /* host, 4 u32 per ray */
+    uint32_t *leaf_nid;        /* host, optional */
+    float *bary;               /* host, optional */
+} tim_rt_request;
+typedef struct {
+    uint64_t submitted, completed, rays_completed, steps;
+    uint64_t arena_bytes, arena_peak_bytes;   /* arena size and the most of it ever admitted */
+    float p50_ms, p99_ms, mean_ms, max_ms;   /* request latency, submit -> results on the host */
+    float queue_p50_ms, queue_p99_ms;        /* submit -> admission */
+    float wall_s;                            /* seconds since the first submit after the last reset */
+} tim_rt_server_stats;
+int tim_rt_server_create(tim_rt_ctx *ctx, const tim_rt_server_params *params, tim_rt_server **out);
+/* Queues a request; never blocks on the GPU. *ticket identifies it. */
+int tim_rt_server_submit(tim_rt_server *srv, const tim_rt_request *req, uint64_t *ticket);
+/* Waits until the request completes (timeout_ms 0 = no limit): TIM_RT_OK, or
+ * TIM_RT_ETIMEOUT with the request still pending. */
+int tim_rt_server_wait(tim_rt_server *srv, uint64_t ticket, uint32_t timeout_ms);
+/* Waits until every submitted request has completed. */
+int tim_rt_server_drain(tim_rt_server *srv, uint32_t timeout_ms);
+/* Statistics over the requests completed since the last reset (reset != 0 clears them afterwards). */
+int tim_rt_server_stats_get(tim_rt_server *srv, tim_rt_server_stats *stats, int reset);
+/* Drains, stops the worker and frees the arena. */
+int tim_rt_server_destroy(tim_rt_server *srv);
 
 /* Camera trace step: cameraPass.comp with TRACING_STEP (src/Shaders/cameraPass.comp:44-76),
  * dispatched by RayTracingPass::tracePass (src/Renderer/raytracingPass.cpp:89-110).

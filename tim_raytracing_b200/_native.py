@@ -29,8 +29,14 @@ EXPORTED = [
     "tim_rt_trace_camera", "tim_rt_cull_lights", "tim_rt_build_params_default", "tim_rt_build_bvh",
     "tim_rt_bvh_blob_info", "tim_rt_bvh_blob_free", "tim_rt_validate_bvh", "tim_rt_trace_camera_dev",
     "tim_rt_cull_lights_dev", "tim_rt_get_launch_config", "tim_rt_set_launch_config", "tim_rt_trace_camera_noalloc",
-    "tim_rt_measure_l2_bandwidth", "tim_rt_update_probes",
+    "tim_rt_measure_l2_bandwidth", "tim_rt_update_probes", "tim_rt_batch_create", "tim_rt_batch_launch",
+    "tim_rt_batch_info", "tim_rt_batch_destroy", "tim_rt_autotune_batch", "tim_rt_server_create",
+    "tim_rt_server_submit", "tim_rt_server_wait", "tim_rt_server_drain", "tim_rt_server_stats_get",
+    "tim_rt_server_destroy",
 ]
+SORT_NONE, SORT_OCTANT, SORT_MORTON = 0, 1, 2
+BATCH_WIDE = 0x100
+TUNE_WIDTH = 1
 PROBE_OCTA, PROBE_WIDE = 1, 0x100
 
 
@@ -77,7 +83,39 @@ class Stats(ctypes.Structure):
 
 class LaunchConfig(ctypes.Structure):
     _fields_ = [("block", ctypes.c_uint32), ("stack_depth", ctypes.c_uint32), ("refill_min", ctypes.c_uint32),
-                ("reserved", ctypes.c_uint32)]
+                ("ray_sort", ctypes.c_uint32)]
+
+
+class Job(ctypes.Structure):
+    """tim_rt_job: one ray buffer of a batch, traced against one resident scene (device pointers)."""
+    _fields_ = [("scene", ctypes.c_uint32), ("mode", ctypes.c_uint32), ("n", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32), ("d_rays", ctypes.c_void_p), ("d_hit", ctypes.c_void_p),
+                ("d_leaf_nid", ctypes.c_void_p), ("d_bary", ctypes.c_void_p)]
+
+
+class ServerParams(ctypes.Structure):
+    _fields_ = [("memory_budget_bytes", ctypes.c_uint64), ("max_rays_per_step", ctypes.c_uint32),
+                ("max_inflight_steps", ctypes.c_uint32), ("max_jobs_per_step", ctypes.c_uint32),
+                ("flags", ctypes.c_uint32)]
+
+
+class Request(ctypes.Structure):
+    _fields_ = [("scene", ctypes.c_uint32), ("mode", ctypes.c_uint32), ("n", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32), ("rays", ctypes.c_void_p), ("hit", ctypes.c_void_p),
+                ("leaf_nid", ctypes.c_void_p), ("bary", ctypes.c_void_p)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_uint64), ("completed", ctypes.c_uint64), ("rays_completed", ctypes.c_uint64),
+                ("steps", ctypes.c_uint64), ("arena_bytes", ctypes.c_uint64), ("arena_peak_bytes", ctypes.c_uint64),
+                ("p50_ms", ctypes.c_float), ("p99_ms", ctypes.c_float), ("mean_ms", ctypes.c_float),
+                ("max_ms", ctypes.c_float), ("queue_p50_ms", ctypes.c_float), ("queue_p99_ms", ctypes.c_float),
+                ("wall_s", ctypes.c_float)]
+
+
+class TuneResult(ctypes.Structure):
+    _fields_ = [("best", LaunchConfig), ("wide", ctypes.c_uint32), ("tried", ctypes.c_uint32),
+                ("best_ms", ctypes.c_float), ("start_ms", ctypes.c_float)]
 
 
 class BuildParams(ctypes.Structure):
@@ -126,6 +164,17 @@ def lib() -> ctypes.CDLL:
     L.tim_rt_trace_camera_noalloc.argtypes = [vp, vp, ctypes.POINTER(PushConstants), vp, u32, u32, vp, u32, u32, vp,
                                               vp, vp, vp, vp]
     L.tim_rt_set_launch_config.argtypes = [vp, ctypes.POINTER(LaunchConfig)]
+    L.tim_rt_batch_create.argtypes = [vp, ctypes.POINTER(Job), u32, u32, ctypes.POINTER(vp)]
+    L.tim_rt_batch_launch.argtypes = [vp, vp, vp]
+    L.tim_rt_batch_info.argtypes = [vp, vp, ctypes.POINTER(u64), ctypes.POINTER(u64)]
+    L.tim_rt_batch_destroy.argtypes = [vp, vp]
+    L.tim_rt_autotune_batch.argtypes = [vp, vp, u32, u32, ctypes.POINTER(TuneResult)]
+    L.tim_rt_server_create.argtypes = [vp, ctypes.POINTER(ServerParams), ctypes.POINTER(vp)]
+    L.tim_rt_server_submit.argtypes = [vp, ctypes.POINTER(Request), ctypes.POINTER(u64)]
+    L.tim_rt_server_wait.argtypes = [vp, u64, u32]
+    L.tim_rt_server_drain.argtypes = [vp, u32]
+    L.tim_rt_server_stats_get.argtypes = [vp, ctypes.POINTER(ServerStats), i32]
+    L.tim_rt_server_destroy.argtypes = [vp]
     for name in EXPORTED:
         if name not in ("tim_rt_version", "tim_rt_last_error", "tim_rt_build_params_default", "tim_rt_bvh_blob_free"):
             getattr(L, name).restype = i32
@@ -254,11 +303,41 @@ class Context:
     def launch_config(self) -> dict:
         c = LaunchConfig()
         _check(self._L.tim_rt_get_launch_config(self._c, ctypes.byref(c)))
-        return {"block": c.block, "stack_depth": c.stack_depth, "refill_min": c.refill_min}
+        return {"block": c.block, "stack_depth": c.stack_depth, "refill_min": c.refill_min, "ray_sort": c.ray_sort}
 
-    def set_launch_config(self, block: int = 128, stack_depth: int = 0, refill_min: int = 1):
-        c = LaunchConfig(block, stack_depth, refill_min, 0)
+    def set_launch_config(self, block: int = 128, stack_depth: int = 0, refill_min: int = 16, ray_sort: int = 0):
+        c = LaunchConfig(block, stack_depth, refill_min, ray_sort)
         _check(self._L.tim_rt_set_launch_config(self._c, ctypes.byref(c)))
+
+    # -- batched multi-scene trace
+    def batch_create(self, jobs, wide: bool = False):
+        """jobs: iterable of (scene_id, mode, n, d_rays, d_hit, d_leaf_nid, d_bary); device buffers are
+        torch tensors or raw pointers. Returns an opaque batch handle."""
+        jobs = list(jobs)
+        arr = (Job * max(1, len(jobs)))()
+        for i, (sid, mode, n, r, h, nid, bary) in enumerate(jobs):
+            arr[i] = Job(sid, mode, n, 0, _ptr(r), _ptr(h), _ptr(nid), _ptr(bary))
+        out = ctypes.c_void_p()
+        _check(self._L.tim_rt_batch_create(self._c, arr, len(jobs), BATCH_WIDE if wide else 0, ctypes.byref(out)))
+        return out
+
+    def batch_launch(self, batch, stream=None):
+        _check(self._L.tim_rt_batch_launch(self._c, batch, _ptr(stream) if stream is not None else None))
+
+    def batch_info(self, batch) -> tuple:
+        rays, nbytes = ctypes.c_uint64(), ctypes.c_uint64()
+        _check(self._L.tim_rt_batch_info(self._c, batch, ctypes.byref(rays), ctypes.byref(nbytes)))
+        return rays.value, nbytes.value
+
+    def batch_destroy(self, batch):
+        _check(self._L.tim_rt_batch_destroy(self._c, batch))
+
+    def autotune_batch(self, batch, width: bool = False, reps: int = 3) -> dict:
+        r = TuneResult()
+        _check(self._L.tim_rt_autotune_batch(self._c, batch, TUNE_WIDTH if width else 0, reps, ctypes.byref(r)))
+        return {"block": r.best.block, "stack_depth": r.best.stack_depth, "refill_min": r.best.refill_min,
+                "ray_sort": r.best.ray_sort, "wide": bool(r.wide), "tried": r.tried, "best_ms": r.best_ms,
+                "start_ms": r.start_ms}
 
     def memory_used(self) -> int:
         v = ctypes.c_uint64()
@@ -353,3 +432,46 @@ class Context:
         _check(self._L.tim_rt_trace_camera(self._c, sid, pd.ctypes.data, flags, seed, _ptr(tile_counts),
                                            _ptr(tile_lists), _ptr(out), _ptr(bounce_out), ctypes.byref(st)))
         return out, bounce_out, st
+
+
+class Server:
+    """tim_rt_server_*: a serving loop over a context's resident scenes. Host
+    buffers passed to submit() are kept referenced until the request completes."""
+
+    def __init__(self, ctx: "Context", memory_budget_bytes: int = 1 << 30, max_rays_per_step: int = 0,
+                 max_inflight_steps: int = 0, max_jobs_per_step: int = 0, wide: bool = False):
+        self._L = lib()
+        self._ctx = ctx
+        p = ServerParams(memory_budget_bytes, max_rays_per_step, max_inflight_steps, max_jobs_per_step,
+                         BATCH_WIDE if wide else 0)
+        h = ctypes.c_void_p()
+        _check(self._L.tim_rt_server_create(ctx._c, ctypes.byref(p), ctypes.byref(h)))
+        self._s = h
+        self._keep = {}
+
+    def submit(self, sid: int, rays, mode: int, hit, nid=None, bary=None) -> int:
+        n = int(rays.shape[0])
+        r = Request(sid, mode, n, 0, _ptr(rays), _ptr(hit), _ptr(nid), _ptr(bary))
+        t = ctypes.c_uint64()
+        _check(self._L.tim_rt_server_submit(self._s, ctypes.byref(r), ctypes.byref(t)))
+        self._keep[t.value] = (rays, hit, nid, bary)
+        return t.value
+
+    def wait(self, ticket: int, timeout_ms: int = 0):
+        _check(self._L.tim_rt_server_wait(self._s, ticket, timeout_ms))
+        self._keep.pop(ticket, None)
+
+    def drain(self, timeout_ms: int = 0):
+        _check(self._L.tim_rt_server_drain(self._s, timeout_ms))
+        self._keep.clear()
+
+    def stats(self, reset: bool = False) -> dict:
+        st = ServerStats()
+        _check(self._L.tim_rt_server_stats_get(self._s, ctypes.byref(st), 1 if reset else 0))
+        return {name: getattr(st, name) for name, _ in ServerStats._fields_}
+
+    def close(self):
+        if self._s:
+            _check(self._L.tim_rt_server_destroy(self._s))
+            self._s = None
+            self._keep.clear()

@@ -6,10 +6,10 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <set>
 #include <string>
 #include <vector>
-#include "internal.h"
-#include "kernels.h"
+#include "context.h"
 
 namespace timrt {
 
@@ -25,49 +25,11 @@ void set_error(const std::string& msg) { g_last_error = msg; }
         }                                                                                        \
     } while (0)
 
-struct DevBuf {
-    void* ptr = nullptr;
-    uint64_t bytes = 0;
-};
-
-struct Scene {
-    DevBuf blob, pos, nrm, uv, wnodes, wtris, wnid;
-    SceneView view{};
-    uint32_t ranges[7][2];
-    tim_rt_push_constants pc{};
-    uint32_t depth = 0;
-    bool has_wide = false;
-    uint64_t bytes = 0;
-};
-
 }  // namespace timrt
 
 using namespace timrt;
 
-struct tim_rt_ctx {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    uint64_t budget = 0;
-    uint64_t used = 0;
-    std::map<uint32_t, std::unique_ptr<Scene>> scenes;
-    uint32_t next_id = 1;
-    // scratch
-    DevBuf rays, hits, nid, bary;
-    DevBuf counters;            // [0..63] per-call work counters, [64] device error word, ring after
-    uint32_t ring = 0;
-    DevBuf cam_out, cam_bounce, cam_nid, q_rays, q_pixel, tiles_counts, tiles_lists;
-    DevBuf dstats;              // 8 x u64 work counters of the counting kernels
-    DevBuf p_dirs, p_basis, p_out, p_nid, p_irr, p_sh16, p_sh32, p_octa;   // light-probe update
-    cudaEvent_t ev[4] = {};
-    cudaEvent_t pev[4] = {};   // camera phases
-    LaunchConfig cfg;
-};
-
-namespace {
-
-constexpr uint32_t kCounterWords = 64 + 1 + 4096;   // fixed counters, error word, trace_dev ring
-constexpr uint32_t kErrWord = 64;
-constexpr uint32_t kRingBase = 65, kRingSize = 4096;
+namespace timrt {
 
 int dev_alloc(tim_rt_ctx* c, DevBuf& b, uint64_t bytes) {
     if (bytes == 0) bytes = 16;
@@ -97,6 +59,10 @@ void dev_free(tim_rt_ctx* c, DevBuf& b) {
     b.bytes = 0;
 }
 
+}  // namespace timrt
+
+namespace {
+
 // Grows a scratch buffer to at least `bytes` (contents not preserved).
 int ensure(tim_rt_ctx* c, DevBuf& b, uint64_t bytes) {
     if (b.bytes >= bytes && b.ptr) return TIM_RT_OK;
@@ -106,6 +72,10 @@ int ensure(tim_rt_ctx* c, DevBuf& b, uint64_t bytes) {
     }
     return dev_alloc(c, b, bytes);
 }
+
+}  // namespace
+
+namespace timrt {
 
 int check_ctx(tim_rt_ctx* c) {
     if (!c) {
@@ -128,6 +98,10 @@ Scene* find_scene(tim_rt_ctx* c, tim_rt_scene_id id) {
     }
     return it->second.get();
 }
+
+}  // namespace timrt
+
+namespace {
 
 // Reads and clears the device error word; a set bit means a kernel guard fired.
 int check_device_error(tim_rt_ctx* c) {
@@ -204,7 +178,14 @@ int tim_rt_create(int device, uint64_t mem_budget_bytes, tim_rt_ctx** out) {
 int tim_rt_destroy(tim_rt_ctx* c) {
     if (!c) return TIM_RT_OK;
     cudaSetDevice(c->device);
+    while (!c->servers.empty()) server_shutdown(c, *c->servers.begin());
     cudaStreamSynchronize(c->stream);
+    for (tim_rt_batch* b : c->batches) {
+        dev_free(c, b->table);
+        dev_free(c, b->sort);
+        delete b;
+    }
+    c->batches.clear();
     for (auto& kv : c->scenes) {
         Scene* s = kv.second.get();
         for (DevBuf* b : {&s->blob, &s->pos, &s->nrm, &s->uv, &s->wnodes, &s->wtris, &s->wnid}) dev_free(c, *b);
@@ -231,19 +212,21 @@ int tim_rt_get_launch_config(tim_rt_ctx* c, tim_rt_launch_config* cfg) {
     cfg->block = (uint32_t)c->cfg.block;
     cfg->stack_depth = (uint32_t)c->cfg.stack_depth;
     cfg->refill_min = (uint32_t)c->cfg.refill_min;
-    cfg->reserved = 0;
+    cfg->ray_sort = (uint32_t)c->cfg.ray_sort;
     return TIM_RT_OK;
 }
 
 int tim_rt_set_launch_config(tim_rt_ctx* c, const tim_rt_launch_config* cfg) {
     if (!c || !cfg || (cfg->block != 64 && cfg->block != 128 && cfg->block != 256) || cfg->stack_depth > 32 ||
-        cfg->refill_min < 1 || cfg->refill_min > 32) {
-        set_error("tim_rt_set_launch_config: block must be 64/128/256, stack_depth <= 32, refill_min 1..32");
+        cfg->refill_min < 1 || cfg->refill_min > 32 || cfg->ray_sort > TIM_RT_SORT_MORTON) {
+        set_error("tim_rt_set_launch_config: block must be 64/128/256, stack_depth <= 32, refill_min 1..32, "
+                  "ray_sort 0..2");
         return TIM_RT_EINVAL;
     }
     c->cfg.block = (int)cfg->block;
     c->cfg.stack_depth = (int)cfg->stack_depth;
     c->cfg.refill_min = (int)cfg->refill_min;
+    c->cfg.ray_sort = (int)cfg->ray_sort;
     return TIM_RT_OK;
 }
 
@@ -277,6 +260,15 @@ int tim_rt_upload_bvh(tim_rt_ctx* c, const void* bvh_bytes, uint64_t n_bytes, co
     std::memcpy(s->ranges, ranges, sizeof(s->ranges));
     s->pc = *pc;
     s->depth = depth;
+    for (int a = 0; a < 3; ++a) {
+        float lo = pos[a], hi = pos[a];
+        for (uint32_t i = 1; i < num_vertex; ++i) {
+            lo = std::min(lo, pos[3ull * i + a]);
+            hi = std::max(hi, pos[3ull * i + a]);
+        }
+        s->bounds[a] = lo;
+        s->bounds[3 + a] = hi;
+    }
     WideHost wh;
     if (flags & TIM_RT_UPLOAD_QUANT8) {
         if (pc->numBlas) {
@@ -366,6 +358,11 @@ int tim_rt_free_scene(tim_rt_ctx* c, tim_rt_scene_id id) {
     if (rc) return rc;
     Scene* s = find_scene(c, id);
     if (!s) return TIM_RT_ENOTFOUND;
+    if (s->batch_refs) {
+        set_error("tim_rt_free_scene: scene " + std::to_string(id) + " is used by " + std::to_string(s->batch_refs) +
+                  " live batch(es)");
+        return TIM_RT_EINVAL;
+    }
     cudaStreamSynchronize(c->stream);
     for (DevBuf* b : {&s->blob, &s->pos, &s->nrm, &s->uv, &s->wnodes, &s->wtris, &s->wnid}) dev_free(c, *b);
     c->scenes.erase(id);
@@ -728,6 +725,270 @@ int tim_rt_trace_camera(tim_rt_ctx* c, tim_rt_scene_id id, const tim_rt_pass_dat
         cudaEventElapsedTime(&stats->secondary_ms, c->pev[2], c->pev[3]);
         if (count) read_counts(c, stats);
     }
+    return TIM_RT_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- batched multi-scene trace
+
+namespace {
+
+// Sort scratch of a batch: keys[2] (8 B per ray each), vals[2] (4 B per ray each),
+// then the radix sort's temporary storage, each part 256-byte aligned.
+int batch_sort_scratch(tim_rt_ctx* c, tim_rt_batch* b) {
+    if (b->sort.ptr) return TIM_RT_OK;
+    auto up = [](uint64_t x) { return (x + 255ull) & ~255ull; };
+    const uint64_t n = b->total;
+    const uint64_t o_k1 = up(8 * n), o_v0 = o_k1 + up(8 * n), o_v1 = o_v0 + up(4 * n), o_t = o_v1 + up(4 * n);
+    const size_t tb = multi_sort_temp_bytes(b->total);
+    int rc = dev_alloc(c, b->sort, o_t + tb);
+    if (rc) return rc;
+    uint8_t* base = static_cast<uint8_t*>(b->sort.ptr);
+    b->ss.keys[0] = reinterpret_cast<unsigned long long*>(base);
+    b->ss.keys[1] = reinterpret_cast<unsigned long long*>(base + o_k1);
+    b->ss.vals[0] = reinterpret_cast<uint32_t*>(base + o_v0);
+    b->ss.vals[1] = reinterpret_cast<uint32_t*>(base + o_v1);
+    b->ss.temp = base + o_t;
+    b->ss.temp_bytes = tb;
+    return TIM_RT_OK;
+}
+
+bool live_batch(tim_rt_ctx* c, const tim_rt_batch* b) {
+    if (b && c->batches.count(const_cast<tim_rt_batch*>(b))) return true;
+    set_error("unknown batch");
+    return false;
+}
+
+int batch_run(tim_rt_ctx* c, tim_rt_batch* b, const LaunchConfig& cfg, bool wide, cudaStream_t st) {
+    if (b->total == 0) return TIM_RT_OK;
+    int rc;
+    if (cfg.ray_sort != TIM_RT_SORT_NONE && (rc = batch_sort_scratch(c, b))) return rc;
+    int depth = wide ? b->wide_depth : b->depth;
+    if (cfg.stack_depth > depth) depth = cfg.stack_depth;
+    uint32_t* err = static_cast<uint32_t*>(c->counters.ptr) + kErrWord;
+    TIMRT_CUDA(launch_multi(b->d_views, b->d_jobs, b->njobs, b->total, b->d_counter, err, depth, wide,
+                            cfg.ray_sort != TIM_RT_SORT_NONE ? &b->ss : nullptr, st, cfg));
+    return TIM_RT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tim_rt_batch_create(tim_rt_ctx* c, const tim_rt_job* jobs, uint32_t num_jobs, uint32_t flags,
+                        tim_rt_batch** out) {
+    int rc = check_ctx(c);
+    if (rc) return rc;
+    if (!out || (num_jobs && !jobs) || (flags & ~TIM_RT_BATCH_WIDE)) {
+        set_error("tim_rt_batch_create: null argument or unknown flag");
+        return TIM_RT_EINVAL;
+    }
+    *out = nullptr;
+    const bool wide = (flags & TIM_RT_BATCH_WIDE) != 0;
+    std::map<uint32_t, uint32_t> slot_of;
+    std::vector<SceneView> views;
+    std::vector<MultiJob> table;
+    auto b = std::make_unique<tim_rt_batch>();
+    uint64_t total = 0;
+    for (uint32_t j = 0; j < num_jobs; ++j) {
+        const tim_rt_job& J = jobs[j];
+        Scene* s = find_scene(c, J.scene);
+        if (!s) return TIM_RT_ENOTFOUND;
+        if (J.mode > TIM_RT_MODE_PER_RAY || (J.n && (!J.d_rays || !J.d_hit)) ||
+            (reinterpret_cast<uintptr_t>(J.d_rays) & 15u) || (reinterpret_cast<uintptr_t>(J.d_hit) & 15u) ||
+            (reinterpret_cast<uintptr_t>(J.d_bary) & 7u) || (reinterpret_cast<uintptr_t>(J.d_leaf_nid) & 3u)) {
+            set_error("tim_rt_batch_create: job " + std::to_string(j) + ": bad mode, null or misaligned buffer");
+            return TIM_RT_EINVAL;
+        }
+        if (wide && !s->has_wide) {
+            set_error("tim_rt_batch_create: scene " + std::to_string(J.scene) +
+                      " was uploaded without TIM_RT_UPLOAD_QUANT8");
+            return TIM_RT_EUNSUPPORTED;
+        }
+        if (J.n == 0) continue;
+        auto it = slot_of.find(J.scene);
+        if (it == slot_of.end()) {
+            it = slot_of.emplace(J.scene, (uint32_t)views.size()).first;
+            views.push_back(s->view);
+            b->scene_ids.push_back(J.scene);
+            b->depth = std::max(b->depth, (int)s->depth);
+            b->wide_depth = std::max(b->wide_depth, (int)s->view.wide_depth);
+        }
+        MultiJob m{};
+        m.rays = J.d_rays;
+        m.hit = reinterpret_cast<uint4*>(J.d_hit);
+        m.nid = J.d_leaf_nid;
+        m.bary = reinterpret_cast<float2*>(J.d_bary);
+        m.scene_slot = it->second;
+        m.mode = J.mode;
+        m.first = (uint32_t)total;
+        m.n = J.n;
+        for (int a = 0; a < 3; ++a) {
+            m.lo[a] = s->bounds[a];
+            const float ext = s->bounds[3 + a] - s->bounds[a];
+            m.scale[a] = ext > 0.f ? 1024.0f / ext : 0.f;
+        }
+        table.push_back(m);
+        total += J.n;
+        if (total > 0x7FFFFFFFull) {
+            set_error("tim_rt_batch_create: more than 2^31 - 1 rays in one batch");
+            return TIM_RT_EINVAL;
+        }
+    }
+    b->njobs = (uint32_t)table.size();
+    b->total = (uint32_t)total;
+    b->wide = wide;
+    const uint64_t vb = (sizeof(SceneView) * views.size() + 15ull) & ~15ull;
+    const uint64_t jb = (sizeof(MultiJob) * table.size() + 15ull) & ~15ull;
+    if ((rc = dev_alloc(c, b->table, vb + jb + 16))) return rc;
+    uint8_t* base = static_cast<uint8_t*>(b->table.ptr);
+    b->d_views = reinterpret_cast<SceneView*>(base);
+    b->d_jobs = reinterpret_cast<MultiJob*>(base + vb);
+    b->d_counter = reinterpret_cast<uint32_t*>(base + vb + jb);
+    if ((!views.empty() && cudaMemcpy(b->d_views, views.data(), sizeof(SceneView) * views.size(),
+                                      cudaMemcpyHostToDevice) != cudaSuccess) ||
+        (!table.empty() && cudaMemcpy(b->d_jobs, table.data(), sizeof(MultiJob) * table.size(),
+                                      cudaMemcpyHostToDevice) != cudaSuccess)) {
+        dev_free(c, b->table);
+        set_error("tim_rt_batch_create: host-to-device copy of the job table failed");
+        return TIM_RT_EDEVICE;
+    }
+    for (uint32_t id : b->scene_ids) c->scenes[id]->batch_refs++;
+    *out = b.release();
+    c->batches.insert(*out);
+    return TIM_RT_OK;
+}
+
+int tim_rt_batch_launch(tim_rt_ctx* c, tim_rt_batch* b, void* cuda_stream) {
+    int rc = check_ctx(c);
+    if (rc) return rc;
+    if (!live_batch(c, b)) return TIM_RT_EINVAL;
+    cudaStream_t st = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : c->stream;
+    LaunchConfig cfg = c->cfg;
+    cfg.stats = nullptr;
+    return batch_run(c, b, cfg, b->wide, st);
+}
+
+int tim_rt_batch_info(tim_rt_ctx* c, const tim_rt_batch* b, uint64_t* rays, uint64_t* bytes) {
+    if (!c || !live_batch(c, b)) return TIM_RT_EINVAL;
+    if (rays) *rays = b->total;
+    if (bytes) *bytes = b->table.bytes + b->sort.bytes;
+    return TIM_RT_OK;
+}
+
+int tim_rt_batch_destroy(tim_rt_ctx* c, tim_rt_batch* b) {
+    int rc = check_ctx(c);
+    if (rc) return rc;
+    if (!b) return TIM_RT_OK;
+    if (!live_batch(c, b)) return TIM_RT_EINVAL;
+    cudaStreamSynchronize(c->stream);
+    cudaDeviceSynchronize();   // launches may have gone to caller streams
+    for (uint32_t id : b->scene_ids) {
+        auto it = c->scenes.find(id);
+        if (it != c->scenes.end() && it->second->batch_refs) it->second->batch_refs--;
+    }
+    dev_free(c, b->table);
+    dev_free(c, b->sort);
+    c->batches.erase(b);
+    delete b;
+    return TIM_RT_OK;
+}
+
+int tim_rt_autotune_batch(tim_rt_ctx* c, tim_rt_batch* b, uint32_t flags, uint32_t reps, tim_rt_tune_result* res) {
+    int rc = check_ctx(c);
+    if (rc) return rc;
+    if (!live_batch(c, b) || !res || (flags & ~TIM_RT_TUNE_WIDTH)) {
+        if (!res) set_error("tim_rt_autotune_batch: null result");
+        return TIM_RT_EINVAL;
+    }
+    std::memset(res, 0, sizeof(*res));
+    reps = reps == 0 ? 3 : std::min(reps, 50u);
+    bool can_wide = true;
+    for (uint32_t id : b->scene_ids) can_wide = can_wide && c->scenes[id]->has_wide;
+    cudaEvent_t e0, e1;
+    TIMRT_CUDA(cudaEventCreate(&e0));
+    TIMRT_CUDA(cudaEventCreate(&e1));
+    int err = TIM_RT_OK;
+    uint32_t tried = 0;
+    // median device time of one launch under (cfg, wide); negative on error
+    auto time_cfg = [&](const LaunchConfig& cfg, bool wide) -> float {
+        // a ray-sort key whose scratch does not fit the budget is not a candidate
+        if (cfg.ray_sort != TIM_RT_SORT_NONE && batch_sort_scratch(c, b) != TIM_RT_OK) return -1.f;
+        ++tried;
+        std::vector<float> ms;
+        for (uint32_t r = 0; r <= reps; ++r) {
+            cudaEventRecord(e0, c->stream);
+            int rc2 = batch_run(c, b, cfg, wide, c->stream);
+            cudaEventRecord(e1, c->stream);
+            if (rc2 || cudaEventSynchronize(e1) != cudaSuccess) {
+                err = rc2 ? rc2 : TIM_RT_EDEVICE;
+                return -1.f;
+            }
+            float t = 0.f;
+            cudaEventElapsedTime(&t, e0, e1);
+            if (r) ms.push_back(t);   // launch 0 is the warm-up
+        }
+        std::sort(ms.begin(), ms.end());
+        return ms[ms.size() / 2];
+    };
+    LaunchConfig best = c->cfg;
+    best.stats = nullptr;
+    best.phase_ev = nullptr;
+    bool best_wide = b->wide;
+    float best_ms = time_cfg(best, best_wide);
+    res->start_ms = best_ms;
+    auto consider = [&](LaunchConfig cand, bool wide) {
+        if (err) return;
+        const float t = time_cfg(cand, wide);
+        if (t >= 0.f && t < best_ms) {
+            best_ms = t;
+            best = cand;
+            best_wide = wide;
+        }
+    };
+    for (int pass = 0; pass < 2 && !err; ++pass) {
+        for (int blk : {64, 128, 256}) {
+            LaunchConfig cand = best;
+            if (cand.block == blk) continue;
+            cand.block = blk;
+            consider(cand, best_wide);
+        }
+        for (int refill : {4, 8, 12, 16, 20, 24, 28, 32}) {
+            LaunchConfig cand = best;
+            if (cand.refill_min == refill) continue;
+            cand.refill_min = refill;
+            consider(cand, best_wide);
+        }
+        for (int srt : {0, 1, 2}) {
+            LaunchConfig cand = best;
+            if (cand.ray_sort == srt) continue;
+            cand.ray_sort = srt;
+            consider(cand, best_wide);
+        }
+        for (int sd : {0, 32}) {
+            LaunchConfig cand = best;
+            if (cand.stack_depth == sd) continue;
+            cand.stack_depth = sd;
+            consider(cand, best_wide);
+        }
+        if ((flags & TIM_RT_TUNE_WIDTH) && can_wide) consider(best, !best_wide);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (err) return err;
+    c->cfg.block = best.block;
+    c->cfg.refill_min = best.refill_min;
+    c->cfg.ray_sort = best.ray_sort;
+    c->cfg.stack_depth = best.stack_depth;
+    b->wide = best_wide;
+    res->best.block = (uint32_t)best.block;
+    res->best.stack_depth = (uint32_t)best.stack_depth;
+    res->best.refill_min = (uint32_t)best.refill_min;
+    res->best.ray_sort = (uint32_t)best.ray_sort;
+    res->wide = best_wide ? 1u : 0u;
+    res->tried = tried;
+    res->best_ms = best_ms;
     return TIM_RT_OK;
 }
 

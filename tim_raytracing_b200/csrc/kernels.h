@@ -13,6 +13,7 @@ struct LaunchConfig {
     int stack_depth = 0;  // traversal-stack entries per thread; 0 = the scene's tree depth
     int refill_min = 16;  // a warp fetches new rays once this many lanes are idle (1..32)
     int wide_order = 1;   // 8-wide slot order: 1 = full nearest-first sort, 0 = nearest first, rest by slot
+    int ray_sort = 0;     // batched traces: TIM_RT_SORT_* key
     bool wide = false;  // 8-wide quantised BVH instead of the reference binary layout
     // when set, a counting variant of the kernel adds per-ray work to
     // stats[0..4] = (rays, node visits, leaf visits, triangle tests, node reloads)
@@ -35,6 +36,34 @@ cudaError_t launch_camera(const SceneView& s, const tim_rt_pass_data& pd, uint32
                           uint32_t* leaf_nid, tim_rt_ray* q_rays, uint32_t* q_pixel, uint32_t seg_cap,
                           uint32_t* counters, uint32_t* err, uint64_t* d_ray_count, cudaStream_t stream,
                           const LaunchConfig& cfg);
+
+// One job of a batched multi-scene trace (device table entry).
+struct MultiJob {
+    const tim_rt_ray* rays;
+    uint4* hit;
+    uint32_t* nid;
+    float2* bary;
+    uint32_t scene_slot;    // index into the context's device SceneView table
+    uint32_t mode;          // TIM_RT_MODE_*
+    uint32_t first;         // first work item of the job (prefix over the batch)
+    uint32_t n;
+    float lo[3];            // scene bounds, for the Morton ray-sort key
+    float scale[3];         // 1024 / extent per axis
+};
+// Ray-sort scratch of a batch: two key/value buffers of `total` entries and the
+// radix sort's temporary storage.
+struct SortScratch {
+    unsigned long long* keys[2];
+    uint32_t* vals[2];
+    void* temp;
+    size_t temp_bytes;
+};
+size_t multi_sort_temp_bytes(uint32_t total);
+// Resets `counter` and launches one persistent kernel over all jobs; with
+// cfg.ray_sort != 0 the rays are first ordered by the coherence key.
+cudaError_t launch_multi(const SceneView* views, const MultiJob* jobs, uint32_t njobs, uint32_t total, uint32_t* counter,
+                         uint32_t* err, int depth, bool wide, const SortScratch* sort, cudaStream_t stream,
+                         const LaunchConfig& cfg);
 
 // Light-probe update of probes [p0, p0 + np), nd directions each.
 struct ProbeArgs {
