@@ -186,13 +186,158 @@ def run_reference(args, rank, world):
     return 0
 
 
+def bench_batched(N, ctx, dev, steps, warmup):
+    """Batched multi-scene workload: 64 scenes of random triangles (counts log-U
+    [1K, 1M], edges log-U [1e-3, 1e-1] in the unit cube), each with its own batch
+    of log-U [4K, 2M] rays (origins uniform in the cube, directions uniform, half
+    closest-hit, half any-hit), traced by ONE persistent launch captured in a CUDA
+    graph with the autotuner's configuration; plain and 8-wide forms. Inputs
+    (~0.7 GB of rays) exceed L2, so no flush between steps."""
+    import torch
+    from tim_raytracing_b200 import scenes
+    rng = np.random.default_rng(3)
+    tris = np.exp(rng.uniform(np.log(1e3), np.log(1e6), 64)).astype(np.int64)
+    nrays = np.exp(rng.uniform(np.log(4e3), np.log(2e6), 64)).astype(np.int64)
+    t0 = time.perf_counter()
+    sids, d_rays = [], []
+    for k in range(64):
+        s = scenes.random_triangles(10_000 + k, int(tris[k]))
+        sids.append(ctx.upload(N.build_bvh(s), s, quant8=True))
+        d_rays.append(torch.from_numpy(scenes.random_rays(20_000 + k, int(nrays[k]))).to(dev))
+    setup_s = time.perf_counter() - t0
+    total = int(nrays.sum())
+    stream = torch.cuda.Stream(device=dev)
+    out = {}
+    hits = {}
+    for form in ("plain", "wide"):
+        hits[form] = [torch.empty((int(n), 4), dtype=torch.int32, device=dev) for n in nrays]
+        jobs = [(sids[k], N.MODE_PER_RAY, int(nrays[k]), d_rays[k], hits[form][k], None, None) for k in range(64)]
+        b = ctx.batch_create(jobs, wide=form == "wide")
+        ctx.set_launch_config()
+        tune = ctx.autotune_batch(b, width=False, reps=3)
+        ctx.batch_launch(b, stream=stream.cuda_stream)      # sizes the sort scratch before capture
+        stream.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=stream):
+            ctx.batch_launch(b, stream=stream.cuda_stream)
+        with torch.cuda.stream(stream):
+            for _ in range(warmup):
+                g.replay()
+        torch.cuda.synchronize()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        with torch.cuda.stream(stream):
+            for k in range(steps):
+                evs[k][0].record(stream)
+                g.replay()
+                evs[k][1].record(stream)
+        torch.cuda.synchronize()
+        ms = [a.elapsed_time(c) for a, c in evs]
+        # the same rays as 64 separate single-scene launches (default configuration)
+        ctx.set_launch_config()
+        sep = []
+        for rep in range(3):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for k in range(64):
+                ctx.trace_dev(sids[k], d_rays[k], int(nrays[k]), N.MODE_PER_RAY | (N.TRACE_WIDE if form == "wide" else 0),
+                              hits[form][k], stream=stream.cuda_stream)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            sep.append(e0.elapsed_time(e1))
+        del g
+        ctx.batch_destroy(b)
+        med = float(np.median(ms))
+        out[form] = {"value": total / (sum(ms) / len(ms) / 1e3) / 1e6, "ms_per_launch_median": med,
+                     "autotuned": {k: tune[k] for k in ("block", "refill_min", "ray_sort", "stack_depth")},
+                     "autotune_ms": {"start": tune["start_ms"], "best": tune["best_ms"], "tried": tune["tried"]},
+                     "separate_launches_ms": float(np.median(sep)),
+                     "separate_launches_value": total / (float(np.median(sep)) / 1e3) / 1e6}
+    ctx.set_launch_config()
+    differing = 0
+    for k in range(64):
+        a, c = hits["plain"][k], hits["wide"][k]
+        differing += int((a != c).any(dim=1).sum().item())
+    for sid in sids:
+        ctx.free_scene(sid)
+    return {"workload": "64 random-triangle scenes (log-U 1K..1M tris), log-U 4K..2M rays each, 50% any-hit",
+            "triangles": int(tris.sum()), "rays": total, "setup_s": round(setup_s, 2),
+            "quantised_8wide": out["wide"], "plain_binary": out["plain"],
+            "speedup_quantised_over_plain": out["wide"]["value"] / out["plain"]["value"],
+            "hit_records_differing": differing, "l2": "not flushed: inputs exceed L2"}
+
+
+def bench_serving(N, ctx, dev, jobs_per_rate=1500):
+    """Serving workload: 16 resident heightfield + icosphere scenes (log-U [10K, 2M]
+    tris), Poisson arrivals of jobs of log-U [1K, 1M] mixed primary / shadow /
+    probe-update rays, a 40 GB device arena. First the saturation throughput
+    (jobs submitted back to back), then p50/p99 latency at 0.5x, 0.8x and 1.0x of
+    the saturation job rate. Host buffers are pinned."""
+    import torch
+    from tim_raytracing_b200 import scenes
+    rng = np.random.default_rng(5)
+    tris = np.exp(rng.uniform(np.log(1e4), np.log(2e6), 16)).astype(np.int64)
+    t0 = time.perf_counter()
+    sids, ntris = [], 0
+    for k in range(16):
+        s = scenes.scaled_heightfield(40 + k, int(tris[k]))
+        sids.append(ctx.upload(N.build_bvh(s), s, quant8=True))
+        ntris += s.num_tris
+    pool = []
+    for e in range(64):
+        n = int(np.exp(rng.uniform(np.log(1e3), np.log(1e6))))
+        r = torch.from_numpy(scenes.serving_rays(60_000 + e, n)).pin_memory()
+        h = torch.empty((n, 4), dtype=torch.int32).pin_memory()
+        pool.append((r, h))
+    setup_s = time.perf_counter() - t0
+    srv = N.Server(ctx, memory_budget_bytes=40 << 30, max_rays_per_step=4 << 20, max_inflight_steps=2, wide=True)
+    owner = [0] * len(pool)           # ticket of the job that last used each pool entry
+
+    def run(n_jobs, rate, seed):
+        """Submits n_jobs at Poisson times of `rate` jobs/s (0 = back to back)."""
+        rg = np.random.default_rng(seed)
+        srv.stats(reset=True)
+        gaps = rg.exponential(1.0 / rate, n_jobs) if rate else np.zeros(n_jobs)
+        t_next = time.perf_counter()
+        offered = 0
+        for j in range(n_jobs):
+            t_next += gaps[j]
+            while time.perf_counter() < t_next:
+                pass
+            e = int(rg.integers(len(pool)))
+            if owner[e]:
+                srv.wait(owner[e])
+            r, h = pool[e]
+            owner[e] = srv.submit(sids[int(rg.integers(16))], r, N.MODE_PER_RAY, h)
+            offered += r.shape[0]
+        srv.drain()
+        st = srv.stats()
+        return {"jobs": n_jobs, "rate_jobs_per_s": rate, "value": st["rays_completed"] / st["wall_s"] / 1e6,
+                "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"], "max_ms": st["max_ms"],
+                "queue_p50_ms": st["queue_p50_ms"], "queue_p99_ms": st["queue_p99_ms"], "steps": st["steps"],
+                "arena_peak_gb": st["arena_peak_bytes"] / 1e9, "wall_s": st["wall_s"]}
+
+    run(64, 0, 1)    # warm-up
+    sat = run(jobs_per_rate, 0, 2)
+    sat_rate = sat["jobs"] / sat["wall_s"]
+    rates = [run(jobs_per_rate, f * sat_rate, 10 + i) | {"load": f} for i, f in enumerate((0.5, 0.8, 1.0))]
+    srv.close()
+    for sid in sids:
+        ctx.free_scene(sid)
+    return {"workload": "16 heightfield+icosphere scenes (log-U 10K..2M tris), Poisson jobs of log-U 1K..1M mixed "
+                        "primary/shadow/probe rays, 40 GB arena, 8-wide BVHs",
+            "triangles": int(ntris), "setup_s": round(setup_s, 2), "saturation": sat,
+            "saturation_jobs_per_s": sat_rate, "rates": rates}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="tim")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched multi-scene workload")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving workload")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -356,6 +501,12 @@ def main():
                                   "tri_tests": stc.secondary_tri_tests / r, "node_reloads": stc.secondary_node_reloads / r,
                                   "bytes": abytes / r}}
     l2_gbs = N.measure_l2_gbs(local)
+    # the batched multi-scene and serving workloads (one GPU; skipped in scaling runs)
+    batched = serving = None
+    if world == 1 and not args.no_batched:
+        batched = bench_batched(N, ctx, dev, args.steps, args.warmup)
+    if world == 1 and not args.no_serving:
+        serving = bench_serving(N, ctx, dev)
 
     if rank == 0:
         line = {
@@ -387,6 +538,14 @@ def main():
             "peak_source": peak_src, "l2_peak_gbs_measured": l2_gbs, "frac_of_l2": achieved / l2_gbs,
             "note": "the 11 MB scene is L2-resident; DRAM carries only the ray queue (see traffic)"}
         line["kernels"] = kern
+        if batched:
+            line["batched"] = batched
+        if serving:
+            line["serving"] = serving
+            r8 = serving["rates"][1]
+            line["latency"] = {"p50_ms": r8["p50_ms"], "p99_ms": r8["p99_ms"], "unit": "ms",
+                               "arrival": f"Poisson, {r8['rate_jobs_per_s']:.0f} jobs/s (0.8x saturation)",
+                               "throughput": r8["value"]}
         if not args.no_cpu_baseline and world == 1:
             from oracle import oracle as O
             line["cpu_baseline"] = cpu_baseline(scene, img, pd, O.threads_available())

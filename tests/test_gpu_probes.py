@@ -62,12 +62,6 @@ def test_probe_update_matches_oracle(ctx, native, oracle_mod, wide):
         otr, oirr, ocounts = O.probe_trace(sc, od, dirs, p0, p1)
         otr = otr.reshape(tr.shape)
         oirr = oirr.reshape(irr.shape)
-        if wide:
-            # the quantised walk may resolve near-ties differently; everything else must agree
-            same = np.all(tr == otr, axis=2)
-            assert same.mean() > 0.999
-            assert np.array_equal(irr[same].view(np.uint32), oirr[same].view(np.uint32))
-            return
         assert np.array_equal(tr, otr)
         assert np.array_equal(irr.view(np.uint32), oirr.view(np.uint32))
         assert st.rays == int(ocounts[0] + ocounts[1])

@@ -81,9 +81,12 @@ namespace {
 struct Slot {
     uint32_t id;        // binary node id | kLeafBit for leaves
     float lo[3], hi[3]; // box the reference stores for this subtree (in its parent record)
+    // per axis, the intersection of this box and the boxes of all its binary
+    // ancestors (each box's two planes taken as min / max)
+    float elo[3], ehi[3];
 };
 
-void child_slots(const PNode& n, Slot& a, Slot& b) {
+void child_slots(const PNode& n, Slot& a, Slot& b, const Slot* parent) {
     const uint32_t left = n.nid[2] & kMask;
     a.id = left | ((n.nid[2] & kLeftLeaf) ? kLeafBit : 0u);
     b.id = (left + 1u) | ((n.nid[2] & kRightLeaf) ? kLeafBit : 0u);
@@ -91,6 +94,12 @@ void child_slots(const PNode& n, Slot& a, Slot& b) {
     a.hi[0] = n.n0xy[2]; a.hi[1] = n.n0xy[3]; a.hi[2] = n.nz[1];
     b.lo[0] = n.n1xy[0]; b.lo[1] = n.n1xy[1]; b.lo[2] = n.nz[2];
     b.hi[0] = n.n1xy[2]; b.hi[1] = n.n1xy[3]; b.hi[2] = n.nz[3];
+    for (Slot* c : {&a, &b})
+        for (int ax = 0; ax < 3; ++ax) {
+            const float lo = std::min(c->lo[ax], c->hi[ax]), hi = std::max(c->lo[ax], c->hi[ax]);
+            c->elo[ax] = parent ? std::max(parent->elo[ax], lo) : lo;
+            c->ehi[ax] = parent ? std::min(parent->ehi[ax], hi) : hi;
+        }
 }
 
 double area(const Slot& s) {
@@ -209,8 +218,18 @@ bool build_wide(const uint8_t* blob, const uint32_t ranges[7][2], uint32_t num_n
         if (off == 0xFFFFFFFFu || off >= leaf_words) return 0u;
         return leaf[off] & 0xFFFu;
     };
-    auto emit_tris = [&](uint32_t nid) {
+    auto emit_tris = [&](uint32_t nid, const Slot& box, bool no_box_test) {
         const uint32_t nm = nid & kMask;
+        const uint32_t entry = (uint32_t)(out.leaves.size() / 8);
+        uint32_t e[8];
+        std::memcpy(&e[0], box.elo, 12);
+        e[3] = nm;
+        std::memcpy(&e[4], box.ehi, 12);
+        // 1: tested without a box; 2: the boxes on its path do not overlap, so
+        // reachability cannot be shown from E (the kernel uses the binary walk)
+        const bool empty = box.elo[0] > box.ehi[0] || box.elo[1] > box.ehi[1] || box.elo[2] > box.ehi[2];
+        e[7] = no_box_test ? 1u : (empty ? 2u : 0u);
+        out.leaves.insert(out.leaves.end(), e, e + 8);
         const uint32_t off = nodes[nm].nid[3];
         const uint32_t nt = leaf_tris(nid);
         for (uint32_t t = 0; t < nt; ++t) {
@@ -227,7 +246,7 @@ bool build_wide(const uint8_t* blob, const uint32_t ranges[7][2], uint32_t num_n
             std::memcpy(&w[7], &r[1], 4);
             std::memcpy(&w[11], &r[2], 4);
             out.tris.insert(out.tris.end(), w, w + 12);
-            out.tri_nid.push_back(nm);
+            out.tri_leaf.push_back(entry);
         }
     };
 
@@ -244,7 +263,7 @@ bool build_wide(const uint8_t* blob, const uint32_t ranges[7][2], uint32_t num_n
                 if (!(fr[k].id & kLeafBit) && area(fr[k]) > ba) { ba = area(fr[k]); best = (int)k; }
             if (best < 0) break;
             Slot a, b;
-            child_slots(nodes[fr[best].id], a, b);
+            child_slots(nodes[fr[best].id], a, b, &fr[best]);
             fr.erase(fr.begin() + best);
             fr.push_back(a);
             fr.push_back(b);
@@ -262,12 +281,12 @@ bool build_wide(const uint8_t* blob, const uint32_t ranges[7][2], uint32_t num_n
     if (num_nodes == 1u) {
         Slot s;
         s.id = kLeafBit;
-        for (int a = 0; a < 3; ++a) { s.lo[a] = 0.f; s.hi[a] = 0.f; }
+        for (int a = 0; a < 3; ++a) { s.lo[a] = s.hi[a] = s.elo[a] = s.ehi[a] = 0.f; }
         q.push_back({0u, {s}, 1u});
         out.root_is_leaf = 1u;
     } else {
         Slot a, b;
-        child_slots(nodes[0], a, b);
+        child_slots(nodes[0], a, b, nullptr);
         q.push_back({0u, expand({a, b}), 1u});
     }
     while (!q.empty()) {
@@ -328,7 +347,7 @@ bool build_wide(const uint8_t* blob, const uint32_t ranges[7][2], uint32_t num_n
                 const uint32_t nt = leaf_tris(sl[k].id);
                 if (nt > 255u) { err = "a leaf holds more than 255 triangles (8-wide slot limit)"; return false; }
                 meta[k] = (uint8_t)nt;
-                emit_tris(sl[k].id);
+                emit_tris(sl[k].id, sl[k], out.root_is_leaf != 0);
             }
         }
         std::memcpy(&w[6], meta, 8);
@@ -341,7 +360,7 @@ bool build_wide(const uint8_t* blob, const uint32_t ranges[7][2], uint32_t num_n
         for (int k = 0; k < n; ++k) {
             if (used[k] && !(sl[k].id & kLeafBit)) {
                 Slot a, b;
-                child_slots(nodes[sl[k].id], a, b);
+                child_slots(nodes[sl[k].id], a, b, &sl[k]);
                 q.push_back({ci++, expand({a, b}), job.depth + 1u});
             }
         }

@@ -19,7 +19,7 @@ struct DevBuf {
 };
 
 struct Scene {
-    DevBuf blob, pos, nrm, uv, wnodes, wtris, wnid;
+    DevBuf blob, pos, nrm, uv, wnodes, wtris, wnid, wleaf;
     SceneView view{};
     uint32_t ranges[7][2];
     tim_rt_push_constants pc{};

@@ -13,7 +13,12 @@ void set_error(const std::string& msg);
 struct WideHost {
     std::vector<uint32_t> nodes;     // 20 words per node
     std::vector<float> tris;         // 12 floats per leaf triangle
-    std::vector<uint32_t> tri_nid;   // binary leaf nid per leaf triangle
+    std::vector<uint32_t> tri_leaf;  // per leaf triangle: its binary leaf's entry in `leaves`
+    // per binary leaf, 8 words: lo.xyz of the intersection of its box and all its
+    // ancestors' boxes, its nid, hi.xyz of that intersection, and a flag: 1 when
+    // the reference tests it without a box (single-leaf tree), 2 when the
+    // intersection is empty
+    std::vector<uint32_t> leaves;
     uint32_t num_nodes = 0;
     uint32_t root_is_leaf = 0;
     uint32_t max_depth = 0;

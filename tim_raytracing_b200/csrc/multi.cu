@@ -122,8 +122,12 @@ __global__ void __launch_bounds__(BLOCK) k_multi(const SceneView* __restrict__ v
             continue;
         }
         if (active) {
-            if (WIDE) wide_step<BLOCK>(sv, st, stk, err, sdepth);
-            else plain_step<BLOCK>(sv, st, stk, err, sdepth);
+            if (WIDE && !st.plain) {
+                wide_step<BLOCK>(sv, st, stk, err, sdepth);
+                if (st.done) wide_finish(sv, st);   // false: restarted with the binary walk
+            } else {
+                plain_step<BLOCK>(sv, st, stk, err, sdepth);
+            }
             if (st.done) {
                 if (st.any) {
                     job.hit[idx] = make_uint4(st.hit ? 1u : 0u, 0u, 0u, __float_as_uint(tmax0));

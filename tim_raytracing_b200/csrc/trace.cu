@@ -221,8 +221,12 @@ __global__ void __launch_bounds__(BLOCK) k_persistent(SceneView s, Policy P, uin
             continue;
         }
         if (active) {
-            if (WIDE) wide_step<BLOCK>(s, st, stk, err, sdepth);
-            else plain_step<BLOCK>(s, st, stk, err, sdepth);
+            if (WIDE && !st.plain) {
+                wide_step<BLOCK>(s, st, stk, err, sdepth);
+                if (st.done) wide_finish(s, st);   // false: restarted with the binary walk
+            } else {
+                plain_step<BLOCK>(s, st, stk, err, sdepth);
+            }
             if (st.done) {
                 P.store(s, idx, st, tmax0);
                 if (STATS) {

@@ -35,6 +35,9 @@ struct TravState {
     uint32_t oct;       // ray octant: bit a set when the direction's component a is negative
     uint32_t first;     // rank of the nearest hit slot still to visit first (8 = none)
     WideHdr h;          // header of the current wide node
+    float t0;           // the ray's tmax
+    float t1, t2;       // closest: the smallest and second-smallest hit t; any: t of the hit
+    bool plain;         // the lane finishes this ray with the binary walk
 };
 
 __device__ __forceinline__ void trav_init(TravState& st, uint32_t root) {

@@ -33,6 +33,29 @@
 // So tmin_here <= tmin_reference and tmax_here >= tmax_reference for every
 // child: the quantised traversal visits a superset of the binary traversal's
 // leaves and never loses a hit.
+//
+// Same hit as the binary walk, for every ray. The reference's closest-hit rule
+// is order-dependent: a hit at t is accepted iff t < c, and then c = t - 1e-5,
+// so of two hits less than 1e-5 apart the one visited first wins. The 8-wide
+// walk visits leaves in another order, so it finds the smallest hit t1 exactly
+// (every candidate below c = min(tmax, t1 + 1e-5 + 2^-20 t1 + 2^-30) is tested) and the
+// second smallest t2, and keeps its answer only when the binary walk provably
+// gives the same one:
+//   (a) RN(t2 - 1e-5) > t1: no other hit can block the nearest one whatever the
+//       order, and after it is accepted none can replace it; and
+//   (b) its binary leaf is reached: the intersection E of the leaf's box and the
+//       boxes of all its binary ancestors (per axis the largest lower and the
+//       smallest upper plane, precomputed per leaf) passes CollideBox with
+//       tmin <= t1. For a direction without zero components IEEE subtraction and
+//       division are monotonic, so E's slab entry is the largest entry and its
+//       exit the smallest exit of all those boxes: each of them then passes its
+//       own test with any c > t1, which is every value c takes before the
+//       nearest hit is accepted. (The reference builder's child boxes can stick
+//       out of the parent's by an ulp, so the leaf box alone would not do.)
+// Any-hit rays keep their first hit under (b) alone. A ray failing a test (a
+// near-tie, a hit grazing its leaf box: about one ray in 10^5) is traced again
+// from the root with the binary walk by the same lane, which reproduces the
+// reference's order exactly.
 #pragma once
 #include "common.cuh"
 #include "trace_plain.cuh"
@@ -132,16 +155,27 @@ __device__ __forceinline__ void wide_leaf(const SceneView& s, TravState& st, con
             if (st.any) {
                 st.hit = true;
                 st.done = true;
+                st.t1 = t;
+                st.nid = __ldg(s.wtri_leaf + first + i);
                 return;
             }
-            st.t = t - kOffsetRayCollision;
-            st.rec0 = __float_as_uint(A.w);
-            st.rec1 = __float_as_uint(B.w);
-            st.rec2 = __float_as_uint(C.w);
-            st.nid = __ldg(s.wtri_nid + first + i);
-            st.u = u;
-            st.v = v;
-            st.hit = true;
+            if (t < st.t1) {
+                st.t2 = st.t1;
+                st.t1 = t;
+                // test every hit that could still block or replace the nearest one
+                // (c = t + 1e-5 + 2^-20 t + 2^-30: the margin exceeds the rounding of
+                // RN(t2 - 1e-5) and of this sum, so every t2 that matters is below c)
+                st.t = fminf(st.t0, t + (kOffsetRayCollision + (t * 9.5367431640625e-07f + 9.313225746154785e-10f)));
+                st.rec0 = __float_as_uint(A.w);
+                st.rec1 = __float_as_uint(B.w);
+                st.rec2 = __float_as_uint(C.w);
+                st.nid = __ldg(s.wtri_leaf + first + i);
+                st.u = u;
+                st.v = v;
+                st.hit = true;
+            } else {
+                st.t2 = fminf(st.t2, t);
+            }
         }
     }
 }
@@ -162,6 +196,9 @@ __device__ __forceinline__ void wide_init(const SceneView& s, TravState& st, uin
     st.u = st.v = 0.0f;
     st.node = 0u;
     st.c_node = st.c_leaf = st.c_tri = st.c_reload = 0u;
+    st.t0 = st.t;
+    st.t1 = st.t2 = __int_as_float(0x7F800000);   // +inf
+    st.plain = false;
     if (s.num_wnodes == 0u) {
         st.done = true;
         return;
@@ -225,6 +262,32 @@ __device__ __forceinline__ void wide_step(const SceneView& s, TravState& st, uin
             return;
         }
     }
+}
+
+// Called when the 8-wide walk of a ray ends: keeps its answer (binary leaf nid,
+// closest t - 1e-5) when tests (a) and (b) above hold and returns true;
+// otherwise restarts the ray from the root with the binary walk and returns false.
+__device__ __forceinline__ bool wide_finish(const SceneView& s, TravState& st) {
+    if (!st.hit) return true;   // no hit below tmax anywhere: the binary walk finds none either
+    const uint4 lo = __ldg(s.wleaf + 2u * st.nid), hi = __ldg(s.wleaf + 2u * st.nid + 1u);
+    bool same = hi.w == 1u;     // a single-leaf tree is intersected without a box test
+    // a zero direction component makes the reference divide by zero, and an empty
+    // E proves nothing: binary walk
+    if (hi.w == 0u && st.r.dx != 0.0f && st.r.dy != 0.0f && st.r.dz != 0.0f) {
+        const float d = collide_box(st.r, __uint_as_float(lo.x), __uint_as_float(lo.y), __uint_as_float(lo.z),
+                                    __uint_as_float(hi.x), __uint_as_float(hi.y), __uint_as_float(hi.z), st.t0);
+        same = d >= 0.0f && d <= st.t1;
+    }
+    if (!st.any) same = same && (st.t2 - kOffsetRayCollision > st.t1);
+    if (same) {
+        st.nid = lo.w;
+        if (!st.any) st.t = st.t1 - kOffsetRayCollision;
+        return true;
+    }
+    st.t = st.t0;
+    trav_init(st, s.num_nodes == 1u ? kNidLeafBit : 0u);
+    st.plain = true;
+    return false;
 }
 
 }  // namespace timrt

@@ -219,6 +219,46 @@ def heightfield_scene(seed: int = 2, grid: int = 128, n_spheres: int = 53, exten
                    cam_target=(extent * 0.5, extent * 0.6, 0.0), sun_dir=(-0.4, 0.3, -1.0), seed=seed)
 
 
+def scaled_heightfield(seed: int, target_tris: int, extent: float = 20.0) -> Scene:
+    """The heightfield + icosphere generator at about target_tris triangles, with
+    the ~100K scene's split (one third heightfield, two thirds icospheres)."""
+    grid = max(4, int(round(math.sqrt(target_tris / 6.0))))
+    n_spheres = max(0, int(round((target_tris - 2 * grid * grid) / 1280.0)))
+    return heightfield_scene(seed=seed, grid=grid, n_spheres=n_spheres, extent=extent)
+
+
+def serving_rays(seed: int, n: int, extent: float = 20.0, lights=None) -> np.ndarray:
+    """Mixed rays of a serving job over a heightfield scene, one third each:
+    primary (from z = 8 looking down, closest hit), shadow (from a point above the
+    terrain towards a light, any hit, tmax = the light distance) and probe-update
+    (from a point in the probe box, uniform direction, closest hit). Ray records as
+    random_rays; flags bit 0 marks the shadow rays."""
+    rng = np.random.default_rng(seed)
+    r = np.zeros((n, 8), np.float32)
+    kind = rng.integers(0, 3, size=n)
+    o = np.empty((n, 3))
+    d = rng.normal(size=(n, 3))
+    tmax = np.full(n, TMAX)
+    p = kind == 0
+    o[p] = np.column_stack([rng.uniform(0, extent, (p.sum(), 2)), np.full(p.sum(), 8.0)])
+    d[p, 2] = -np.abs(d[p, 2]) - 2.0
+    s = kind == 1
+    o[s] = rng.uniform((0.0, 0.0, 0.0), (extent, extent, 2.5), size=(s.sum(), 3))
+    lp = (np.asarray(lights, np.float64)[:, :3] if lights is not None and len(lights)
+          else rng.uniform((0, 0, 0.5), (extent, extent, 5.0), size=(16, 3)))
+    tgt = lp[rng.integers(0, len(lp), size=s.sum())]
+    d[s] = tgt - o[s]
+    tmax[s] = np.linalg.norm(d[s], axis=1)
+    q = kind == 2
+    o[q] = rng.uniform((0.0, 0.0, 0.5), (extent, extent, 5.0), size=(q.sum(), 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    r[:, 0:3] = o
+    r[:, 3] = tmax
+    r[:, 4:7] = d
+    r.view(np.uint32)[:, 7] = s.astype(np.uint32)
+    return r
+
+
 def random_triangles(seed: int, n: int) -> Scene:
     """Config 3 scenes: n triangles in the unit cube; each has a vertex uniform in
     [0,1]^3 and two edges of length log-uniform in [1e-3, 1e-1] with uniform direction."""
