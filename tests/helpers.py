@@ -118,3 +118,23 @@ def adjudicate_closest(scene, rays, hit_a, hit_b, window=2.5e-5):
         if abs(da - db) > window:
             unexplained += 1
     return len(idx), unexplained, worst
+
+
+def near_tie_scene(seed, n):
+    """Random triangles, each present three times: as generated, as an exact copy
+    (equal t, different record) and moved 3e-6 along its normal (t within the
+    reference's 1e-5 acceptance window), so most closest hits are order-dependent
+    near-ties."""
+    from tim_raytracing_b200 import scenes
+    base = scenes.random_triangles(seed, n)
+    P = base.positions.reshape(-1, 3, 3)
+    N = base.normals.reshape(-1, 3, 3)
+    b = scenes._Builder()
+    per = 21845
+    for shift in (0.0, 0.0, 3e-6):
+        Q = (P + N * np.float32(shift)).astype(np.float32)
+        for s0 in range(0, len(Q), per):
+            q = Q[s0:s0 + per]
+            b.add(q.reshape(-1, 3), N[s0:s0 + per].reshape(-1, 3), np.arange(3 * len(q), dtype=np.uint32).reshape(-1, 3),
+                  (0.7, 0.7, 0.7))
+    return b.scene("near_ties", [], seed=seed)

@@ -161,6 +161,40 @@ def test_autotune_installs_a_config(mctx, native, world):
         mctx.batch_destroy(b)
 
 
+def test_batch_near_ties_match_oracle(mctx, native, oracle_mod):
+    """A batch whose scene is mostly near-ties (exercises the 8-wide walk's hand-over
+    to the binary walk inside the multi-scene kernel), next to an ordinary scene."""
+    import torch
+    from helpers import near_tie_scene
+    from tim_raytracing_b200 import scenes
+    s1 = near_tie_scene(41, 3000)
+    s2 = scenes.random_triangles(42, 5000)
+    imgs = [native.build_bvh(s1), native.build_bvh(s2)]
+    sids = [mctx.upload(imgs[0], s1, quant8=True), mctx.upload(imgs[1], s2, quant8=True)]
+    b = None
+    try:
+        rays = [scenes.random_rays(43, 20000, any_fraction=0.3), scenes.random_rays(44, 7000)]
+        d = [torch.from_numpy(r).cuda() for r in rays]
+        hits = [torch.zeros((len(r), 4), dtype=torch.int32, device="cuda") for r in rays]
+        nids = [torch.zeros(len(r), dtype=torch.int32, device="cuda") for r in rays]
+        b = mctx.batch_create([(sids[k], native.MODE_PER_RAY, len(rays[k]), d[k], hits[k], nids[k], None)
+                               for k in range(2)], wide=True)
+        for refill in (16, 1):
+            mctx.set_launch_config(block=128, refill_min=refill)
+            mctx.batch_launch(b)
+            torch.cuda.synchronize()
+            for k, (s, img) in enumerate(((s1, imgs[0]), (s2, imgs[1]))):
+                oh, on, _, _ = oracle_mod.trace(oracle_mod.Scene(img, s.positions, s.normals), rays[k], 2)
+                assert np.array_equal(hits[k].cpu().numpy().view(np.uint32), oh), (k, refill)
+                assert np.array_equal(nids[k].cpu().numpy().view(np.uint32), on), (k, refill)
+    finally:
+        mctx.set_launch_config()
+        if b is not None:
+            mctx.batch_destroy(b)
+        for sid in sids:
+            mctx.free_scene(sid)
+
+
 def test_batch_errors(mctx, native, world):
     built, jobs = world
     b = mctx.batch_create(_outputs(jobs[:2]))

@@ -6,7 +6,7 @@ whose answer it cannot prove equal with the binary walk)."""
 import numpy as np
 import pytest
 
-from helpers import load_room, load_room_golden
+from helpers import load_room, load_room_golden, near_tie_scene
 
 pytestmark = pytest.mark.gpu
 
@@ -99,31 +99,11 @@ def test_random_scene_mixed_rays(ctx, native, oracle_mod, n_tris, seed):
         ctx.free_scene(sid)
 
 
-def _near_tie_scene(seed, n):
-    """Random triangles, each present three times: as generated, as an exact copy
-    (equal t, different record) and moved 3e-6 along its normal (t within the
-    reference's 1e-5 acceptance window), so most closest hits are order-dependent
-    near-ties."""
-    from tim_raytracing_b200 import scenes
-    base = scenes.random_triangles(seed, n)
-    P = base.positions.reshape(-1, 3, 3)
-    N = base.normals.reshape(-1, 3, 3)
-    b = scenes._Builder()
-    per = 21845
-    for shift in (0.0, 0.0, 3e-6):
-        Q = (P + N * np.float32(shift)).astype(np.float32)
-        for s0 in range(0, len(Q), per):
-            q = Q[s0:s0 + per]
-            b.add(q.reshape(-1, 3), N[s0:s0 + per].reshape(-1, 3), np.arange(3 * len(q), dtype=np.uint32).reshape(-1, 3),
-                  (0.7, 0.7, 0.7))
-    return b.scene("near_ties", [], seed=seed)
-
-
 def test_wide_near_ties_match_oracle(ctx, native, oracle_mod):
     """Scenes built to be mostly near-ties: the 8-wide walk must still return the
     binary walk's (the reference's order-dependent) answer on every ray."""
     from tim_raytracing_b200 import scenes
-    s = _near_tie_scene(31, 4000)
+    s = near_tie_scene(31, 4000)
     img = native.build_bvh(s)
     sid = ctx.upload(img, s, quant8=True)
     try:

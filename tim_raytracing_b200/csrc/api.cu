@@ -188,7 +188,7 @@ int tim_rt_destroy(tim_rt_ctx* c) {
     c->batches.clear();
     for (auto& kv : c->scenes) {
         Scene* s = kv.second.get();
-        for (DevBuf* b : {&s->blob, &s->pos, &s->nrm, &s->uv, &s->wnodes, &s->wtris, &s->wnid, &s->wleaf}) dev_free(c, *b);
+        for (DevBuf* b : {&s->blob, &s->pos, &s->nrm, &s->uv, &s->wnodes, &s->wtris, &s->wnid}) dev_free(c, *b);
     }
     c->scenes.clear();
     for (DevBuf* b : {&c->rays, &c->hits, &c->nid, &c->bary, &c->counters, &c->cam_out, &c->cam_bounce, &c->cam_nid,
@@ -281,7 +281,7 @@ int tim_rt_upload_bvh(tim_rt_ctx* c, const void* bvh_bytes, uint64_t n_bytes, co
         }
     }
     auto fail = [&](int code) {
-        for (DevBuf* b : {&s->blob, &s->pos, &s->nrm, &s->uv, &s->wnodes, &s->wtris, &s->wnid, &s->wleaf}) dev_free(c, *b);
+        for (DevBuf* b : {&s->blob, &s->pos, &s->nrm, &s->uv, &s->wnodes, &s->wtris, &s->wnid}) dev_free(c, *b);
         return code;
     };
     if ((rc = dev_alloc(c, s->blob, n_bytes))) return fail(rc);
@@ -299,11 +299,9 @@ int tim_rt_upload_bvh(tim_rt_ctx* c, const void* bvh_bytes, uint64_t n_bytes, co
         if ((rc = dev_alloc(c, s->wnodes, 4ull * wh.nodes.size()))) return fail(rc);
         if ((rc = dev_alloc(c, s->wtris, 4ull * wh.tris.size()))) return fail(rc);
         if ((rc = dev_alloc(c, s->wnid, 4ull * wh.tri_leaf.size()))) return fail(rc);
-        if ((rc = dev_alloc(c, s->wleaf, 4ull * wh.leaves.size()))) return fail(rc);
         if (cudaMemcpyAsync(s->wnodes.ptr, wh.nodes.data(), 4ull * wh.nodes.size(), cudaMemcpyHostToDevice, c->stream) ||
             (!wh.tris.empty() && cudaMemcpyAsync(s->wtris.ptr, wh.tris.data(), 4ull * wh.tris.size(), cudaMemcpyHostToDevice, c->stream)) ||
-            (!wh.tri_leaf.empty() && cudaMemcpyAsync(s->wnid.ptr, wh.tri_leaf.data(), 4ull * wh.tri_leaf.size(), cudaMemcpyHostToDevice, c->stream)) ||
-            (!wh.leaves.empty() && cudaMemcpyAsync(s->wleaf.ptr, wh.leaves.data(), 4ull * wh.leaves.size(), cudaMemcpyHostToDevice, c->stream))) {
+            (!wh.tri_leaf.empty() && cudaMemcpyAsync(s->wnid.ptr, wh.tri_leaf.data(), 4ull * wh.tri_leaf.size(), cudaMemcpyHostToDevice, c->stream))) {
             set_error("tim_rt_upload_bvh: host-to-device copy of the 8-wide form failed");
             return fail(TIM_RT_EDEVICE);
         }
@@ -327,15 +325,13 @@ int tim_rt_upload_bvh(tim_rt_ctx* c, const void* bvh_bytes, uint64_t n_bytes, co
     v.leaf_words = ranges[TIM_RT_RANGE_LEAF][1] / 4u;
     v.num_vertex = num_vertex;
     v.depth = depth;
-    v.wide_depth = std::max(wh.max_depth, depth);   // the binary walk finishes ambiguous rays
+    v.wide_depth = wh.max_depth;
     v.wnodes = static_cast<const uint4*>(s->wnodes.ptr);
     v.wtris = static_cast<const float4*>(s->wtris.ptr);
-    v.wtri_leaf = static_cast<const uint32_t*>(s->wnid.ptr);
-    v.wleaf = static_cast<const uint4*>(s->wleaf.ptr);
+    v.wtri_leaf = static_cast<const uint4*>(s->wnid.ptr);
     v.num_wnodes = s->has_wide ? wh.num_nodes : 0u;
     v.wide_root_is_leaf = wh.root_is_leaf;
-    s->bytes = s->blob.bytes + s->pos.bytes + s->nrm.bytes + s->uv.bytes + s->wnodes.bytes + s->wtris.bytes + s->wnid.bytes +
-               s->wleaf.bytes;
+    s->bytes = s->blob.bytes + s->pos.bytes + s->nrm.bytes + s->uv.bytes + s->wnodes.bytes + s->wtris.bytes + s->wnid.bytes;
     const uint32_t id = c->next_id++;
     c->scenes[id] = std::move(s);
     *out = id;
@@ -368,7 +364,7 @@ int tim_rt_free_scene(tim_rt_ctx* c, tim_rt_scene_id id) {
         return TIM_RT_EINVAL;
     }
     cudaStreamSynchronize(c->stream);
-    for (DevBuf* b : {&s->blob, &s->pos, &s->nrm, &s->uv, &s->wnodes, &s->wtris, &s->wnid, &s->wleaf}) dev_free(c, *b);
+    for (DevBuf* b : {&s->blob, &s->pos, &s->nrm, &s->uv, &s->wnodes, &s->wtris, &s->wnid}) dev_free(c, *b);
     c->scenes.erase(id);
     return TIM_RT_OK;
 }

@@ -220,7 +220,6 @@ bool build_wide(const uint8_t* blob, const uint32_t ranges[7][2], uint32_t num_n
     };
     auto emit_tris = [&](uint32_t nid, const Slot& box, bool no_box_test) {
         const uint32_t nm = nid & kMask;
-        const uint32_t entry = (uint32_t)(out.leaves.size() / 8);
         uint32_t e[8];
         std::memcpy(&e[0], box.elo, 12);
         e[3] = nm;
@@ -229,7 +228,6 @@ bool build_wide(const uint8_t* blob, const uint32_t ranges[7][2], uint32_t num_n
         // reachability cannot be shown from E (the kernel uses the binary walk)
         const bool empty = box.elo[0] > box.ehi[0] || box.elo[1] > box.ehi[1] || box.elo[2] > box.ehi[2];
         e[7] = no_box_test ? 1u : (empty ? 2u : 0u);
-        out.leaves.insert(out.leaves.end(), e, e + 8);
         const uint32_t off = nodes[nm].nid[3];
         const uint32_t nt = leaf_tris(nid);
         for (uint32_t t = 0; t < nt; ++t) {
@@ -246,7 +244,7 @@ bool build_wide(const uint8_t* blob, const uint32_t ranges[7][2], uint32_t num_n
             std::memcpy(&w[7], &r[1], 4);
             std::memcpy(&w[11], &r[2], 4);
             out.tris.insert(out.tris.end(), w, w + 12);
-            out.tri_leaf.push_back(entry);
+            out.tri_leaf.insert(out.tri_leaf.end(), e, e + 8);
         }
     };
 

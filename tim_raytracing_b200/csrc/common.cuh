@@ -37,13 +37,11 @@ struct SceneView {
     uint32_t leaf_words;
     uint32_t num_vertex;
     uint32_t depth;             // binary tree depth (stack entries needed)
-    uint32_t wide_depth;        // stack entries of the 8-wide kernel: max(8-wide depth, binary depth),
-                                // since an ambiguous ray finishes with the binary walk
+    uint32_t wide_depth;        // 8-wide tree depth
     // 8-wide quantised form (null when not built)
     const uint4* wnodes;        // WideNode, 5 x 16 B
     const float4* wtris;        // 3 x float4 per leaf triangle: (p0, vo) (e1, i01) (e2, i2m)
-    const uint32_t* wtri_leaf;  // binary leaf entry (in wleaf) of each wide triangle
-    const uint4* wleaf;         // per binary leaf: (box lo.xyz, nid), (box hi.xyz, no-box-test flag)
+    const uint4* wtri_leaf;     // per wide triangle, its binary leaf: (E lo.xyz, nid), (E hi.xyz, flag)
     uint32_t num_wnodes;
     uint32_t wide_root_is_leaf; // scene is a single leaf
 };

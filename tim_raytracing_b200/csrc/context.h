@@ -19,7 +19,7 @@ struct DevBuf {
 };
 
 struct Scene {
-    DevBuf blob, pos, nrm, uv, wnodes, wtris, wnid, wleaf;
+    DevBuf blob, pos, nrm, uv, wnodes, wtris, wnid;
     SceneView view{};
     uint32_t ranges[7][2];
     tim_rt_push_constants pc{};

@@ -13,12 +13,11 @@ void set_error(const std::string& msg);
 struct WideHost {
     std::vector<uint32_t> nodes;     // 20 words per node
     std::vector<float> tris;         // 12 floats per leaf triangle
-    std::vector<uint32_t> tri_leaf;  // per leaf triangle: its binary leaf's entry in `leaves`
-    // per binary leaf, 8 words: lo.xyz of the intersection of its box and all its
-    // ancestors' boxes, its nid, hi.xyz of that intersection, and a flag: 1 when
-    // the reference tests it without a box (single-leaf tree), 2 when the
-    // intersection is empty
-    std::vector<uint32_t> leaves;
+    // per leaf triangle, 8 words about its binary leaf: lo.xyz of the intersection
+    // of the leaf's box and all its ancestors' boxes, the leaf's nid, hi.xyz of
+    // that intersection, and a flag: 1 when the reference tests the leaf without a
+    // box (single-leaf tree), 2 when the intersection is empty
+    std::vector<uint32_t> tri_leaf;
     uint32_t num_nodes = 0;
     uint32_t root_is_leaf = 0;
     uint32_t max_depth = 0;

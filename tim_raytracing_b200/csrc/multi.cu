@@ -73,7 +73,7 @@ __global__ void k_sort_keys(const MultiJob* __restrict__ jobs, uint32_t njobs, u
 // job up (binary search) and loads that job's scene view, so the lanes of one
 // warp may trace different scenes.
 template <int BLOCK, bool WIDE>
-__global__ void __launch_bounds__(BLOCK) k_multi(const SceneView* __restrict__ views, const MultiJob* __restrict__ jobs,
+__global__ void __launch_bounds__(BLOCK, WIDE ? 768 / BLOCK : 1) k_multi(const SceneView* __restrict__ views, const MultiJob* __restrict__ jobs,
                                                  uint32_t njobs, uint32_t total, const uint32_t* __restrict__ perm,
                                                  uint32_t* counter, uint32_t* err, int sdepth, int refill_min) {
     extern __shared__ uint32_t stack_mem[];
@@ -82,14 +82,34 @@ __global__ void __launch_bounds__(BLOCK) k_multi(const SceneView* __restrict__ v
     TravState st;
     st.done = true;
     SceneView sv;
-    MultiJob job;
-    bool active = false, exhausted = false;
-    uint32_t idx = 0;
-    float tmax0 = 0.f;
+    // active / pending as in k_persistent: lanes whose ray ended are finished
+    // (8-wide proof, binary walk when it fails) and stored together when the warp
+    // refills. The job's output pointers are read again at store time, so only
+    // its index stays live during the traversal.
+    bool active = false, pending = false, exhausted = false;
+    uint32_t idx = 0, jidx = 0;
     for (;;) {
-        if (!exhausted) {
-            const uint32_t need = __ballot_sync(0xFFFFFFFFu, !active);
-            if (need && (__popc(need) >= refill_min || need == 0xFFFFFFFFu)) {
+        const uint32_t idle = __ballot_sync(0xFFFFFFFFu, !active);
+        if (idle && (exhausted || __popc(idle) >= refill_min || idle == 0xFFFFFFFFu)) {
+            if (pending) {
+                pending = false;
+                if (WIDE) wide_finish_or_walk(sv, st, err);
+                const MultiJob& J = jobs[jidx];
+                uint4* hit = J.hit;
+                uint32_t* nid = J.nid;
+                float2* bary = J.bary;
+                if (st.any) {
+                    hit[idx] = make_uint4(st.hit ? 1u : 0u, 0u, 0u, __float_as_uint(st.t0));
+                    if (nid) nid[idx] = 0xFFFFFFFFu;
+                    if (bary) bary[idx] = make_float2(0.f, 0.f);
+                } else {
+                    hit[idx] = make_uint4(st.rec0, st.rec1, st.rec2, __float_as_uint(st.t));
+                    if (nid) nid[idx] = st.hit ? st.nid : 0xFFFFFFFFu;
+                    if (bary) bary[idx] = make_float2(st.u, st.v);
+                }
+            }
+            if (!exhausted) {
+                const uint32_t need = __ballot_sync(0xFFFFFFFFu, !active);
                 const int leader = __ffs(need) - 1;
                 uint32_t base = 0;
                 if ((int)lane == leader) base = atomicAdd(counter, (uint32_t)__popc(need));
@@ -99,17 +119,19 @@ __global__ void __launch_bounds__(BLOCK) k_multi(const SceneView* __restrict__ v
                     const uint32_t my = base + __popc(need & lanemask_lt());
                     if (my < total) {
                         const uint32_t item = perm ? __ldg(perm + my) : my;
-                        job = jobs[find_job(jobs, njobs, item)];
-                        sv = views[job.scene_slot];
-                        idx = item - job.first;
-                        const float4* rp = reinterpret_cast<const float4*>(job.rays + idx);
+                        jidx = find_job(jobs, njobs, item);
+                        const MultiJob& J = jobs[jidx];
+                        sv = views[J.scene_slot];
+                        idx = item - J.first;
+                        const uint32_t mode = J.mode;
+                        const float4* rp = reinterpret_cast<const float4*>(J.rays + idx);
                         const float4 a = __ldg(rp), b = __ldg(rp + 1);
                         st.r.ox = a.x; st.r.oy = a.y; st.r.oz = a.z;
                         st.r.dx = b.x; st.r.dy = b.y; st.r.dz = b.z;
                         st.t = a.w;
-                        tmax0 = a.w;
-                        st.any = (job.mode == TIM_RT_MODE_ANY) ||
-                                 (job.mode == TIM_RT_MODE_PER_RAY && (__float_as_uint(b.w) & TIM_RT_RAY_ANY));
+                        st.t0 = a.w;
+                        st.any = (mode == TIM_RT_MODE_ANY) ||
+                                 (mode == TIM_RT_MODE_PER_RAY && (__float_as_uint(b.w) & TIM_RT_RAY_ANY));
                         if (WIDE) wide_init(sv, st, stk);
                         else trav_init(st, sv.num_nodes == 1u ? kNidLeafBit : 0u);
                         active = true;
@@ -117,28 +139,16 @@ __global__ void __launch_bounds__(BLOCK) k_multi(const SceneView* __restrict__ v
                 }
             }
         }
-        if (__ballot_sync(0xFFFFFFFFu, active) == 0u) {
+        if (__ballot_sync(0xFFFFFFFFu, active || pending) == 0u) {
             if (exhausted) break;
             continue;
         }
         if (active) {
-            if (WIDE && !st.plain) {
-                wide_step<BLOCK>(sv, st, stk, err, sdepth);
-                if (st.done) wide_finish(sv, st);   // false: restarted with the binary walk
-            } else {
-                plain_step<BLOCK>(sv, st, stk, err, sdepth);
-            }
+            if (WIDE) wide_step<BLOCK>(sv, st, stk, err, sdepth);
+            else plain_step<BLOCK>(sv, st, stk, err, sdepth);
             if (st.done) {
-                if (st.any) {
-                    job.hit[idx] = make_uint4(st.hit ? 1u : 0u, 0u, 0u, __float_as_uint(tmax0));
-                    if (job.nid) job.nid[idx] = 0xFFFFFFFFu;
-                    if (job.bary) job.bary[idx] = make_float2(0.f, 0.f);
-                } else {
-                    job.hit[idx] = make_uint4(st.rec0, st.rec1, st.rec2, __float_as_uint(st.t));
-                    if (job.nid) job.nid[idx] = st.hit ? st.nid : 0xFFFFFFFFu;
-                    if (job.bary) job.bary[idx] = make_float2(st.u, st.v);
-                }
                 active = false;
+                pending = true;
             }
         }
     }

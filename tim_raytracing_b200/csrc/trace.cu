@@ -175,7 +175,7 @@ struct SecondaryPolicy {
 // lives in dynamic shared memory, entry k of thread t at [k * BLOCK + t]
 // (binary form) or [(2k, 2k+1) * BLOCK + t] (8-wide form).
 template <int BLOCK, bool WIDE, bool STATS, class Policy>
-__global__ void __launch_bounds__(BLOCK) k_persistent(SceneView s, Policy P, uint32_t n_static,
+__global__ void __launch_bounds__(BLOCK, WIDE ? 896 / BLOCK : 1) k_persistent(SceneView s, Policy P, uint32_t n_static,
                                                       const uint32_t* n_dev, uint32_t* counter, uint32_t* err,
                                                       unsigned long long* stats, int sdepth, int refill_min) {
     extern __shared__ uint32_t stack_mem[];
@@ -186,15 +186,32 @@ __global__ void __launch_bounds__(BLOCK) k_persistent(SceneView s, Policy P, uin
 
     TravState st;
     st.done = true;
-    bool active = false, exhausted = false;
+    // active: a ray is being traversed; pending: its traversal ended and its
+    // result waits to be finished (8-wide proof) and stored. Pending lanes are
+    // finished together when the warp refills, so that end-of-ray work runs
+    // converged instead of once per lane as lanes end at different steps.
+    bool active = false, pending = false, exhausted = false;
     uint32_t idx = 0;
-    float tmax0 = 0.f;
     for (;;) {
-        if (!exhausted) {
-            const uint32_t need = __ballot_sync(0xFFFFFFFFu, !active);
-            // refill once at least refill_min lanes are idle (32: whole-warp
-            // batches, which keeps coherent rays of a batch in lockstep)
-            if (need && (__popc(need) >= refill_min || need == 0xFFFFFFFFu)) {
+        const uint32_t idle = __ballot_sync(0xFFFFFFFFu, !active);
+        // refill once at least refill_min lanes are idle (32: whole-warp
+        // batches, which keeps coherent rays of a batch in lockstep); after the
+        // last ray was handed out, finish pending lanes as they come
+        if (idle && (exhausted || __popc(idle) >= refill_min || idle == 0xFFFFFFFFu)) {
+            if (pending) {
+                pending = false;
+                if (WIDE) wide_finish_or_walk(s, st, err);
+                P.store(s, idx, st, st.t0);
+                if (STATS) {
+                    atomicAdd(stats + 0, 1ull);
+                    atomicAdd(stats + 1, (unsigned long long)st.c_node);
+                    atomicAdd(stats + 2, (unsigned long long)st.c_leaf);
+                    atomicAdd(stats + 3, (unsigned long long)st.c_tri);
+                    atomicAdd(stats + 4, (unsigned long long)st.c_reload);
+                }
+            }
+            if (!exhausted) {
+                const uint32_t need = __ballot_sync(0xFFFFFFFFu, !active);
                 const int leader = __ffs(need) - 1;
                 uint32_t base = 0;
                 if ((int)lane == leader) base = atomicAdd(counter, (uint32_t)__popc(need));
@@ -205,7 +222,7 @@ __global__ void __launch_bounds__(BLOCK) k_persistent(SceneView s, Policy P, uin
                     if (my < n) {
                         idx = my;
                         if (P.load(s, idx, st)) {
-                            tmax0 = st.t;
+                            st.t0 = st.t;
                             if (WIDE) wide_init(s, st, stk);
                             else trav_init(st, root);
                             active = true;
@@ -216,27 +233,16 @@ __global__ void __launch_bounds__(BLOCK) k_persistent(SceneView s, Policy P, uin
                 }
             }
         }
-        if (__ballot_sync(0xFFFFFFFFu, active) == 0u) {
+        if (__ballot_sync(0xFFFFFFFFu, active || pending) == 0u) {
             if (exhausted) break;
             continue;
         }
         if (active) {
-            if (WIDE && !st.plain) {
-                wide_step<BLOCK>(s, st, stk, err, sdepth);
-                if (st.done) wide_finish(s, st);   // false: restarted with the binary walk
-            } else {
-                plain_step<BLOCK>(s, st, stk, err, sdepth);
-            }
+            if (WIDE) wide_step<BLOCK>(s, st, stk, err, sdepth);
+            else plain_step<BLOCK>(s, st, stk, err, sdepth);
             if (st.done) {
-                P.store(s, idx, st, tmax0);
-                if (STATS) {
-                    atomicAdd(stats + 0, 1ull);
-                    atomicAdd(stats + 1, (unsigned long long)st.c_node);
-                    atomicAdd(stats + 2, (unsigned long long)st.c_leaf);
-                    atomicAdd(stats + 3, (unsigned long long)st.c_tri);
-                    atomicAdd(stats + 4, (unsigned long long)st.c_reload);
-                }
                 active = false;
+                pending = true;
             }
         }
     }

@@ -36,8 +36,8 @@ struct TravState {
     uint32_t first;     // rank of the nearest hit slot still to visit first (8 = none)
     WideHdr h;          // header of the current wide node
     float t0;           // the ray's tmax
-    float t1, t2;       // closest: the smallest and second-smallest hit t; any: t of the hit
-    bool plain;         // the lane finishes this ray with the binary walk
+    float t1;           // closest: the smallest hit t; any: t of the hit
+    bool near2;         // closest: another hit t2 has RN(t2 - 1e-5) <= t1
 };
 
 __device__ __forceinline__ void trav_init(TravState& st, uint32_t root) {

@@ -38,9 +38,9 @@
 // is order-dependent: a hit at t is accepted iff t < c, and then c = t - 1e-5,
 // so of two hits less than 1e-5 apart the one visited first wins. The 8-wide
 // walk visits leaves in another order, so it finds the smallest hit t1 exactly
-// (every candidate below c = min(tmax, t1 + 1e-5 + 2^-20 t1 + 2^-30) is tested) and the
-// second smallest t2, and keeps its answer only when the binary walk provably
-// gives the same one:
+// (every candidate below c = min(tmax, t1 + 1e-5 + 2^-20 t1 + 2^-30) is tested),
+// tracks whether the second smallest t2 lies in its window, and keeps its answer
+// only when the binary walk provably gives the same one:
 //   (a) RN(t2 - 1e-5) > t1: no other hit can block the nearest one whatever the
 //       order, and after it is accepted none can replace it; and
 //   (b) its binary leaf is reached: the intersection E of the leaf's box and the
@@ -54,7 +54,7 @@
 //       out of the parent's by an ulp, so the leaf box alone would not do.)
 // Any-hit rays keep their first hit under (b) alone. A ray failing a test (a
 // near-tie, a hit grazing its leaf box: about one ray in 10^5) is traced again
-// from the root with the binary walk by the same lane, which reproduces the
+// from the root by the binary walk (binary_walk below), which reproduces the
 // reference's order exactly.
 #pragma once
 #include "common.cuh"
@@ -156,11 +156,12 @@ __device__ __forceinline__ void wide_leaf(const SceneView& s, TravState& st, con
                 st.hit = true;
                 st.done = true;
                 st.t1 = t;
-                st.nid = __ldg(s.wtri_leaf + first + i);
+                st.nid = first + i;   // wide triangle; wide_finish turns it into the leaf nid
                 return;
             }
             if (t < st.t1) {
-                st.t2 = st.t1;
+                // the old nearest becomes the second nearest (it is <= any other hit)
+                st.near2 = st.t1 - kOffsetRayCollision <= t;
                 st.t1 = t;
                 // test every hit that could still block or replace the nearest one
                 // (c = t + 1e-5 + 2^-20 t + 2^-30: the margin exceeds the rounding of
@@ -169,12 +170,14 @@ __device__ __forceinline__ void wide_leaf(const SceneView& s, TravState& st, con
                 st.rec0 = __float_as_uint(A.w);
                 st.rec1 = __float_as_uint(B.w);
                 st.rec2 = __float_as_uint(C.w);
-                st.nid = __ldg(s.wtri_leaf + first + i);
+                st.nid = first + i;
+                // wide_finish reads this triangle's leaf record: start fetching it now
+                asm volatile("prefetch.global.L1 [%0];" ::"l"(s.wtri_leaf + 2u * (first + i)));
                 st.u = u;
                 st.v = v;
                 st.hit = true;
             } else {
-                st.t2 = fminf(st.t2, t);
+                st.near2 = st.near2 || (t - kOffsetRayCollision <= st.t1);
             }
         }
     }
@@ -196,9 +199,8 @@ __device__ __forceinline__ void wide_init(const SceneView& s, TravState& st, uin
     st.u = st.v = 0.0f;
     st.node = 0u;
     st.c_node = st.c_leaf = st.c_tri = st.c_reload = 0u;
-    st.t0 = st.t;
-    st.t1 = st.t2 = __int_as_float(0x7F800000);   // +inf
-    st.plain = false;
+    st.t1 = __int_as_float(0x7F800000);   // +inf (st.t0 = tmax is set by the caller)
+    st.near2 = false;
     if (s.num_wnodes == 0u) {
         st.done = true;
         return;
@@ -266,28 +268,91 @@ __device__ __forceinline__ void wide_step(const SceneView& s, TravState& st, uin
 
 // Called when the 8-wide walk of a ray ends: keeps its answer (binary leaf nid,
 // closest t - 1e-5) when tests (a) and (b) above hold and returns true;
-// otherwise restarts the ray from the root with the binary walk and returns false.
+// otherwise returns false and the caller has the ray traced by the binary walk.
 __device__ __forceinline__ bool wide_finish(const SceneView& s, TravState& st) {
     if (!st.hit) return true;   // no hit below tmax anywhere: the binary walk finds none either
-    const uint4 lo = __ldg(s.wleaf + 2u * st.nid), hi = __ldg(s.wleaf + 2u * st.nid + 1u);
+    const uint4 lo = __ldg(s.wtri_leaf + 2u * st.nid), hi = __ldg(s.wtri_leaf + 2u * st.nid + 1u);
     bool same = hi.w == 1u;     // a single-leaf tree is intersected without a box test
     // a zero direction component makes the reference divide by zero, and an empty
     // E proves nothing: binary walk
     if (hi.w == 0u && st.r.dx != 0.0f && st.r.dy != 0.0f && st.r.dz != 0.0f) {
-        const float d = collide_box(st.r, __uint_as_float(lo.x), __uint_as_float(lo.y), __uint_as_float(lo.z),
-                                    __uint_as_float(hi.x), __uint_as_float(hi.y), __uint_as_float(hi.z), st.t0);
-        same = d >= 0.0f && d <= st.t1;
+        const float lx = __uint_as_float(lo.x), ly = __uint_as_float(lo.y), lz = __uint_as_float(lo.z);
+        const float hx = __uint_as_float(hi.x), hy = __uint_as_float(hi.y), hz = __uint_as_float(hi.z);
+        // Fast proof first: with inv = RN(1/d) (d != 0 here), RN((p - o) * inv) is
+        // within 2^-22 |t| of CollideBox's RN((p - o) / d), so moving every entry up
+        // and every exit down by 2^-21 |t| bounds the reference's tmin from above and
+        // its exit from below. (An infinite plane distance makes t +- |t| e NaN only
+        // on the side fminf / fmaxf then ignore, which is the side that does not
+        // constrain the reference either; the 2^-100 terms cover underflow.) Rays
+        // this cannot settle take the exact test with the reference's divisions.
+        constexpr float e = 4.76837158203125e-07f;   // 2^-21
+        constexpr float a = 7.888609052210118e-31f;  // 2^-100
+        const float ax = (lx - st.r.ox) * st.ix, bx = (hx - st.r.ox) * st.ix;
+        const float ay = (ly - st.r.oy) * st.iy, by = (hy - st.r.oy) * st.iy;
+        const float az = (lz - st.r.oz) * st.iz, bz = (hz - st.r.oz) * st.iz;
+        const float sx = fminf(ax, bx), sy = fminf(ay, by), sz = fminf(az, bz);
+        const float fx = fmaxf(ax, bx), fy = fmaxf(ay, by), fz = fmaxf(az, bz);
+        const float up = fmaxf(0.0f, fmaxf(sx + fabsf(sx) * e, fmaxf(sy + fabsf(sy) * e, sz + fabsf(sz) * e))) + a;
+        const float dn = fminf(fx - fabsf(fx) * e, fminf(fy - fabsf(fy) * e, fz - fabsf(fz) * e)) - a;
+        same = up <= st.t1 && up < dn;
+        if (!same) {
+            const float d = collide_box(st.r, lx, ly, lz, hx, hy, hz, st.t0);
+            same = d >= 0.0f && d <= st.t1;
+        }
     }
-    if (!st.any) same = same && (st.t2 - kOffsetRayCollision > st.t1);
+    if (!st.any) same = same && !st.near2;
     if (same) {
         st.nid = lo.w;
         if (!st.any) st.t = st.t1 - kOffsetRayCollision;
         return true;
     }
-    st.t = st.t0;
-    trav_init(st, s.num_nodes == 1u ? kNidLeafBit : 0u);
-    st.plain = true;
     return false;
+}
+
+// The binary walk of one ray from the root to the end, for the rays wide_finish
+// could not prove. Not inlined: its code and registers stay out of the 8-wide
+// kernels' hot loop (inlined, even unexecuted, it slowed them by about 5%); the
+// lane that calls it runs the whole walk while the warp's other lanes wait, which
+// costs little at about one ray in 10^5, and other warps hide its latency.
+struct BinaryResult {
+    uint32_t rec0, rec1, rec2, nid;
+    float t, u, v;
+    uint32_t hit;
+};
+
+static __device__ __noinline__ BinaryResult binary_walk(const float4* nodes, const uint32_t* leaf, const float* pos,
+                                                        const float* blas, uint32_t num_nodes, uint32_t leaf_words,
+                                                        float ox, float oy, float oz, float dx, float dy, float dz,
+                                                        float tmax, bool any, uint32_t* err) {
+    SceneView v{};
+    v.nodes = nodes;
+    v.leaf = leaf;
+    v.pos = pos;
+    v.blas = blas;
+    v.num_nodes = num_nodes;
+    v.leaf_words = leaf_words;
+    TravState st;
+    st.r.ox = ox; st.r.oy = oy; st.r.oz = oz;
+    st.r.dx = dx; st.r.dy = dy; st.r.dz = dz;
+    st.t = tmax;
+    st.any = any;
+    trav_init(st, num_nodes == 1u ? kNidLeafBit : 0u);
+    uint32_t stk[kStackSize];
+    do {
+        plain_step<1>(v, st, stk, err, kStackSize);
+    } while (!st.done);
+    return {st.rec0, st.rec1, st.rec2, st.nid, st.t, st.u, st.v, st.hit ? 1u : 0u};
+}
+
+// wide_finish, and the binary walk when it fails: afterwards st holds the
+// reference's answer for the ray.
+__device__ __forceinline__ void wide_finish_or_walk(const SceneView& s, TravState& st, uint32_t* err) {
+    if (wide_finish(s, st)) return;
+    const BinaryResult b = binary_walk(s.nodes, s.leaf, s.pos, s.blas, s.num_nodes, s.leaf_words, st.r.ox, st.r.oy,
+                                       st.r.oz, st.r.dx, st.r.dy, st.r.dz, st.t0, st.any, err);
+    st.rec0 = b.rec0; st.rec1 = b.rec1; st.rec2 = b.rec2; st.nid = b.nid;
+    st.t = b.t; st.u = b.u; st.v = b.v;
+    st.hit = b.hit != 0u;
 }
 
 }  // namespace timrt
