@@ -125,9 +125,10 @@ int tim_rt_memory_used(tim_rt_ctx *ctx, uint64_t *bytes);
 
 /* Launch shape of the persistent trace kernels (the knobs the autotuner picks). */
 typedef struct {
-    uint32_t block;        /* threads per block: 64, 128 or 256 */
+    uint32_t block;        /* threads per block: 64, 128 or 256 (default 256) */
     uint32_t stack_depth;  /* traversal-stack entries per thread; 0 = the scene's tree depth (<= 32) */
-    uint32_t refill_min;   /* a warp fetches new rays once this many of its 32 lanes are idle (1..32) */
+    uint32_t refill_min;   /* a warp fetches new rays once this many of its 32 lanes are idle (1..32);
+                              camera primary rays always refill whole warps (one 8x4-pixel tile) */
     uint32_t ray_sort;     /* batched traces: TIM_RT_SORT_* coherence key the rays are reordered by */
 } tim_rt_launch_config;
 #define TIM_RT_SORT_NONE 0u     /* trace in input order */

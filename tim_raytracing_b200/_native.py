@@ -305,7 +305,7 @@ class Context:
         _check(self._L.tim_rt_get_launch_config(self._c, ctypes.byref(c)))
         return {"block": c.block, "stack_depth": c.stack_depth, "refill_min": c.refill_min, "ray_sort": c.ray_sort}
 
-    def set_launch_config(self, block: int = 128, stack_depth: int = 0, refill_min: int = 16, ray_sort: int = 0):
+    def set_launch_config(self, block: int = 256, stack_depth: int = 0, refill_min: int = 16, ray_sort: int = 0):
         c = LaunchConfig(block, stack_depth, refill_min, ray_sort)
         _check(self._L.tim_rt_set_launch_config(self._c, ctypes.byref(c)))
 

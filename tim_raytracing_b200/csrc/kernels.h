@@ -9,10 +9,9 @@ namespace timrt {
 
 // Launch shape of the persistent trace kernels (chosen by the autotuner).
 struct LaunchConfig {
-    int block = 128;    // threads per block: 64, 128 or 256
+    int block = 256;    // threads per block: 64, 128 or 256
     int stack_depth = 0;  // traversal-stack entries per thread; 0 = the scene's tree depth
     int refill_min = 16;  // a warp fetches new rays once this many lanes are idle (1..32)
-    int wide_order = 1;   // 8-wide slot order: 1 = full nearest-first sort, 0 = nearest first, rest by slot
     int ray_sort = 0;     // batched traces: TIM_RT_SORT_* key
     bool wide = false;  // 8-wide quantised BVH instead of the reference binary layout
     // when set, a counting variant of the kernel adds per-ray work to
