@@ -189,6 +189,19 @@ def run_reference(args, rank, world):
     return 0
 
 
+def aggregate(t, rays, dist, dev):
+    """Whole-job figures of a replica run: the slowest rank's time and the rays of
+    all ranks (every rank calls this with its own numbers; no-op on one rank)."""
+    if not dist:
+        return float(t), float(rays)
+    import torch
+    tt = torch.tensor([float(t)], dtype=torch.float64, device=dev)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    rr = torch.tensor([float(rays)], dtype=torch.float64, device=dev)
+    dist.all_reduce(rr)
+    return float(tt.item()), float(rr.item())
+
+
 def bench_batched(N, ctx, dev, steps, warmup):
     """Batched multi-scene workload: 64 scenes of random triangles (counts log-U
     [1K, 1M], edges log-U [1e-3, 1e-1] in the unit cube), each with its own batch
@@ -257,16 +270,76 @@ def bench_batched(N, ctx, dev, steps, warmup):
                      "separate_launches_value": total / (float(np.median(sep)) / 1e3) / 1e6}
     ctx.set_launch_config()
     differing = 0
+    ver = {"hits_checked": 0, "fp64_misses": 0, "max_abs_t_err": 0.0, "max_rel_t_err": 0.0}
     for k in range(64):
         a, c = hits["plain"][k], hits["wide"][k]
         differing += int((a != c).any(dim=1).sum().item())
+        v = ctx.verify_hits(sids[k], d_rays[k], int(nrays[k]), hits["wide"][k])
+        ver["hits_checked"] += v["hits_checked"]
+        ver["fp64_misses"] += v["fp64_misses"]
+        ver["max_abs_t_err"] = max(ver["max_abs_t_err"], v["max_abs_t_err"])
+        ver["max_rel_t_err"] = max(ver["max_rel_t_err"], v["max_rel_t_err"])
     for sid in sids:
         ctx.free_scene(sid)
     return {"workload": "64 random-triangle scenes (log-U 1K..1M tris), log-U 4K..2M rays each, 50% any-hit",
             "triangles": int(tris.sum()), "rays": total, "setup_s": round(setup_s, 2),
             "quantised_8wide": out["wide"], "plain_binary": out["plain"],
             "speedup_quantised_over_plain": out["wide"]["value"] / out["plain"]["value"],
-            "hit_records_differing": differing, "l2": "not flushed: inputs exceed L2"}
+            "hit_records_differing": differing, "l2": "not flushed: inputs exceed L2",
+            "fp64_check": dict(ver, note="closest-hit records re-intersected in FP64 on the GPU (tim_rt_verify_hits); "
+                                         "any-hit records carry no t and are not checked")}
+
+
+def bench_probes(N, ctx, reps=5):
+    """Light-probe field workload: the heightfield + icosphere generator at 1M
+    triangles, a 32x32x8 probe grid, 256 octahedrally distributed rays per probe
+    per update (closest hit, then sun and leaf-light shadow rays), FP32 radiance
+    averaged into 8x8 FP32 octahedral texels per probe and SH9 stored as FP16.
+    Throughput is rays (probe + shadow) per second of the update's device time.
+    FP16 storage error: the FP32 texels rounded to FP16 against texels averaged in
+    FP64 from the same per-ray radiance."""
+    from tim_raytracing_b200 import scenes
+    t0 = time.perf_counter()
+    scene = scenes.scaled_heightfield(77, 1_000_000)
+    img = N.build_bvh(scene)
+    sid = ctx.upload(img, scene, quant8=True)
+    setup_s = time.perf_counter() - t0
+    res = (32, 32, 8)
+    side = 16
+    dirs = scenes.octahedral_dirs(side)
+    basis = scenes.sh9_basis(dirs)
+    lo, hi = img.aabb[:3], img.aabb[3:]
+    out = {"workload": "probe field 32x32x8, 256 rays per probe, heightfield+icospheres",
+           "triangles": int(scene.num_tris), "setup_s": round(setup_s, 2)}
+    total = res[0] * res[1] * res[2]
+    for form, flag in (("quantised_8wide", N.PROBE_WIDE), ("plain_binary", 0)):
+        desc = N.probe_desc(lo, hi, res, (-0.4, 0.3, -1.0), (1.0, 0.95, 0.9), len(dirs), 0.03,
+                            N.PROBE_OCTA | flag)
+        sh16 = np.zeros((7, res[2], res[1], res[0], 4), np.uint16)
+        ms, rays = [], 0
+        for k in range(reps + 2):
+            _, _, _, _, st = ctx.update_probes(sid, desc, dirs, basis, sh16)
+            if k >= 2:
+                ms.append(st.kernel_ms)
+                rays = st.rays
+        med = float(np.median(ms))
+        out[form] = {"value": rays / (med / 1e3) / 1e6, "update_ms": med, "rays_per_update": int(rays)}
+    # FP16 texel storage error against FP64 averaging of the same radiance
+    desc = N.probe_desc(lo, hi, res, (-0.4, 0.3, -1.0), (1.0, 0.95, 0.9), len(dirs), 0.03,
+                        N.PROBE_OCTA | N.PROBE_WIDE)
+    sh16 = np.zeros((7, res[2], res[1], res[0], 4), np.uint16)
+    _, irr, _, octa, _ = ctx.update_probes(sid, desc, dirs, basis, sh16, want_irr=True, want_octa=True)
+    step = side // 8
+    tex64 = irr.astype(np.float64).reshape(total, 8, step, 8, step, 3).mean(axis=(2, 4)).reshape(total, 64, 3)
+    tex16 = octa.astype(np.float16).astype(np.float64)
+    mag = np.maximum(np.abs(tex64), 1e-6)
+    rel16 = np.abs(tex16 - tex64) / mag
+    rel32 = np.abs(octa.astype(np.float64) - tex64) / mag
+    out["octa_texels"] = {"texels": int(tex64.size // 3), "fp16_max_rel_err": float(rel16.max()),
+                          "fp16_mean_rel_err": float(rel16.mean()), "fp32_max_rel_err": float(rel32.max()),
+                          "reference": "FP64 mean of the same per-ray FP32 radiance"}
+    ctx.free_scene(sid)
+    return out
 
 
 def bench_serving(N, ctx, dev, jobs_per_rate=1500):
@@ -359,6 +432,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched multi-scene workload")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving workload")
+    ap.add_argument("--no-probes", action="store_true", help="skip the light-probe field workload")
     ap.add_argument("--profile", choices=["plain", "wide"],
                     help="only trace two frames of one form through the host API and exit (a small, fixed "
                          "launch sequence for ncu: per frame one primary and one secondary k_persistent launch)")
@@ -449,17 +523,8 @@ def main():
     clocks = sampler.summary()
 
     # identical work per frame on every rank: aggregate rays, max time
-    def agg(ms, rays):
-        if dist:
-            t = torch.tensor([ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            r = torch.tensor([rays], dtype=torch.float64, device=dev)
-            dist.all_reduce(r)
-            return float(t.item()), float(r.item())
-        return ms, float(rays)
-
-    ms_w, rays_w = agg(*results["wide"])
-    ms_p, rays_p = agg(*results["plain"])
+    ms_w, rays_w = aggregate(*results["wide"], dist, dev)
+    ms_p, rays_p = aggregate(*results["plain"], dist, dev)
     v_w = rays_w / (ms_w / 1e3) / 1e6
     v_p = rays_p / (ms_p / 1e3) / 1e6
     rays_per_frame = rays_w / world / args.steps
@@ -495,13 +560,7 @@ def main():
     t0 = time.perf_counter()
     e2e_rays = sum(e2e_step() for _ in range(args.steps))
     e2e_s = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([e2e_s], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-        r = torch.tensor([float(e2e_rays)], dtype=torch.float64, device=dev)
-        dist.all_reduce(r)
-        e2e_rays = float(r.item())
+    e2e_s, e2e_rays = aggregate(e2e_s, e2e_rays, dist, dev)
     e2e_v = e2e_rays / e2e_s / 1e6
 
     # Dominant kernel (the secondary trace): its launch duration from CUDA events
@@ -533,6 +592,9 @@ def main():
         batched = bench_batched(N, ctx, dev, args.steps, args.warmup)
     if world == 1 and not args.no_serving:
         serving = bench_serving(N, ctx, dev)
+    probes = None
+    if world == 1 and not args.no_probes:
+        probes = bench_probes(N, ctx)
 
     if rank == 0:
         line = {
@@ -569,6 +631,8 @@ def main():
         line["kernels"] = kern
         if batched:
             line["batched"] = batched
+        if probes:
+            line["probes"] = probes
         if serving:
             line["serving"] = serving
             r8 = serving["rates"][1]

@@ -181,6 +181,20 @@ int tim_rt_trace(tim_rt_ctx *ctx, tim_rt_scene_id scene, const tim_rt_ray *rays,
 int tim_rt_trace_dev(tim_rt_ctx *ctx, tim_rt_scene_id scene, const tim_rt_ray *d_rays, uint32_t n, uint32_t mode,
                      uint32_t *d_hit, uint32_t *d_leaf_nid, float *d_bary, void *cuda_stream);
 
+/* Verification (not in the reference, and never on the trace path): re-runs the
+ * Moller-Trumbore test of each closest-hit record's triangle in FP64 and reports
+ * the largest |(t + 1e-5) - t_fp64| (absolute and relative to t_fp64) over the
+ * records with a hit, the records without one (t = ray tmax), and hits the FP64
+ * test does not confirm (u, v outside [-1e-6, 1 + 1e-6] or t <= 0: grazing hits
+ * accepted by the FP32 arithmetic). The only FP64 arithmetic on the GPU.
+ * d_hit: closest-hit records of d_rays (tim_rt_trace_dev layout). Synchronous. */
+typedef struct {
+    uint64_t hits_checked, misses, fp64_misses;
+    double max_abs_t_err, max_rel_t_err;
+} tim_rt_verify_result;
+int tim_rt_verify_hits(tim_rt_ctx *ctx, tim_rt_scene_id scene, const tim_rt_ray *d_rays, uint32_t n,
+                       const uint32_t *d_hit, tim_rt_verify_result *result);
+
 /* ---------------------------------------------------------------- batched multi-scene trace */
 /* Not in the reference, which dispatches one scene per compute pass. A batch is
  * a device-resident table of jobs, each a ray buffer traced against one resident

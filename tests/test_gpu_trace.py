@@ -99,6 +99,32 @@ def test_random_scene_mixed_rays(ctx, native, oracle_mod, n_tris, seed):
         ctx.free_scene(sid)
 
 
+def test_fp64_verification(ctx, native, oracle_mod):
+    """tim_rt_verify_hits re-intersects every reported closest hit in FP64: all
+    hits are counted, and the FP32 t of the reference arithmetic is close to FP64."""
+    import torch
+    from tim_raytracing_b200 import scenes
+    s = scenes.heightfield_scene(seed=6, grid=32, n_spheres=5)
+    img = native.build_bvh(s)
+    sid = ctx.upload(img, s, quant8=True)
+    try:
+        n = 50000
+        rays = scenes.random_rays(61, n, any_fraction=0.0)
+        rays[:, 0:3] = np.random.default_rng(62).uniform((0, 0, 0.5), (20, 20, 5), size=(n, 3))
+        d_rays = torch.from_numpy(rays).cuda()
+        d_hit = torch.empty((n, 4), dtype=torch.int32, device="cuda")
+        ctx.trace_dev(sid, d_rays, n, native.MODE_CLOSEST | native.TRACE_WIDE, d_hit)
+        torch.cuda.synchronize()
+        r = ctx.verify_hits(sid, d_rays, n, d_hit)
+        h = d_hit.cpu().numpy().view(np.uint32)
+        n_hit = int((h[:, 3].view(np.float32) != rays[:, 3]).sum())
+        assert r["hits_checked"] == n_hit and r["misses"] == n - n_hit and n_hit > 10000
+        assert r["fp64_misses"] <= n_hit * 1e-3
+        assert 0 < r["max_rel_t_err"] < 1e-3 and r["max_abs_t_err"] < 1e-2
+    finally:
+        ctx.free_scene(sid)
+
+
 def test_wide_near_ties_match_oracle(ctx, native, oracle_mod):
     """Scenes built to be mostly near-ties: the 8-wide walk must still return the
     binary walk's (the reference's order-dependent) answer on every ray."""

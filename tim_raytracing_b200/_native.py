@@ -32,7 +32,7 @@ EXPORTED = [
     "tim_rt_measure_l2_bandwidth", "tim_rt_update_probes", "tim_rt_batch_create", "tim_rt_batch_launch",
     "tim_rt_batch_info", "tim_rt_batch_destroy", "tim_rt_autotune_batch", "tim_rt_server_create",
     "tim_rt_server_submit", "tim_rt_server_wait", "tim_rt_server_drain", "tim_rt_server_stats_get",
-    "tim_rt_server_destroy",
+    "tim_rt_server_destroy", "tim_rt_verify_hits",
 ]
 SORT_NONE, SORT_OCTANT, SORT_MORTON = 0, 1, 2
 BATCH_WIDE = 0x100
@@ -113,6 +113,11 @@ class ServerStats(ctypes.Structure):
                 ("wall_s", ctypes.c_float)]
 
 
+class VerifyResult(ctypes.Structure):
+    _fields_ = [("hits_checked", ctypes.c_uint64), ("misses", ctypes.c_uint64), ("fp64_misses", ctypes.c_uint64),
+                ("max_abs_t_err", ctypes.c_double), ("max_rel_t_err", ctypes.c_double)]
+
+
 class TuneResult(ctypes.Structure):
     _fields_ = [("best", LaunchConfig), ("wide", ctypes.c_uint32), ("tried", ctypes.c_uint32),
                 ("best_ms", ctypes.c_float), ("start_ms", ctypes.c_float)]
@@ -175,6 +180,7 @@ def lib() -> ctypes.CDLL:
     L.tim_rt_server_drain.argtypes = [vp, u32]
     L.tim_rt_server_stats_get.argtypes = [vp, ctypes.POINTER(ServerStats), i32]
     L.tim_rt_server_destroy.argtypes = [vp]
+    L.tim_rt_verify_hits.argtypes = [vp, u32, vp, u32, vp, ctypes.POINTER(VerifyResult)]
     for name in EXPORTED:
         if name not in ("tim_rt_version", "tim_rt_last_error", "tim_rt_build_params_default", "tim_rt_bvh_blob_free"):
             getattr(L, name).restype = i32
@@ -308,6 +314,12 @@ class Context:
     def set_launch_config(self, block: int = 256, stack_depth: int = 0, refill_min: int = 16, ray_sort: int = 0):
         c = LaunchConfig(block, stack_depth, refill_min, ray_sort)
         _check(self._L.tim_rt_set_launch_config(self._c, ctypes.byref(c)))
+
+    def verify_hits(self, sid: int, d_rays, n: int, d_hit) -> dict:
+        """tim_rt_verify_hits: FP64 re-intersection of closest-hit records (device buffers)."""
+        r = VerifyResult()
+        _check(self._L.tim_rt_verify_hits(self._c, sid, _ptr(d_rays), n, _ptr(d_hit), ctypes.byref(r)))
+        return {name: getattr(r, name) for name, _ in VerifyResult._fields_}
 
     # -- batched multi-scene trace
     def batch_create(self, jobs, wide: bool = False):

@@ -169,7 +169,7 @@ int tim_rt_create(int device, uint64_t mem_budget_bytes, tim_rt_ctx** out) {
     for (auto& e : c->pev) TIMRT_CUDA(cudaEventCreate(&e));
     int rc = dev_alloc(c.get(), c->counters, 4ull * kCounterWords);
     if (rc) return rc;
-    if ((rc = dev_alloc(c.get(), c->dstats, 128))) return rc;
+    if ((rc = dev_alloc(c.get(), c->dstats, 256))) return rc;   // 16 counter words + 16 verification words
     TIMRT_CUDA(cudaMemset(c->counters.ptr, 0, 4ull * kCounterWords));
     *out = c.release();
     return TIM_RT_OK;

@@ -46,7 +46,7 @@ struct tim_rt_ctx {
     DevBuf counters;            // [0..63] per-call work counters, [64] device error word, ring after
     uint32_t ring = 0;
     DevBuf cam_out, cam_bounce, cam_nid, q_rays, q_pixel, tiles_counts, tiles_lists;
-    DevBuf dstats;              // 8 x u64 work counters of the counting kernels
+    DevBuf dstats;              // [0..15] u64 work counters of the counting kernels, [16..20] verification
     DevBuf p_dirs, p_basis, p_out, p_nid, p_irr, p_sh16, p_sh32, p_octa;   // light-probe update
     cudaEvent_t ev[4] = {};
     cudaEvent_t pev[4] = {};   // camera phases
