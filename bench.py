@@ -211,9 +211,7 @@ def bench_batched(N, ctx, dev, steps, warmup):
     (~0.7 GB of rays) exceed L2, so no flush between steps."""
     import torch
     from tim_raytracing_b200 import scenes
-    rng = np.random.default_rng(3)
-    tris = np.exp(rng.uniform(np.log(1e3), np.log(1e6), 64)).astype(np.int64)
-    nrays = np.exp(rng.uniform(np.log(4e3), np.log(2e6), 64)).astype(np.int64)
+    tris, nrays = batched_workload()
     t0 = time.perf_counter()
     sids, d_rays = [], []
     for k in range(64):
@@ -423,6 +421,40 @@ def profile_frames(form):
     return 0
 
 
+def batched_workload():
+    """Triangle and ray counts of the 64 scenes of the batched workload."""
+    rng = np.random.default_rng(3)
+    tris = np.exp(rng.uniform(np.log(1e3), np.log(1e6), 64)).astype(np.int64)
+    nrays = np.exp(rng.uniform(np.log(4e3), np.log(2e6), 64)).astype(np.int64)
+    return tris, nrays
+
+
+def profile_batched(wide, scenes_used=16):
+    """Two launches of one batch over the first scenes_used scenes of the batched
+    workload (same generators and seeds; a few hundred MB on the device)."""
+    import torch
+    from tim_raytracing_b200 import _native as N, scenes
+    tris, nrays = batched_workload()
+    ctx = N.Context(0)
+    dev = torch.device("cuda", 0)
+    sids, jobs = [], []
+    for k in range(scenes_used):
+        s = scenes.random_triangles(10_000 + k, int(tris[k]))
+        sids.append(ctx.upload(N.build_bvh(s), s, quant8=True))
+        r = torch.from_numpy(scenes.random_rays(20_000 + k, int(nrays[k]))).to(dev)
+        h = torch.empty((int(nrays[k]), 4), dtype=torch.int32, device=dev)
+        jobs.append((sids[k], N.MODE_PER_RAY, int(nrays[k]), r, h, None, None))
+    b = ctx.batch_create(jobs, wide=wide)
+    for _ in range(2):
+        ctx.batch_launch(b)
+    torch.cuda.synchronize()
+    print(json.dumps({"wide": wide, "scenes": scenes_used, "rays": int(nrays[:scenes_used].sum()),
+                      "triangles": int(tris[:scenes_used].sum())}))
+    ctx.batch_destroy(b)
+    ctx.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -433,12 +465,15 @@ def main():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched multi-scene workload")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving workload")
     ap.add_argument("--no-probes", action="store_true", help="skip the light-probe field workload")
-    ap.add_argument("--profile", choices=["plain", "wide"],
-                    help="only trace two frames of one form through the host API and exit (a small, fixed "
-                         "launch sequence for ncu: per frame one primary and one secondary k_persistent launch)")
+    ap.add_argument("--profile", choices=["plain", "wide", "batched-plain", "batched-wide"],
+                    help="only run a small, fixed launch sequence for ncu and exit: plain / wide = two frames of "
+                         "one form (per frame one primary and one secondary k_persistent launch); batched-* = two "
+                         "launches of one k_multi batch over the first 16 scenes of the batched workload")
     args = ap.parse_args()
-    if args.profile:
+    if args.profile in ("plain", "wide"):
         return profile_frames(args.profile)
+    if args.profile:
+        return profile_batched(args.profile == "batched-wide")
     args.warmup = max(args.warmup, 3)
 
     rank = int(os.environ.get("RANK", "0"))

@@ -38,6 +38,7 @@ struct TravState {
     float t0;           // the ray's tmax
     float t1;           // closest: the smallest hit t; any: t of the hit
     bool near2;         // closest: another hit t2 has RN(t2 - 1e-5) <= t1
+    uint32_t leaf;      // pending leaf slot of the current wide node (8 = none)
 };
 
 __device__ __forceinline__ void trav_init(TravState& st, uint32_t root) {

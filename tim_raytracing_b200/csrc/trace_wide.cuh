@@ -201,6 +201,7 @@ __device__ __forceinline__ void wide_init(const SceneView& s, TravState& st, uin
     st.c_node = st.c_leaf = st.c_tri = st.c_reload = 0u;
     st.t1 = __int_as_float(0x7F800000);   // +inf (st.t0 = tmax is set by the caller)
     st.near2 = false;
+    st.leaf = 8u;
     if (s.num_wnodes == 0u) {
         st.done = true;
         return;
@@ -215,54 +216,73 @@ __device__ __forceinline__ void wide_init(const SceneView& s, TravState& st, uin
     }
 }
 
-// One step: walk hit slots in rank order, descending into internal slots (the
-// rest of the current node is pushed as one (node << 8 | rank mask) entry),
-// until one leaf slot has been tested or the traversal ends.
+// One advance of one lane: take the next hit slot in rank order (popping a
+// pending node first when the current one is used up); an internal slot is
+// visited (the rest of the current node is pushed as one (node << 8 | rank
+// mask) entry), a leaf slot becomes the lane's pending leaf (st.leaf). At most
+// one node visit per call, so that lanes calling it together visit together.
 template <int BLOCK>
-__device__ __forceinline__ void wide_step(const SceneView& s, TravState& st, uint32_t* stk, uint32_t* err,
-                                          int sdepth) {
-    for (;;) {
-        if (st.order == 0u) {
-            if (st.sp == 0) {
+__device__ __forceinline__ void wide_advance(const SceneView& s, TravState& st, uint32_t* stk, uint32_t* err,
+                                             int sdepth) {
+    if (st.order == 0u) {
+        if (st.sp == 0) {
+            st.done = true;
+            return;
+        }
+        --st.sp;
+        const uint32_t e = stk[st.sp * BLOCK];
+        st.node = e >> 8;
+        st.order = e & 0xFFu;   // never 0: only non-empty remainders are pushed
+        st.first = 8u;
+        wide_read_hdr(s, st.node, st.h);
+        st.c_reload++;
+    }
+    uint32_t r;
+    if (st.first < 8u) {   // the nearest hit slot of a freshly visited node
+        r = st.first;
+        st.first = 8u;
+    } else {
+        r = (uint32_t)(__ffs(st.order) - 1);
+    }
+    st.order &= ~(1u << r);
+    const uint32_t slot = r ^ st.oct;
+    if ((st.h.imask >> slot) & 1u) {
+        const uint32_t child = st.h.child_base + __popc(st.h.imask & ((1u << slot) - 1u));
+        if (st.order != 0u) {
+            if (st.sp >= sdepth) {   // unreachable: the stack holds the 8-wide tree depth
+                atomicOr(err, 1u);
                 st.done = true;
                 return;
             }
-            --st.sp;
-            const uint32_t e = stk[st.sp * BLOCK];
-            st.node = e >> 8;
-            st.order = e & 0xFFu;
-            st.first = 8u;
-            wide_read_hdr(s, st.node, st.h);
-            st.c_reload++;
-            continue;
+            stk[st.sp * BLOCK] = (st.node << 8) | st.order;   // fewer than 2^24 nodes (checked at build)
+            ++st.sp;
         }
-        uint32_t r;
-        if (st.first < 8u) {   // the nearest hit slot of a freshly visited node
-            r = st.first;
-            st.first = 8u;
-        } else {
-            r = (uint32_t)(__ffs(st.order) - 1);
-        }
-        st.order &= ~(1u << r);
-        const uint32_t slot = r ^ st.oct;
-        if ((st.h.imask >> slot) & 1u) {
-            const uint32_t child = st.h.child_base + __popc(st.h.imask & ((1u << slot) - 1u));
-            if (st.order != 0u) {
-                if (st.sp >= sdepth) {   // unreachable: the stack holds the 8-wide tree depth
-                    atomicOr(err, 1u);
-                    st.done = true;
-                    return;
-                }
-                stk[st.sp * BLOCK] = (st.node << 8) | st.order;   // fewer than 2^24 nodes (checked at build)
-                ++st.sp;
-            }
-            st.node = child;
-            st.c_node++;
-            st.order = wide_visit(s, st, child, st.h, st.first);
-        } else {
-            wide_leaf<BLOCK>(s, st, st.h, slot);
-            return;
-        }
+        st.node = child;
+        st.c_node++;
+        st.order = wide_visit(s, st, child, st.h, st.first);
+    } else {
+        st.leaf = slot;
+    }
+}
+
+// One traversal step of the whole warp, called by all 32 lanes (`active`: the
+// lane has a ray): first every lane advances, one node visit per round and all
+// in the same rounds, until each has a pending leaf slot or has finished; then
+// the lanes test their pending leaves together. Without this the node test and
+// the triangle loop ran in many passes of a few lanes each, as lanes reached
+// them at different iterations of a per-lane loop.
+template <int BLOCK>
+__device__ __forceinline__ void wide_step_warp(const SceneView& s, TravState& st, bool active, uint32_t* stk,
+                                               uint32_t* err, int sdepth) {
+    for (;;) {
+        const bool need = active && !st.done && st.leaf >= 8u;
+        if (!__any_sync(0xFFFFFFFFu, need)) break;
+        if (need) wide_advance<BLOCK>(s, st, stk, err, sdepth);
+    }
+    if (active && st.leaf < 8u) {
+        const uint32_t slot = st.leaf;
+        st.leaf = 8u;
+        wide_leaf<BLOCK>(s, st, st.h, slot);
     }
 }
 
