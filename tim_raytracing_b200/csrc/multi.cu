@@ -145,8 +145,8 @@ __global__ void __launch_bounds__(BLOCK, WIDE ? 768 / BLOCK : 1) k_multi(const S
         }
         if (WIDE) {
             wide_step_warp<BLOCK>(sv, st, active, stk, err, sdepth);   // all lanes: warp-synchronous step
-        } else if (active) {
-            plain_step<BLOCK>(sv, st, stk, err, sdepth);
+        } else {
+            plain_step_warp<BLOCK>(sv, st, active, stk, err, sdepth);
         }
         if (active && st.done) {
             active = false;

@@ -239,8 +239,8 @@ __global__ void __launch_bounds__(BLOCK, WIDE ? 896 / BLOCK : 1) k_persistent(Sc
         }
         if (WIDE) {
             wide_step_warp<BLOCK>(s, st, active, stk, err, sdepth);   // all lanes: warp-synchronous step
-        } else if (active) {
-            plain_step<BLOCK>(s, st, stk, err, sdepth);
+        } else {
+            plain_step_warp<BLOCK>(s, st, active, stk, err, sdepth);
         }
         if (active && st.done) {
             active = false;

@@ -154,4 +154,68 @@ __device__ __forceinline__ void plain_step(const SceneView& s, TravState& st, ui
     st.node = stk[(--st.sp) * BLOCK];
 }
 
+// One advance of one lane from the inner node st.node: test its two child boxes
+// and move to the child the reference enters first (pushing the other when both
+// are hit), or pop the next pending subtree when neither is hit. At most one node
+// per call, so that lanes calling it together test their nodes together.
+template <int BLOCK>
+__device__ __forceinline__ void plain_advance(const SceneView& s, TravState& st, uint32_t* stk, uint32_t* err,
+                                              int sdepth) {
+    const uint32_t node = st.node;
+    const float4* np = s.nodes + 4u * node;
+    st.c_node++;
+    const uint4 nid = __ldg(reinterpret_cast<const uint4*>(np));
+    const float4 a = __ldg(np + 1);
+    const float4 b = __ldg(np + 2);
+    const float4 c = __ldg(np + 3);
+    const float d0 = collide_box(st.r, a.x, a.y, c.x, a.z, a.w, c.y, st.t);
+    const float d1 = collide_box(st.r, b.x, b.y, c.z, b.z, b.w, c.w, st.t);
+    const uint32_t packed = nid.z;
+    uint32_t c0 = packed & kNidMask;
+    uint32_t c1 = c0 + 1u;
+    c0 |= (packed & kNidLeftLeafBit) ? kNidLeafBit : 0u;
+    c1 |= (packed & kNidRightLeafBit) ? kNidLeafBit : 0u;
+    if (d0 < 0.0f && d1 < 0.0f) {
+        if (st.sp == 0) {
+            st.done = true;
+            return;
+        }
+        st.node = stk[(--st.sp) * BLOCK];
+        return;
+    }
+    if (d0 >= 0.0f && d1 >= 0.0f) {
+        const bool first1 = d1 < d0;
+        if (st.sp >= sdepth) {   // unreachable: the stack holds the tree depth
+            atomicOr(err, 1u);
+            st.done = true;
+            return;
+        }
+        stk[(st.sp++) * BLOCK] = first1 ? c0 : c1;
+        st.node = first1 ? c1 : c0;
+    } else {
+        st.node = (d0 >= 0.0f) ? c0 : c1;
+    }
+}
+
+// One traversal step of the whole warp, called by all 32 lanes (`active`: the
+// lane has a ray): node rounds in lockstep until every lane stands on a leaf or
+// has finished, then the leaves are tested together and each lane pops its next
+// pending subtree. Same per-ray visit order as plain_step.
+template <int BLOCK>
+__device__ __forceinline__ void plain_step_warp(const SceneView& s, TravState& st, bool active, uint32_t* stk,
+                                                uint32_t* err, int sdepth) {
+    for (;;) {
+        const bool need = active && !st.done && !(st.node & kNidLeafBit);
+        if (!__any_sync(0xFFFFFFFFu, need)) break;
+        if (need) plain_advance<BLOCK>(s, st, stk, err, sdepth);
+    }
+    if (active && !st.done) {
+        plain_leaf(s, st, st.node);
+        if (!st.done) {
+            if (st.sp == 0) st.done = true;
+            else st.node = stk[(--st.sp) * BLOCK];
+        }
+    }
+}
+
 }  // namespace timrt
