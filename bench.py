@@ -262,7 +262,7 @@ def bench_batched(N, ctx, dev, steps, warmup):
         ctx.batch_destroy(b)
         med = float(np.median(ms))
         out[form] = {"value": total / (sum(ms) / len(ms) / 1e3) / 1e6, "ms_per_launch_median": med,
-                     "autotuned": {k: tune[k] for k in ("block", "refill_min", "ray_sort", "stack_depth")},
+                     "autotuned": {k: tune[k] for k in ("block", "refill_min", "ray_sort", "stack_depth", "phase_switch")},
                      "autotune_ms": {"start": tune["start_ms"], "best": tune["best_ms"], "tried": tune["tried"]},
                      "separate_launches_ms": float(np.median(sep)),
                      "separate_launches_value": total / (float(np.median(sep)) / 1e3) / 1e6}

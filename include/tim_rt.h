@@ -130,6 +130,8 @@ typedef struct {
     uint32_t refill_min;   /* a warp fetches new rays once this many of its 32 lanes are idle (1..32);
                               camera primary rays always refill whole warps (one 8x4-pixel tile) */
     uint32_t ray_sort;     /* batched traces: TIM_RT_SORT_* coherence key the rays are reordered by */
+    uint32_t phase_switch; /* 0..31 (default 10): a warp stops its lockstep node rounds and tests the leaves
+                              its lanes hold once only this many lanes still need nodes */
 } tim_rt_launch_config;
 #define TIM_RT_SORT_NONE 0u     /* trace in input order */
 #define TIM_RT_SORT_OCTANT 1u   /* group each job's rays by direction octant (stable) */

@@ -177,20 +177,26 @@ def test_batch_near_ties_match_oracle(mctx, native, oracle_mod):
         d = [torch.from_numpy(r).cuda() for r in rays]
         hits = [torch.zeros((len(r), 4), dtype=torch.int32, device="cuda") for r in rays]
         nids = [torch.zeros(len(r), dtype=torch.int32, device="cuda") for r in rays]
+        hits_p = [torch.zeros((len(r), 4), dtype=torch.int32, device="cuda") for r in rays]
         b = mctx.batch_create([(sids[k], native.MODE_PER_RAY, len(rays[k]), d[k], hits[k], nids[k], None)
                                for k in range(2)], wide=True)
-        for refill in (16, 1):
-            mctx.set_launch_config(block=128, refill_min=refill)
+        bp = mctx.batch_create([(sids[k], native.MODE_PER_RAY, len(rays[k]), d[k], hits_p[k], None, None)
+                                for k in range(2)], wide=False)
+        for refill, sw in ((16, 10), (1, 0), (4, 31)):
+            mctx.set_launch_config(block=128, refill_min=refill, phase_switch=sw)
             mctx.batch_launch(b)
+            mctx.batch_launch(bp)
             torch.cuda.synchronize()
             for k, (s, img) in enumerate(((s1, imgs[0]), (s2, imgs[1]))):
                 oh, on, _, _ = oracle_mod.trace(oracle_mod.Scene(img, s.positions, s.normals), rays[k], 2)
-                assert np.array_equal(hits[k].cpu().numpy().view(np.uint32), oh), (k, refill)
-                assert np.array_equal(nids[k].cpu().numpy().view(np.uint32), on), (k, refill)
+                assert np.array_equal(hits[k].cpu().numpy().view(np.uint32), oh), (k, refill, sw)
+                assert np.array_equal(nids[k].cpu().numpy().view(np.uint32), on), (k, refill, sw)
+                assert np.array_equal(hits_p[k].cpu().numpy().view(np.uint32), oh), (k, refill, sw)
     finally:
         mctx.set_launch_config()
         if b is not None:
             mctx.batch_destroy(b)
+            mctx.batch_destroy(bp)
         for sid in sids:
             mctx.free_scene(sid)
 

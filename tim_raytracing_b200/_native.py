@@ -83,7 +83,7 @@ class Stats(ctypes.Structure):
 
 class LaunchConfig(ctypes.Structure):
     _fields_ = [("block", ctypes.c_uint32), ("stack_depth", ctypes.c_uint32), ("refill_min", ctypes.c_uint32),
-                ("ray_sort", ctypes.c_uint32)]
+                ("ray_sort", ctypes.c_uint32), ("phase_switch", ctypes.c_uint32)]
 
 
 class Job(ctypes.Structure):
@@ -309,10 +309,12 @@ class Context:
     def launch_config(self) -> dict:
         c = LaunchConfig()
         _check(self._L.tim_rt_get_launch_config(self._c, ctypes.byref(c)))
-        return {"block": c.block, "stack_depth": c.stack_depth, "refill_min": c.refill_min, "ray_sort": c.ray_sort}
+        return {"block": c.block, "stack_depth": c.stack_depth, "refill_min": c.refill_min, "ray_sort": c.ray_sort,
+                "phase_switch": c.phase_switch}
 
-    def set_launch_config(self, block: int = 256, stack_depth: int = 0, refill_min: int = 16, ray_sort: int = 0):
-        c = LaunchConfig(block, stack_depth, refill_min, ray_sort)
+    def set_launch_config(self, block: int = 256, stack_depth: int = 0, refill_min: int = 16, ray_sort: int = 0,
+                          phase_switch: int = 10):
+        c = LaunchConfig(block, stack_depth, refill_min, ray_sort, phase_switch)
         _check(self._L.tim_rt_set_launch_config(self._c, ctypes.byref(c)))
 
     def verify_hits(self, sid: int, d_rays, n: int, d_hit) -> dict:
@@ -348,7 +350,8 @@ class Context:
         r = TuneResult()
         _check(self._L.tim_rt_autotune_batch(self._c, batch, TUNE_WIDTH if width else 0, reps, ctypes.byref(r)))
         return {"block": r.best.block, "stack_depth": r.best.stack_depth, "refill_min": r.best.refill_min,
-                "ray_sort": r.best.ray_sort, "wide": bool(r.wide), "tried": r.tried, "best_ms": r.best_ms,
+                "ray_sort": r.best.ray_sort, "phase_switch": r.best.phase_switch, "wide": bool(r.wide),
+                "tried": r.tried, "best_ms": r.best_ms,
                 "start_ms": r.start_ms}
 
     def memory_used(self) -> int:

@@ -213,20 +213,22 @@ int tim_rt_get_launch_config(tim_rt_ctx* c, tim_rt_launch_config* cfg) {
     cfg->stack_depth = (uint32_t)c->cfg.stack_depth;
     cfg->refill_min = (uint32_t)c->cfg.refill_min;
     cfg->ray_sort = (uint32_t)c->cfg.ray_sort;
+    cfg->phase_switch = (uint32_t)c->cfg.phase_switch;
     return TIM_RT_OK;
 }
 
 int tim_rt_set_launch_config(tim_rt_ctx* c, const tim_rt_launch_config* cfg) {
     if (!c || !cfg || (cfg->block != 64 && cfg->block != 128 && cfg->block != 256) || cfg->stack_depth > 32 ||
-        cfg->refill_min < 1 || cfg->refill_min > 32 || cfg->ray_sort > TIM_RT_SORT_MORTON) {
+        cfg->refill_min < 1 || cfg->refill_min > 32 || cfg->ray_sort > TIM_RT_SORT_MORTON || cfg->phase_switch > 31) {
         set_error("tim_rt_set_launch_config: block must be 64/128/256, stack_depth <= 32, refill_min 1..32, "
-                  "ray_sort 0..2");
+                  "ray_sort 0..2, phase_switch 0..31");
         return TIM_RT_EINVAL;
     }
     c->cfg.block = (int)cfg->block;
     c->cfg.stack_depth = (int)cfg->stack_depth;
     c->cfg.refill_min = (int)cfg->refill_min;
     c->cfg.ray_sort = (int)cfg->ray_sort;
+    c->cfg.phase_switch = (int)cfg->phase_switch;
     return TIM_RT_OK;
 }
 
@@ -954,7 +956,7 @@ int tim_rt_autotune_batch(tim_rt_ctx* c, tim_rt_batch* b, uint32_t flags, uint32
             cand.block = blk;
             consider(cand, best_wide);
         }
-        for (int refill : {4, 8, 12, 16, 20, 24, 28, 32}) {
+        for (int refill : {1, 2, 4, 8, 12, 16, 20, 24, 28, 32}) {
             LaunchConfig cand = best;
             if (cand.refill_min == refill) continue;
             cand.refill_min = refill;
@@ -964,6 +966,12 @@ int tim_rt_autotune_batch(tim_rt_ctx* c, tim_rt_batch* b, uint32_t flags, uint32
             LaunchConfig cand = best;
             if (cand.ray_sort == srt) continue;
             cand.ray_sort = srt;
+            consider(cand, best_wide);
+        }
+        for (int sw : {0, 4, 8, 12, 16}) {
+            LaunchConfig cand = best;
+            if (cand.phase_switch == sw) continue;
+            cand.phase_switch = sw;
             consider(cand, best_wide);
         }
         for (int sd : {0, 32}) {
@@ -981,11 +989,13 @@ int tim_rt_autotune_batch(tim_rt_ctx* c, tim_rt_batch* b, uint32_t flags, uint32
     c->cfg.refill_min = best.refill_min;
     c->cfg.ray_sort = best.ray_sort;
     c->cfg.stack_depth = best.stack_depth;
+    c->cfg.phase_switch = best.phase_switch;
     b->wide = best_wide;
     res->best.block = (uint32_t)best.block;
     res->best.stack_depth = (uint32_t)best.stack_depth;
     res->best.refill_min = (uint32_t)best.refill_min;
     res->best.ray_sort = (uint32_t)best.ray_sort;
+    res->best.phase_switch = (uint32_t)best.phase_switch;
     res->wide = best_wide ? 1u : 0u;
     res->tried = tried;
     res->best_ms = best_ms;

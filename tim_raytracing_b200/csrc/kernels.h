@@ -13,6 +13,7 @@ struct LaunchConfig {
     int stack_depth = 0;  // traversal-stack entries per thread; 0 = the scene's tree depth
     int refill_min = 16;  // a warp fetches new rays once this many lanes are idle (1..32)
     int ray_sort = 0;     // batched traces: TIM_RT_SORT_* key
+    int phase_switch = 10;  // a warp's node rounds end once only this many lanes still need nodes (0..31)
     bool wide = false;  // 8-wide quantised BVH instead of the reference binary layout
     // when set, a counting variant of the kernel adds per-ray work to
     // stats[0..4] = (rays, node visits, leaf visits, triangle tests, node reloads)
@@ -20,6 +21,13 @@ struct LaunchConfig {
     // when set, the camera launcher records ev[0..3] around its three phases
     cudaEvent_t* phase_ev = nullptr;
 };
+
+// The kernels' packed knob word: refill threshold (1..32) | phase switch (0..31) << 8.
+inline int launch_knobs(const LaunchConfig& cfg) {
+    const int refill = cfg.refill_min < 1 ? 1 : (cfg.refill_min > 32 ? 32 : cfg.refill_min);
+    const int sw = cfg.phase_switch < 0 ? 0 : (cfg.phase_switch > 31 ? 31 : cfg.phase_switch);
+    return refill | (sw << 8);
+}
 
 cudaError_t launch_trace_batch(const SceneView& s, const tim_rt_ray* rays, uint32_t n, uint32_t mode, uint32_t* hit,
                                uint32_t* nid, float* bary, uint32_t* counter, uint32_t* err, cudaStream_t stream,

@@ -75,8 +75,11 @@ __global__ void k_sort_keys(const MultiJob* __restrict__ jobs, uint32_t njobs, u
 template <int BLOCK, bool WIDE>
 __global__ void __launch_bounds__(BLOCK, WIDE ? 768 / BLOCK : 1) k_multi(const SceneView* __restrict__ views, const MultiJob* __restrict__ jobs,
                                                  uint32_t njobs, uint32_t total, const uint32_t* __restrict__ perm,
-                                                 uint32_t* counter, uint32_t* err, int sdepth, int refill_min) {
+                                                 uint32_t* counter, uint32_t* err, int sdepth, int knobs) {
     extern __shared__ uint32_t stack_mem[];
+    // knobs: refill threshold (bits 0..7), phase-switch threshold (bits 8..15)
+    const int refill_min = knobs & 0xFF;
+    const uint32_t phase_sw = (uint32_t)(knobs >> 8) & 0xFFu;
     uint32_t* stk = stack_mem + threadIdx.x;
     const uint32_t lane = threadIdx.x & 31u;
     TravState st;
@@ -144,9 +147,9 @@ __global__ void __launch_bounds__(BLOCK, WIDE ? 768 / BLOCK : 1) k_multi(const S
             continue;
         }
         if (WIDE) {
-            wide_step_warp<BLOCK>(sv, st, active, stk, err, sdepth);   // all lanes: warp-synchronous step
+            wide_step_warp<BLOCK>(sv, st, active, stk, err, sdepth, phase_sw);   // all lanes: warp-synchronous step
         } else {
-            plain_step_warp<BLOCK>(sv, st, active, stk, err, sdepth);
+            plain_step_warp<BLOCK>(sv, st, active, stk, err, sdepth, phase_sw);
         }
         if (active && st.done) {
             active = false;
@@ -196,7 +199,7 @@ cudaError_t launch_multi(const SceneView* views, const MultiJob* jobs, uint32_t 
                          uint32_t* err, int depth, bool wide, const SortScratch* sort, cudaStream_t stream,
                          const LaunchConfig& cfg) {
     depth = depth < 1 ? 1 : (depth > kStackSize ? kStackSize : depth);
-    const int refill = cfg.refill_min < 1 ? 1 : (cfg.refill_min > 32 ? 32 : cfg.refill_min);
+    const int refill = launch_knobs(cfg);
     const uint32_t* perm = nullptr;
     if (cfg.ray_sort != TIM_RT_SORT_NONE) {
         if (!sort) return cudaErrorInvalidValue;

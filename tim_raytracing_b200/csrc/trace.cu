@@ -177,8 +177,11 @@ struct SecondaryPolicy {
 template <int BLOCK, bool WIDE, bool STATS, class Policy>
 __global__ void __launch_bounds__(BLOCK, WIDE ? 896 / BLOCK : 1) k_persistent(SceneView s, Policy P, uint32_t n_static,
                                                       const uint32_t* n_dev, uint32_t* counter, uint32_t* err,
-                                                      unsigned long long* stats, int sdepth, int refill_min) {
+                                                      unsigned long long* stats, int sdepth, int knobs) {
     extern __shared__ uint32_t stack_mem[];
+    // knobs: refill threshold (bits 0..7), phase-switch threshold (bits 8..15)
+    const int refill_min = knobs & 0xFF;
+    const uint32_t phase_sw = (uint32_t)(knobs >> 8) & 0xFFu;
     uint32_t* stk = stack_mem + threadIdx.x;
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t n = n_dev ? *n_dev : n_static;
@@ -238,9 +241,9 @@ __global__ void __launch_bounds__(BLOCK, WIDE ? 896 / BLOCK : 1) k_persistent(Sc
             continue;
         }
         if (WIDE) {
-            wide_step_warp<BLOCK>(s, st, active, stk, err, sdepth);   // all lanes: warp-synchronous step
+            wide_step_warp<BLOCK>(s, st, active, stk, err, sdepth, phase_sw);   // all lanes: warp-synchronous step
         } else {
-            plain_step_warp<BLOCK>(s, st, active, stk, err, sdepth);
+            plain_step_warp<BLOCK>(s, st, active, stk, err, sdepth, phase_sw);
         }
         if (active && st.done) {
             active = false;
@@ -571,7 +574,7 @@ static cudaError_t launch_persistent(const SceneView& s, const Policy& P, uint32
     int depth = WIDE ? (int)s.wide_depth : (int)s.depth;
     if (cfg.stack_depth > depth) depth = cfg.stack_depth;
     depth = depth < 1 ? 1 : (depth > kStackSize ? kStackSize : depth);
-    const int refill = cfg.refill_min < 1 ? 1 : (cfg.refill_min > 32 ? 32 : cfg.refill_min);
+    const int refill = launch_knobs(cfg);
     if (cfg.stats) {
         launch_block<128, WIDE, true>(s, P, n_static, n_dev, counter, err, cfg.stats, depth, refill, stream);
         return cudaGetLastError();

@@ -199,17 +199,21 @@ __device__ __forceinline__ void plain_advance(const SceneView& s, TravState& st,
 
 // One traversal step of the whole warp, called by all 32 lanes (`active`: the
 // lane has a ray): node rounds in lockstep until every lane stands on a leaf or
-// has finished, then the leaves are tested together and each lane pops its next
+// has finished, or until only `sw` lanes still need nodes while some lane stands
+// on a leaf; then the leaves are tested together and each lane pops its next
 // pending subtree. Same per-ray visit order as plain_step.
 template <int BLOCK>
 __device__ __forceinline__ void plain_step_warp(const SceneView& s, TravState& st, bool active, uint32_t* stk,
-                                                uint32_t* err, int sdepth) {
+                                                uint32_t* err, int sdepth, uint32_t sw) {
     for (;;) {
         const bool need = active && !st.done && !(st.node & kNidLeafBit);
-        if (!__any_sync(0xFFFFFFFFu, need)) break;
+        const uint32_t nm = __ballot_sync(0xFFFFFFFFu, need);
+        if (nm == 0u) break;
+        if ((uint32_t)__popc(nm) <= sw &&
+            __any_sync(0xFFFFFFFFu, active && !st.done && (st.node & kNidLeafBit))) break;
         if (need) plain_advance<BLOCK>(s, st, stk, err, sdepth);
     }
-    if (active && !st.done) {
+    if (active && !st.done && (st.node & kNidLeafBit)) {
         plain_leaf(s, st, st.node);
         if (!st.done) {
             if (st.sp == 0) st.done = true;

@@ -266,17 +266,21 @@ __device__ __forceinline__ void wide_advance(const SceneView& s, TravState& st, 
 }
 
 // One traversal step of the whole warp, called by all 32 lanes (`active`: the
-// lane has a ray): first every lane advances, one node visit per round and all
-// in the same rounds, until each has a pending leaf slot or has finished; then
+// lane has a ray): first the lanes advance, one node visit per round and all in
+// the same rounds, until each has a pending leaf slot or has finished -- or until
+// only `sw` lanes still need nodes while some lane holds a leaf (those few lanes
+// go on in the next step instead of making the warp run near-empty rounds); then
 // the lanes test their pending leaves together. Without this the node test and
 // the triangle loop ran in many passes of a few lanes each, as lanes reached
 // them at different iterations of a per-lane loop.
 template <int BLOCK>
 __device__ __forceinline__ void wide_step_warp(const SceneView& s, TravState& st, bool active, uint32_t* stk,
-                                               uint32_t* err, int sdepth) {
+                                               uint32_t* err, int sdepth, uint32_t sw) {
     for (;;) {
         const bool need = active && !st.done && st.leaf >= 8u;
-        if (!__any_sync(0xFFFFFFFFu, need)) break;
+        const uint32_t nm = __ballot_sync(0xFFFFFFFFu, need);
+        if (nm == 0u) break;
+        if ((uint32_t)__popc(nm) <= sw && __any_sync(0xFFFFFFFFu, active && st.leaf < 8u)) break;
         if (need) wide_advance<BLOCK>(s, st, stk, err, sdepth);
     }
     if (active && st.leaf < 8u) {
