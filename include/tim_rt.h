@@ -331,6 +331,8 @@ int tim_rt_server_destroy(tim_rt_server *srv);
 #define TIM_RT_CAM_BOUNCE 4u
 #define TIM_RT_CAM_WIDE 0x100u   /* use the quantised 8-wide BVH */
 #define TIM_RT_CAM_COUNT 0x200u  /* counting kernel variant; fills the work counters of tim_rt_stats */
+#define TIM_RT_CAM_PRIMARY_BINARY 0x400u /* with TIM_RT_CAM_WIDE: primary rays take the binary walk (faster for
+                                          coherent camera rays here; both walks give identical results) */
 int tim_rt_trace_camera(tim_rt_ctx *ctx, tim_rt_scene_id scene, const tim_rt_pass_data *pd, uint32_t flags,
                         uint32_t seed, const uint32_t *tile_counts, const uint32_t *tile_lists,
                         uint32_t *out, uint32_t *bounce_out, tim_rt_stats *stats);

@@ -54,7 +54,7 @@ def test_camera_room_matches_golden(ctx, native, room):
     assert st.primary_rays == 256 * 255
 
 
-@pytest.mark.parametrize("wide", [False, True])
+@pytest.mark.parametrize("wide", [0, 1, 2])
 def test_camera_heightfield_tile_lights_bounce(ctx, native, oracle_mod, wide):
     from tim_raytracing_b200 import scenes
     s = scenes.heightfield_scene(seed=9, grid=32, n_spheres=6, n_lights=16, light_radius=5.0)
@@ -70,7 +70,8 @@ def test_camera_heightfield_tile_lights_bounce(ctx, native, oracle_mod, wide):
         assert np.array_equal(counts, oc)
         assert np.array_equal(lists, ol)
         flags = native.CAM_TILE_LIGHTS | native.CAM_BOUNCE | native.CAM_PROB_MASK
-        out, bounce, st = ctx.trace_camera(sid, pd, flags=flags | (native.CAM_WIDE if wide else 0), seed=17,
+        form = [0, native.CAM_WIDE, native.CAM_WIDE | native.CAM_PRIMARY_BINARY][wide]
+        out, bounce, st = ctx.trace_camera(sid, pd, flags=flags | form, seed=17,
                                            tile_counts=counts, tile_lists=lists)
         o_out, o_bounce, o_counts = oracle_mod.camera(sc, pd, flags=flags, seed=17, tile_counts=oc, tile_lists=ol)
         assert np.array_equal(out, o_out)

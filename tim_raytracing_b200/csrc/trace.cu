@@ -616,8 +616,9 @@ cudaError_t launch_camera(const SceneView& s, const tim_rt_pass_data& pd, uint32
     // coherent rays; the secondary launch keeps the configured threshold)
     LaunchConfig pcfg = cfg;
     pcfg.refill_min = 32;
-    cudaError_t e = cfg.wide ? launch_persistent<true>(s, CP, items, nullptr, counters + 0, err, stream, pcfg)
-                             : launch_persistent<false>(s, CP, items, nullptr, counters + 0, err, stream, pcfg);
+    if (flags & TIM_RT_CAM_PRIMARY_BINARY) pcfg.wide = false;
+    cudaError_t e = pcfg.wide ? launch_persistent<true>(s, CP, items, nullptr, counters + 0, err, stream, pcfg)
+                              : launch_persistent<false>(s, CP, items, nullptr, counters + 0, err, stream, pcfg);
     if (e != cudaSuccess) return e;
     if (cfg.phase_ev) cudaEventRecord(cfg.phase_ev[1], stream);
     GenParams g;
