@@ -313,7 +313,8 @@ def bench_probes(N, ctx, reps=5):
     out = {"workload": "probe field 32x32x8, 256 rays per probe, heightfield+icospheres",
            "triangles": int(scene.num_tris), "setup_s": round(setup_s, 2)}
     total = res[0] * res[1] * res[2]
-    for form, flag in (("quantised_8wide", N.PROBE_WIDE), ("plain_binary", 0)):
+    # quantised form: 8-wide walk for the shadow rays, binary walk for the probe rays
+    for form, flag in (("quantised_8wide", N.PROBE_WIDE | N.PROBE_PRIMARY_BINARY), ("plain_binary", 0)):
         desc = N.probe_desc(lo, hi, res, (-0.4, 0.3, -1.0), (1.0, 0.95, 0.9), len(dirs), 0.03,
                             N.PROBE_OCTA | flag)
         sh16 = np.zeros((7, res[2], res[1], res[0], 4), np.uint16)
@@ -325,6 +326,8 @@ def bench_probes(N, ctx, reps=5):
                 rays = st.rays
         med = float(np.median(ms))
         out[form] = {"value": rays / (med / 1e3) / 1e6, "update_ms": med, "rays_per_update": int(rays)}
+        if flag:
+            out[form]["walks"] = "binary for the probe rays, 8-wide for their shadow rays"
     # FP16 texel storage error against FP64 averaging of the same radiance
     desc = N.probe_desc(lo, hi, res, (-0.4, 0.3, -1.0), (1.0, 0.95, 0.9), len(dirs), 0.03,
                         N.PROBE_OCTA | N.PROBE_WIDE)

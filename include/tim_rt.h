@@ -416,6 +416,8 @@ typedef struct {
 } tim_rt_probe_desc;
 #define TIM_RT_PROBE_OCTA 1u
 #define TIM_RT_PROBE_WIDE 0x100u
+#define TIM_RT_PROBE_PRIMARY_BINARY 0x400u /* with TIM_RT_PROBE_WIDE: the probe rays take the binary walk and
+                                            only their shadow rays the 8-wide one (identical results) */
 int tim_rt_update_probes(tim_rt_ctx *ctx, tim_rt_scene_id scene, const tim_rt_probe_desc *desc, const float *dirs,
                          const float *sh_basis, uint32_t probe_begin, uint32_t probe_end, uint32_t *trace_out,
                          float *irradiance, uint16_t *sh9_fp16, float *sh9_fp32, float *octa, tim_rt_stats *stats);

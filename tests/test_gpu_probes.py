@@ -34,7 +34,7 @@ def probe_coord(index, res):
     return x * 4 + inn % 4, y * 4 + (inn // 4) % 4, z * 4 + (inn // 16) % 4
 
 
-@pytest.mark.parametrize("wide", [False, True])
+@pytest.mark.parametrize("wide", [0, 1, 2])
 def test_probe_update_matches_oracle(ctx, native, oracle_mod, wide):
     from tim_raytracing_b200 import scenes
     O = oracle_mod
@@ -49,7 +49,7 @@ def test_probe_update_matches_oracle(ctx, native, oracle_mod, wide):
         lo, hi = img.aabb[:3], img.aabb[3:]
         sun = np.array([-0.4, 0.3, -1.0], np.float32)      # not normalised, as the reference passes it
         sunc = np.array([1.0, 0.95, 0.9], np.float32)
-        flags = native.PROBE_OCTA | (native.PROBE_WIDE if wide else 0)
+        flags = native.PROBE_OCTA | [0, native.PROBE_WIDE, native.PROBE_WIDE | native.PROBE_PRIMARY_BINARY][wide]
         desc = native.probe_desc(lo, hi, res, sun, sunc, len(dirs), 0.03, flags)
         rng = np.random.default_rng(5)
         sh16 = rng.uniform(-1, 1, size=(7, res[2], res[1], res[0], 4)).astype(np.float16).view(np.uint16).copy()

@@ -38,7 +38,7 @@ EXPORTED = [
 SORT_NONE, SORT_OCTANT, SORT_MORTON = 0, 1, 2
 BATCH_WIDE = 0x100
 TUNE_WIDTH = 1
-PROBE_OCTA, PROBE_WIDE = 1, 0x100
+PROBE_OCTA, PROBE_WIDE, PROBE_PRIMARY_BINARY = 1, 0x100, 0x400
 
 
 class ProbeDesc(ctypes.Structure):

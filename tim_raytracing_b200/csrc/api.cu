@@ -635,6 +635,7 @@ int tim_rt_update_probes(tim_rt_ctx* c, tim_rt_scene_id id, const tim_rt_probe_d
     TIMRT_CUDA(cudaMemsetAsync(ctr, 0, 4 * kCamCounterWords, c->stream));
     TIMRT_CUDA(cudaEventRecord(c->ev[1], c->stream));
     LaunchConfig cfg = cfg_for(c, s, (desc->flags & TIM_RT_PROBE_WIDE) != 0);
+    cfg.primary_binary = (desc->flags & TIM_RT_PROBE_PRIMARY_BINARY) != 0;
     cfg.phase_ev = c->pev;
     TIMRT_CUDA(launch_probes(s->view, d, static_cast<uint32_t*>(c->p_out.ptr), static_cast<uint32_t*>(c->p_nid.ptr),
                              static_cast<tim_rt_ray*>(c->q_rays.ptr), static_cast<uint32_t*>(c->q_pixel.ptr), ctr,

@@ -15,6 +15,7 @@ struct LaunchConfig {
     int ray_sort = 0;     // batched traces: TIM_RT_SORT_* key
     int phase_switch = 10;  // a warp's node rounds end once only this many lanes still need nodes (0..31)
     bool wide = false;  // 8-wide quantised BVH instead of the reference binary layout
+    bool primary_binary = false;   // probe updates with `wide`: the probe rays take the binary walk
     // when set, a counting variant of the kernel adds per-ray work to
     // stats[0..4] = (rays, node visits, leaf visits, triangle tests, node reloads)
     unsigned long long* stats = nullptr;

@@ -969,8 +969,9 @@ cudaError_t launch_probes(const SceneView& s, const ProbeArgs& d, uint32_t* out,
     uint32_t* prefix = counters + 2 + kNumKinds;
     ProbePolicy PP{d, reinterpret_cast<uint4*>(out), leaf_nid};
     if (cfg.phase_ev) cudaEventRecord(cfg.phase_ev[0], stream);
-    cudaError_t e = cfg.wide ? launch_persistent<true>(s, PP, n, nullptr, counters + 0, err, stream, cfg)
-                             : launch_persistent<false>(s, PP, n, nullptr, counters + 0, err, stream, cfg);
+    const bool probe_wide = cfg.wide && !cfg.primary_binary;
+    cudaError_t e = probe_wide ? launch_persistent<true>(s, PP, n, nullptr, counters + 0, err, stream, cfg)
+                               : launch_persistent<false>(s, PP, n, nullptr, counters + 0, err, stream, cfg);
     if (e != cudaSuccess) return e;
     if (cfg.phase_ev) cudaEventRecord(cfg.phase_ev[1], stream);
     GenParams g{};
