@@ -461,6 +461,26 @@ def profile_batched(wide, scenes_used=16):
     return 0
 
 
+def profile_probes(wide):
+    """Two updates of the probe-field workload in one walk (pure 8-wide or binary)."""
+    from tim_raytracing_b200 import _native as N, scenes
+    scene = scenes.scaled_heightfield(77, 1_000_000)
+    img = N.build_bvh(scene)
+    ctx = N.Context(0)
+    sid = ctx.upload(img, scene, quant8=True)
+    res = (32, 32, 8)
+    dirs = scenes.octahedral_dirs(16)
+    basis = scenes.sh9_basis(dirs)
+    desc = N.probe_desc(img.aabb[:3], img.aabb[3:], res, (-0.4, 0.3, -1.0), (1.0, 0.95, 0.9), len(dirs), 0.03,
+                        N.PROBE_OCTA | (N.PROBE_WIDE if wide else 0))
+    sh16 = np.zeros((7, res[2], res[1], res[0], 4), np.uint16)
+    for _ in range(2):
+        _, _, _, _, st = ctx.update_probes(sid, desc, dirs, basis, sh16)
+    print(json.dumps({"wide": wide, "probe_ms": st.primary_ms, "shadow_ms": st.secondary_ms, "rays": int(st.rays)}))
+    ctx.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -471,15 +491,20 @@ def main():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched multi-scene workload")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving workload")
     ap.add_argument("--no-probes", action="store_true", help="skip the light-probe field workload")
-    ap.add_argument("--profile", choices=["plain", "wide", "batched-plain", "batched-wide"],
+    ap.add_argument("--profile", choices=["plain", "wide", "batched-plain", "batched-wide", "probes-plain",
+                                          "probes-wide"],
                     help="only run a small, fixed launch sequence for ncu and exit: plain / wide = two frames of "
                          "one form (per frame one primary and one secondary k_persistent launch); batched-* = two "
-                         "launches of one k_multi batch over the first 16 scenes of the batched workload")
+                         "launches of one k_multi batch over the first 16 scenes of the batched workload; "
+                         "probes-* = two probe-field updates of one form (per update one probe-ray and one "
+                         "shadow-ray k_persistent launch)")
     args = ap.parse_args()
     if args.profile in ("plain", "wide"):
         return profile_frames(args.profile)
-    if args.profile:
+    if args.profile in ("batched-plain", "batched-wide"):
         return profile_batched(args.profile == "batched-wide")
+    if args.profile:
+        return profile_probes(args.profile == "probes-wide")
     args.warmup = max(args.warmup, 3)
 
     rank = int(os.environ.get("RANK", "0"))

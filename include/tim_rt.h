@@ -85,7 +85,6 @@ typedef struct { float o[3]; float tmax; float d[3]; uint32_t flags; } tim_rt_ra
 #define TIM_RT_MODE_ANY 1u       /* traverseBvhFast, bvhTraversal_inline.glsl:83-151 */
 #define TIM_RT_MODE_PER_RAY 2u   /* ray.flags bit 0 selects any-hit */
 #define TIM_RT_TRACE_WIDE 0x100u /* trace the 8-wide quantised BVH (needs TIM_RT_UPLOAD_QUANT8) */
-#define TIM_RT_TRACE_SORT 0x200u /* reorder rays by a coherence key before tracing (results keep input order) */
 #define TIM_RT_TRACE_COUNT 0x400u /* run the counting kernel variant and fill the work counters of tim_rt_stats */
 
 /* Upload flags. */

@@ -17,7 +17,6 @@ LIB_PATH = Path(__file__).resolve().parent / "libtim_rt.so"
 OK, EINVAL, ENOMEM, ETIMEOUT, EDEVICE, ENOTFOUND, EUNSUPPORTED = range(7)
 MODE_CLOSEST, MODE_ANY, MODE_PER_RAY = 0, 1, 2
 TRACE_WIDE = 0x100
-TRACE_SORT = 0x200
 TRACE_COUNT = 0x400
 UPLOAD_QUANT8 = 0x2
 CAM_PROB_MASK, CAM_TILE_LIGHTS, CAM_BOUNCE, CAM_WIDE, CAM_COUNT = 1, 2, 4, 0x100, 0x200

@@ -388,7 +388,7 @@ int tim_rt_trace_dev(tim_rt_ctx* c, tim_rt_scene_id id, const tim_rt_ray* d_rays
     if (rc) return rc;
     Scene* s = find_scene(c, id);
     if (!s) return TIM_RT_ENOTFOUND;
-    if ((mode & 0xFFu) > TIM_RT_MODE_PER_RAY || n > 0x7FFFFFFFu || (n && (!d_rays || !d_hit))) {
+    if ((mode & 0xFFu) > TIM_RT_MODE_PER_RAY || (mode & ~(0xFFu | TIM_RT_TRACE_WIDE | TIM_RT_TRACE_COUNT)) || n > 0x7FFFFFFFu || (n && (!d_rays || !d_hit))) {
         set_error("tim_rt_trace_dev: bad mode, size or null buffer");
         return TIM_RT_EINVAL;
     }
@@ -412,7 +412,7 @@ int tim_rt_trace(tim_rt_ctx* c, tim_rt_scene_id id, const tim_rt_ray* rays, uint
     if (rc) return rc;
     Scene* s = find_scene(c, id);
     if (!s) return TIM_RT_ENOTFOUND;
-    if ((mode & 0xFFu) > TIM_RT_MODE_PER_RAY || n > 0x7FFFFFFFu || (n && (!rays || !hit))) {
+    if ((mode & 0xFFu) > TIM_RT_MODE_PER_RAY || (mode & ~(0xFFu | TIM_RT_TRACE_WIDE | TIM_RT_TRACE_COUNT)) || n > 0x7FFFFFFFu || (n && (!rays || !hit))) {
         set_error("tim_rt_trace: bad mode, size or null buffer");
         return TIM_RT_EINVAL;
     }
