@@ -6,10 +6,11 @@
   sources by oracle/Makefile, single-threaded so node numbering is stable) run
   on the config-1 room scene (scenes.room_scene(1)): the fillGpuBuffer bytes,
   the seven ranges and the push constants. GPU tests trace this exact buffer.
-* room_golden.npz -- camera and random-ray results on that buffer from the
-  reference's GLSL traversal compiled as C++ (oracle/refglsl, when built) and
-  from the C restatement (oracle/reftrace.c); the tests check both against
-  each other and the CUDA kernels against them.
+* room_golden.npz -- camera, random-ray and light-probe results on that buffer
+  from the C restatement (oracle/reftrace.c) and, under the glsl_* keys, from the
+  reference's own compute shaders compiled as C++ (oracle/refglsl, built by
+  oracle/Makefile from the reference tree); the tests check the two against each
+  other and the CUDA kernels against them.
 """
 from __future__ import annotations
 
@@ -56,6 +57,19 @@ def main():
     cam, _, _ = O.camera(sc, pd, flags=1)
     out = dict(rays=rays, hit_closest=hit_c, nid_closest=nid_c, bary_closest=bary_c, hit_any=hit_a,
                pass_data=pd.view(np.uint8).reshape(-1), camera=cam)
+    # light-probe field of the room: 4x4x4 probes, 64 octahedral directions
+    res = (4, 4, 4)
+    total = res[0] * res[1] * res[2]
+    dirs = scenes.octahedral_dirs(8)
+    basis = scenes.sh9_basis(dirs)
+    sun = np.array([-0.4, 0.3, -1.0], np.float32)
+    sunc = np.array([1.0, 0.95, 0.9], np.float32)
+    od = O.probe_desc(img.aabb[:3], img.aabb[3:], res, sun, sunc, len(dirs), 0.03)
+    ptr, pirr, _ = O.probe_trace(sc, od, dirs, 0, total)
+    prev16 = np.random.default_rng(11).uniform(-1, 1, size=(7, res[2], res[1], res[0], 4)).astype(np.float16)
+    out.update(probe_res=np.array(res, np.uint32), probe_dirs=dirs, probe_basis=basis,
+               probe_sun=np.stack([sun, sunc]), probe_prev16=prev16.view(np.uint16),
+               probe_trace=ptr.reshape(-1, 8), probe_irradiance=pirr.reshape(-1, 3))
     try:
         from oracle import refglsl
         g = refglsl.available()
@@ -65,8 +79,12 @@ def main():
         gs = refglsl.Scene(img, s.positions, s.normals)
         gh, gn = refglsl.trace(gs, rays, 0)
         ga, _ = refglsl.trace(gs, rays, 1)
-        gcam = refglsl.camera(gs, pd, prob_mask=True)
-        out.update(glsl_hit_closest=gh, glsl_nid_closest=gn, glsl_hit_any=ga, glsl_camera=gcam)
+        gcam = refglsl.camera(gs, pd)
+        gptr = refglsl.probe_trace(gs, od, dirs)
+        girr = refglsl.probe_light(gs, od, dirs, gptr)
+        gimg = refglsl.probe_update(od, basis, girr, prev16.view(np.uint16))
+        out.update(glsl_hit_closest=gh, glsl_nid_closest=gn, glsl_hit_any=ga, glsl_camera=gcam,
+                   glsl_probe_trace=gptr, glsl_probe_irradiance=girr, glsl_probe_images16=gimg)
     np.savez_compressed(HERE / "room_golden.npz", **out)
     print("wrote", HERE / "room_refbvh.npz", HERE / "room_golden.npz", "glsl:", bool(g))
 

@@ -138,3 +138,46 @@ def near_tie_scene(seed, n):
             b.add(q.reshape(-1, 3), N[s0:s0 + per].reshape(-1, 3), np.arange(3 * len(q), dtype=np.uint32).reshape(-1, 3),
                   (0.7, 0.7, 0.7))
     return b.scene("near_ties", [], seed=seed)
+
+
+def sh16_to_prev27(sh16, res, probes):
+    """The previous SH9 (FP32, [probe][j][c]) as fetchSH9 reads it from the 7 images
+    (lightprob/fetchSH_inline.glsl:6-31)."""
+    rx, ry, rz = res
+    img = sh16.view(np.float16).astype(np.float32).reshape(7, rz, ry, rx, 4)
+    out = np.zeros((len(probes), 27), np.float32)
+    for n, p in enumerate(probes):
+        x, y, z = probe_coord(p, res)
+        out[n, 0:3] = img[0, z, y, x, 0:3]
+        for j in range(1, 9):
+            for ch in range(3):
+                image = 1 + 2 * ch if j <= 4 else 2 + 2 * ch
+                comp = j - 1 if j <= 4 else j - 5
+                out[n, 3 * j + ch] = img[image, z, y, x, comp]
+    return out
+
+
+def probe_coord(index, res):
+    """Probe index -> (x, y, z), lightprobHelpers.glsl getLightProbCoord (4x4x4 tiles)."""
+    trx, try_ = res[0] // 4, res[1] // 4
+    tile, inn = index // 64, index % 64
+    z = tile // (trx * try_)
+    tile = tile % (trx * try_)
+    y, x = tile // trx, tile % trx
+    return x * 4 + inn % 4, y * 4 + (inn // 4) % 4, z * 4 + (inn // 16) % 4
+
+
+def sh27_to_images16(sh27, res, probes, images16):
+    """Inverse of sh16_to_prev27: the 7 rgba16f images (u16 bits) after storeSH9
+    (lightprob/storeSH_inline.glsl:6-17) wrote each probe's FP32 SH9, rounded to
+    FP16 (w of image 0 is 0); other probes keep their texels."""
+    rx, ry, rz = res
+    img = np.array(images16, np.uint16).view(np.float16).reshape(7, rz, ry, rx, 4).copy()
+    for n, p in enumerate(probes):
+        x, y, z = probe_coord(p, res)
+        w = np.asarray(sh27[n], np.float32).reshape(9, 3)
+        img[0, z, y, x] = (w[0, 0], w[0, 1], w[0, 2], 0.0)
+        for ch in range(3):
+            img[1 + 2 * ch, z, y, x] = w[1:5, ch]
+            img[2 + 2 * ch, z, y, x] = w[5:9, ch]
+    return img.view(np.uint16).reshape(np.shape(images16))

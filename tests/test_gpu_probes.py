@@ -4,34 +4,9 @@ images) and octahedral texels are all computed in the oracle's operation order,
 so they must be bit-identical."""
 import numpy as np
 import pytest
+from helpers import probe_coord, sh16_to_prev27
 
 pytestmark = pytest.mark.gpu
-
-
-def sh16_to_prev27(sh16, res, probes):
-    """The previous SH9 (FP32, [probe][j][c]) as fetchSH9 reads it from the 7 images
-    (lightprob/fetchSH_inline.glsl:6-31)."""
-    rx, ry, rz = res
-    img = sh16.view(np.float16).astype(np.float32).reshape(7, rz, ry, rx, 4)
-    out = np.zeros((len(probes), 27), np.float32)
-    for n, p in enumerate(probes):
-        x, y, z = probe_coord(p, res)
-        out[n, 0:3] = img[0, z, y, x, 0:3]
-        for j in range(1, 9):
-            for ch in range(3):
-                image = 1 + 2 * ch if j <= 4 else 2 + 2 * ch
-                comp = j - 1 if j <= 4 else j - 5
-                out[n, 3 * j + ch] = img[image, z, y, x, comp]
-    return out
-
-
-def probe_coord(index, res):
-    trx, try_ = res[0] // 4, res[1] // 4
-    tile, inn = index // 64, index % 64
-    z = tile // (trx * try_)
-    tile = tile % (trx * try_)
-    y, x = tile // trx, tile % trx
-    return x * 4 + inn % 4, y * 4 + (inn // 4) % 4, z * 4 + (inn // 16) % 4
 
 
 @pytest.mark.parametrize("wide", [0, 1, 2])
