@@ -688,14 +688,14 @@ def main():
         line["roofline"] = {
             "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": traffic,
-            "kernel": "k_persistent<128, wide, SecondaryPolicy> (secondary trace of the frame)",
+            "kernel": "k_persistent<256, 1, 0, SecondaryPolicy> (8-wide secondary trace of the frame)",
             "algorithmic_bytes_per_launch": kw["algorithmic_bytes"], "launch_ms": kw["secondary_ms"],
             "bytes_per_ray": "80 per 8-wide node + 32 per node-header reload + 48 per triangle test (device counts)",
             "peak_source": peak_src, "l2_peak_gbs_measured": l2_gbs, "frac_of_l2": achieved / l2_gbs,
             "traffic_source": "profiles/secondary_trace_heightfield_1080p.md (ncu dram read + write, one launch)",
             "note": ("the 11 MB scene is L2-resident, so DRAM carries only the ray queue (traffic << algorithmic "
-                     "bytes); the kernel's actual limiter is instruction issue (ncu: ~79% issue-active, "
-                     "~11/32 active lanes), not HBM")}
+                     "bytes); the kernel's actual limiter is instruction issue (ncu: 75% issue-active, "
+                     "17/32 active lanes per instruction), not HBM")}
         line["kernels"] = kern
         if batched:
             line["batched"] = batched
