@@ -348,8 +348,10 @@ def bench_probes(N, ctx, reps=5):
 
 def bench_serving(N, ctx, dev, jobs_per_rate=1500):
     """Serving workload: 16 resident heightfield + icosphere scenes (log-U [10K, 2M]
-    tris), Poisson arrivals of jobs of log-U [1K, 1M] mixed primary / shadow /
-    probe-update rays, a 40 GB device arena. First the saturation throughput
+    tris), Poisson arrivals of jobs, a 40 GB device arena. A job is a ray batch of
+    log-U [1K, 1M] mixed primary / shadow / probe-direction rays, or, one job in
+    16, a probe-field update (tim_rt_server_submit_probes) of 64 probes x 256
+    directions of a 16x16x8 field on its scene. First the saturation throughput
     (jobs submitted back to back), then p50/p99 latency at 0.5x, 0.8x and 1.0x of
     the saturation job rate. Host buffers are pinned."""
     import torch
@@ -357,11 +359,18 @@ def bench_serving(N, ctx, dev, jobs_per_rate=1500):
     rng = np.random.default_rng(5)
     tris = np.exp(rng.uniform(np.log(1e4), np.log(2e6), 16)).astype(np.int64)
     t0 = time.perf_counter()
-    sids, ntris = [], 0
+    sids, ntris, descs = [], 0, []
     for k in range(16):
         s = scenes.scaled_heightfield(40 + k, int(tris[k]))
-        sids.append(ctx.upload(N.build_bvh(s), s, quant8=True))
+        img = N.build_bvh(s)
+        sids.append(ctx.upload(img, s, quant8=True))
         ntris += s.num_tris
+        descs.append(N.probe_desc(img.aabb[:3], img.aabb[3:], (16, 16, 8), (-0.4, 0.3, -1.0), (1.0, 0.95, 0.9), 256,
+                                  0.03, N.PROBE_WIDE | N.PROBE_PRIMARY_BINARY))
+    dirs = scenes.octahedral_dirs(16)
+    basis = scenes.sh9_basis(dirs)
+    fields = [torch.zeros((7, 8, 16, 16, 4), dtype=torch.int16).pin_memory() for _ in range(8)]
+    field_owner = [0] * len(fields)
     pool = []
     for e in range(64):
         n = int(np.exp(rng.uniform(np.log(1e3), np.log(1e6))))
@@ -378,20 +387,30 @@ def bench_serving(N, ctx, dev, jobs_per_rate=1500):
         srv.stats(reset=True)
         gaps = rg.exponential(1.0 / rate, n_jobs) if rate else np.zeros(n_jobs)
         t_next = time.perf_counter()
-        offered = 0
+        probe_jobs = 0
         for j in range(n_jobs):
             t_next += gaps[j]
             while time.perf_counter() < t_next:
                 pass
+            k = int(rg.integers(16))
+            if rg.uniform() < 1.0 / 16:
+                f = int(rg.integers(len(fields)))
+                if field_owner[f]:
+                    srv.wait(field_owner[f])
+                p0 = 64 * int(rg.integers(32))
+                field_owner[f] = srv.submit_probes(sids[k], descs[k], dirs, basis,
+                                                   fields[f].numpy().view(np.uint16), p0, p0 + 64)
+                probe_jobs += 1
+                continue
             e = int(rg.integers(len(pool)))
             if owner[e]:
                 srv.wait(owner[e])
             r, h = pool[e]
-            owner[e] = srv.submit(sids[int(rg.integers(16))], r, N.MODE_PER_RAY, h)
-            offered += r.shape[0]
+            owner[e] = srv.submit(sids[k], r, N.MODE_PER_RAY, h)
         srv.drain()
         st = srv.stats()
-        return {"jobs": n_jobs, "rate_jobs_per_s": rate, "value": st["rays_completed"] / st["wall_s"] / 1e6,
+        return {"jobs": n_jobs, "probe_update_jobs": probe_jobs, "rate_jobs_per_s": rate,
+                "value": st["rays_completed"] / st["wall_s"] / 1e6,
                 "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"], "max_ms": st["max_ms"],
                 "queue_p50_ms": st["queue_p50_ms"], "queue_p99_ms": st["queue_p99_ms"], "steps": st["steps"],
                 "arena_peak_gb": st["arena_peak_bytes"] / 1e9, "wall_s": st["wall_s"]}
@@ -403,8 +422,11 @@ def bench_serving(N, ctx, dev, jobs_per_rate=1500):
     srv.close()
     for sid in sids:
         ctx.free_scene(sid)
-    return {"workload": "16 heightfield+icosphere scenes (log-U 10K..2M tris), Poisson jobs of log-U 1K..1M mixed "
-                        "primary/shadow/probe rays, 40 GB arena, 8-wide BVHs",
+    return {"workload": "16 heightfield+icosphere scenes (log-U 10K..2M tris), Poisson jobs: log-U 1K..1M mixed "
+                        "primary/shadow/probe rays, or (1 in 16) a probe-field update of 64 probes x 256 rays, "
+                        "40 GB arena, 8-wide BVHs",
+            "note": "value counts traced rays: ray-batch rays plus the probe rays of probe updates (their shadow "
+                    "rays are traced but not counted)",
             "triangles": int(ntris), "setup_s": round(setup_s, 2), "saturation": sat,
             "saturation_jobs_per_s": sat_rate, "rates": rates}
 

@@ -305,6 +305,28 @@ typedef struct {
 int tim_rt_server_create(tim_rt_ctx *ctx, const tim_rt_server_params *params, tim_rt_server **out);
 /* Queues a request; never blocks on the GPU. *ticket identifies it. */
 int tim_rt_server_submit(tim_rt_server *srv, const tim_rt_request *req, uint64_t *ticket);
+/* A light-probe field update as a server request: the work and outputs of
+ * tim_rt_update_probes (declared below) on probes [probe_begin, probe_end) of a
+ * resident scene, with the same validation. sh9_fp16 (the whole field, host) is
+ * read when the request is admitted and rewritten when it completes; octa is
+ * optional (TIM_RT_PROBE_OCTA). Admission counts its whole device staging
+ * (directions, basis, the FP16 field, per-ray records, lit values, the shadow-ray
+ * queue and the optional texels) against the same arena as trace requests, in the
+ * same FIFO. Once admitted it runs as one probe-update launch sequence on the
+ * server's compute stream between batched trace steps; the outputs equal those
+ * of tim_rt_update_probes on the same inputs. */
+typedef struct tim_rt_probe_desc tim_rt_probe_desc;
+typedef struct {
+    tim_rt_scene_id scene;
+    uint32_t probe_begin, probe_end;
+    uint32_t reserved;
+    const tim_rt_probe_desc *desc;  /* copied at submit */
+    const float *dirs;              /* host, 4 floats per direction */
+    const float *sh_basis;          /* host, 9 floats per direction */
+    uint16_t *sh9_fp16;             /* host, in/out: [7][res_z][res_y][res_x][4] */
+    float *octa;                    /* host, optional: [probes][64][3] */
+} tim_rt_probe_request;
+int tim_rt_server_submit_probes(tim_rt_server *srv, const tim_rt_probe_request *req, uint64_t *ticket);
 /* Waits until the request completes (timeout_ms 0 = no limit): TIM_RT_OK, or
  * TIM_RT_ETIMEOUT with the request still pending. */
 int tim_rt_server_wait(tim_rt_server *srv, uint64_t ticket, uint32_t timeout_ms);
@@ -404,7 +426,7 @@ int tim_rt_cull_lights_dev(tim_rt_ctx *ctx, tim_rt_scene_id scene, const tim_rt_
  * Outputs of probes [probe_begin, probe_end) only; all optional except sh9_fp16.
  * trace_out: [probes][num_dirs][8] u32 tracingData; irradiance: [probes][num_dirs][3];
  * sh9_fp32: the new SH9 before FP16 rounding, [probes][9][3]. */
-typedef struct {
+struct tim_rt_probe_desc {
     float aabbMin[4]; float aabbMax[4];
     uint32_t resolution[4];
     float sunDir[4]; float sunColor[4];
@@ -412,7 +434,7 @@ typedef struct {
     uint32_t num_dirs;
     uint32_t flags;            /* TIM_RT_PROBE_* */
     uint32_t reserved;
-} tim_rt_probe_desc;
+};
 #define TIM_RT_PROBE_OCTA 1u
 #define TIM_RT_PROBE_WIDE 0x100u
 #define TIM_RT_PROBE_PRIMARY_BINARY 0x400u /* with TIM_RT_PROBE_WIDE: the probe rays take the binary walk and

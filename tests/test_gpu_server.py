@@ -113,3 +113,84 @@ def test_server_errors(ctx, native, served):
         assert srv.stats()["completed"] == 0
     finally:
         srv.close()
+
+
+def test_server_probe_updates_in_the_mix(ctx, native, served):
+    """Probe-field update requests (tim_rt_server_submit_probes) submitted while
+    trace requests stream in from other threads: each update's FP16 field and
+    octahedral texels equal tim_rt_update_probes on the same inputs, and the
+    trace requests still equal tracing alone."""
+    import torch
+    from tim_raytracing_b200 import scenes
+    sid = served[-1]
+    res = (8, 8, 4)
+    dirs = scenes.octahedral_dirs(8)
+    basis = scenes.sh9_basis(dirs)
+    lo, hi = np.zeros(3, np.float32), np.array([20, 20, 4], np.float32)
+    forms = [(0, 0, 64, False), (native.PROBE_WIDE | native.PROBE_PRIMARY_BINARY, 64, 192, True),
+             (native.PROBE_WIDE, 16, 48, True), (0, 200, 256, True)]
+    probes = []
+    rng = np.random.default_rng(4)
+    for k, (flag, p0, p1, octa) in enumerate(forms):
+        desc = native.probe_desc(lo, hi, res, (-0.4, 0.3, -1.0), (1.0, 0.95, 0.9), len(dirs), 0.03,
+                                 flag | (native.PROBE_OCTA if octa else 0))
+        sh = rng.uniform(-1, 1, size=(7, res[2], res[1], res[0], 4)).astype(np.float16).view(np.uint16)
+        want = sh.copy()
+        _, _, _, want_octa, _ = ctx.update_probes(sid, desc, dirs, basis, want, p0, p1, want_octa=octa)
+        t16, got = _pinned(sh.shape, torch.int16)
+        got = got.view(np.uint16)
+        got[:] = sh
+        to, go = _pinned((p1 - p0, 64, 3), torch.float32) if octa else (None, None)
+        probes.append(dict(desc=desc, p0=p0, p1=p1, want=want, want_octa=want_octa, got=got, octa=go,
+                           keep=(t16, to)))
+    reqs = _requests(served, 24, seed=29)
+    srv = native.Server(ctx, memory_budget_bytes=16 << 20, max_rays_per_step=16384, max_inflight_steps=2, wide=True)
+    try:
+        def submit(part):
+            for q in part:
+                q["ticket"] = srv.submit(q["sid"], q["rays"], q["mode"], q["hit"], q["nid"], q["bary"])
+
+        def submit_probes():
+            for P in probes:
+                P["ticket"] = srv.submit_probes(sid, P["desc"], dirs, basis, P["got"], P["p0"], P["p1"], P["octa"])
+
+        threads = [threading.Thread(target=submit, args=(reqs[k::2],)) for k in range(2)]
+        threads.append(threading.Thread(target=submit_probes))
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+        srv.drain(timeout_ms=120000)
+        st = srv.stats()
+        assert st["completed"] == st["submitted"] == len(reqs) + len(probes)
+        assert st["rays_completed"] == sum(len(q["rays"]) for q in reqs) + sum(
+            (P["p1"] - P["p0"]) * len(dirs) for P in probes)
+    finally:
+        srv.close()
+    for P in probes:
+        assert np.array_equal(P["got"], P["want"])
+        if P["octa"] is not None:
+            assert np.array_equal(P["octa"].view(np.uint32), P["want_octa"].view(np.uint32))
+    _check(ctx, native, reqs, True)
+
+
+def test_server_probe_request_errors(ctx, native, served):
+    from tim_raytracing_b200 import scenes
+    dirs = scenes.octahedral_dirs(8)
+    basis = scenes.sh9_basis(dirs)
+    sh = np.zeros((7, 4, 8, 8, 4), np.uint16)
+    srv = native.Server(ctx, memory_budget_bytes=1 << 20)
+    try:
+        bad_res = native.probe_desc((0, 0, 0), (1, 1, 1), (8, 8, 6), (0, 0, -1), (1, 1, 1), len(dirs), 0.03, 0)
+        with pytest.raises(native.TimRtError) as e:
+            srv.submit_probes(served[-1], bad_res, dirs, basis, sh, 0, 64)
+        assert e.value.code == native.EINVAL
+        desc = native.probe_desc((0, 0, 0), (1, 1, 1), (8, 8, 4), (0, 0, -1), (1, 1, 1), len(dirs), 0.03, 0)
+        with pytest.raises(native.TimRtError) as e:
+            srv.submit_probes(served[-1], desc, dirs, basis, sh, 0, 256)    # ~17 MB of staging
+        assert e.value.code == native.ENOMEM
+        with pytest.raises(native.TimRtError) as e:
+            srv.submit_probes(served[-1], desc, dirs, basis, sh, 10, 5)
+        assert e.value.code == native.EINVAL
+    finally:
+        srv.close()

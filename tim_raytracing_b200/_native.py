@@ -32,7 +32,7 @@ EXPORTED = [
     "tim_rt_measure_l2_bandwidth", "tim_rt_update_probes", "tim_rt_batch_create", "tim_rt_batch_launch",
     "tim_rt_batch_info", "tim_rt_batch_destroy", "tim_rt_autotune_batch", "tim_rt_server_create",
     "tim_rt_server_submit", "tim_rt_server_wait", "tim_rt_server_drain", "tim_rt_server_stats_get",
-    "tim_rt_server_destroy", "tim_rt_verify_hits",
+    "tim_rt_server_destroy", "tim_rt_verify_hits", "tim_rt_server_submit_probes",
 ]
 SORT_NONE, SORT_OCTANT, SORT_MORTON = 0, 1, 2
 BATCH_WIDE = 0x100
@@ -103,6 +103,12 @@ class Request(ctypes.Structure):
     _fields_ = [("scene", ctypes.c_uint32), ("mode", ctypes.c_uint32), ("n", ctypes.c_uint32),
                 ("reserved", ctypes.c_uint32), ("rays", ctypes.c_void_p), ("hit", ctypes.c_void_p),
                 ("leaf_nid", ctypes.c_void_p), ("bary", ctypes.c_void_p)]
+
+
+class ProbeRequest(ctypes.Structure):
+    _fields_ = [("scene", ctypes.c_uint32), ("probe_begin", ctypes.c_uint32), ("probe_end", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32), ("desc", ctypes.c_void_p), ("dirs", ctypes.c_void_p),
+                ("sh_basis", ctypes.c_void_p), ("sh9_fp16", ctypes.c_void_p), ("octa", ctypes.c_void_p)]
 
 
 class ServerStats(ctypes.Structure):
@@ -176,6 +182,7 @@ def lib() -> ctypes.CDLL:
     L.tim_rt_autotune_batch.argtypes = [vp, vp, u32, u32, ctypes.POINTER(TuneResult)]
     L.tim_rt_server_create.argtypes = [vp, ctypes.POINTER(ServerParams), ctypes.POINTER(vp)]
     L.tim_rt_server_submit.argtypes = [vp, ctypes.POINTER(Request), ctypes.POINTER(u64)]
+    L.tim_rt_server_submit_probes.argtypes = [vp, ctypes.POINTER(ProbeRequest), ctypes.POINTER(u64)]
     L.tim_rt_server_wait.argtypes = [vp, u64, u32]
     L.tim_rt_server_drain.argtypes = [vp, u32]
     L.tim_rt_server_stats_get.argtypes = [vp, ctypes.POINTER(ServerStats), i32]
@@ -470,6 +477,21 @@ class Server:
         t = ctypes.c_uint64()
         _check(self._L.tim_rt_server_submit(self._s, ctypes.byref(r), ctypes.byref(t)))
         self._keep[t.value] = (rays, hit, nid, bary)
+        return t.value
+
+    def submit_probes(self, sid: int, desc: "ProbeDesc", dirs, sh_basis, sh16, probe_begin: int, probe_end: int,
+                      octa=None) -> int:
+        """A probe-field update request (tim_rt_server_submit_probes): sh16 (uint16
+        [7][rz][ry][rx][4], host) is read at admission and rewritten on completion;
+        octa (float32 [probes][64][3]) is optional."""
+        dirs = np.ascontiguousarray(dirs, np.float32)
+        basis = np.ascontiguousarray(sh_basis, np.float32)
+        assert sh16.dtype == np.uint16 and sh16.flags.c_contiguous
+        r = ProbeRequest(sid, probe_begin, probe_end, 0, ctypes.cast(ctypes.byref(desc), ctypes.c_void_p), _ptr(dirs),
+                         _ptr(basis), _ptr(sh16), _ptr(octa))
+        t = ctypes.c_uint64()
+        _check(self._L.tim_rt_server_submit_probes(self._s, ctypes.byref(r), ctypes.byref(t)))
+        self._keep[t.value] = (desc, dirs, basis, sh16, octa)
         return t.value
 
     def wait(self, ticket: int, timeout_ms: int = 0):

@@ -126,6 +126,73 @@ LaunchConfig cfg_for(tim_rt_ctx* c, const Scene* s, bool wide, bool count = fals
     return cfg;
 }
 
+}  // namespace
+
+namespace timrt {
+
+int probe_plan(Scene* s, const tim_rt_probe_desc* desc, uint32_t probe_begin, uint32_t probe_end, const char* who,
+               ProbePlan* out) {
+    const std::string w(who);
+    if (!desc || desc->num_dirs == 0 || desc->num_dirs > 4096) {
+        set_error(w + ": null description or num_dirs outside 1..4096");
+        return TIM_RT_EINVAL;
+    }
+    const uint32_t* res = desc->resolution;
+    if (res[0] == 0 || res[1] == 0 || res[2] == 0 || res[0] % 4u || res[1] % 4u || res[2] % 4u) {
+        set_error(w + ": the probe resolution must be a positive multiple of 4 per axis "
+                      "(4x4x4 probe tiles, lightprobHelpers.glsl:16-61)");
+        return TIM_RT_EINVAL;
+    }
+    const uint64_t total = (uint64_t)res[0] * res[1] * res[2];
+    if (probe_begin >= probe_end || probe_end > total || total > (1u << 24)) {
+        set_error(w + ": bad probe range");
+        return TIM_RT_EINVAL;
+    }
+    const uint32_t nd = desc->num_dirs, np = probe_end - probe_begin;
+    const uint64_t n = (uint64_t)np * nd;
+    if (n * camera_queue_kinds() > 0xFFFFFFFFull) {
+        set_error(w + ": too many probe rays in one call");
+        return TIM_RT_EINVAL;
+    }
+    uint32_t side = 0;
+    if (desc->flags & TIM_RT_PROBE_OCTA) {
+        while ((uint64_t)side * side < nd) ++side;
+        if ((uint64_t)side * side != nd || side % 8u) {
+            set_error(w + ": OCTA needs num_dirs = side^2 with side a multiple of 8");
+            return TIM_RT_EINVAL;
+        }
+    }
+    if ((desc->flags & TIM_RT_PROBE_WIDE) && !s->has_wide) {
+        set_error(w + ": scene was uploaded without TIM_RT_UPLOAD_QUANT8");
+        return TIM_RT_EUNSUPPORTED;
+    }
+    if (!s->nrm.ptr) {
+        set_error(w + ": the lit value needs vertex normals (upload with nrm)");
+        return TIM_RT_EINVAL;
+    }
+    ProbeArgs d{};
+    for (int a = 0; a < 3; ++a) {
+        d.mn[a] = desc->aabbMin[a];
+        d.mx[a] = desc->aabbMax[a];
+        d.res[a] = res[a];
+        d.sun[a] = desc->sunDir[a];
+        d.sunc[a] = desc->sunColor[a];
+    }
+    d.hyst = desc->hysteresis;
+    d.nd = nd;
+    d.p0 = probe_begin;
+    d.np = np;
+    out->args = d;
+    out->side = side;
+    out->n = n;
+    out->total = total;
+    return TIM_RT_OK;
+}
+
+}  // namespace timrt
+
+namespace {
+
 // Copies the counting kernels' totals into the caller's stats (after a sync).
 void read_counts(tim_rt_ctx* c, tim_rt_stats* st) {
     unsigned long long v[16] = {};
@@ -568,43 +635,14 @@ int tim_rt_update_probes(tim_rt_ctx* c, tim_rt_scene_id id, const tim_rt_probe_d
     if (rc) return rc;
     Scene* s = find_scene(c, id);
     if (!s) return TIM_RT_ENOTFOUND;
-    if (!desc || !dirs || !sh_basis || !sh9_fp16 || desc->num_dirs == 0 || desc->num_dirs > 4096) {
-        set_error("tim_rt_update_probes: null argument or num_dirs outside 1..4096");
+    if (!dirs || !sh_basis || !sh9_fp16) {
+        set_error("tim_rt_update_probes: null argument");
         return TIM_RT_EINVAL;
     }
-    const uint32_t* res = desc->resolution;
-    if (res[0] == 0 || res[1] == 0 || res[2] == 0 || res[0] % 4u || res[1] % 4u || res[2] % 4u) {
-        set_error("tim_rt_update_probes: the probe resolution must be a positive multiple of 4 per axis "
-                  "(4x4x4 probe tiles, lightprobHelpers.glsl:16-61)");
-        return TIM_RT_EINVAL;
-    }
-    const uint64_t total = (uint64_t)res[0] * res[1] * res[2];
-    if (probe_begin >= probe_end || probe_end > total || total > (1u << 24)) {
-        set_error("tim_rt_update_probes: bad probe range");
-        return TIM_RT_EINVAL;
-    }
-    const uint32_t nd = desc->num_dirs, np = probe_end - probe_begin;
-    const uint64_t n = (uint64_t)np * nd;
-    if (n * camera_queue_kinds() > 0xFFFFFFFFull) {
-        set_error("tim_rt_update_probes: too many probe rays in one call");
-        return TIM_RT_EINVAL;
-    }
-    uint32_t side = 0;
-    if (desc->flags & TIM_RT_PROBE_OCTA) {
-        while ((uint64_t)side * side < nd) ++side;
-        if ((uint64_t)side * side != nd || side % 8u) {
-            set_error("tim_rt_update_probes: OCTA needs num_dirs = side^2 with side a multiple of 8");
-            return TIM_RT_EINVAL;
-        }
-    }
-    if ((desc->flags & TIM_RT_PROBE_WIDE) && !s->has_wide) {
-        set_error("tim_rt_update_probes: scene was uploaded without TIM_RT_UPLOAD_QUANT8");
-        return TIM_RT_EUNSUPPORTED;
-    }
-    if (!s->nrm.ptr) {
-        set_error("tim_rt_update_probes: the lit value needs vertex normals (upload with nrm)");
-        return TIM_RT_EINVAL;
-    }
+    ProbePlan P;
+    if ((rc = probe_plan(s, desc, probe_begin, probe_end, "tim_rt_update_probes", &P))) return rc;
+    const uint32_t nd = P.args.nd, np = P.args.np, side = P.side;
+    const uint64_t n = P.n, total = P.total;
     if ((rc = ensure(c, c->p_dirs, 16ull * nd)) || (rc = ensure(c, c->p_basis, 36ull * nd)) ||
         (rc = ensure(c, c->p_out, 32ull * n)) || (rc = ensure(c, c->p_nid, 4ull * n)) ||
         (rc = ensure(c, c->p_irr, 12ull * n)) || (rc = ensure(c, c->p_sh16, 56ull * total)) ||
@@ -613,18 +651,7 @@ int tim_rt_update_probes(tim_rt_ctx* c, tim_rt_scene_id id, const tim_rt_probe_d
         return rc;
     if (sh9_fp32 && (rc = ensure(c, c->p_sh32, 108ull * np))) return rc;
     if (octa && side && (rc = ensure(c, c->p_octa, 768ull * np))) return rc;
-    ProbeArgs d{};
-    for (int a = 0; a < 3; ++a) {
-        d.mn[a] = desc->aabbMin[a];
-        d.mx[a] = desc->aabbMax[a];
-        d.res[a] = res[a];
-        d.sun[a] = desc->sunDir[a];
-        d.sunc[a] = desc->sunColor[a];
-    }
-    d.hyst = desc->hysteresis;
-    d.nd = nd;
-    d.p0 = probe_begin;
-    d.np = np;
+    ProbeArgs d = P.args;
     d.dirs = static_cast<const float4*>(c->p_dirs.ptr);
     d.basis = static_cast<const float*>(c->p_basis.ptr);
     uint32_t* ctr = static_cast<uint32_t*>(c->counters.ptr);

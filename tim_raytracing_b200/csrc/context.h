@@ -84,4 +84,16 @@ Scene* find_scene(tim_rt_ctx* c, tim_rt_scene_id id);
 // Stops a server's worker and releases its device memory (context teardown).
 void server_shutdown(tim_rt_ctx* c, tim_rt_server* s);
 
+// A validated light-probe update: kernel arguments (without the device
+// direction / basis pointers), octahedral side (0 = no texels), rays and probes.
+struct ProbePlan {
+    ProbeArgs args{};
+    uint32_t side = 0;
+    uint64_t n = 0, total = 0;
+};
+// Checks a probe description and range against a scene (messages prefixed with
+// `who`); TIM_RT_OK and *out filled, or an error code with the message set.
+int probe_plan(Scene* s, const tim_rt_probe_desc* desc, uint32_t probe_begin, uint32_t probe_end, const char* who,
+               ProbePlan* out);
+
 }  // namespace timrt

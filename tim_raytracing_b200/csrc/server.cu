@@ -1,6 +1,7 @@
 // server.cu -- the serving loop of include/tim_rt.h (tim_rt_server_*): admission
-// of trace requests against a device arena, continuous batching of request
-// chunks into batched multi-scene launches (launch_multi), asynchronous result
+// of trace and probe-update requests against a device arena, continuous batching
+// of trace-request chunks into batched multi-scene launches (launch_multi),
+// probe updates (launch_probes) between those launches, asynchronous result
 // copies and latency statistics.
 //
 // Threads: callers submit and wait; one worker thread per server issues every
@@ -73,6 +74,7 @@ struct Req {
     tim_rt_request r{};
     Scene* scene = nullptr;
     uint64_t off = 0, bytes = 0;
+    uint64_t rays = 0;            // rays the request traces (probe updates: the probe rays)
     tim_rt_ray* d_rays = nullptr;
     uint4* d_hit = nullptr;
     uint32_t* d_nid = nullptr;
@@ -81,7 +83,44 @@ struct Req {
     bool first_chunk = true;      // the next step must wait for the upload
     Clock::time_point t_submit, t_admit;
     cudaEvent_t uploaded = nullptr;
+    // probe-field update requests
+    bool probe = false;
+    tim_rt_probe_request pr{};
+    tim_rt_probe_desc pdesc{};
+    ProbePlan plan;
+    cudaEvent_t ran = nullptr;
+    float4* d_dirs = nullptr;
+    float* d_basis = nullptr;
+    uint32_t* d_out = nullptr;
+    uint32_t* d_pnid = nullptr;
+    float* d_irr = nullptr;
+    uint16_t* d_sh16 = nullptr;
+    tim_rt_ray* d_qrays = nullptr;
+    uint32_t* d_qpix = nullptr;
+    uint32_t* d_ctr = nullptr;
+    float* d_octa = nullptr;
 };
+
+// Device staging of a probe-update request, in arena order (256-byte aligned parts).
+struct ProbeStaging {
+    uint64_t dirs, basis, out, nid, irr, sh16, qrays, qpix, ctr, octa;
+    uint64_t total() const { return dirs + basis + out + nid + irr + sh16 + qrays + qpix + ctr + octa; }
+};
+inline ProbeStaging probe_staging(const ProbePlan& P, bool octa) {
+    const uint64_t n = P.n, nd = P.args.nd, kinds = camera_queue_kinds();
+    ProbeStaging b;
+    b.dirs = round256(16 * nd);
+    b.basis = round256(36 * nd);
+    b.out = round256(32 * n);
+    b.nid = round256(4 * n);
+    b.irr = round256(12 * n);
+    b.sh16 = round256(56 * P.total);
+    b.qrays = round256(32 * n * kinds);
+    b.qpix = round256(4 * n * kinds);
+    b.ctr = round256(4ull * kCamCounterWords);
+    b.octa = (octa && P.side) ? round256(768ull * P.args.np) : 0;
+    return b;
+}
 
 struct Slot {
     DevBuf dev;                   // SceneView[max_jobs], MultiJob[max_jobs], counter
@@ -149,7 +188,7 @@ void CUDART_CB on_requests_done(void* p) {
             s->lat_ms.push_back(std::chrono::duration<float, std::milli>(now - r->t_submit).count());
             s->queue_ms.push_back(std::chrono::duration<float, std::milli>(r->t_admit - r->t_submit).count());
             s->completed++;
-            s->rays_completed += r->r.n;
+            s->rays_completed += r->rays;
             s->pending.erase(r->ticket);
             s->finished.push_back(r);
         }
@@ -271,6 +310,71 @@ int issue_step(tim_rt_server* s, Plan& P) {
     return TIM_RT_OK;
 }
 
+// Uploads nothing: the request's inputs went up on the upload stream at
+// admission. Runs the probe update on the compute stream, then copies the FP16
+// field (and the texels) back and completes the request.
+int issue_probe(tim_rt_server* s, Req* r) {
+    ProbeArgs d = r->plan.args;
+    d.dirs = r->d_dirs;
+    d.basis = r->d_basis;
+    LaunchConfig cfg = s->ctx->cfg;
+    cfg.stats = nullptr;
+    cfg.phase_ev = nullptr;
+    cfg.wide = (r->pdesc.flags & TIM_RT_PROBE_WIDE) != 0 && r->scene->has_wide;
+    cfg.primary_binary = (r->pdesc.flags & TIM_RT_PROBE_PRIMARY_BINARY) != 0;
+    uint32_t* err = static_cast<uint32_t*>(s->ctx->counters.ptr) + kErrWord;
+    if (cudaStreamWaitEvent(s->comp, r->uploaded, 0) ||
+        cudaMemsetAsync(r->d_ctr, 0, 4ull * kCamCounterWords, s->comp) ||
+        launch_probes(r->scene->view, d, r->d_out, r->d_pnid, r->d_qrays, r->d_qpix, r->d_ctr, err, r->d_irr,
+                      r->d_sh16, nullptr, r->d_octa, r->d_octa ? r->plan.side : 0, s->comp, cfg) != cudaSuccess ||
+        cudaEventCreateWithFlags(&r->ran, cudaEventDisableTiming) || cudaEventRecord(r->ran, s->comp) ||
+        cudaStreamWaitEvent(s->down, r->ran, 0) ||
+        cudaMemcpyAsync(r->pr.sh9_fp16, r->d_sh16, 56ull * r->plan.total, cudaMemcpyDeviceToHost, s->down) ||
+        (r->d_octa && cudaMemcpyAsync(r->pr.octa, r->d_octa, 768ull * r->plan.args.np, cudaMemcpyDeviceToHost, s->down)))
+        return TIM_RT_EDEVICE;
+    if (cudaLaunchHostFunc(s->down, on_requests_done, new DoneMsg{s, {r}}) != cudaSuccess) return TIM_RT_EDEVICE;
+    return TIM_RT_OK;
+}
+
+// Points a probe request's staging into its arena block and queues its uploads.
+int stage_probe(tim_rt_server* s, Req* r, uint8_t* p) {
+    const ProbeStaging b = probe_staging(r->plan, r->pr.octa != nullptr);
+    r->d_dirs = reinterpret_cast<float4*>(p);
+    p += b.dirs;
+    r->d_basis = reinterpret_cast<float*>(p);
+    p += b.basis;
+    r->d_out = reinterpret_cast<uint32_t*>(p);
+    p += b.out;
+    r->d_pnid = reinterpret_cast<uint32_t*>(p);
+    p += b.nid;
+    r->d_irr = reinterpret_cast<float*>(p);
+    p += b.irr;
+    r->d_sh16 = reinterpret_cast<uint16_t*>(p);
+    p += b.sh16;
+    r->d_qrays = reinterpret_cast<tim_rt_ray*>(p);
+    p += b.qrays;
+    r->d_qpix = reinterpret_cast<uint32_t*>(p);
+    p += b.qpix;
+    r->d_ctr = reinterpret_cast<uint32_t*>(p);
+    p += b.ctr;
+    r->d_octa = b.octa ? reinterpret_cast<float*>(p) : nullptr;
+    const uint64_t nd = r->plan.args.nd;
+    if (cudaEventCreateWithFlags(&r->uploaded, cudaEventDisableTiming) ||
+        cudaMemcpyAsync(r->d_dirs, r->pr.dirs, 16 * nd, cudaMemcpyHostToDevice, s->up) ||
+        cudaMemcpyAsync(r->d_basis, r->pr.sh_basis, 36 * nd, cudaMemcpyHostToDevice, s->up) ||
+        cudaMemcpyAsync(r->d_sh16, r->pr.sh9_fp16, 56ull * r->plan.total, cudaMemcpyHostToDevice, s->up) ||
+        cudaEventRecord(r->uploaded, s->up))
+        return TIM_RT_EDEVICE;
+    return TIM_RT_OK;
+}
+
+void release_req(Req* r) {
+    r->scene->batch_refs--;
+    if (r->uploaded) cudaEventDestroy(r->uploaded);
+    if (r->ran) cudaEventDestroy(r->ran);
+    delete r;
+}
+
 void worker_main(tim_rt_server* s) {
     cudaSetDevice(s->ctx->device);
     for (;;) {
@@ -303,7 +407,7 @@ void worker_main(tim_rt_server* s) {
                     r->t_admit = Clock::now();
                     s->waiting.pop_front();
                     admitted.push_back(r);
-                    s->active.push_back(r);
+                    if (!r->probe) s->active.push_back(r);
                 }
                 if (!s->active.empty() && !s->free_slots.empty()) {
                     P.slot = s->free_slots.back();
@@ -313,14 +417,14 @@ void worker_main(tim_rt_server* s) {
                 }
             }
         }
-        for (Req* r : release) {
-            r->scene->batch_refs--;
-            if (r->uploaded) cudaEventDestroy(r->uploaded);
-            delete r;
-        }
+        for (Req* r : release) release_req(r);
         int rc = TIM_RT_OK;
         uint8_t* base = static_cast<uint8_t*>(s->arena_buf.ptr);
         for (Req* r : admitted) {
+            if (r->probe) {
+                if (stage_probe(s, r, base + r->off) != TIM_RT_OK) rc = TIM_RT_EDEVICE;
+                continue;
+            }
             const uint64_t n = r->r.n;
             uint8_t* p = base + r->off;
             r->d_rays = reinterpret_cast<tim_rt_ray*>(p);
@@ -337,6 +441,9 @@ void worker_main(tim_rt_server* s) {
                 cudaEventRecord(r->uploaded, s->up))
                 rc = TIM_RT_EDEVICE;
         }
+        // admitted probe updates run on the compute stream ahead of the next trace step
+        for (Req* r : admitted)
+            if (r->probe && rc == TIM_RT_OK) rc = issue_probe(s, r);
         if (P.slot >= 0 && rc == TIM_RT_OK) {
             // requests whose last rays this step traces leave the active list
             for (auto& ch : P.chunks)
@@ -364,11 +471,7 @@ int server_teardown(tim_rt_server* s) {
     // requests left behind (only after a device error or a failed create)
     std::set<Req*> left(s->finished.begin(), s->finished.end());
     for (auto& kv : s->pending) left.insert(kv.second);
-    for (Req* r : left) {
-        r->scene->batch_refs--;
-        if (r->uploaded) cudaEventDestroy(r->uploaded);
-        delete r;
-    }
+    for (Req* r : left) release_req(r);
     s->finished.clear();
     s->pending.clear();
     s->waiting.clear();
@@ -483,6 +586,57 @@ int tim_rt_server_submit(tim_rt_server* s, const tim_rt_request* req, uint64_t* 
     Req* r = new Req;
     r->ticket = s->next_ticket++;
     r->r = *req;
+    r->rays = req->n;
+    r->scene = sc;
+    r->bytes = bytes;
+    r->t_submit = Clock::now();
+    sc->batch_refs++;
+    if (!s->t0_set) {
+        s->t0 = r->t_submit;
+        s->t0_set = true;
+    }
+    s->submitted++;
+    s->pending[r->ticket] = r;
+    s->waiting.push_back(r);
+    *ticket = r->ticket;
+    lk.unlock();
+    s->cv.notify_all();
+    return TIM_RT_OK;
+}
+
+int tim_rt_server_submit_probes(tim_rt_server* s, const tim_rt_probe_request* req, uint64_t* ticket) {
+    if (!s || !req || !ticket || !req->desc || !req->dirs || !req->sh_basis || !req->sh9_fp16) {
+        set_error("tim_rt_server_submit_probes: null argument");
+        return TIM_RT_EINVAL;
+    }
+    std::unique_lock<std::mutex> lk(s->m);
+    if (s->error) {
+        set_error(s->error_msg);
+        return s->error;
+    }
+    if (s->stop) {
+        set_error("tim_rt_server_submit_probes: server is stopping");
+        return TIM_RT_EINVAL;
+    }
+    Scene* sc = find_scene(s->ctx, req->scene);
+    if (!sc) return TIM_RT_ENOTFOUND;
+    ProbePlan plan;
+    int rc = probe_plan(sc, req->desc, req->probe_begin, req->probe_end, "tim_rt_server_submit_probes", &plan);
+    if (rc) return rc;
+    const uint64_t bytes = probe_staging(plan, req->octa != nullptr).total();
+    if (bytes > s->p.memory_budget_bytes) {
+        set_error("tim_rt_server_submit_probes: request needs " + std::to_string(bytes) + " B, the arena holds " +
+                  std::to_string(s->p.memory_budget_bytes));
+        return TIM_RT_ENOMEM;
+    }
+    Req* r = new Req;
+    r->ticket = s->next_ticket++;
+    r->probe = true;
+    r->pr = *req;
+    r->pdesc = *req->desc;
+    r->pr.desc = &r->pdesc;
+    r->plan = plan;
+    r->rays = plan.n;
     r->scene = sc;
     r->bytes = bytes;
     r->t_submit = Clock::now();
