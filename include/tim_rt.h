@@ -468,6 +468,27 @@ int tim_rt_bvh_blob_info(const tim_rt_bvh_blob *blob, const uint8_t **bytes, uin
                          uint32_t ranges[7][2], tim_rt_push_constants *pc, float aabb[6]);
 void tim_rt_bvh_blob_free(tim_rt_bvh_blob *blob);
 
+/* ---------------------------------------------------------------- on-disk BVH file */
+/* Not in the reference (BVHData::build rebuilds every run, BVHData.cpp:28-49, and
+ * its threaded builder is not deterministic, BVHBuilder.cpp:851-894). A versioned
+ * file holding a fillGpuBuffer image (bytes, seven ranges, push constants, bounds)
+ * and the BVHGeometry vertex arrays (positions; normals and uvs when given), with
+ * an FNV-1a 64 checksum. Writing validates the BVH first and replaces the file
+ * atomically; reading checks magic, version, sizes, checksum and the BVH, and
+ * returns TIM_RT_EINVAL (corrupt) or TIM_RT_EUNSUPPORTED (other version). */
+typedef struct tim_rt_bvh_file tim_rt_bvh_file;
+int tim_rt_bvh_file_write(const char *path, const void *bvh_bytes, uint64_t n_bytes, const uint32_t ranges[7][2],
+                          const tim_rt_push_constants *pc, const float aabb[6], const float *pos, const float *nrm,
+                          const float *uv, uint32_t max_vertex, uint32_t num_vertex);
+int tim_rt_bvh_file_read(const char *path, tim_rt_bvh_file **out);
+/* Pointers stay valid until tim_rt_bvh_file_free; nrm / uv are NULL when absent. */
+int tim_rt_bvh_file_info(const tim_rt_bvh_file *file, const uint8_t **bytes, uint64_t *size, uint32_t ranges[7][2],
+                         tim_rt_push_constants *pc, float aabb[6], const float **pos, const float **nrm,
+                         const float **uv, uint32_t *max_vertex, uint32_t *num_vertex);
+void tim_rt_bvh_file_free(tim_rt_bvh_file *file);
+/* tim_rt_bvh_file_read followed by tim_rt_upload_bvh with `flags`. */
+int tim_rt_upload_bvh_file(tim_rt_ctx *ctx, const char *path, uint32_t flags, tim_rt_scene_id *out);
+
 #ifdef __cplusplus
 }
 #endif

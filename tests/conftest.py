@@ -38,3 +38,16 @@ def ctx(native):
     c = native.Context(0)
     yield c
     c.close()
+
+
+@pytest.fixture
+def tmp_path(request):
+    """Scratch folder inside the repository (tests/_tmp/<test>, git-ignored),
+    replacing pytest's system-wide temporary directory."""
+    import re
+    import shutil
+    d = ROOT / "tests" / "_tmp" / re.sub(r"[^\w.-]", "_", request.node.name)
+    if d.exists():
+        shutil.rmtree(d)
+    d.mkdir(parents=True)
+    return d

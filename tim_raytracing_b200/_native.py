@@ -32,7 +32,8 @@ EXPORTED = [
     "tim_rt_measure_l2_bandwidth", "tim_rt_update_probes", "tim_rt_batch_create", "tim_rt_batch_launch",
     "tim_rt_batch_info", "tim_rt_batch_destroy", "tim_rt_autotune_batch", "tim_rt_server_create",
     "tim_rt_server_submit", "tim_rt_server_wait", "tim_rt_server_drain", "tim_rt_server_stats_get",
-    "tim_rt_server_destroy", "tim_rt_verify_hits", "tim_rt_server_submit_probes",
+    "tim_rt_server_destroy", "tim_rt_verify_hits", "tim_rt_server_submit_probes", "tim_rt_bvh_file_write",
+    "tim_rt_bvh_file_read", "tim_rt_bvh_file_info", "tim_rt_bvh_file_free", "tim_rt_upload_bvh_file",
 ]
 SORT_NONE, SORT_OCTANT, SORT_MORTON = 0, 1, 2
 BATCH_WIDE = 0x100
@@ -188,8 +189,18 @@ def lib() -> ctypes.CDLL:
     L.tim_rt_server_stats_get.argtypes = [vp, ctypes.POINTER(ServerStats), i32]
     L.tim_rt_server_destroy.argtypes = [vp]
     L.tim_rt_verify_hits.argtypes = [vp, u32, vp, u32, vp, ctypes.POINTER(VerifyResult)]
+    L.tim_rt_bvh_file_write.argtypes = [ctypes.c_char_p, vp, u64, vp, ctypes.POINTER(PushConstants), vp, vp, vp, vp,
+                                        u32, u32]
+    L.tim_rt_bvh_file_read.argtypes = [ctypes.c_char_p, ctypes.POINTER(vp)]
+    L.tim_rt_bvh_file_info.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(u64), vp, ctypes.POINTER(PushConstants),
+                                       vp, ctypes.POINTER(vp), ctypes.POINTER(vp), ctypes.POINTER(vp),
+                                       ctypes.POINTER(u32), ctypes.POINTER(u32)]
+    L.tim_rt_bvh_file_free.argtypes = [vp]
+    L.tim_rt_bvh_file_free.restype = None
+    L.tim_rt_upload_bvh_file.argtypes = [vp, ctypes.c_char_p, u32, ctypes.POINTER(u32)]
     for name in EXPORTED:
-        if name not in ("tim_rt_version", "tim_rt_last_error", "tim_rt_build_params_default", "tim_rt_bvh_blob_free"):
+        if name not in ("tim_rt_version", "tim_rt_last_error", "tim_rt_build_params_default", "tim_rt_bvh_blob_free",
+                        "tim_rt_bvh_file_free"):
             getattr(L, name).restype = i32
     _lib = L
     return L
@@ -284,6 +295,50 @@ def build_bvh(scene, **params) -> BvhImage:
     return BvhImage(data, ranges, (pc.numTriangles, pc.numBlas, pc.numPrimitives, pc.numLights, pc.numNodes), aabb)
 
 
+def save_bvh_file(path, img: BvhImage, positions, normals=None, uvs=None) -> None:
+    """tim_rt_bvh_file_write: the BVH image and the vertex arrays to a versioned file."""
+    pos = np.ascontiguousarray(positions, np.float32)
+    nrm = np.ascontiguousarray(normals, np.float32) if normals is not None else None
+    uv = np.ascontiguousarray(uvs, np.float32) if uvs is not None else None
+    ranges = np.ascontiguousarray(img.ranges, np.uint32)
+    aabb = np.ascontiguousarray(img.aabb, np.float32)
+    pc = PushConstants(*[int(x) for x in img.pc])
+    data = np.ascontiguousarray(img.data, np.uint8)
+    _check(lib().tim_rt_bvh_file_write(str(path).encode(), data.ctypes.data, data.nbytes, ranges.ctypes.data,
+                                       ctypes.byref(pc), aabb.ctypes.data, pos.ctypes.data, _ptr(nrm), _ptr(uv),
+                                       pos.shape[0], pos.shape[0]))
+
+
+def load_bvh_file(path):
+    """tim_rt_bvh_file_read: (BvhImage, positions, normals or None, uvs or None), copied out of the file."""
+    L = lib()
+    f = ctypes.c_void_p()
+    _check(L.tim_rt_bvh_file_read(str(path).encode(), ctypes.byref(f)))
+    try:
+        bp, size = ctypes.c_void_p(), ctypes.c_uint64()
+        ranges = np.zeros((7, 2), np.uint32)
+        pc = PushConstants()
+        aabb = np.zeros(6, np.float32)
+        pp, pn, pu = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+        mx, nv = ctypes.c_uint32(), ctypes.c_uint32()
+        _check(L.tim_rt_bvh_file_info(f, ctypes.byref(bp), ctypes.byref(size), ranges.ctypes.data, ctypes.byref(pc),
+                                      aabb.ctypes.data, ctypes.byref(pp), ctypes.byref(pn), ctypes.byref(pu),
+                                      ctypes.byref(mx), ctypes.byref(nv)))
+        data = np.frombuffer(ctypes.string_at(bp.value, size.value), dtype=np.uint8).copy()
+        n = nv.value
+
+        def arr(ptr, k):
+            if not ptr.value:
+                return None
+            return np.frombuffer(ctypes.string_at(ptr.value, 4 * k * n), dtype=np.float32).reshape(n, k).copy()
+
+        pos, nrm, uv = arr(pp, 3), arr(pn, 3), arr(pu, 2)
+    finally:
+        L.tim_rt_bvh_file_free(f)
+    img = BvhImage(data, ranges, (pc.numTriangles, pc.numBlas, pc.numPrimitives, pc.numLights, pc.numNodes), aabb)
+    return img, pos, nrm, uv
+
+
 class Context:
     """A tim_rt_ctx: one device, one CUDA stream, resident scenes."""
 
@@ -375,6 +430,13 @@ class Context:
         _check(self._L.tim_rt_upload_bvh(self._c, img.data.ctypes.data, img.data.nbytes, ranges.ctypes.data,
                                          pos.ctypes.data, nrm.ctypes.data, None, pos.shape[0], pos.shape[0],
                                          ctypes.byref(pc), UPLOAD_QUANT8 if quant8 else 0, ctypes.byref(sid)))
+        return sid.value
+
+    def upload_file(self, path, quant8: bool = False) -> int:
+        """tim_rt_upload_bvh_file: a scene straight from a BVH file."""
+        sid = ctypes.c_uint32()
+        _check(self._L.tim_rt_upload_bvh_file(self._c, str(path).encode(), UPLOAD_QUANT8 if quant8 else 0,
+                                              ctypes.byref(sid)))
         return sid.value
 
     def free_scene(self, sid: int):
