@@ -400,6 +400,28 @@ int tim_rt_cull_lights(tim_rt_ctx *ctx, tim_rt_scene_id scene, const tim_rt_pass
 int tim_rt_cull_lights_dev(tim_rt_ctx *ctx, tim_rt_scene_id scene, const tim_rt_pass_data *pd,
                            uint32_t tiles_x, uint32_t tiles_y, uint32_t *d_counts, uint32_t *d_lists, void *cuda_stream);
 
+/* Lighting step of the camera pass: cameraPass.comp without TRACING_STEP, as
+ * RayTracingPass::lightingPass dispatches it (src/Renderer/raytracingPass.cpp:113-135:
+ * USE_LPF, USE_LPF_MASK; cameraPass.comp:78-88). Per pixel, from the tracing step's
+ * output (tracing: W*H*8 u32 as tim_rt_trace_camera writes it): the hit point and
+ * interpolated normal (baseRaytracingPass.glsl:38-82); direct light of the lights
+ * whose shadow-mask bit is clear and of the sun (bvhLighting.glsl:42-85, a light
+ * out of range adds nothing); unless TIM_RT_SHADE_NO_LPF, the light-probe term:
+ * the probe-masked trilinear SH9 sample of the 7 RGBA16F images that
+ * tim_rt_update_probes writes (resolution pd->lpfResolution, at least 2 per axis,
+ * over pd->sceneMinExtent..sceneMaxExtent; fetchSH_inline.glsl:82-118), evalSH and
+ * computeIndirectLighting; the sky colour on a miss. Materials are taken as
+ * untextured (texColor 1). out_rgba16: W*H*4 halves (lit rgb, alpha 1), written
+ * for every pixel, output row 0 (which the reference's dispatch never reaches) as
+ * 0; out_rgb32: optional W*H*3 floats before the FP16 rounding. */
+#define TIM_RT_SHADE_NO_LPF 1u
+int tim_rt_shade_camera(tim_rt_ctx *ctx, tim_rt_scene_id scene, const tim_rt_pass_data *pd, uint32_t flags,
+                        const uint32_t *tracing, const uint16_t *sh9_fp16, uint16_t *out_rgba16, float *out_rgb32,
+                        tim_rt_stats *stats);
+int tim_rt_shade_camera_dev(tim_rt_ctx *ctx, tim_rt_scene_id scene, const tim_rt_pass_data *pd, uint32_t flags,
+                            const uint32_t *d_tracing, const uint16_t *d_sh9_fp16, uint16_t *d_out_rgba16,
+                            float *d_out_rgb32, void *cuda_stream);
+
 /* ---------------------------------------------------------------- light-probe field */
 /* Probe field update: genLightProbField.comp (trace step and lighting step,
  * src/Shaders/genLightProbField.comp:41-81) followed by updateLightProbField.comp

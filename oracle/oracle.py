@@ -84,6 +84,8 @@ def orc():
         L.orc_probe_octa.restype = None
         L.orc_bounce_dir.argtypes = [vp, u32, u32, vp]
         L.orc_bounce_dir.restype = None
+        L.orc_shade_camera.argtypes = [vp, vp, u32, vp, vp, vp, vp, i32]
+        L.orc_shade_camera.restype = None
         L.orc_hash32.argtypes = [u32]
         L.orc_hash32.restype = u32
         _orc = L
@@ -195,6 +197,20 @@ def camera(sc: Scene, pd: np.ndarray, flags: int = 0, seed: int = 0, tile_counts
                      tl.ctypes.data if tl is not None else None, out.ctypes.data, bounce.ctypes.data,
                      counts.ctypes.data, b, e, threads)
     return out, bounce, counts
+
+
+def shade_camera(sc: Scene, pd: np.ndarray, tracing: np.ndarray, sh16: np.ndarray, no_lpf: bool = False,
+                 threads: int = 0):
+    """orc_shade_camera: the camera pass's lighting step -> (RGBA16F u16 [W*H, 4], FP32 rgb [W*H, 3])."""
+    W, H = (int(x) for x in np.asarray(pd["frameSize"]).reshape(-1)[:2])
+    pd = np.ascontiguousarray(pd)
+    tr = np.ascontiguousarray(tracing, np.uint32)
+    sh = np.ascontiguousarray(sh16, np.uint16)
+    out = np.zeros((W * H, 4), np.uint16)
+    f32 = np.zeros((W * H, 3), np.float32)
+    orc().orc_shade_camera(sc.ref, pd.ctypes.data, 1 if no_lpf else 0, tr.ctypes.data, sh.ctypes.data,
+                           out.ctypes.data, f32.ctypes.data, threads)
+    return out, f32
 
 
 def cull_lights(sc: Scene, pd: np.ndarray, tiles_x: int, tiles_y: int, threads: int = 0):

@@ -1,8 +1,8 @@
 """oracle/refglsl -- TEST INFRASTRUCTURE ONLY.
 
 ctypes wrapper around oracle/_ref/librefglsl.so: the reference's own compute
-shaders (cameraPass.comp, genLightProbField.comp, updateLightProbField.comp and
-the BVH traversal they include), rewritten mechanically into C++ by
+shaders (cameraPass.comp in its tracing and lighting steps, genLightProbField.comp,
+updateLightProbField.comp and the BVH traversal they include), rewritten mechanically into C++ by
 make_refglsl.py and compiled with glsl_shim.h by oracle/Makefile. It is a second
 oracle, used only by the tests and the golden-fixture script to pin the C
 restatement (oracle/reftrace.c) to the reference's code. Scenes are the same
@@ -38,8 +38,9 @@ def lib():
         L.refglsl_probe_trace.argtypes = [vp, vp, vp, vp]
         L.refglsl_probe_light.argtypes = [vp, vp, vp, vp, vp]
         L.refglsl_probe_update.argtypes = [vp, vp, vp, vp]
+        L.refglsl_shade.argtypes = [vp, vp, vp, vp, vp]
         for f in (L.refglsl_trace, L.refglsl_camera, L.refglsl_probe_trace, L.refglsl_probe_light,
-                  L.refglsl_probe_update):
+                  L.refglsl_probe_update, L.refglsl_shade):
             f.restype = ctypes.c_int
         _lib = L
     return _lib
@@ -98,3 +99,14 @@ def probe_update(desc, sh_basis: np.ndarray, irradiance: np.ndarray, images16: n
     img = np.array(images16, np.uint16, copy=True, order="C")
     _check(lib().refglsl_probe_update(ctypes.byref(desc), _ptr(b), _ptr(irr), _ptr(img)), "probe_update")
     return img
+
+
+def shade(sc, pd: np.ndarray, tracing: np.ndarray, sh16: np.ndarray) -> np.ndarray:
+    """cameraPass.comp lighting step (USE_LPF, USE_LPF_MASK): RGBA16F [W*H, 4] as u16."""
+    pd = np.ascontiguousarray(pd)
+    W, H = (int(x) for x in np.asarray(pd["frameSize"]).reshape(-1)[:2])
+    tr = np.ascontiguousarray(tracing, np.uint32)
+    sh = np.ascontiguousarray(sh16, np.uint16)
+    out = np.zeros((W * H, 4), np.uint16)
+    _check(lib().refglsl_shade(sc.ref, _ptr(pd), _ptr(tr), _ptr(sh), _ptr(out)), "shade")
+    return out

@@ -261,8 +261,6 @@ struct sampler2D { int unit = 0; };
 inline vec4 texture(const sampler2D&, const vec2&) { g_refglsl_error |= 1u; return vec4(1.0f); }
 inline vec4 textureLod(const sampler2D&, const vec2&, float) { g_refglsl_error |= 1u; return vec4(1.0f); }
 
-struct image2D { int unit = 0; };
-inline void imageStore(image2D&, const ivec2&, const vec4&) {}
 
 /* rgba16f 3D image: four halves per texel, x fastest. */
 struct image3D {
@@ -281,6 +279,18 @@ inline vec4 imageLoad(const image3D& im, const ivec3& c) {
 inline void imageStore(image3D& im, const ivec3& c, const vec4& v) {
     if (!im.inside(c)) { g_refglsl_error |= 2u; return; }
     uint16_t* t = im.data + im.at(c);
+    for (int i = 0; i < 4; ++i) t[i] = float_to_half(v.v[i]);
+}
+
+/* rgba16f 2D image (x fastest); with no storage bound, stores are dropped. */
+struct image2D {
+    uint16_t* data = nullptr;
+    int w = 0, h = 0;
+};
+inline void imageStore(image2D& im, const ivec2& c, const vec4& v) {
+    if (!im.data) return;
+    if (c.x < 0 || c.y < 0 || c.x >= im.w || c.y >= im.h) { g_refglsl_error |= 2u; return; }
+    uint16_t* t = im.data + 4ull * ((uint64_t)c.y * im.w + c.x);
     for (int i = 0; i < 4; ++i) t[i] = float_to_half(v.v[i]);
 }
 

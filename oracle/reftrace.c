@@ -667,13 +667,12 @@ static v3 interp_normal(const orc_scene *s, const uint32_t *rec, v3 pos) {
     return add(add(muls(n0, u), muls(n1, v)), muls(n2, w));
 }
 
-/* bvhLighting.glsl:42-85 computeLighting with NO_LPF (genLightProbField.comp:5), and
- * baseRaytracingPass.glsl:67-82 for the miss colour. */
-static v3 probe_lit(const orc_scene *s, const orc_probe_desc *pd, const ray_t *r, float t, const uint32_t *rec, uint32_t mask) {
-    if (!(t < TMAX)) return divs(muls(mk(200.0f, 220.0f, 255.0f), 0.3f), 255.0f);   /* 0.3 * vec3(...) / 255 */
-    v3 pos = add(r->from, muls(r->dir, t));
-    v3 N = interp_normal(s, rec, pos);
-    const material *m = material_at(s, (rec[2] & 0xFFFF0000u) >> 16);
+/* bvhLighting.glsl:42-85 computeLighting, direct part: texColor 1 (untextured
+ * materials), the lights whose mask bit is clear (evalLighting -> evalSphereLight;
+ * a light out of range contributes 0, where lighting.glsl:92-101 falls off the end
+ * of a non-void function), then the sun (evalSunLight), summed in that order. */
+static v3 direct_lit(const orc_scene *s, const material *m, v3 pos, v3 N, v3 eye, uint32_t mask, v3 sunDir,
+                     v3 sunColor) {
     v3 lit = mk(0, 0, 0);
     for (uint32_t i = 0; i < s->num_lights && i < 31u; ++i) {
         if ((mask & (1u << (i + 1u))) != 0u) continue;
@@ -684,13 +683,26 @@ static v3 probe_lit(const orc_scene *s, const orc_probe_desc *pd, const ray_t *r
         if (d < L->fparam[3]) {
             v3 Ld = divs(sub(lp, pos), d);
             d = fmaxf(0.01f, d - L->fparam[7]);
-            lit = add(lit, compute_lighting(m, mk(L->fparam[4], L->fparam[5], L->fparam[6]), pos, Ld, N, r->from,
+            lit = add(lit, compute_lighting(m, mk(L->fparam[4], L->fparam[5], L->fparam[6]), pos, Ld, N, eye,
                                             attenuation(d, L->fparam[3])));
         }
     }
-    if ((mask & 1u) == 0u)
-        lit = add(lit, compute_lighting(m, ld3(pd->sunColor), pos, neg(ld3(pd->sunDir)), N, r->from, 1.0f));
+    if ((mask & 1u) == 0u) lit = add(lit, compute_lighting(m, sunColor, pos, neg(sunDir), N, eye, 1.0f));
     return lit;
+}
+
+static inline v3 sky_colour(void) {   /* baseRaytracingPass.glsl:81: 0.3 * vec3(200,220,255) / 255 */
+    return divs(muls(mk(200.0f, 220.0f, 255.0f), 0.3f), 255.0f);
+}
+
+/* bvhLighting.glsl:42-85 computeLighting with NO_LPF (genLightProbField.comp:5), and
+ * baseRaytracingPass.glsl:67-82 for the miss colour. */
+static v3 probe_lit(const orc_scene *s, const orc_probe_desc *pd, const ray_t *r, float t, const uint32_t *rec, uint32_t mask) {
+    if (!(t < TMAX)) return sky_colour();
+    v3 pos = add(r->from, muls(r->dir, t));
+    v3 N = interp_normal(s, rec, pos);
+    const material *m = material_at(s, (rec[2] & 0xFFFF0000u) >> 16);
+    return direct_lit(s, m, pos, N, r->from, mask, ld3(pd->sunDir), ld3(pd->sunColor));
 }
 
 /* genLightProbField.comp:41-81: trace step (closest hit + leaf-light shadow mask;
@@ -785,5 +797,126 @@ void orc_probe_octa(const orc_probe_desc *pd, const float *irradiance,
         }
         float inv = 1.0f / (float)(per ? per : 1u);
         for (uint32_t q = 0; q < 192u; ++q) o[q] *= inv;
+    }
+}
+
+/* ------------------------------------------------------------ camera lighting step */
+static inline float half_to_float(uint16_t h) { _Float16 f; memcpy(&f, &h, 2); return (float)f; }
+static inline uint16_t float_to_half(float x) { _Float16 f = (_Float16)x; uint16_t h; memcpy(&h, &f, 2); return h; }
+static inline float mixf(float a, float b, float x) { return a * (1.0f - x) + b * x; }   /* GLSL mix */
+
+/* fetchSH_inline.glsl:82-118 sampleSH9 with the probe mask, per image channel:
+ * v[x + 2y + 4z] are the eight corner values, bit (x + 2y + 4z) of mask set =
+ * corner masked. The same lerp tree as the shader, so the same rounding. */
+static float masked_trilinear(const float v[8], v3 f, uint32_t mask) {
+#define M(i) (((mask >> (i)) & 1u) == 0u)
+    float shx0 = M(0) && M(1) ? mixf(v[0], v[1], f.x) : (M(0) ? v[0] : v[1]);
+    float shx1 = M(2) && M(3) ? mixf(v[2], v[3], f.x) : (M(2) ? v[2] : v[3]);
+    int b00 = M(0) || M(1), b10 = M(2) || M(3);
+    float z0 = b00 && b10 ? mixf(shx0, shx1, f.y) : (b00 ? shx0 : shx1);
+    shx0 = M(4) && M(5) ? mixf(v[4], v[5], f.x) : (M(4) ? v[4] : v[5]);
+    shx1 = M(6) && M(7) ? mixf(v[6], v[7], f.x) : (M(6) ? v[6] : v[7]);
+    int b01 = M(4) || M(5), b11 = M(6) || M(7);
+    float z1 = b01 && b11 ? mixf(shx0, shx1, f.y) : (b01 ? shx0 : shx1);
+    int bxy0 = b00 || b10, bxy1 = b01 || b11;
+#undef M
+    return bxy0 && bxy1 ? mixf(z0, z1, f.z) : (bxy0 ? z0 : z1);
+}
+
+/* bvhLighting.glsl:24-40 computeLPFLighting with USE_LPF_MASK: probe-grid uvw
+ * (lightprobHelpers.glsl:71-77), masked SH9 sample from the 7 FP16 images
+ * (fetchSH_inline.glsl:6-31 channel layout), evalSH (lightprobHelpers.glsl:90-101)
+ * and computeIndirectLighting (core/lighting.glsl:59-74, texColor 1). */
+static v3 lpf_lit(const orc_pass_data *pd, const uint16_t *sh16, const material *m, v3 pos, v3 N, uint32_t mask) {
+    const uint32_t *res = pd->lpfResolution;
+    v3 step = lpf_step(pd->sceneMinExtent, pd->sceneMaxExtent, res);
+    v3 uvw = sub(mk((pos.x - pd->sceneMinExtent[0]) / step.x, (pos.y - pd->sceneMinExtent[1]) / step.y,
+                    (pos.z - pd->sceneMinExtent[2]) / step.z), mk(0.5f, 0.5f, 0.5f));
+    uvw = mk(fminf(fmaxf(uvw.x, 0.0f), (float)res[0] - 1.0f), fminf(fmaxf(uvw.y, 0.0f), (float)res[1] - 1.0f),
+             fminf(fmaxf(uvw.z, 0.0f), (float)res[2] - 1.0f));
+    /* min(int(uvw), res - 2) in GLSL's int -> uint conversion */
+    uint32_t ix = (uint32_t)(int32_t)uvw.x, iy = (uint32_t)(int32_t)uvw.y, iz = (uint32_t)(int32_t)uvw.z;
+    ix = ix < res[0] - 2u ? ix : res[0] - 2u;
+    iy = iy < res[1] - 2u ? iy : res[1] - 2u;
+    iz = iz < res[2] - 2u ? iz : res[2] - 2u;
+    v3 f = sub(uvw, mk((float)(int32_t)ix, (float)(int32_t)iy, (float)(int32_t)iz));
+    const uint64_t img = (uint64_t)res[0] * res[1] * res[2];
+    float ch[7][4];
+    for (int k = 0; k < 7; ++k)
+        for (int c = 0; c < 4; ++c) {
+            float v[8];
+            for (int q = 0; q < 8; ++q) {
+                uint64_t x = ix + (q & 1), y = iy + ((q >> 1) & 1), z = iz + ((q >> 2) & 1);
+                v[q] = half_to_float(sh16[4u * (k * img + (z * res[1] + y) * res[0] + x) + c]);
+            }
+            ch[k][c] = masked_trilinear(v, f, mask);
+        }
+    float w[9][3];   /* SH9Color.w[j].rgb from the storeSH9 layout */
+    for (int c = 0; c < 3; ++c) w[0][c] = ch[0][c];
+    for (int j = 1; j <= 8; ++j)
+        for (int c = 0; c < 3; ++c) w[j][c] = j <= 4 ? ch[1 + 2 * c][j - 1] : ch[2 + 2 * c][j - 5];
+    const float c1 = 0.429043f, c2 = 0.511664f, c3 = 0.743125f, c4 = 0.886227f, c5 = 0.247708f;
+    /* SH_Y00 0, Y11 1, Y10 2, Y1_1 3, Y21 4, Y2_1 5, Y2_2 6, Y20 7, Y22 8 (lightprob.glsl) */
+    float L[3];
+    for (int c = 0; c < 3; ++c) {
+        float t1 = (c1 * (N.x * N.x - N.y * N.y)) * w[8][c];
+        float t2 = ((c3 * w[7][c]) * N.z) * N.z;
+        float t3 = c4 * w[0][c];
+        float t4 = c5 * w[7][c];
+        float t5 = (2.0f * c1) * (((w[6][c] * N.x) * N.y + (w[4][c] * N.x) * N.z) + (w[5][c] * N.y) * N.z);
+        float t6 = (2.0f * c2) * ((w[1][c] * N.x + w[3][c] * N.y) + w[2][c] * N.z);
+        L[c] = ((((t1 + t2) + t3) - t4) + t5) + t6;
+    }
+    const float pi = 3.14159265359f;   /* TIM_PI, core/math.glsl:4 */
+    if (m->type_ids[0] == MAT_PBR) {
+        float k = 1.0f - m->params[0];
+        return mk(((k * m->color[0]) * L[0]) / pi, ((k * m->color[1]) * L[1]) / pi, ((k * m->color[2]) * L[2]) / pi);
+    }
+    if (m->type_ids[0] == MAT_LAMBERT)
+        return mk((L[0] * m->color[0]) / pi, (L[1] * m->color[1]) / pi, (L[2] * m->color[2]) / pi);
+    return mk(0, 0, 0);
+}
+
+/* cameraPass.comp:78-88, the lighting step (RayTracingPass::lightingPass,
+ * raytracingPass.cpp:113-135: USE_LPF, USE_LPF_MASK): per pixel the tracing
+ * record and masks -> computeLighting (baseRaytracingPass.glsl:67-82) -> RGBA16F. */
+void orc_shade_camera(const orc_scene *s, const orc_pass_data *pd, uint32_t flags, const uint32_t *tracing,
+                      const uint16_t *sh16, uint16_t *out_rgba16, float *out_rgb32, int threads) {
+    const uint32_t W = pd->frameSize[0], H = pd->frameSize[1];
+    const uint32_t ngy = (H + 15u) / 16u;
+    v3 c00 = ld3(pd->frustumCorner00), c10 = ld3(pd->frustumCorner10), c01 = ld3(pd->frustumCorner01);
+    v3 cam = ld3(pd->cameraPos);
+    v3 stepW = muls(sub(c10, c00), pd->invFrameSize[0]);
+    v3 stepH = muls(sub(c01, c00), pd->invFrameSize[1]);
+    int nt = nthreads(threads);
+    (void)nt;
+    int64_t npix = (int64_t)W * H;
+#pragma omp parallel for schedule(dynamic, 256) num_threads(nt)
+    for (int64_t pix = 0; pix < npix; ++pix) {
+        uint32_t px = (uint32_t)(pix % W), py = (uint32_t)(pix / W);
+        uint16_t *o = out_rgba16 + 4u * (uint64_t)pix;
+        float *of = out_rgb32 ? out_rgb32 + 3u * (uint64_t)pix : 0;
+        memset(o, 0, 8);
+        if (of) memset(of, 0, 12);
+        if (py == 0u) continue;   /* the dispatch never reaches output row 0 */
+        uint32_t gx = px, gy = ngy * 16u - py;
+        v3 target = add(add(c00, muls(stepW, (float)gx)), muls(stepH, (float)gy));
+        ray_t r; r.from = cam; r.dir = normalize3(sub(target, cam));
+        const uint32_t *rec = tracing + 8u * (uint64_t)pix;
+        float t;
+        memcpy(&t, rec + 3, 4);
+        v3 lit;
+        if (!(t < TMAX)) {
+            lit = sky_colour();
+        } else {
+            v3 pos = add(r.from, muls(r.dir, t));
+            v3 N = interp_normal(s, rec, pos);
+            const material *m = material_at(s, (rec[2] & 0xFFFF0000u) >> 16);
+            lit = direct_lit(s, m, pos, N, r.from, rec[4], ld3(pd->sunDir), ld3(pd->sunColor));
+            if (!(flags & ORC_SHADE_NO_LPF)) lit = add(lit, lpf_lit(pd, sh16, m, pos, N, rec[5]));
+        }
+        o[0] = float_to_half(lit.x); o[1] = float_to_half(lit.y); o[2] = float_to_half(lit.z);
+        o[3] = float_to_half(1.0f);
+        if (of) { of[0] = lit.x; of[1] = lit.y; of[2] = lit.z; }
     }
 }

@@ -102,6 +102,14 @@ void orc_probe_sh9(const orc_probe_desc *pd, const float *sh_basis, const float 
 void orc_probe_octa(const orc_probe_desc *pd, const float *irradiance,
                     uint32_t probe_begin, uint32_t probe_end, float *out_texels);
 
+/* cameraPass.comp lighting step (USE_LPF, USE_LPF_MASK): per pixel, from the
+ * tracing step's records (tracing: W*H*8 u32) and the light-probe field's 7 RGBA16F
+ * images (sh16, resolution pd->lpfResolution, the layout of orc_probe_sh9's images),
+ * the lit colour as RGBA16F (out_rgba16, W*H*4) and optionally FP32 rgb (W*H*3).
+ * Output row 0 is never reached by the reference's dispatch and is written as 0. */
+#define ORC_SHADE_NO_LPF 1u   /* leave out the light-probe term */
+void orc_shade_camera(const orc_scene *s, const orc_pass_data *pd, uint32_t flags, const uint32_t *tracing,
+                      const uint16_t *sh16, uint16_t *out_rgba16, float *out_rgb32, int threads);
 /* Bounce direction and basis helpers exposed for tests. */
 void orc_bounce_dir(const float n[3], uint32_t pixel, uint32_t seed, float out[3]);
 uint32_t orc_hash32(uint32_t x);

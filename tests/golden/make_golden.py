@@ -6,7 +6,8 @@
   sources by oracle/Makefile, single-threaded so node numbering is stable) run
   on the config-1 room scene (scenes.room_scene(1)): the fillGpuBuffer bytes,
   the seven ranges and the push constants. GPU tests trace this exact buffer.
-* room_golden.npz -- camera, random-ray and light-probe results on that buffer
+* room_golden.npz -- camera (tracing and lighting steps), random-ray and
+  light-probe results on that buffer
   from the C restatement (oracle/reftrace.c) and, under the glsl_* keys, from the
   reference's own compute shaders compiled as C++ (oracle/refglsl, built by
   oracle/Makefile from the reference tree); the tests check the two against each
@@ -67,6 +68,10 @@ def main():
     od = O.probe_desc(img.aabb[:3], img.aabb[3:], res, sun, sunc, len(dirs), 0.03)
     ptr, pirr, _ = O.probe_trace(sc, od, dirs, 0, total)
     prev16 = np.random.default_rng(11).uniform(-1, 1, size=(7, res[2], res[1], res[0], 4)).astype(np.float16)
+    # camera lighting step over the camera records, with a seeded FP16 probe field
+    lpf16 = np.random.default_rng(13).uniform(-0.5, 1.5, size=(7, 8, 8, 8, 4)).astype(np.float16).view(np.uint16)
+    shade16, _ = O.shade_camera(sc, pd, cam, lpf16)
+    out.update(lpf16=lpf16, shade16=shade16)
     out.update(probe_res=np.array(res, np.uint32), probe_dirs=dirs, probe_basis=basis,
                probe_sun=np.stack([sun, sunc]), probe_prev16=prev16.view(np.uint16),
                probe_trace=ptr.reshape(-1, 8), probe_irradiance=pirr.reshape(-1, 3))
@@ -83,6 +88,7 @@ def main():
         gptr = refglsl.probe_trace(gs, od, dirs)
         girr = refglsl.probe_light(gs, od, dirs, gptr)
         gimg = refglsl.probe_update(od, basis, girr, prev16.view(np.uint16))
+        out.update(glsl_shade16=refglsl.shade(gs, pd, cam, lpf16))
         out.update(glsl_hit_closest=gh, glsl_nid_closest=gn, glsl_hit_any=ga, glsl_camera=gcam,
                    glsl_probe_trace=gptr, glsl_probe_irradiance=girr, glsl_probe_images16=gimg)
     np.savez_compressed(HERE / "room_golden.npz", **out)

@@ -38,8 +38,11 @@ def test_fixture_pins_restatement(oracle_mod):
     assert np.array_equal(hit, g["glsl_hit_closest"]) and np.array_equal(nid, g["glsl_nid_closest"])
     ha, _, _, _ = O.trace(sc, g["rays"], 1)
     assert np.array_equal(ha, g["glsl_hit_any"])
-    cam, _, _ = O.camera(sc, g["pass_data"].view(scenes.PASS_DATA_DTYPE), flags=O_CAM_PROB_MASK)
+    pd = g["pass_data"].view(scenes.PASS_DATA_DTYPE)
+    cam, _, _ = O.camera(sc, pd, flags=O_CAM_PROB_MASK)
     assert np.array_equal(cam, g["glsl_camera"])
+    shade16, _ = O.shade_camera(sc, pd, cam, g["lpf16"])
+    assert np.array_equal(shade16, g["glsl_shade16"])
     res, dirs, basis, sun, sunc, prev16 = _probe_inputs(g)
     total = res[0] * res[1] * res[2]
     od = O.probe_desc(img.aabb[:3], img.aabb[3:], res, sun, sunc, len(dirs), 0.03)
@@ -146,3 +149,28 @@ def test_probe_passes(oracle_mod, G):
     probes = list(range(total))
     sh = O.probe_sh9(od, basis, irr.reshape(-1, 3), 0, total, sh16_to_prev27(prev16, res, probes))
     assert np.array_equal(G.probe_update(od, basis, girr, prev16), sh27_to_images16(sh, res, probes, prev16))
+
+
+@pytest.mark.parametrize("mask_frac", [0.0, 0.5])
+def test_camera_lighting_step(oracle_mod, G, mask_frac):
+    """cameraPass.comp lighting step (USE_LPF, USE_LPF_MASK): direct light from the
+    tracing step's shadow masks, the probe-masked SH9 sample of the FP16 field,
+    evalSH and computeIndirectLighting, stored as RGBA16F."""
+    from tim_raytracing_b200 import scenes
+    O = oracle_mod
+    s = scenes.heightfield_scene(seed=9, grid=20, n_spheres=6, n_lights=12, light_radius=5.0)
+    img = O.ref_build(s)
+    sc = O.Scene(img, s.positions, s.normals)
+    pd = scenes.pass_data(s, 80, 56, lpf_res=(8, 8, 4), aabb=(img.aabb[:3], img.aabb[3:]))
+    cam, _, _ = O.camera(sc, pd, flags=O_CAM_PROB_MASK)
+    rng = np.random.default_rng(17)
+    if mask_frac:   # random probe masks exercise every branch of the masked trilinear tree
+        hit = cam[:, 3].view(np.float32) < 100.0
+        cam[hit, 5] = rng.integers(0, 256, size=int(hit.sum())).astype(np.uint32)
+    sh16 = rng.uniform(-0.5, 1.5, size=(7, 4, 8, 8, 4)).astype(np.float16).view(np.uint16)
+    o16, _ = O.shade_camera(sc, pd, cam, sh16)
+    g16 = G.shade(G.Scene(img, s.positions, s.normals), pd, cam, sh16)
+    bad = np.flatnonzero((o16 != g16).any(1))
+    assert bad.size == 0, bad[:8]
+    hit = cam[:, 3].view(np.float32) < 100.0
+    assert hit.sum() > 100

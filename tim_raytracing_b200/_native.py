@@ -34,11 +34,13 @@ EXPORTED = [
     "tim_rt_server_submit", "tim_rt_server_wait", "tim_rt_server_drain", "tim_rt_server_stats_get",
     "tim_rt_server_destroy", "tim_rt_verify_hits", "tim_rt_server_submit_probes", "tim_rt_bvh_file_write",
     "tim_rt_bvh_file_read", "tim_rt_bvh_file_info", "tim_rt_bvh_file_free", "tim_rt_upload_bvh_file",
+    "tim_rt_shade_camera", "tim_rt_shade_camera_dev",
 ]
 SORT_NONE, SORT_OCTANT, SORT_MORTON = 0, 1, 2
 BATCH_WIDE = 0x100
 TUNE_WIDTH = 1
 PROBE_OCTA, PROBE_WIDE, PROBE_PRIMARY_BINARY = 1, 0x100, 0x400
+SHADE_NO_LPF = 1
 
 
 class ProbeDesc(ctypes.Structure):
@@ -198,6 +200,8 @@ def lib() -> ctypes.CDLL:
     L.tim_rt_bvh_file_free.argtypes = [vp]
     L.tim_rt_bvh_file_free.restype = None
     L.tim_rt_upload_bvh_file.argtypes = [vp, ctypes.c_char_p, u32, ctypes.POINTER(u32)]
+    L.tim_rt_shade_camera.argtypes = [vp, u32, vp, u32, vp, vp, vp, vp, ctypes.POINTER(Stats)]
+    L.tim_rt_shade_camera_dev.argtypes = [vp, u32, vp, u32, vp, vp, vp, vp, vp]
     for name in EXPORTED:
         if name not in ("tim_rt_version", "tim_rt_last_error", "tim_rt_build_params_default", "tim_rt_bvh_blob_free",
                         "tim_rt_bvh_file_free"):
@@ -504,6 +508,20 @@ class Context:
                                             probe_begin, probe_end, _ptr(tr), _ptr(irr), sh16.ctypes.data, _ptr(s32),
                                             _ptr(octa), ctypes.byref(st)))
         return tr, irr, s32, octa, st
+
+    def shade_camera(self, sid: int, pd: np.ndarray, tracing: np.ndarray, sh16=None, flags: int = 0,
+                     want_f32: bool = False):
+        """tim_rt_shade_camera: (RGBA16F u16 [W*H, 4], FP32 rgb [W*H, 3] or None, Stats)."""
+        W, H = (int(x) for x in np.asarray(pd["frameSize"]).reshape(-1)[:2])
+        pd = np.ascontiguousarray(pd)
+        tr = np.ascontiguousarray(tracing, np.uint32)
+        sh = np.ascontiguousarray(sh16, np.uint16) if sh16 is not None else None
+        out = np.empty((W * H, 4), np.uint16)
+        f32 = np.empty((W * H, 3), np.float32) if want_f32 else None
+        st = Stats()
+        _check(self._L.tim_rt_shade_camera(self._c, sid, pd.ctypes.data, flags, tr.ctypes.data, _ptr(sh),
+                                           out.ctypes.data, _ptr(f32), ctypes.byref(st)))
+        return out, f32, st
 
     def trace_camera(self, sid: int, pd: np.ndarray, flags: int = 0, seed: int = 0, tile_counts=None, tile_lists=None,
                      out=None, bounce_out=None):

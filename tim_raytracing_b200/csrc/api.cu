@@ -260,7 +260,7 @@ int tim_rt_destroy(tim_rt_ctx* c) {
     c->scenes.clear();
     for (DevBuf* b : {&c->rays, &c->hits, &c->nid, &c->bary, &c->counters, &c->cam_out, &c->cam_bounce, &c->cam_nid,
                       &c->q_rays, &c->q_pixel, &c->tiles_counts, &c->tiles_lists, &c->dstats, &c->p_dirs, &c->p_basis,
-                      &c->p_out, &c->p_nid, &c->p_irr, &c->p_sh16, &c->p_sh32, &c->p_octa})
+                      &c->p_out, &c->p_nid, &c->p_irr, &c->p_sh16, &c->p_sh32, &c->p_octa, &c->sh_out, &c->sh_f32})
         dev_free(c, *b);
     for (auto& e : c->ev)
         if (e) cudaEventDestroy(e);
@@ -625,6 +625,82 @@ int tim_rt_trace_camera_dev(tim_rt_ctx* c, tim_rt_scene_id id, const tim_rt_pass
                              static_cast<tim_rt_ray*>(c->q_rays.ptr), static_cast<uint32_t*>(c->q_pixel.ptr),
                              (uint32_t)qcap, ctr, ctr + kErrWord, d_ray_count, st,
                              cfg_for(c, s, (flags & TIM_RT_CAM_WIDE) != 0)));
+    return TIM_RT_OK;
+}
+
+// Checks of tim_rt_shade_camera(_dev): frame size, light-probe resolution, normals.
+static int shade_check(Scene* s, const tim_rt_pass_data* pd, uint32_t flags, const void* tracing, const void* sh16,
+                       const void* out16, const char* who) {
+    const std::string w(who);
+    if (!pd || !tracing || !out16 || (!(flags & TIM_RT_SHADE_NO_LPF) && !sh16) || (flags & ~TIM_RT_SHADE_NO_LPF)) {
+        set_error(w + ": null argument or unknown flag");
+        return TIM_RT_EINVAL;
+    }
+    const uint64_t npix = (uint64_t)pd->frameSize[0] * pd->frameSize[1];
+    if (pd->frameSize[0] == 0 || pd->frameSize[1] == 0 || npix > (1ull << 30)) {
+        set_error(w + ": frame size must be 1..2^30 pixels");
+        return TIM_RT_EINVAL;
+    }
+    if (!(flags & TIM_RT_SHADE_NO_LPF)) {
+        const uint32_t* r = pd->lpfResolution;
+        if (r[0] < 2 || r[1] < 2 || r[2] < 2 || (uint64_t)r[0] * r[1] * r[2] > (1ull << 24)) {
+            set_error(w + ": light-probe resolution must be 2..2^24 probes with at least 2 per axis "
+                          "(sampleSH9 interpolates between neighbours)");
+            return TIM_RT_EINVAL;
+        }
+    }
+    if (!s->nrm.ptr) {
+        set_error(w + ": the lit value needs vertex normals (upload with nrm)");
+        return TIM_RT_EINVAL;
+    }
+    return TIM_RT_OK;
+}
+
+int tim_rt_shade_camera(tim_rt_ctx* c, tim_rt_scene_id id, const tim_rt_pass_data* pd, uint32_t flags,
+                        const uint32_t* tracing, const uint16_t* sh9_fp16, uint16_t* out_rgba16, float* out_rgb32,
+                        tim_rt_stats* stats) {
+    int rc = check_ctx(c);
+    if (rc) return rc;
+    Scene* s = find_scene(c, id);
+    if (!s) return TIM_RT_ENOTFOUND;
+    if ((rc = shade_check(s, pd, flags, tracing, sh9_fp16, out_rgba16, "tim_rt_shade_camera"))) return rc;
+    const uint64_t npix = (uint64_t)pd->frameSize[0] * pd->frameSize[1];
+    const bool lpf = !(flags & TIM_RT_SHADE_NO_LPF);
+    const uint64_t field = lpf ? 56ull * pd->lpfResolution[0] * pd->lpfResolution[1] * pd->lpfResolution[2] : 0;
+    if ((rc = ensure(c, c->cam_out, 32ull * npix)) || (rc = ensure(c, c->sh_out, 8ull * npix)) ||
+        (lpf && (rc = ensure(c, c->p_sh16, field))) || (out_rgb32 && (rc = ensure(c, c->sh_f32, 12ull * npix))))
+        return rc;
+    TIMRT_CUDA(cudaEventRecord(c->ev[0], c->stream));
+    TIMRT_CUDA(cudaMemcpyAsync(c->cam_out.ptr, tracing, 32ull * npix, cudaMemcpyHostToDevice, c->stream));
+    if (lpf) TIMRT_CUDA(cudaMemcpyAsync(c->p_sh16.ptr, sh9_fp16, field, cudaMemcpyHostToDevice, c->stream));
+    TIMRT_CUDA(cudaEventRecord(c->ev[1], c->stream));
+    TIMRT_CUDA(launch_shade(s->view, *pd, flags, static_cast<const uint32_t*>(c->cam_out.ptr),
+                            lpf ? static_cast<const uint16_t*>(c->p_sh16.ptr) : nullptr,
+                            static_cast<uint16_t*>(c->sh_out.ptr), out_rgb32 ? static_cast<float*>(c->sh_f32.ptr) : nullptr,
+                            c->stream));
+    TIMRT_CUDA(cudaEventRecord(c->ev[2], c->stream));
+    TIMRT_CUDA(cudaMemcpyAsync(out_rgba16, c->sh_out.ptr, 8ull * npix, cudaMemcpyDeviceToHost, c->stream));
+    if (out_rgb32) TIMRT_CUDA(cudaMemcpyAsync(out_rgb32, c->sh_f32.ptr, 12ull * npix, cudaMemcpyDeviceToHost, c->stream));
+    TIMRT_CUDA(cudaEventRecord(c->ev[3], c->stream));
+    TIMRT_CUDA(cudaStreamSynchronize(c->stream));
+    if (stats) {
+        std::memset(stats, 0, sizeof(*stats));
+        cudaEventElapsedTime(&stats->kernel_ms, c->ev[1], c->ev[2]);
+        cudaEventElapsedTime(&stats->total_ms, c->ev[0], c->ev[3]);
+    }
+    return TIM_RT_OK;
+}
+
+int tim_rt_shade_camera_dev(tim_rt_ctx* c, tim_rt_scene_id id, const tim_rt_pass_data* pd, uint32_t flags,
+                            const uint32_t* d_tracing, const uint16_t* d_sh9_fp16, uint16_t* d_out_rgba16,
+                            float* d_out_rgb32, void* cuda_stream) {
+    int rc = check_ctx(c);
+    if (rc) return rc;
+    Scene* s = find_scene(c, id);
+    if (!s) return TIM_RT_ENOTFOUND;
+    if ((rc = shade_check(s, pd, flags, d_tracing, d_sh9_fp16, d_out_rgba16, "tim_rt_shade_camera_dev"))) return rc;
+    cudaStream_t st = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : c->stream;
+    TIMRT_CUDA(launch_shade(s->view, *pd, flags, d_tracing, d_sh9_fp16, d_out_rgba16, d_out_rgb32, st));
     return TIM_RT_OK;
 }
 

@@ -91,6 +91,12 @@ cudaError_t launch_probes(const SceneView& s, const ProbeArgs& d, uint32_t* out,
                           uint32_t* q_pixel, uint32_t* counters, uint32_t* err, float* irr, uint16_t* sh16, float* sh32,
                           float* octa, uint32_t side, cudaStream_t stream, const LaunchConfig& cfg);
 
+// Camera lighting step: tracing = W*H*8 u32 (tim_rt_trace_camera's output), sh16 =
+// the 7 RGBA16F light-probe images of pd.lpfResolution (unused with
+// TIM_RT_SHADE_NO_LPF), out16 = W*H*4 halves, out32 optional W*H*3 floats.
+cudaError_t launch_shade(const SceneView& s, const tim_rt_pass_data& pd, uint32_t flags, const uint32_t* tracing,
+                         const uint16_t* sh16, uint16_t* out16, float* out32, cudaStream_t stream);
+
 cudaError_t launch_cull_lights(const SceneView& s, const tim_rt_pass_data& pd, uint32_t tiles_x, uint32_t tiles_y,
                                uint32_t* counts, uint32_t* lists, cudaStream_t stream);
 

@@ -835,6 +835,65 @@ __device__ void compute_lighting(const float* m, float lcx, float lcy, float lcz
     oz = rz * att;
 }
 
+// baseRaytracingPass.glsl:38-64 fillUvNormal, the normal: barycentric weights of
+// the hit point in the hit triangle (record rec) and the interpolated vertex normal.
+__device__ __forceinline__ void hit_normal(const SceneView& s, const uint4& rec, float px, float py, float pz,
+                                           float& Nx, float& Ny, float& Nz) {
+    const uint32_t i0 = rec.x + (rec.y & 0xFFFFu), i1 = rec.x + (rec.y >> 16), i2 = rec.x + (rec.z & 0xFFFFu);
+    const float* P = s.pos;
+    const float v0x = P[3 * i1] - P[3 * i0], v0y = P[3 * i1 + 1] - P[3 * i0 + 1], v0z = P[3 * i1 + 2] - P[3 * i0 + 2];
+    const float v1x = P[3 * i2] - P[3 * i0], v1y = P[3 * i2 + 1] - P[3 * i0 + 1], v1z = P[3 * i2 + 2] - P[3 * i0 + 2];
+    const float v2x = px - P[3 * i0], v2y = py - P[3 * i0 + 1], v2z = pz - P[3 * i0 + 2];
+    const float d00 = dot3(v0x, v0y, v0z, v0x, v0y, v0z), d01 = dot3(v0x, v0y, v0z, v1x, v1y, v1z);
+    const float d11 = dot3(v1x, v1y, v1z, v1x, v1y, v1z);
+    const float d20 = dot3(v2x, v2y, v2z, v0x, v0y, v0z), d21 = dot3(v2x, v2y, v2z, v1x, v1y, v1z);
+    const float denom = d00 * d11 - d01 * d01;
+    const float v = (d11 * d20 - d01 * d21) / denom;
+    const float w = (d00 * d21 - d01 * d20) / denom;
+    const float u = 1.0f - v - w;
+    const float* Nn = s.nrm;
+    Nx = (Nn[3 * i0] * u + Nn[3 * i1] * v) + Nn[3 * i2] * w;
+    Ny = (Nn[3 * i0 + 1] * u + Nn[3 * i1 + 1] * v) + Nn[3 * i2 + 1] * w;
+    Nz = (Nn[3 * i0 + 2] * u + Nn[3 * i1 + 2] * v) + Nn[3 * i2 + 2] * w;
+}
+
+// bvhLighting.glsl:42-85 computeLighting, direct part (texColor 1): the lights whose
+// shadow-mask bit is clear (evalLighting -> evalSphereLight; an out-of-range light
+// adds nothing), then the sun (evalSunLight), summed in the shader's order.
+__device__ void direct_lit(const SceneView& s, const float* m, float px, float py, float pz, float Nx, float Ny,
+                           float Nz, float ex, float ey, float ez, uint32_t mask, const float* sun, const float* sunc,
+                           float& lx, float& ly, float& lz) {
+    lx = 0.f; ly = 0.f; lz = 0.f;
+    for (uint32_t li = 0; li < s.num_lights && li < 31u; ++li) {
+        if (mask & (1u << (li + 1u))) continue;
+        const float* L = s.lights + 14u * li;
+        if (__float_as_uint(__ldg(L)) != kLightSphere) continue;
+        const float ax = __ldg(L + 1) - px, ay = __ldg(L + 2) - py, az = __ldg(L + 3) - pz;
+        float dd = sqrtf(dot3(ax, ay, az, ax, ay, az));
+        if (dd < __ldg(L + 4)) {
+            const float Lx = ax / dd, Ly = ay / dd, Lz = az / dd;
+            dd = fmaxf(0.01f, dd - __ldg(L + 8));
+            float cx, cy, cz;
+            compute_lighting(m, __ldg(L + 5), __ldg(L + 6), __ldg(L + 7), px, py, pz, Lx, Ly, Lz, Nx, Ny, Nz, ex, ey,
+                             ez, attenuation(dd, __ldg(L + 4)), cx, cy, cz);
+            lx = lx + cx; ly = ly + cy; lz = lz + cz;
+        }
+    }
+    if ((mask & 1u) == 0u) {
+        float cx, cy, cz;
+        compute_lighting(m, sunc[0], sunc[1], sunc[2], px, py, pz, -sun[0], -sun[1], -sun[2], Nx, Ny, Nz, ex, ey, ez,
+                         1.0f, cx, cy, cz);
+        lx = lx + cx; ly = ly + cy; lz = lz + cz;
+    }
+}
+
+// baseRaytracingPass.glsl:81: the colour of a miss, 0.3 * vec3(200, 220, 255) / 255.
+__device__ __forceinline__ void sky_colour(float& lx, float& ly, float& lz) {
+    lx = (0.3f * 200.0f) / 255.0f;
+    ly = (0.3f * 220.0f) / 255.0f;
+    lz = (0.3f * 255.0f) / 255.0f;
+}
+
 // Lit value of one probe ray: bvhLighting.glsl:42-85 computeLighting with NO_LPF
 // (genLightProbField.comp:5), normal from baseRaytracingPass.glsl:38-64, sky
 // colour on a miss (baseRaytracingPass.glsl:81).
@@ -845,54 +904,18 @@ __global__ void __launch_bounds__(256) k_probe_light(SceneView s, ProbeArgs d, c
     const uint4 rec = reinterpret_cast<const uint4*>(out_words)[2u * sample];
     const uint32_t mask = out_words[8u * sample + 4u];
     const float t = __uint_as_float(rec.w);
-    float lx = 0.f, ly = 0.f, lz = 0.f;
+    float lx, ly, lz;
     if (!(t < kTMax)) {
-        lx = (0.3f * 200.0f) / 255.0f;
-        ly = (0.3f * 220.0f) / 255.0f;
-        lz = (0.3f * 255.0f) / 255.0f;
+        sky_colour(lx, ly, lz);
     } else {
         float ox, oy, oz;
         probe_position(d, d.p0 + pl, ox, oy, oz);
         const float4 dir = __ldg(d.dirs + r);
         const float px = ox + dir.x * t, py = oy + dir.y * t, pz = oz + dir.z * t;
-        const uint32_t i0 = rec.x + (rec.y & 0xFFFFu), i1 = rec.x + (rec.y >> 16), i2 = rec.x + (rec.z & 0xFFFFu);
-        const float* P = s.pos;
-        const float v0x = P[3 * i1] - P[3 * i0], v0y = P[3 * i1 + 1] - P[3 * i0 + 1], v0z = P[3 * i1 + 2] - P[3 * i0 + 2];
-        const float v1x = P[3 * i2] - P[3 * i0], v1y = P[3 * i2 + 1] - P[3 * i0 + 1], v1z = P[3 * i2 + 2] - P[3 * i0 + 2];
-        const float v2x = px - P[3 * i0], v2y = py - P[3 * i0 + 1], v2z = pz - P[3 * i0 + 2];
-        const float d00 = dot3(v0x, v0y, v0z, v0x, v0y, v0z), d01 = dot3(v0x, v0y, v0z, v1x, v1y, v1z);
-        const float d11 = dot3(v1x, v1y, v1z, v1x, v1y, v1z);
-        const float d20 = dot3(v2x, v2y, v2z, v0x, v0y, v0z), d21 = dot3(v2x, v2y, v2z, v1x, v1y, v1z);
-        const float denom = d00 * d11 - d01 * d01;
-        const float v = (d11 * d20 - d01 * d21) / denom;
-        const float w = (d00 * d21 - d01 * d20) / denom;
-        const float u = 1.0f - v - w;
-        const float* Nn = s.nrm;
-        const float Nx = (Nn[3 * i0] * u + Nn[3 * i1] * v) + Nn[3 * i2] * w;
-        const float Ny = (Nn[3 * i0 + 1] * u + Nn[3 * i1 + 1] * v) + Nn[3 * i2 + 1] * w;
-        const float Nz = (Nn[3 * i0 + 2] * u + Nn[3 * i1 + 2] * v) + Nn[3 * i2 + 2] * w;
+        float Nx, Ny, Nz;
+        hit_normal(s, rec, px, py, pz, Nx, Ny, Nz);
         const float* m = s.materials + 12u * (rec.z >> 16);
-        for (uint32_t li = 0; li < s.num_lights && li < 31u; ++li) {
-            if (mask & (1u << (li + 1u))) continue;
-            const float* L = s.lights + 14u * li;
-            if (__float_as_uint(__ldg(L)) != kLightSphere) continue;
-            const float ax = __ldg(L + 1) - px, ay = __ldg(L + 2) - py, az = __ldg(L + 3) - pz;
-            float dd = sqrtf(dot3(ax, ay, az, ax, ay, az));
-            if (dd < __ldg(L + 4)) {
-                const float Lx = ax / dd, Ly = ay / dd, Lz = az / dd;
-                dd = fmaxf(0.01f, dd - __ldg(L + 8));
-                float cx, cy, cz;
-                compute_lighting(m, __ldg(L + 5), __ldg(L + 6), __ldg(L + 7), px, py, pz, Lx, Ly, Lz, Nx, Ny, Nz, ox,
-                                 oy, oz, attenuation(dd, __ldg(L + 4)), cx, cy, cz);
-                lx = lx + cx; ly = ly + cy; lz = lz + cz;
-            }
-        }
-        if ((mask & 1u) == 0u) {
-            float cx, cy, cz;
-            compute_lighting(m, d.sunc[0], d.sunc[1], d.sunc[2], px, py, pz, -d.sun[0], -d.sun[1], -d.sun[2], Nx, Ny,
-                             Nz, ox, oy, oz, 1.0f, cx, cy, cz);
-            lx = lx + cx; ly = ly + cy; lz = lz + cz;
-        }
+        direct_lit(s, m, px, py, pz, Nx, Ny, Nz, ox, oy, oz, mask, d.sun, d.sunc, lx, ly, lz);
     }
     irr[3u * sample] = lx;
     irr[3u * sample + 1u] = ly;
@@ -959,6 +982,152 @@ __global__ void __launch_bounds__(128) k_probe_accum(ProbeArgs d, const float* i
             o[3 * q + 2] = sb * inv;
         }
     }
+}
+
+// ------------------------------------------------------------ camera lighting step
+__device__ __forceinline__ float mixf(float a, float b, float x) { return a * (1.0f - x) + b * x; }   // GLSL mix
+
+// fetchSH_inline.glsl:82-118 sampleSH9 with the probe mask, for one image channel:
+// v[x + 2y + 4z] are the corner values, mask bit (x + 2y + 4z) set = corner
+// masked; the shader's lerp tree, so the shader's rounding.
+__device__ __forceinline__ float masked_trilinear(const float (&v)[8], float fx, float fy, float fz, uint32_t mask) {
+    const bool m0 = !(mask & 1u), m1 = !(mask & 2u), m2 = !(mask & 4u), m3 = !(mask & 8u);
+    const bool m4 = !(mask & 16u), m5 = !(mask & 32u), m6 = !(mask & 64u), m7 = !(mask & 128u);
+    float x0 = m0 && m1 ? mixf(v[0], v[1], fx) : (m0 ? v[0] : v[1]);
+    float x1 = m2 && m3 ? mixf(v[2], v[3], fx) : (m2 ? v[2] : v[3]);
+    const bool b00 = m0 || m1, b10 = m2 || m3;
+    const float z0 = b00 && b10 ? mixf(x0, x1, fy) : (b00 ? x0 : x1);
+    x0 = m4 && m5 ? mixf(v[4], v[5], fx) : (m4 ? v[4] : v[5]);
+    x1 = m6 && m7 ? mixf(v[6], v[7], fx) : (m6 ? v[6] : v[7]);
+    const bool b01 = m4 || m5, b11 = m6 || m7;
+    const float z1 = b01 && b11 ? mixf(x0, x1, fy) : (b01 ? x0 : x1);
+    const bool bxy0 = b00 || b10, bxy1 = b01 || b11;
+    return bxy0 && bxy1 ? mixf(z0, z1, fz) : (bxy0 ? z0 : z1);
+}
+
+// bvhLighting.glsl:24-40 computeLPFLighting with USE_LPF_MASK: probe-grid uvw
+// (lightprobHelpers.glsl:10-14,71-77), masked SH9 sample of the 7 RGBA16F images
+// (fetchSH_inline.glsl:6-31 channel layout), evalSH (lightprobHelpers.glsl:90-101)
+// and computeIndirectLighting (core/lighting.glsl:59-74, texColor 1).
+__device__ void lpf_lit(const tim_rt_pass_data& pd, const uint2* sh16, const float* m, float px, float py, float pz,
+                        float Nx, float Ny, float Nz, uint32_t mask, float& lx, float& ly, float& lz) {
+    const uint32_t rx = pd.lpfResolution[0], ry = pd.lpfResolution[1], rz = pd.lpfResolution[2];
+    const float sx = (pd.sceneMaxExtent[0] - pd.sceneMinExtent[0]) / (float)rx;
+    const float sy = (pd.sceneMaxExtent[1] - pd.sceneMinExtent[1]) / (float)ry;
+    const float sz = (pd.sceneMaxExtent[2] - pd.sceneMinExtent[2]) / (float)rz;
+    float u = (px - pd.sceneMinExtent[0]) / sx - 0.5f;
+    float v = (py - pd.sceneMinExtent[1]) / sy - 0.5f;
+    float w = (pz - pd.sceneMinExtent[2]) / sz - 0.5f;
+    u = fminf(fmaxf(u, 0.0f), (float)rx - 1.0f);
+    v = fminf(fmaxf(v, 0.0f), (float)ry - 1.0f);
+    w = fminf(fmaxf(w, 0.0f), (float)rz - 1.0f);
+    // min(int(uvw), res - 2) in GLSL's int -> uint conversion
+    const uint32_t ix = min((uint32_t)(int)u, rx - 2u), iy = min((uint32_t)(int)v, ry - 2u),
+                   iz = min((uint32_t)(int)w, rz - 2u);
+    const float fx = u - (float)(int)ix, fy = v - (float)(int)iy, fz = w - (float)(int)iz;
+    const uint64_t img = (uint64_t)rx * ry * rz;
+    float ch[7][4];
+#pragma unroll
+    for (int k = 0; k < 7; ++k) {
+        float c[4][8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const uint64_t texel = ((uint64_t)(iz + ((q >> 2) & 1)) * ry + (iy + ((q >> 1) & 1))) * rx + ix + (q & 1);
+            const uint2 h = __ldg(sh16 + k * img + texel);
+            c[0][q] = __half2float(__ushort_as_half((unsigned short)(h.x & 0xFFFFu)));
+            c[1][q] = __half2float(__ushort_as_half((unsigned short)(h.x >> 16)));
+            c[2][q] = __half2float(__ushort_as_half((unsigned short)(h.y & 0xFFFFu)));
+            c[3][q] = __half2float(__ushort_as_half((unsigned short)(h.y >> 16)));
+        }
+#pragma unroll
+        for (int cc = 0; cc < 4; ++cc) ch[k][cc] = masked_trilinear(c[cc], fx, fy, fz, mask);
+    }
+    const float c1 = 0.429043f, c2 = 0.511664f, c3 = 0.743125f, c4 = 0.886227f, c5 = 0.247708f;
+    float L[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        // SH9Color.w[j] from the storeSH9 layout: w0 = image 0; w1..4 = images 1/3/5, w5..8 = images 2/4/6
+        const float w0 = ch[0][c], w1 = ch[1 + 2 * c][0], w2 = ch[1 + 2 * c][1], w3 = ch[1 + 2 * c][2];
+        const float w4 = ch[1 + 2 * c][3], w5 = ch[2 + 2 * c][0], w6 = ch[2 + 2 * c][1], w7 = ch[2 + 2 * c][2];
+        const float w8 = ch[2 + 2 * c][3];
+        // SH_Y00 0, Y11 1, Y10 2, Y1_1 3, Y21 4, Y2_1 5, Y2_2 6, Y20 7, Y22 8 (lightprob/lightprob.glsl)
+        const float t1 = (c1 * (Nx * Nx - Ny * Ny)) * w8;
+        const float t2 = ((c3 * w7) * Nz) * Nz;
+        const float t3 = c4 * w0;
+        const float t4 = c5 * w7;
+        const float t5 = (2.0f * c1) * (((w6 * Nx) * Ny + (w4 * Nx) * Nz) + (w5 * Ny) * Nz);
+        const float t6 = (2.0f * c2) * ((w1 * Nx + w3 * Ny) + w2 * Nz);
+        L[c] = ((((t1 + t2) + t3) - t4) + t5) + t6;
+    }
+    const uint32_t type = __float_as_uint(__ldg(m));
+    const float cr = __ldg(m + 4), cg = __ldg(m + 5), cb = __ldg(m + 6);
+    const float pi = 3.14159265359f;   // TIM_PI, core/math.glsl:4
+    if (type == 5u) {                  // Material_PBR
+        const float k = 1.0f - __ldg(m + 8);
+        lx = ((k * cr) * L[0]) / pi; ly = ((k * cg) * L[1]) / pi; lz = ((k * cb) * L[2]) / pi;
+    } else if (type == 2u) {           // Material_Lambert
+        lx = (L[0] * cr) / pi; ly = (L[1] * cg) / pi; lz = (L[2] * cb) / pi;
+    } else {
+        lx = ly = lz = 0.0f;
+    }
+}
+
+// cameraPass.comp:78-88, the lighting step (RayTracingPass::lightingPass,
+// raytracingPass.cpp:113-135: USE_LPF, USE_LPF_MASK). One thread per output pixel
+// in row-major order (coalesced record reads and image writes); the pixel's ray is
+// the tracing step's (cameraPass.comp:46-56), output row 0 is never reached by the
+// reference's dispatch and is written as 0.
+__global__ void __launch_bounds__(256) k_shade_camera(SceneView s, tim_rt_pass_data pd, uint32_t flags,
+                                                      const uint4* tracing, const uint2* sh16, uint2* out16,
+                                                      float* out32) {
+    const uint32_t W = pd.frameSize[0], H = pd.frameSize[1];
+    const uint64_t pix = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (pix >= (uint64_t)W * H) return;
+    const uint32_t px = (uint32_t)(pix % W), py = (uint32_t)(pix / W);
+    float lx = 0.f, ly = 0.f, lz = 0.f;
+    bool reached = py != 0u;
+    if (reached) {
+        const uint4 rec = __ldg(tracing + 2u * pix);
+        const uint4 masks = __ldg(tracing + 2u * pix + 1u);
+        const float t = __uint_as_float(rec.w);
+        if (!(t < kTMax)) {
+            sky_colour(lx, ly, lz);
+        } else {
+            const uint32_t ngy16 = 16u * ((H + 15u) / 16u);
+            float dx, dy, dz;
+            camera_ray(pd, px, ngy16 - py, dx, dy, dz);
+            const float ex = pd.cameraPos[0], ey = pd.cameraPos[1], ez = pd.cameraPos[2];
+            const float hx = ex + dx * t, hy = ey + dy * t, hz = ez + dz * t;
+            float Nx, Ny, Nz;
+            hit_normal(s, rec, hx, hy, hz, Nx, Ny, Nz);
+            const float* m = s.materials + 12u * (rec.z >> 16);
+            direct_lit(s, m, hx, hy, hz, Nx, Ny, Nz, ex, ey, ez, masks.x, pd.sunDir, pd.sunColor, lx, ly, lz);
+            if (!(flags & TIM_RT_SHADE_NO_LPF)) {
+                float ix, iy, iz;
+                lpf_lit(pd, sh16, m, hx, hy, hz, Nx, Ny, Nz, masks.y, ix, iy, iz);
+                lx = lx + ix; ly = ly + iy; lz = lz + iz;
+            }
+        }
+    }
+    const uint32_t hr = __half_as_ushort(__float2half_rn(lx)), hg = __half_as_ushort(__float2half_rn(ly));
+    const uint32_t hb = __half_as_ushort(__float2half_rn(lz));
+    const uint32_t ha = reached ? 0x3C00u : 0u;   // alpha 1
+    out16[pix] = make_uint2(hr | (hg << 16), hb | (ha << 16));
+    if (out32) {
+        out32[3u * pix] = lx;
+        out32[3u * pix + 1u] = ly;
+        out32[3u * pix + 2u] = lz;
+    }
+}
+
+cudaError_t launch_shade(const SceneView& s, const tim_rt_pass_data& pd, uint32_t flags, const uint32_t* tracing,
+                         const uint16_t* sh16, uint16_t* out16, float* out32, cudaStream_t stream) {
+    const uint64_t npix = (uint64_t)pd.frameSize[0] * pd.frameSize[1];
+    if (npix == 0) return cudaSuccess;
+    k_shade_camera<<<(unsigned)((npix + 255u) / 256u), 256, 0, stream>>>(
+        s, pd, flags, reinterpret_cast<const uint4*>(tracing), reinterpret_cast<const uint2*>(sh16),
+        reinterpret_cast<uint2*>(out16), out32);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_probes(const SceneView& s, const ProbeArgs& d, uint32_t* out, uint32_t* leaf_nid, tim_rt_ray* q_rays,
