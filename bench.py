@@ -674,6 +674,21 @@ def main():
                                   "tri_tests": stc.secondary_tri_tests / r, "node_reloads": stc.secondary_node_reloads / r,
                                   "bytes": abytes / r}}
     l2_gbs = N.measure_l2_gbs(local)
+    # the lighting step of the same frame (tim_rt_shade_camera) on the quantised
+    # frame's records, with a seeded FP16 light-probe field of the frame's grid
+    cam_h = outs["wide"].cpu().numpy().view(np.uint32).reshape(-1, 8)
+    lres = [int(x) for x in np.asarray(pd["lpfResolution"]).reshape(-1)[:3]]
+    field = np.random.default_rng(3).uniform(0.0, 1.0, size=(7, lres[2], lres[1], lres[0], 4)).astype(np.float16)
+    sk = []
+    for _ in range(7):
+        img16, _, st = ctx.shade_camera(sid, pd, cam_h, field.view(np.uint16))
+        sk.append(st.kernel_ms)
+    shade_ms = float(np.median(sk[2:]))
+    shade = {"kernel_ms": shade_ms, "mpix_per_s": W * H / shade_ms / 1e3,
+             "lit_pixels": int((img16[:, 3] != 0).sum()),
+             "workload": "cameraPass.comp lighting step of the 1080p frame: direct light of the 16 lights and the "
+                         f"sun from the shadow masks, probe-masked SH9 sample of a {lres[0]}x{lres[1]}x{lres[2]} "
+                         "FP16 probe field, RGBA16F out"}
     # the batched multi-scene and serving workloads (one GPU; skipped in scaling runs)
     batched = serving = None
     if world == 1 and not args.no_batched:
@@ -723,6 +738,7 @@ def main():
             line["batched"] = batched
         if probes:
             line["probes"] = probes
+        line["shade"] = shade
         if serving:
             line["serving"] = serving
             r8 = serving["rates"][1]
