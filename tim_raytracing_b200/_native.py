@@ -34,7 +34,7 @@ EXPORTED = [
     "tim_rt_server_submit", "tim_rt_server_wait", "tim_rt_server_drain", "tim_rt_server_stats_get",
     "tim_rt_server_destroy", "tim_rt_verify_hits", "tim_rt_server_submit_probes", "tim_rt_bvh_file_write",
     "tim_rt_bvh_file_read", "tim_rt_bvh_file_info", "tim_rt_bvh_file_free", "tim_rt_upload_bvh_file",
-    "tim_rt_shade_camera", "tim_rt_shade_camera_dev",
+    "tim_rt_shade_camera", "tim_rt_shade_camera_dev", "tim_rt_build_bvh_gpu",
 ]
 SORT_NONE, SORT_OCTANT, SORT_MORTON = 0, 1, 2
 BATCH_WIDE = 0x100
@@ -201,6 +201,8 @@ def lib() -> ctypes.CDLL:
     L.tim_rt_bvh_file_free.restype = None
     L.tim_rt_upload_bvh_file.argtypes = [vp, ctypes.c_char_p, u32, ctypes.POINTER(u32)]
     L.tim_rt_shade_camera.argtypes = [vp, u32, vp, u32, vp, vp, vp, vp, ctypes.POINTER(Stats)]
+    L.tim_rt_build_bvh_gpu.argtypes = [vp, vp, u32, vp, u32, vp, u32, vp, u32, ctypes.POINTER(BuildParams),
+                                       ctypes.POINTER(vp)]
     L.tim_rt_shade_camera_dev.argtypes = [vp, u32, vp, u32, vp, vp, vp, vp, vp]
     for name in EXPORTED:
         if name not in ("tim_rt_version", "tim_rt_last_error", "tim_rt_build_params_default", "tim_rt_bvh_blob_free",
@@ -273,8 +275,9 @@ def build_params(**kw) -> BuildParams:
     return p
 
 
-def build_bvh(scene, **params) -> BvhImage:
-    """Product-side builder (tim_rt_build_bvh) over a scenes.Scene."""
+def build_bvh(scene, ctx: "Context" = None, **params) -> BvhImage:
+    """Product-side builder over a scenes.Scene: tim_rt_build_bvh (binned SAH on the
+    host), or tim_rt_build_bvh_gpu on ctx's GPU when a context is given."""
     L = lib()
     pos = np.ascontiguousarray(scene.positions, np.float32)
     rec = np.ascontiguousarray(scene.tri_records())
@@ -284,8 +287,12 @@ def build_bvh(scene, **params) -> BvhImage:
     nl = len(lights) // 56
     p = build_params(**params)
     out = ctypes.c_void_p()
-    _check(L.tim_rt_build_bvh(pos.ctypes.data, pos.shape[0], rec.ctypes.data, rec.shape[0], mats, nmat,
-                              lights if nl else None, nl, ctypes.byref(p), ctypes.byref(out)))
+    if ctx is not None:
+        _check(L.tim_rt_build_bvh_gpu(ctx._c, pos.ctypes.data, pos.shape[0], rec.ctypes.data, rec.shape[0], mats, nmat,
+                                      lights if nl else None, nl, ctypes.byref(p), ctypes.byref(out)))
+    else:
+        _check(L.tim_rt_build_bvh(pos.ctypes.data, pos.shape[0], rec.ctypes.data, rec.shape[0], mats, nmat,
+                                  lights if nl else None, nl, ctypes.byref(p), ctypes.byref(out)))
     try:
         bp, size = ctypes.c_void_p(), ctypes.c_uint64()
         ranges = np.zeros((7, 2), np.uint32)

@@ -1,0 +1,539 @@
+// bvh_build_gpu.cu -- GPU BVH builder writing the reference's fillGpuBuffer
+// layout (BVHBuilder.cpp:1319-1534), with the node numbering and leaf-data order
+// of the host builder (bvh_build.cpp), for fast scene turnaround:
+//   1. triangle boxes and centroids, centroid bounds;
+//   2. 63-bit Morton codes of the centroids, radix sort (CUB, stable);
+//   3. radix tree over the sorted codes (Karras 2012, "Maximizing parallelism in
+//      the construction of BVHs, octrees, and k-d trees"): internal node i covers
+//      a key range split at its highest differing bit, equal keys split by index;
+//   4. subtrees of at most max_leaf_size triangles become leaves;
+//   5. bottom-up boxes and internal-node counts (the second child to arrive at a
+//      node merges), then per node its depth and pre-order rank among internal
+//      nodes by walking to the root, which gives the host builder's numbering:
+//      root 0, the children of the internal node of rank r at 2r+1 and 2r+2;
+//   6. leaf sizes, exclusive scan in node order, leaf data (header, triangle
+//      records in Morton order, light ids: sphere vs widened leaf box, at most
+//      15) and node records (parent, sibling, children, leaf offset, widened
+//      child boxes), copied back into the host image.
+// Trees deeper than max_depth (the reference's traversal keeps a 32-bit
+// bitstack) are refused with TIM_RT_EUNSUPPORTED.
+#include <cuda_runtime.h>
+#include <cub/cub.cuh>
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+#include "context.h"
+
+struct tim_rt_bvh_blob {   // same definition as bvh_build.cpp
+    std::vector<uint8_t> bytes;
+    uint32_t ranges[7][2];
+    tim_rt_push_constants pc;
+    float aabb[6];
+};
+
+namespace timrt {
+namespace {
+
+constexpr uint32_t kNone = 0x3FFFFFFFu;
+
+struct Aabb {
+    float lo[3], hi[3];
+};
+
+__device__ __forceinline__ uint32_t f2ord(float f) {   // order-preserving float -> uint
+    const uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float ord2f(uint32_t u) {
+    return __uint_as_float((u & 0x80000000u) ? (u & 0x7FFFFFFFu) : ~u);
+}
+
+// Triangle boxes and centroids (the host builder's: box of the three vertices,
+// centroid = its midpoint); bounds of the centroids; bad indices or non-finite
+// positions set err.
+__global__ void k_tri_boxes(const float* pos, uint32_t nv, const uint32_t* tri, uint32_t n, Aabb* boxes,
+                            float4* cen, uint32_t* cbounds, uint32_t* err) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    float c[3] = {0.f, 0.f, 0.f};
+    bool ok = false;
+    if (t < n) {
+        const uint32_t r0 = tri[3 * t], r1 = tri[3 * t + 1], r2 = tri[3 * t + 2];
+        const uint64_t i0 = (uint64_t)r0 + (r1 & 0xFFFFu), i1 = (uint64_t)r0 + (r1 >> 16), i2 = (uint64_t)r0 + (r2 & 0xFFFFu);
+        if (i0 >= nv || i1 >= nv || i2 >= nv) {
+            atomicOr(err, 1u);
+        } else {
+            Aabb b;
+            bool fin = true;
+            for (int a = 0; a < 3; ++a) {
+                const float p0 = pos[3 * i0 + a], p1 = pos[3 * i1 + a], p2 = pos[3 * i2 + a];
+                b.lo[a] = fminf(fminf(p0, p1), p2);
+                b.hi[a] = fmaxf(fmaxf(p0, p1), p2);
+                fin = fin && isfinite(p0) && isfinite(p1) && isfinite(p2);
+                c[a] = 0.5f * (b.lo[a] + b.hi[a]);
+            }
+            if (!fin) atomicOr(err, 2u);
+            boxes[t] = b;
+            cen[t] = make_float4(c[0], c[1], c[2], 0.f);
+            ok = fin;
+        }
+    }
+    // block-wide min / max of the centroids, then one atomic per block and axis
+    __shared__ uint32_t smin[3], smax[3];
+    if (threadIdx.x < 3) { smin[threadIdx.x] = 0xFFFFFFFFu; smax[threadIdx.x] = 0u; }
+    __syncthreads();
+    if (ok)
+        for (int a = 0; a < 3; ++a) {
+            atomicMin(&smin[a], f2ord(c[a]));
+            atomicMax(&smax[a], f2ord(c[a]));
+        }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        atomicMin(cbounds + threadIdx.x, smin[threadIdx.x]);
+        atomicMax(cbounds + 3 + threadIdx.x, smax[threadIdx.x]);
+    }
+}
+
+__device__ __forceinline__ uint64_t spread21(uint64_t v) {
+    v &= 0x1FFFFFull;
+    v = (v | (v << 32)) & 0x1F00000000FFFFull;
+    v = (v | (v << 16)) & 0x1F0000FF0000FFull;
+    v = (v | (v << 8)) & 0x100F00F00F00F00Full;
+    v = (v | (v << 4)) & 0x10C30C30C30C30C3ull;
+    v = (v | (v << 2)) & 0x1249249249249249ull;
+    return v;
+}
+
+__global__ void k_morton(const float4* cen, uint32_t n, const uint32_t* cbounds, uint64_t* keys, uint32_t* vals) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const float4 c = cen[t];
+    const float cv[3] = {c.x, c.y, c.z};
+    uint64_t q[3];
+    for (int a = 0; a < 3; ++a) {
+        const float lo = ord2f(cbounds[a]), hi = ord2f(cbounds[3 + a]);
+        const float ext = hi - lo;
+        float u = ext > 0.f ? (cv[a] - lo) / ext : 0.f;
+        u = fminf(fmaxf(u, 0.f), 1.f);
+        q[a] = (uint64_t)(u * 2097151.0f);
+    }
+    keys[t] = (spread21(q[0]) << 2) | (spread21(q[1]) << 1) | spread21(q[2]);
+    vals[t] = t;
+}
+
+// Common-prefix length of keys i and j (equal keys: 64 + that of the indices).
+__device__ __forceinline__ int delta(const uint64_t* k, uint32_t n, int i, int j) {
+    if (j < 0 || j >= (int)n) return -1;
+    const uint64_t a = k[i], b = k[j];
+    return a == b ? 64 + __clz((uint32_t)(i ^ j)) : __clzll(a ^ b);
+}
+
+// Radix tree: internal node i in [0, n-2], handle i; leaf j at handle n-1+j.
+__global__ void k_radix_tree(const uint64_t* k, uint32_t n, uint32_t* left, uint32_t* right, uint32_t* first,
+                             uint32_t* last, uint32_t* parent) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (int)n - 1) return;
+    const int d = (delta(k, n, i, i + 1) - delta(k, n, i, i - 1)) >= 0 ? 1 : -1;
+    const int dmin = delta(k, n, i, i - d);
+    int lmax = 2;
+    while (delta(k, n, i, i + lmax * d) > dmin) lmax <<= 1;
+    int l = 0;
+    for (int t = lmax >> 1; t >= 1; t >>= 1)
+        if (delta(k, n, i, i + (l + t) * d) > dmin) l += t;
+    const int j = i + l * d;
+    const int dnode = delta(k, n, i, j);
+    int s = 0;
+    for (int div = 2;; div <<= 1) {
+        const int t = (l + div - 1) / div;
+        if (delta(k, n, i, i + (s + t) * d) > dnode) s += t;
+        if (t <= 1) break;
+    }
+    const int gamma = i + s * d + min(d, 0);
+    const int lo = min(i, j), hi = max(i, j);
+    const uint32_t L = lo == gamma ? (n - 1u) + (uint32_t)gamma : (uint32_t)gamma;
+    const uint32_t R = hi == gamma + 1 ? (n - 1u) + (uint32_t)(gamma + 1) : (uint32_t)(gamma + 1);
+    left[i] = L;
+    right[i] = R;
+    first[i] = (uint32_t)lo;
+    last[i] = (uint32_t)hi;
+    parent[L] = (uint32_t)i;
+    parent[R] = (uint32_t)i;
+    if (i == 0) parent[0] = kNone;
+}
+
+// A box written by another thread, read past L1 (after its writer's fence).
+__device__ __forceinline__ Aabb load_box_cg(const Aabb* p) {
+    const float* f = reinterpret_cast<const float*>(p);
+    Aabb b;
+    for (int a = 0; a < 3; ++a) {
+        b.lo[a] = __ldcg(f + a);
+        b.hi[a] = __ldcg(f + 3 + a);
+    }
+    return b;
+}
+
+__device__ __forceinline__ uint32_t hsize(uint32_t h, uint32_t n, const uint32_t* first, const uint32_t* last) {
+    return h < n - 1u ? last[h] - first[h] + 1u : 1u;
+}
+__device__ __forceinline__ uint32_t hfirst(uint32_t h, uint32_t n, const uint32_t* first) {
+    return h < n - 1u ? first[h] : h - (n - 1u);
+}
+
+// From every leaf of the final tree (a handle of at most max_leaf triangles whose
+// parent has more) up to the root: the second child to arrive at a node merges the
+// boxes and internal counts of both children and goes on.
+__global__ void k_bottom_up(uint32_t n, uint32_t max_leaf, const uint32_t* left, const uint32_t* right,
+                            const uint32_t* first, const uint32_t* last, const uint32_t* parent, const uint32_t* order,
+                            const Aabb* tri_box, Aabb* box, uint32_t* icount, uint32_t* arrive) {
+    const uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
+    if (h >= 2u * n - 1u || h == 0u) return;
+    const uint32_t sz = hsize(h, n, first, last);
+    if (sz > max_leaf || hsize(parent[h], n, first, last) <= max_leaf) return;
+    Aabb b;
+    for (int a = 0; a < 3; ++a) { b.lo[a] = INFINITY; b.hi[a] = -INFINITY; }
+    const uint32_t f = hfirst(h, n, first);
+    for (uint32_t q = 0; q < sz; ++q) {
+        const Aabb t = tri_box[order[f + q]];
+        for (int a = 0; a < 3; ++a) { b.lo[a] = fminf(b.lo[a], t.lo[a]); b.hi[a] = fmaxf(b.hi[a], t.hi[a]); }
+    }
+    box[h] = b;
+    icount[h] = 0;
+    uint32_t cur = h;
+    while (cur != 0u) {
+        const uint32_t p = parent[cur];
+        __threadfence();
+        if (atomicAdd(arrive + p, 1u) == 0u) return;   // the sibling finishes this node
+        __threadfence();
+        const uint32_t L = left[p], R = right[p];
+        const Aabb bl = load_box_cg(box + L);
+        const Aabb br = load_box_cg(box + R);
+        Aabb m;
+        for (int a = 0; a < 3; ++a) { m.lo[a] = fminf(bl.lo[a], br.lo[a]); m.hi[a] = fmaxf(bl.hi[a], br.hi[a]); }
+        box[p] = m;
+        icount[p] = 1u + __ldcg(icount + L) + __ldcg(icount + R);
+        cur = p;
+    }
+}
+
+// Per node of the final tree: depth, and output id from the pre-order rank of
+// internal nodes (rank(child) = rank(parent) + 1, plus the left sibling's internal
+// count for a right child); the root is 0, the children of rank r are 2r+1, 2r+2.
+__global__ void k_number(uint32_t n, uint32_t max_leaf, const uint32_t* left, const uint32_t* first,
+                         const uint32_t* last, const uint32_t* parent, const uint32_t* icount, uint32_t* out_id,
+                         uint32_t* rank_of, uint32_t* max_depth) {
+    const uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
+    if (h >= 2u * n - 1u) return;
+    const uint32_t sz = hsize(h, n, first, last);
+    const bool in_tree = h == 0u || hsize(parent[h], n, first, last) > max_leaf;
+    if (!in_tree) return;
+    // rank of h (meaningful for internal nodes) and depth
+    uint32_t rank = 0, depth = 0, cur = h;
+    while (cur != 0u) {
+        const uint32_t p = parent[cur];
+        rank += 1u;
+        if (left[p] != cur) rank += icount[left[p]];
+        ++depth;
+        cur = p;
+    }
+    if (sz > max_leaf) rank_of[h] = rank;
+    atomicMax(max_depth, depth);
+    if (h == 0u) {
+        out_id[0] = 0u;
+        return;
+    }
+    const uint32_t p = parent[h];
+    uint32_t prank = 0, c2 = p;
+    while (c2 != 0u) {
+        const uint32_t pp = parent[c2];
+        prank += 1u;
+        if (left[pp] != c2) prank += icount[left[pp]];
+        c2 = pp;
+    }
+    out_id[h] = 1u + 2u * prank + (left[p] == h ? 0u : 1u);
+}
+
+__device__ __forceinline__ float widen_lo(float x) { return x - (1e-6f + fabsf(x) * 9.5367431640625e-07f); }   // 2^-20
+__device__ __forceinline__ float widen_hi(float x) { return x + (1e-6f + fabsf(x) * 9.5367431640625e-07f); }
+
+// Leaf sizes (header + 3 words per triangle + light ids), indexed by output id;
+// internal nodes 0. Light ids: sphere (centre, radius) vs the widened leaf box,
+// at most 15 (BVHBuilder.cpp:36-42,749-756 with the 4-bit count kept below 16).
+__global__ void k_leaf_sizes(uint32_t n, uint32_t max_leaf, const uint32_t* first, const uint32_t* last,
+                             const uint32_t* parent, const uint32_t* out_id, const Aabb* box, const float* lights,
+                             uint32_t num_lights, uint32_t* leaf_size, uint32_t* leaf_nl) {
+    const uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
+    if (h >= 2u * n - 1u || h == 0u) return;
+    const uint32_t sz = hsize(h, n, first, last);
+    if (sz > max_leaf || hsize(parent[h], n, first, last) <= max_leaf) return;
+    const Aabb b = box[h];
+    float lo[3], hi[3];
+    for (int a = 0; a < 3; ++a) { lo[a] = widen_lo(b.lo[a]); hi[a] = widen_hi(b.hi[a]); }
+    uint32_t nl = 0;
+    for (uint32_t l = 0; l < num_lights && nl < 15u; ++l) {
+        const float* f = lights + 14u * l + 1u;
+        const float r = f[3];
+        float d2 = 0.f;
+        for (int a = 0; a < 3; ++a) {
+            const float c = fminf(fmaxf(f[a], lo[a]), hi[a]);
+            d2 += (c - f[a]) * (c - f[a]);
+        }
+        if (d2 < r * r) ++nl;
+    }
+    const uint32_t id = out_id[h];
+    leaf_size[id] = 1u + 3u * sz + nl;
+    leaf_nl[id] = nl;
+}
+
+// Node records (packNodeData, BVHBuilder.cpp:1283-1317) and leaf data.
+__global__ void k_emit(uint32_t n, uint32_t max_leaf, const uint32_t* left, const uint32_t* right,
+                       const uint32_t* first, const uint32_t* last, const uint32_t* parent, const uint32_t* out_id,
+                       const Aabb* box, const uint32_t* order, const uint32_t* tri, const float* lights,
+                       uint32_t num_lights, const uint32_t* leaf_off, const uint32_t* leaf_nl, uint32_t* nodes,
+                       uint32_t* leaf) {
+    const uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
+    if (h >= 2u * n - 1u) return;
+    const uint32_t sz = hsize(h, n, first, last);
+    const bool in_tree = h == 0u || hsize(parent[h], n, first, last) > max_leaf;
+    if (!in_tree) return;
+    const bool inner = sz > max_leaf;
+    const uint32_t id = out_id[h];
+    uint32_t* w = nodes + 16ull * id;
+    if (h == 0u) {
+        w[0] = kNone;
+        w[1] = kNone;
+    } else {
+        const uint32_t p = parent[h];
+        const uint32_t sib = left[p] == h ? right[p] : left[p];
+        w[0] = out_id[p];
+        w[1] = out_id[sib] | (hsize(sib, n, first, last) <= max_leaf ? 0x80000000u : 0u);
+    }
+    float f[12] = {};
+    if (inner) {
+        const uint32_t L = left[h], R = right[h];
+        w[2] = out_id[L] | (hsize(L, n, first, last) <= max_leaf ? 0x80000000u : 0u) |
+               (hsize(R, n, first, last) <= max_leaf ? 0x40000000u : 0u);
+        w[3] = 0xFFFFFFFFu;
+        const Aabb b0 = box[L], b1 = box[R];
+        f[0] = widen_lo(b0.lo[0]); f[1] = widen_lo(b0.lo[1]); f[2] = widen_hi(b0.hi[0]); f[3] = widen_hi(b0.hi[1]);
+        f[4] = widen_lo(b1.lo[0]); f[5] = widen_lo(b1.lo[1]); f[6] = widen_hi(b1.hi[0]); f[7] = widen_hi(b1.hi[1]);
+        f[8] = widen_lo(b0.lo[2]); f[9] = widen_hi(b0.hi[2]); f[10] = widen_lo(b1.lo[2]); f[11] = widen_hi(b1.hi[2]);
+    } else {
+        w[2] = kNone;
+        const uint32_t off = leaf_off[id], nl = leaf_nl[id];
+        w[3] = off;
+        uint32_t* o = leaf + off;
+        o[0] = sz | (nl << 28);
+        const uint32_t fs = hfirst(h, n, first);
+        for (uint32_t q = 0; q < sz; ++q) {
+            const uint32_t t = order[fs + q];
+            o[1 + 3 * q] = tri[3 * t];
+            o[2 + 3 * q] = tri[3 * t + 1];
+            o[3 + 3 * q] = tri[3 * t + 2];
+        }
+        // light ids, the same test as k_leaf_sizes
+        const Aabb b = box[h];
+        float lo[3], hi[3];
+        for (int a = 0; a < 3; ++a) { lo[a] = widen_lo(b.lo[a]); hi[a] = widen_hi(b.hi[a]); }
+        uint32_t k = 0;
+        for (uint32_t l = 0; l < num_lights && k < nl; ++l) {
+            const float* fl = lights + 14u * l + 1u;
+            const float r = fl[3];
+            float d2 = 0.f;
+            for (int a = 0; a < 3; ++a) {
+                const float c = fminf(fmaxf(fl[a], lo[a]), hi[a]);
+                d2 += (c - fl[a]) * (c - fl[a]);
+            }
+            if (d2 < r * r) o[1 + 3 * sz + k++] = l;
+        }
+    }
+    for (int q = 0; q < 12; ++q) w[4 + q] = __float_as_uint(f[q]);
+}
+
+uint32_t align32(uint32_t x) { return (x + 31u) & ~31u; }
+
+// Device scratch of one build, freed on every exit path.
+struct Scratch {
+    tim_rt_ctx* c;
+    std::vector<DevBuf> bufs;
+    explicit Scratch(tim_rt_ctx* cc) : c(cc) {}
+    ~Scratch() {
+        for (DevBuf& b : bufs) dev_free(c, b);
+    }
+    template <class T>
+    int get(T*& p, uint64_t count) {
+        bufs.emplace_back();
+        const int rc = dev_alloc(c, bufs.back(), std::max<uint64_t>(16, sizeof(T) * count));
+        p = static_cast<T*>(bufs.back().ptr);
+        return rc;
+    }
+};
+
+#define GB_CUDA(x)                                                                        \
+    do {                                                                                  \
+        cudaError_t e_ = (x);                                                             \
+        if (e_ != cudaSuccess) {                                                          \
+            set_error(std::string("tim_rt_build_bvh_gpu: ") + cudaGetErrorString(e_));    \
+            return TIM_RT_EDEVICE;                                                        \
+        }                                                                                 \
+    } while (0)
+
+}  // namespace
+}  // namespace timrt
+
+using namespace timrt;
+
+extern "C" {
+
+int tim_rt_build_bvh_gpu(tim_rt_ctx* c, const float* pos, uint32_t num_vertex, const uint32_t* tri, uint32_t num_tris,
+                         const void* materials, uint32_t num_materials, const void* lights, uint32_t num_lights,
+                         const tim_rt_build_params* params, tim_rt_bvh_blob** out) {
+    int rc = check_ctx(c);
+    if (rc) return rc;
+    if (!out || !pos || !tri || num_tris == 0 || num_vertex == 0) {
+        set_error("tim_rt_build_bvh_gpu: null argument, no triangles or no vertices");
+        return TIM_RT_EINVAL;
+    }
+    *out = nullptr;
+    tim_rt_build_params p;
+    tim_rt_build_params_default(&p);
+    if (params) p = *params;
+    if (p.max_leaf_size == 0 || p.max_leaf_size > 4095u || p.max_depth == 0 || p.max_depth > 32u) {
+        set_error("tim_rt_build_bvh_gpu: max_leaf_size must be 1..4095 and max_depth 1..32");
+        return TIM_RT_EINVAL;
+    }
+    if (num_lights && !lights) {
+        set_error("tim_rt_build_bvh_gpu: lights pointer is null");
+        return TIM_RT_EINVAL;
+    }
+    if (num_tris <= p.max_leaf_size || num_tris >= (1u << 29)) {
+        // a single leaf (or a size the 32-bit handles cannot hold): the host builder
+        return tim_rt_build_bvh(pos, num_vertex, tri, num_tris, materials, num_materials, lights, num_lights, &p, out);
+    }
+    const uint32_t n = num_tris, nh = 2u * n - 1u;
+    cudaStream_t st = c->stream;
+    Scratch S(c);
+    float* d_pos;
+    uint32_t *d_tri, *d_err, *d_cb, *d_vals, *d_order, *d_left, *d_right, *d_first, *d_last, *d_parent, *d_icount,
+        *d_arrive, *d_outid, *d_rank, *d_maxd, *d_lsize, *d_lnl, *d_loff;
+    uint64_t *d_keys, *d_keys2;
+    float4* d_cen;
+    Aabb *d_tbox, *d_box;
+    float* d_lights;
+    if ((rc = S.get(d_pos, 3ull * num_vertex)) || (rc = S.get(d_tri, 3ull * n)) || (rc = S.get(d_err, 8)) ||
+        (rc = S.get(d_cb, 8)) || (rc = S.get(d_tbox, n)) || (rc = S.get(d_cen, n)) || (rc = S.get(d_keys, n)) ||
+        (rc = S.get(d_keys2, n)) || (rc = S.get(d_vals, n)) || (rc = S.get(d_order, n)) ||
+        (rc = S.get(d_left, n)) || (rc = S.get(d_right, n)) || (rc = S.get(d_first, n)) || (rc = S.get(d_last, n)) ||
+        (rc = S.get(d_parent, nh)) || (rc = S.get(d_box, nh)) || (rc = S.get(d_icount, nh)) ||
+        (rc = S.get(d_arrive, n)) || (rc = S.get(d_outid, nh)) || (rc = S.get(d_rank, nh)) ||
+        (rc = S.get(d_maxd, 1)) || (rc = S.get(d_lights, 14ull * std::max(num_lights, 1u))))
+        return rc;
+    GB_CUDA(cudaMemcpyAsync(d_pos, pos, 12ull * num_vertex, cudaMemcpyHostToDevice, st));
+    GB_CUDA(cudaMemcpyAsync(d_tri, tri, 12ull * n, cudaMemcpyHostToDevice, st));
+    if (num_lights) GB_CUDA(cudaMemcpyAsync(d_lights, lights, 56ull * num_lights, cudaMemcpyHostToDevice, st));
+    const uint32_t cb_init[8] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0u, 0u, 0u, 0u, 0u};
+    GB_CUDA(cudaMemcpyAsync(d_cb, cb_init, sizeof(cb_init), cudaMemcpyHostToDevice, st));
+    GB_CUDA(cudaMemsetAsync(d_err, 0, 4, st));
+    const uint32_t B = 256, g1 = (n + B - 1) / B, gh = (nh + B - 1) / B;
+    k_tri_boxes<<<g1, B, 0, st>>>(d_pos, num_vertex, d_tri, n, d_tbox, d_cen, d_cb, d_err);
+    GB_CUDA(cudaGetLastError());
+    k_morton<<<g1, B, 0, st>>>(d_cen, n, d_cb, d_keys, d_vals);
+    GB_CUDA(cudaGetLastError());
+    size_t tmp_bytes = 0;
+    GB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, d_keys, d_keys2, d_vals, d_order, (int)n, 0, 63, st));
+    uint8_t* d_tmp;
+    if ((rc = S.get(d_tmp, tmp_bytes))) return rc;
+    GB_CUDA(cub::DeviceRadixSort::SortPairs(d_tmp, tmp_bytes, d_keys, d_keys2, d_vals, d_order, (int)n, 0, 63, st));
+    k_radix_tree<<<(n - 1 + B - 1) / B, B, 0, st>>>(d_keys2, n, d_left, d_right, d_first, d_last, d_parent);
+    GB_CUDA(cudaGetLastError());
+    GB_CUDA(cudaMemsetAsync(d_arrive, 0, 4ull * n, st));
+    GB_CUDA(cudaMemsetAsync(d_maxd, 0, 4, st));
+    k_bottom_up<<<gh, B, 0, st>>>(n, p.max_leaf_size, d_left, d_right, d_first, d_last, d_parent, d_order, d_tbox,
+                                  d_box, d_icount, d_arrive);
+    GB_CUDA(cudaGetLastError());
+    k_number<<<gh, B, 0, st>>>(n, p.max_leaf_size, d_left, d_first, d_last, d_parent, d_icount, d_outid, d_rank,
+                               d_maxd);
+    GB_CUDA(cudaGetLastError());
+    uint32_t h_err = 0, h_maxd = 0, h_root_icount = 0;
+    GB_CUDA(cudaMemcpyAsync(&h_err, d_err, 4, cudaMemcpyDeviceToHost, st));
+    GB_CUDA(cudaMemcpyAsync(&h_maxd, d_maxd, 4, cudaMemcpyDeviceToHost, st));
+    GB_CUDA(cudaMemcpyAsync(&h_root_icount, d_icount, 4, cudaMemcpyDeviceToHost, st));
+    GB_CUDA(cudaStreamSynchronize(st));
+    if (h_err & 1u) {
+        set_error("tim_rt_build_bvh_gpu: a triangle indexes past num_vertex");
+        return TIM_RT_EINVAL;
+    }
+    if (h_err & 2u) {
+        set_error("tim_rt_build_bvh_gpu: non-finite vertex position");
+        return TIM_RT_EINVAL;
+    }
+    if (h_maxd > p.max_depth) {
+        set_error("tim_rt_build_bvh_gpu: the Morton-code tree is " + std::to_string(h_maxd) +
+                  " levels deep, above max_depth " + std::to_string(p.max_depth) +
+                  " (the reference traversal's bitstack); use tim_rt_build_bvh");
+        return TIM_RT_EUNSUPPORTED;
+    }
+    const uint32_t num_nodes = 1u + 2u * h_root_icount;
+    if ((rc = S.get(d_lsize, num_nodes + 1)) || (rc = S.get(d_lnl, num_nodes)) || (rc = S.get(d_loff, num_nodes + 1)))
+        return rc;
+    GB_CUDA(cudaMemsetAsync(d_lsize, 0, 4ull * (num_nodes + 1), st));
+    GB_CUDA(cudaMemsetAsync(d_lnl, 0, 4ull * num_nodes, st));
+    k_leaf_sizes<<<gh, B, 0, st>>>(n, p.max_leaf_size, d_first, d_last, d_parent, d_outid, d_box, d_lights, num_lights,
+                                   d_lsize, d_lnl);
+    GB_CUDA(cudaGetLastError());
+    size_t scan_bytes = 0;
+    GB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, d_lsize, d_loff, (int)num_nodes + 1, st));
+    uint8_t* d_scan;
+    if ((rc = S.get(d_scan, scan_bytes))) return rc;
+    GB_CUDA(cub::DeviceScan::ExclusiveSum(d_scan, scan_bytes, d_lsize, d_loff, (int)num_nodes + 1, st));
+    uint32_t leaf_words = 0;
+    GB_CUDA(cudaMemcpyAsync(&leaf_words, d_loff + num_nodes, 4, cudaMemcpyDeviceToHost, st));
+    GB_CUDA(cudaStreamSynchronize(st));
+    uint32_t *d_nodes, *d_leaf;
+    if ((rc = S.get(d_nodes, 16ull * num_nodes)) || (rc = S.get(d_leaf, leaf_words))) return rc;
+    k_emit<<<gh, B, 0, st>>>(n, p.max_leaf_size, d_left, d_right, d_first, d_last, d_parent, d_outid, d_box, d_order,
+                             d_tri, d_lights, num_lights, d_loff, d_lnl, d_nodes, d_leaf);
+    GB_CUDA(cudaGetLastError());
+
+    // host image: fillGpuBuffer section order and 32-byte alignment
+    auto blob = std::make_unique<tim_rt_bvh_blob>();
+    uint32_t off = 0;
+    auto place = [&](int r, uint32_t bytes) {
+        blob->ranges[r][0] = off;
+        blob->ranges[r][1] = std::max(32u, bytes);
+        off += align32(bytes);
+    };
+    place(TIM_RT_RANGE_BLAS, 0);
+    place(TIM_RT_RANGE_TRI, 12u * n);
+    place(TIM_RT_RANGE_PRIM, 0);
+    place(TIM_RT_RANGE_MAT, 48u * num_materials);
+    place(TIM_RT_RANGE_LIGHT, 56u * num_lights);
+    place(TIM_RT_RANGE_NODE, 64u * num_nodes);
+    blob->ranges[TIM_RT_RANGE_LEAF][0] = off;
+    blob->ranges[TIM_RT_RANGE_LEAF][1] = 4u * leaf_words;
+    blob->bytes.assign((uint64_t)off + 4ull * leaf_words, 0);
+    uint8_t* b = blob->bytes.data();
+    GB_CUDA(cudaMemcpyAsync(b + blob->ranges[TIM_RT_RANGE_NODE][0], d_nodes, 64ull * num_nodes, cudaMemcpyDeviceToHost,
+                            st));
+    GB_CUDA(cudaMemcpyAsync(b + blob->ranges[TIM_RT_RANGE_LEAF][0], d_leaf, 4ull * leaf_words, cudaMemcpyDeviceToHost,
+                            st));
+    Aabb root;
+    GB_CUDA(cudaMemcpyAsync(&root, d_box, sizeof(Aabb), cudaMemcpyDeviceToHost, st));
+    std::memcpy(b + blob->ranges[TIM_RT_RANGE_TRI][0], tri, 12ull * n);
+    if (num_materials && materials) std::memcpy(b + blob->ranges[TIM_RT_RANGE_MAT][0], materials, 48ull * num_materials);
+    if (num_lights) std::memcpy(b + blob->ranges[TIM_RT_RANGE_LIGHT][0], lights, 56ull * num_lights);
+    GB_CUDA(cudaStreamSynchronize(st));
+    blob->pc.numTriangles = n;
+    blob->pc.numBlas = 0;
+    blob->pc.numPrimitives = 0;
+    blob->pc.numLights = num_lights;
+    blob->pc.numNodes = num_nodes;
+    for (int a = 0; a < 3; ++a) {   // the widened root box, as the host builder reports it
+        blob->aabb[a] = root.lo[a] - (1e-6f + std::fabs(root.lo[a]) * 9.5367431640625e-07f);
+        blob->aabb[3 + a] = root.hi[a] + (1e-6f + std::fabs(root.hi[a]) * 9.5367431640625e-07f);
+    }
+    *out = blob.release();
+    return TIM_RT_OK;
+}
+
+}  // extern "C"
