@@ -431,6 +431,39 @@ def bench_serving(N, ctx, dev, jobs_per_rate=1500):
             "saturation_jobs_per_s": sat_rate, "rates": rates}
 
 
+def bench_build(N, ctx, frame_scene, pd, tx, ty):
+    """Builders: the binned-SAH host builder (tim_rt_build_bvh, all host threads)
+    against the GPU builder (tim_rt_build_bvh_gpu, wall time including the copies
+    of the triangles in and of the image out) on the benchmark frame's scene and on
+    the 1M-triangle probe scene, and the frame's trace time on each tree (kernel
+    time of tim_rt_trace_camera, median of 5, quantised form)."""
+    from tim_raytracing_b200 import scenes
+    out = {}
+    for name, sc in (("frame_100k", frame_scene), ("heightfield_1m", scenes.scaled_heightfield(77, 1_000_000))):
+        row = {"triangles": int(sc.num_tris)}
+        for label, kw in (("host_sah", {}), ("gpu_lbvh", {"ctx": ctx})):
+            ts = []
+            for _ in range(3):
+                t0 = time.perf_counter()
+                img = N.build_bvh(sc, **kw)
+                ts.append(time.perf_counter() - t0)
+            row[label] = {"build_ms": 1e3 * min(ts), "nodes": int(img.num_nodes)}
+            if name == "frame_100k":
+                sid = ctx.upload(img, sc, quant8=True)
+                counts, lists = ctx.cull_lights(sid, pd, tx, ty)
+                ks = []
+                for _ in range(5):
+                    _, _, st = ctx.trace_camera(sid, pd, N.CAM_TILE_LIGHTS | N.CAM_BOUNCE | WIDE_FORM_FLAGS, 1, counts,
+                                                lists)
+                    ks.append(st.kernel_ms)
+                row[label]["frame_trace_ms"] = float(np.median(ks))
+                row[label]["frame_mrays_per_s"] = st.rays / float(np.median(ks)) / 1e3
+                ctx.free_scene(sid)
+        row["gpu_speedup"] = row["host_sah"]["build_ms"] / row["gpu_lbvh"]["build_ms"]
+        out[name] = row
+    return out
+
+
 def profile_frames(form):
     """Two frames of the benchmark workload in one form (tim_rt_trace_camera)."""
     from tim_raytracing_b200 import _native as N, scenes
@@ -513,6 +546,7 @@ def main():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched multi-scene workload")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving workload")
     ap.add_argument("--no-probes", action="store_true", help="skip the light-probe field workload")
+    ap.add_argument("--no-build", action="store_true", help="skip the BVH builder comparison")
     ap.add_argument("--profile", choices=["plain", "wide", "batched-plain", "batched-wide", "probes-plain",
                                           "probes-wide"],
                     help="only run a small, fixed launch sequence for ncu and exit: plain / wide = two frames of "
@@ -689,6 +723,7 @@ def main():
              "workload": "cameraPass.comp lighting step of the 1080p frame: direct light of the 16 lights and the "
                          f"sun from the shadow masks, probe-masked SH9 sample of a {lres[0]}x{lres[1]}x{lres[2]} "
                          "FP16 probe field, RGBA16F out"}
+    build = bench_build(N, ctx, scene, pd, tx, ty) if world == 1 and not args.no_build else None
     # the batched multi-scene and serving workloads (one GPU; skipped in scaling runs)
     batched = serving = None
     if world == 1 and not args.no_batched:
@@ -739,6 +774,8 @@ def main():
         if probes:
             line["probes"] = probes
         line["shade"] = shade
+        if build:
+            line["build"] = build
         if serving:
             line["serving"] = serving
             r8 = serving["rates"][1]
