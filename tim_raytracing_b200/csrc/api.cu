@@ -260,7 +260,7 @@ int tim_rt_destroy(tim_rt_ctx* c) {
     c->scenes.clear();
     for (DevBuf* b : {&c->rays, &c->hits, &c->nid, &c->bary, &c->counters, &c->cam_out, &c->cam_bounce, &c->cam_nid,
                       &c->q_rays, &c->q_pixel, &c->tiles_counts, &c->tiles_lists, &c->dstats, &c->p_dirs, &c->p_basis,
-                      &c->p_out, &c->p_nid, &c->p_irr, &c->p_sh16, &c->p_sh32, &c->p_octa, &c->sh_out, &c->sh_f32})
+                      &c->p_out, &c->p_nid, &c->p_irr, &c->p_sh16, &c->p_sh32, &c->p_octa, &c->sh_out, &c->sh_f32, &c->bld})
         dev_free(c, *b);
     for (auto& e : c->ev)
         if (e) cudaEventDestroy(e);

@@ -352,20 +352,17 @@ __global__ void k_emit(uint32_t n, uint32_t max_leaf, const uint32_t* left, cons
 
 uint32_t align32(uint32_t x) { return (x + 31u) & ~31u; }
 
-// Device scratch of one build, freed on every exit path.
-struct Scratch {
-    tim_rt_ctx* c;
-    std::vector<DevBuf> bufs;
-    explicit Scratch(tim_rt_ctx* cc) : c(cc) {}
-    ~Scratch() {
-        for (DevBuf& b : bufs) dev_free(c, b);
-    }
+// Carves the buffers of one build out of the context's build scratch, which
+// grows to the largest build seen and is kept for the next one (no allocation or
+// free per build once warm).
+struct Carve {
+    uint8_t* base = nullptr;
+    uint64_t used = 0;
     template <class T>
-    int get(T*& p, uint64_t count) {
-        bufs.emplace_back();
-        const int rc = dev_alloc(c, bufs.back(), std::max<uint64_t>(16, sizeof(T) * count));
-        p = static_cast<T*>(bufs.back().ptr);
-        return rc;
+    T* take(uint64_t count) {
+        T* p = reinterpret_cast<T*>(base + used);
+        used += (std::max<uint64_t>(16, sizeof(T) * count) + 255ull) & ~255ull;
+        return p;
     }
 };
 
@@ -412,22 +409,64 @@ int tim_rt_build_bvh_gpu(tim_rt_ctx* c, const float* pos, uint32_t num_vertex, c
     }
     const uint32_t n = num_tris, nh = 2u * n - 1u;
     cudaStream_t st = c->stream;
-    Scratch S(c);
-    float* d_pos;
-    uint32_t *d_tri, *d_err, *d_cb, *d_vals, *d_order, *d_left, *d_right, *d_first, *d_last, *d_parent, *d_icount,
-        *d_arrive, *d_outid, *d_rank, *d_maxd, *d_lsize, *d_lnl, *d_loff;
-    uint64_t *d_keys, *d_keys2;
-    float4* d_cen;
-    Aabb *d_tbox, *d_box;
-    float* d_lights;
-    if ((rc = S.get(d_pos, 3ull * num_vertex)) || (rc = S.get(d_tri, 3ull * n)) || (rc = S.get(d_err, 8)) ||
-        (rc = S.get(d_cb, 8)) || (rc = S.get(d_tbox, n)) || (rc = S.get(d_cen, n)) || (rc = S.get(d_keys, n)) ||
-        (rc = S.get(d_keys2, n)) || (rc = S.get(d_vals, n)) || (rc = S.get(d_order, n)) ||
-        (rc = S.get(d_left, n)) || (rc = S.get(d_right, n)) || (rc = S.get(d_first, n)) || (rc = S.get(d_last, n)) ||
-        (rc = S.get(d_parent, nh)) || (rc = S.get(d_box, nh)) || (rc = S.get(d_icount, nh)) ||
-        (rc = S.get(d_arrive, n)) || (rc = S.get(d_outid, nh)) || (rc = S.get(d_rank, nh)) ||
-        (rc = S.get(d_maxd, 1)) || (rc = S.get(d_lights, 14ull * std::max(num_lights, 1u))))
-        return rc;
+    // CUB temporary sizes (the scan's for the largest possible node count)
+    size_t sort_bytes = 0, scan_bytes = 0;
+    GB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, (uint64_t*)nullptr, (uint64_t*)nullptr,
+                                            (uint32_t*)nullptr, (uint32_t*)nullptr, (int)n, 0, 63, st));
+    GB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (uint32_t*)nullptr, (uint32_t*)nullptr, (int)nh + 1, st));
+    // every buffer of the build, with upper bounds for the node and leaf arrays:
+    // at most nh nodes; leaf words at most 16 per leaf (header + 15 lights) + 3 per triangle
+    Carve K;
+    auto plan = [&](Carve& k) {
+        k.take<float>(3ull * num_vertex); k.take<uint32_t>(3ull * n); k.take<uint32_t>(8); k.take<uint32_t>(8);
+        k.take<Aabb>(n); k.take<float4>(n); k.take<uint64_t>(n); k.take<uint64_t>(n); k.take<uint32_t>(n);
+        k.take<uint32_t>(n); k.take<uint32_t>(n); k.take<uint32_t>(n); k.take<uint32_t>(n); k.take<uint32_t>(n);
+        k.take<uint32_t>(nh); k.take<Aabb>(nh); k.take<uint32_t>(nh); k.take<uint32_t>(n); k.take<uint32_t>(nh);
+        k.take<uint32_t>(nh); k.take<uint32_t>(1); k.take<float>(14ull * std::max(num_lights, 1u));
+        k.take<uint8_t>(sort_bytes); k.take<uint32_t>(nh + 1ull); k.take<uint32_t>(nh); k.take<uint32_t>(nh + 1ull);
+        k.take<uint8_t>(scan_bytes); k.take<uint32_t>(16ull * nh); k.take<uint32_t>(19ull * n);
+    };
+    plan(K);
+    if (c->bld.bytes < K.used) {
+        cudaStreamSynchronize(st);
+        dev_free(c, c->bld);
+        if ((rc = dev_alloc(c, c->bld, K.used))) return rc;
+    }
+    K.base = static_cast<uint8_t*>(c->bld.ptr);
+    K.used = 0;
+    float* d_pos = K.take<float>(3ull * num_vertex);
+    uint32_t* d_tri = K.take<uint32_t>(3ull * n);
+    uint32_t* d_err = K.take<uint32_t>(8);
+    uint32_t* d_cb = K.take<uint32_t>(8);
+    Aabb* d_tbox = K.take<Aabb>(n);
+    float4* d_cen = K.take<float4>(n);
+    uint64_t* d_keys = K.take<uint64_t>(n);
+    uint64_t* d_keys2 = K.take<uint64_t>(n);
+    uint32_t* d_vals = K.take<uint32_t>(n);
+    uint32_t* d_order = K.take<uint32_t>(n);
+    uint32_t* d_left = K.take<uint32_t>(n);
+    uint32_t* d_right = K.take<uint32_t>(n);
+    uint32_t* d_first = K.take<uint32_t>(n);
+    uint32_t* d_last = K.take<uint32_t>(n);
+    uint32_t* d_parent = K.take<uint32_t>(nh);
+    Aabb* d_box = K.take<Aabb>(nh);
+    uint32_t* d_icount = K.take<uint32_t>(nh);
+    uint32_t* d_arrive = K.take<uint32_t>(n);
+    uint32_t* d_outid = K.take<uint32_t>(nh);
+    uint32_t* d_rank = K.take<uint32_t>(nh);
+    uint32_t* d_maxd = K.take<uint32_t>(1);
+    float* d_lights = K.take<float>(14ull * std::max(num_lights, 1u));
+    uint8_t* d_tmp = K.take<uint8_t>(sort_bytes);
+    uint32_t* d_lsize = K.take<uint32_t>(nh + 1ull);
+    uint32_t* d_lnl = K.take<uint32_t>(nh);
+    uint32_t* d_loff = K.take<uint32_t>(nh + 1ull);
+    uint8_t* d_scan = K.take<uint8_t>(scan_bytes);
+    uint32_t* d_nodes = K.take<uint32_t>(16ull * nh);
+    uint32_t* d_leaf = K.take<uint32_t>(19ull * n);
+    if (K.used > c->bld.bytes) {   // the plan above and these takes list the same buffers
+        set_error("tim_rt_build_bvh_gpu: scratch plan mismatch");
+        return TIM_RT_EDEVICE;
+    }
     GB_CUDA(cudaMemcpyAsync(d_pos, pos, 12ull * num_vertex, cudaMemcpyHostToDevice, st));
     GB_CUDA(cudaMemcpyAsync(d_tri, tri, 12ull * n, cudaMemcpyHostToDevice, st));
     if (num_lights) GB_CUDA(cudaMemcpyAsync(d_lights, lights, 56ull * num_lights, cudaMemcpyHostToDevice, st));
@@ -439,11 +478,7 @@ int tim_rt_build_bvh_gpu(tim_rt_ctx* c, const float* pos, uint32_t num_vertex, c
     GB_CUDA(cudaGetLastError());
     k_morton<<<g1, B, 0, st>>>(d_cen, n, d_cb, d_keys, d_vals);
     GB_CUDA(cudaGetLastError());
-    size_t tmp_bytes = 0;
-    GB_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, d_keys, d_keys2, d_vals, d_order, (int)n, 0, 63, st));
-    uint8_t* d_tmp;
-    if ((rc = S.get(d_tmp, tmp_bytes))) return rc;
-    GB_CUDA(cub::DeviceRadixSort::SortPairs(d_tmp, tmp_bytes, d_keys, d_keys2, d_vals, d_order, (int)n, 0, 63, st));
+    GB_CUDA(cub::DeviceRadixSort::SortPairs(d_tmp, sort_bytes, d_keys, d_keys2, d_vals, d_order, (int)n, 0, 63, st));
     k_radix_tree<<<(n - 1 + B - 1) / B, B, 0, st>>>(d_keys2, n, d_left, d_right, d_first, d_last, d_parent);
     GB_CUDA(cudaGetLastError());
     GB_CUDA(cudaMemsetAsync(d_arrive, 0, 4ull * n, st));
@@ -474,23 +509,19 @@ int tim_rt_build_bvh_gpu(tim_rt_ctx* c, const float* pos, uint32_t num_vertex, c
         return TIM_RT_EUNSUPPORTED;
     }
     const uint32_t num_nodes = 1u + 2u * h_root_icount;
-    if ((rc = S.get(d_lsize, num_nodes + 1)) || (rc = S.get(d_lnl, num_nodes)) || (rc = S.get(d_loff, num_nodes + 1)))
-        return rc;
     GB_CUDA(cudaMemsetAsync(d_lsize, 0, 4ull * (num_nodes + 1), st));
     GB_CUDA(cudaMemsetAsync(d_lnl, 0, 4ull * num_nodes, st));
     k_leaf_sizes<<<gh, B, 0, st>>>(n, p.max_leaf_size, d_first, d_last, d_parent, d_outid, d_box, d_lights, num_lights,
                                    d_lsize, d_lnl);
     GB_CUDA(cudaGetLastError());
-    size_t scan_bytes = 0;
-    GB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, d_lsize, d_loff, (int)num_nodes + 1, st));
-    uint8_t* d_scan;
-    if ((rc = S.get(d_scan, scan_bytes))) return rc;
     GB_CUDA(cub::DeviceScan::ExclusiveSum(d_scan, scan_bytes, d_lsize, d_loff, (int)num_nodes + 1, st));
     uint32_t leaf_words = 0;
     GB_CUDA(cudaMemcpyAsync(&leaf_words, d_loff + num_nodes, 4, cudaMemcpyDeviceToHost, st));
     GB_CUDA(cudaStreamSynchronize(st));
-    uint32_t *d_nodes, *d_leaf;
-    if ((rc = S.get(d_nodes, 16ull * num_nodes)) || (rc = S.get(d_leaf, leaf_words))) return rc;
+    if (leaf_words > 19ull * n) {   // cannot happen: at most 16 words per leaf plus 3 per triangle
+        set_error("tim_rt_build_bvh_gpu: leaf data larger than its bound");
+        return TIM_RT_EDEVICE;
+    }
     k_emit<<<gh, B, 0, st>>>(n, p.max_leaf_size, d_left, d_right, d_first, d_last, d_parent, d_outid, d_box, d_order,
                              d_tri, d_lights, num_lights, d_loff, d_lnl, d_nodes, d_leaf);
     GB_CUDA(cudaGetLastError());

@@ -49,6 +49,7 @@ struct tim_rt_ctx {
     DevBuf dstats;              // [0..15] u64 work counters of the counting kernels, [16..20] verification
     DevBuf p_dirs, p_basis, p_out, p_nid, p_irr, p_sh16, p_sh32, p_octa;   // light-probe update
     DevBuf sh_out, sh_f32;      // camera lighting step
+    DevBuf bld;                 // GPU BVH builder scratch (kept between builds)
     cudaEvent_t ev[4] = {};
     cudaEvent_t pev[4] = {};   // camera phases
     LaunchConfig cfg;
