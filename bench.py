@@ -536,6 +536,27 @@ def profile_probes(wide):
     return 0
 
 
+def profile_shade():
+    """The benchmark frame traced once (quantised form), then two lighting steps
+    (tim_rt_shade_camera) over its records with a seeded 12x12x12 FP16 probe field."""
+    from tim_raytracing_b200 import _native as N, scenes
+    scene = make_workload()
+    img = N.build_bvh(scene)
+    ctx = N.Context(0)
+    sid = ctx.upload(img, scene, quant8=True)
+    pd = scenes.pass_data(scene, W, H, aabb=(img.aabb[:3], img.aabb[3:]))
+    tx, ty = (W + 15) // 16, (H + 15) // 16
+    counts, lists = ctx.cull_lights(sid, pd, tx, ty)
+    cam, _, _ = ctx.trace_camera(sid, pd, N.CAM_TILE_LIGHTS | N.CAM_BOUNCE | WIDE_FORM_FLAGS, 1, counts, lists)
+    lres = [int(x) for x in np.asarray(pd["lpfResolution"]).reshape(-1)[:3]]
+    field = np.random.default_rng(3).uniform(0.0, 1.0, size=(7, lres[2], lres[1], lres[0], 4)).astype(np.float16)
+    for _ in range(2):
+        _, _, st = ctx.shade_camera(sid, pd, cam, field.view(np.uint16))
+    print(json.dumps({"shade_kernel_ms": st.kernel_ms}))
+    ctx.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -548,17 +569,20 @@ def main():
     ap.add_argument("--no-probes", action="store_true", help="skip the light-probe field workload")
     ap.add_argument("--no-build", action="store_true", help="skip the BVH builder comparison")
     ap.add_argument("--profile", choices=["plain", "wide", "batched-plain", "batched-wide", "probes-plain",
-                                          "probes-wide"],
+                                          "probes-wide", "shade"],
                     help="only run a small, fixed launch sequence for ncu and exit: plain / wide = two frames of "
                          "one form (per frame one primary and one secondary k_persistent launch); batched-* = two "
                          "launches of one k_multi batch over the first 16 scenes of the batched workload; "
                          "probes-* = two probe-field updates of one form (per update one probe-ray and one "
-                         "shadow-ray k_persistent launch)")
+                         "shadow-ray k_persistent launch); shade = one quantised frame, then two k_shade_camera "
+                         "launches")
     args = ap.parse_args()
     if args.profile in ("plain", "wide"):
         return profile_frames(args.profile)
     if args.profile in ("batched-plain", "batched-wide"):
         return profile_batched(args.profile == "batched-wide")
+    if args.profile == "shade":
+        return profile_shade()
     if args.profile:
         return profile_probes(args.profile == "probes-wide")
     args.warmup = max(args.warmup, 3)
