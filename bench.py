@@ -694,7 +694,7 @@ def main():
     def e2e_step():
         N._check(L.tim_rt_cull_lights(ctx.handle, sid, pdc.ctypes.data, tx, ty, counts_h.data_ptr(), lists_h.data_ptr()))
         st = N.Stats()
-        N._check(L.tim_rt_trace_camera(ctx.handle, sid, pdc.ctypes.data, base_flags | WIDE_FORM_FLAGS, 1,
+        N._check(L.tim_rt_trace_camera(ctx.handle, sid, pdc.ctypes.data, base_flags | WIDE_FORM_FLAGS | N.CAM_PIPELINED, 1,
                                        counts_h.data_ptr(), lists_h.data_ptr(), out_h.data_ptr(), bounce_h.data_ptr(),
                                        ctypes.byref(st)))
         return st.rays

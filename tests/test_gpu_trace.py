@@ -81,6 +81,34 @@ def test_camera_heightfield_tile_lights_bounce(ctx, native, oracle_mod, wide):
         ctx.free_scene(sid)
 
 
+@pytest.mark.parametrize("H", [120, 257])
+def test_camera_pipelined_bands_match_oracle(ctx, native, oracle_mod, H):
+    """TIM_RT_CAM_PIPELINED (bands of rows, copies overlapped with tracing) gives the
+    oracle's records, bounce records and ray count, frame heights with and without
+    a partial last tile row."""
+    from tim_raytracing_b200 import scenes
+    s = scenes.heightfield_scene(seed=10, grid=32, n_spheres=6, n_lights=16, light_radius=5.0)
+    img = native.build_bvh(s)
+    sid = ctx.upload(img, s, quant8=True)
+    try:
+        W = 200
+        pd = scenes.pass_data(s, W, H, aabb=(img.aabb[:3], img.aabb[3:]))
+        tx, ty = (W + 15) // 16, (H + 15) // 16
+        counts, lists = ctx.cull_lights(sid, pd, tx, ty)
+        sc = oracle_mod.Scene(img, s.positions, s.normals)
+        flags = native.CAM_TILE_LIGHTS | native.CAM_BOUNCE | native.CAM_PROB_MASK
+        o_out, o_bounce, o_counts = oracle_mod.camera(sc, pd, flags=flags, seed=5, tile_counts=counts,
+                                                      tile_lists=lists)
+        for form in (0, native.CAM_WIDE | native.CAM_PRIMARY_BINARY):
+            out, bounce, st = ctx.trace_camera(sid, pd, flags=flags | form | native.CAM_PIPELINED, seed=5,
+                                               tile_counts=counts, tile_lists=lists)
+            assert np.array_equal(out, o_out)
+            assert np.array_equal(bounce, o_bounce)
+            assert st.rays == int(o_counts.sum())
+    finally:
+        ctx.free_scene(sid)
+
+
 @pytest.mark.parametrize("n_tris,seed", [(2000, 1), (50000, 2)])
 def test_random_scene_mixed_rays(ctx, native, oracle_mod, n_tris, seed):
     from tim_raytracing_b200 import scenes

@@ -234,9 +234,12 @@ int tim_rt_create(int device, uint64_t mem_budget_bytes, tim_rt_ctx** out) {
     TIMRT_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     for (auto& e : c->ev) TIMRT_CUDA(cudaEventCreate(&e));
     for (auto& e : c->pev) TIMRT_CUDA(cudaEventCreate(&e));
+    TIMRT_CUDA(cudaStreamCreateWithFlags(&c->cstream, cudaStreamNonBlocking));
+    for (auto& e : c->bev) TIMRT_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     int rc = dev_alloc(c.get(), c->counters, 4ull * kCounterWords);
     if (rc) return rc;
     if ((rc = dev_alloc(c.get(), c->dstats, 256))) return rc;   // 16 counter words + 16 verification words
+    if ((rc = dev_alloc(c.get(), c->ray_acc, 16))) return rc;
     TIMRT_CUDA(cudaMemset(c->counters.ptr, 0, 4ull * kCounterWords));
     *out = c.release();
     return TIM_RT_OK;
@@ -260,12 +263,18 @@ int tim_rt_destroy(tim_rt_ctx* c) {
     c->scenes.clear();
     for (DevBuf* b : {&c->rays, &c->hits, &c->nid, &c->bary, &c->counters, &c->cam_out, &c->cam_bounce, &c->cam_nid,
                       &c->q_rays, &c->q_pixel, &c->tiles_counts, &c->tiles_lists, &c->dstats, &c->p_dirs, &c->p_basis,
-                      &c->p_out, &c->p_nid, &c->p_irr, &c->p_sh16, &c->p_sh32, &c->p_octa, &c->sh_out, &c->sh_f32, &c->bld})
+                      &c->p_out, &c->p_nid, &c->p_irr, &c->p_sh16, &c->p_sh32, &c->p_octa, &c->sh_out, &c->sh_f32, &c->bld, &c->ray_acc})
         dev_free(c, *b);
     for (auto& e : c->ev)
         if (e) cudaEventDestroy(e);
     for (auto& e : c->pev)
         if (e) cudaEventDestroy(e);
+    for (auto& e : c->bev)
+        if (e) cudaEventDestroy(e);
+    if (c->cstream) {
+        cudaStreamSynchronize(c->cstream);
+        cudaStreamDestroy(c->cstream);
+    }
     cudaStreamDestroy(c->stream);
     delete c;
     return TIM_RT_OK;
@@ -797,24 +806,50 @@ int tim_rt_trace_camera(tim_rt_ctx* c, tim_rt_scene_id id, const tim_rt_pass_dat
         TIMRT_CUDA(cudaMemcpyAsync(c->tiles_counts.ptr, tile_counts, 4ull * tiles, cudaMemcpyHostToDevice, c->stream));
         TIMRT_CUDA(cudaMemcpyAsync(c->tiles_lists.ptr, tile_lists, 64ull * tiles, cudaMemcpyHostToDevice, c->stream));
     }
-    TIMRT_CUDA(cudaMemsetAsync(ctr, 0, 4 * kCamCounterWords, c->stream));
     const bool count = (flags & TIM_RT_CAM_COUNT) != 0;
     if (count) TIMRT_CUDA(cudaMemsetAsync(c->dstats.ptr, 0, 128, c->stream));
-    TIMRT_CUDA(cudaEventRecord(c->ev[1], c->stream));
     LaunchConfig cam_cfg = cfg_for(c, s, (flags & TIM_RT_CAM_WIDE) != 0, count);
-    cam_cfg.phase_ev = c->pev;
-    TIMRT_CUDA(launch_camera(s->view, *pd, flags, seed, static_cast<const uint32_t*>(c->tiles_counts.ptr),
-                             static_cast<const uint32_t*>(c->tiles_lists.ptr), static_cast<uint32_t*>(c->cam_out.ptr),
-                             (flags & TIM_RT_CAM_BOUNCE) ? static_cast<uint32_t*>(c->cam_bounce.ptr) : nullptr,
-                             static_cast<uint32_t*>(c->cam_nid.ptr), static_cast<tim_rt_ray*>(c->q_rays.ptr),
-                             static_cast<uint32_t*>(c->q_pixel.ptr), (uint32_t)qcap, ctr, ctr + kErrWord, nullptr,
-                             c->stream, cam_cfg));
+    // TIM_RT_CAM_PIPELINED: horizontal bands of output rows; each band's records go
+    // down on the copy stream while the next band traces
+    const uint32_t tile_rows = (H + 3u) / 4u;
+    constexpr uint32_t kMaxBands = sizeof(c->bev) / sizeof(c->bev[0]);   // one band-end event each
+    const uint32_t bands = (flags & TIM_RT_CAM_PIPELINED) ? std::min<uint32_t>(kMaxBands, std::max<uint32_t>(1u, tile_rows / 16u))
+                                                           : 1u;
+    cam_cfg.phase_ev = bands == 1u ? c->pev : nullptr;
+    uint64_t* acc = static_cast<uint64_t*>(c->ray_acc.ptr);
+    TIMRT_CUDA(cudaMemsetAsync(acc, 0, 8, c->stream));
+    TIMRT_CUDA(cudaEventRecord(c->ev[1], c->stream));
+    for (uint32_t b = 0; b < bands; ++b) {
+        const uint32_t r0 = 4u * (tile_rows * b / bands), r1 = std::min(H, 4u * (tile_rows * (b + 1u) / bands));
+        TIMRT_CUDA(cudaMemsetAsync(ctr, 0, 4 * kCamCounterWords, c->stream));
+        TIMRT_CUDA(launch_camera(s->view, *pd, flags, seed, static_cast<const uint32_t*>(c->tiles_counts.ptr),
+                                 static_cast<const uint32_t*>(c->tiles_lists.ptr), static_cast<uint32_t*>(c->cam_out.ptr),
+                                 (flags & TIM_RT_CAM_BOUNCE) ? static_cast<uint32_t*>(c->cam_bounce.ptr) : nullptr,
+                                 static_cast<uint32_t*>(c->cam_nid.ptr), static_cast<tim_rt_ray*>(c->q_rays.ptr),
+                                 static_cast<uint32_t*>(c->q_pixel.ptr), (uint32_t)qcap, ctr, ctr + kErrWord, acc,
+                                 c->stream, cam_cfg, r0, r1));
+        if (bands > 1u) {
+            const uint64_t p0 = (uint64_t)W * r0, np = (uint64_t)W * (r1 - r0);
+            TIMRT_CUDA(cudaEventRecord(c->bev[b], c->stream));
+            TIMRT_CUDA(cudaStreamWaitEvent(c->cstream, c->bev[b], 0));
+            TIMRT_CUDA(cudaMemcpyAsync(out + 8ull * p0, static_cast<uint32_t*>(c->cam_out.ptr) + 8ull * p0, 32ull * np,
+                                       cudaMemcpyDeviceToHost, c->cstream));
+            if (flags & TIM_RT_CAM_BOUNCE)
+                TIMRT_CUDA(cudaMemcpyAsync(bounce_out + 4ull * p0, static_cast<uint32_t*>(c->cam_bounce.ptr) + 4ull * p0,
+                                           16ull * np, cudaMemcpyDeviceToHost, c->cstream));
+        }
+    }
     TIMRT_CUDA(cudaEventRecord(c->ev[2], c->stream));
-    TIMRT_CUDA(cudaMemcpyAsync(out, c->cam_out.ptr, 32ull * npix, cudaMemcpyDeviceToHost, c->stream));
-    if (flags & TIM_RT_CAM_BOUNCE)
-        TIMRT_CUDA(cudaMemcpyAsync(bounce_out, c->cam_bounce.ptr, 16ull * npix, cudaMemcpyDeviceToHost, c->stream));
-    uint32_t qn = 0;
-    TIMRT_CUDA(cudaMemcpyAsync(&qn, ctr + kCamTotalWord, 4, cudaMemcpyDeviceToHost, c->stream));
+    if (bands == 1u) {
+        TIMRT_CUDA(cudaMemcpyAsync(out, c->cam_out.ptr, 32ull * npix, cudaMemcpyDeviceToHost, c->stream));
+        if (flags & TIM_RT_CAM_BOUNCE)
+            TIMRT_CUDA(cudaMemcpyAsync(bounce_out, c->cam_bounce.ptr, 16ull * npix, cudaMemcpyDeviceToHost, c->stream));
+    } else {
+        TIMRT_CUDA(cudaEventRecord(c->bev[bands - 1u], c->cstream));
+        TIMRT_CUDA(cudaStreamWaitEvent(c->stream, c->bev[bands - 1u], 0));
+    }
+    uint64_t traced = 0;
+    TIMRT_CUDA(cudaMemcpyAsync(&traced, acc, 8, cudaMemcpyDeviceToHost, c->stream));
     TIMRT_CUDA(cudaEventRecord(c->ev[3], c->stream));
     TIMRT_CUDA(cudaStreamSynchronize(c->stream));
     if ((rc = check_device_error(c))) return rc;
@@ -822,13 +857,15 @@ int tim_rt_trace_camera(tim_rt_ctx* c, tim_rt_scene_id id, const tim_rt_pass_dat
         std::memset(stats, 0, sizeof(*stats));
         const uint64_t primary = (uint64_t)W * (H - 1u);
         stats->primary_rays = primary;
-        stats->rays = primary + qn;
-        stats->shadow_rays = qn;   // all secondary rays (shadow, probe-visibility, bounce)
+        stats->rays = traced;
+        stats->shadow_rays = traced - primary;   // all secondary rays (shadow, probe-visibility, bounce)
         cudaEventElapsedTime(&stats->kernel_ms, c->ev[1], c->ev[2]);
         cudaEventElapsedTime(&stats->total_ms, c->ev[0], c->ev[3]);
-        cudaEventElapsedTime(&stats->primary_ms, c->pev[0], c->pev[1]);
-        cudaEventElapsedTime(&stats->gen_ms, c->pev[1], c->pev[2]);
-        cudaEventElapsedTime(&stats->secondary_ms, c->pev[2], c->pev[3]);
+        if (bands == 1u) {
+            cudaEventElapsedTime(&stats->primary_ms, c->pev[0], c->pev[1]);
+            cudaEventElapsedTime(&stats->gen_ms, c->pev[1], c->pev[2]);
+            cudaEventElapsedTime(&stats->secondary_ms, c->pev[2], c->pev[3]);
+        }
         if (count) read_counts(c, stats);
     }
     return TIM_RT_OK;

@@ -52,6 +52,9 @@ struct tim_rt_ctx {
     DevBuf bld;                 // GPU BVH builder scratch (kept between builds)
     cudaEvent_t ev[4] = {};
     cudaEvent_t pev[4] = {};   // camera phases
+    cudaStream_t cstream = nullptr;   // result copies overlapped with tracing (TIM_RT_CAM_PIPELINED)
+    cudaEvent_t bev[4] = {};          // end of each band of a pipelined camera trace
+    DevBuf ray_acc;                   // rays traced by a pipelined camera trace (u64)
     LaunchConfig cfg;
     std::set<tim_rt_batch*> batches;
     std::set<tim_rt_server*> servers;

@@ -35,6 +35,8 @@ cudaError_t launch_trace_batch(const SceneView& s, const tim_rt_ray* rays, uint3
                                const LaunchConfig& cfg);
 
 // Secondary rays are queued in camera_queue_kinds() segments of seg_cap = W*H slots.
+// row_begin / row_end restrict a launch to a band of output rows (row_begin a
+// multiple of 4); counters must be cleared before each launch.
 // counters: [0] pixel work, [1] secondary work, [2..27] per-kind counts,
 // [28..54] per-kind prefix ([54] = secondary rays traced).
 uint32_t camera_queue_kinds();
@@ -43,7 +45,7 @@ cudaError_t launch_camera(const SceneView& s, const tim_rt_pass_data& pd, uint32
                           const uint32_t* tile_counts, const uint32_t* tile_lists, uint32_t* out, uint32_t* bounce_out,
                           uint32_t* leaf_nid, tim_rt_ray* q_rays, uint32_t* q_pixel, uint32_t seg_cap,
                           uint32_t* counters, uint32_t* err, uint64_t* d_ray_count, cudaStream_t stream,
-                          const LaunchConfig& cfg);
+                          const LaunchConfig& cfg, uint32_t row_begin = 0, uint32_t row_end = 0xFFFFFFFFu);
 
 // One job of a batched multi-scene trace (device table entry).
 struct MultiJob {

@@ -99,10 +99,11 @@ struct CameraPolicy {
     uint32_t ngy16;         // 16 * ceil(H / 16)
     uint4* out;             // 2 x uint4 per pixel
     uint32_t* leaf_nid;     // per pixel, for the leaf-light shadow mask
+    uint32_t item0;         // first work item (8x4-pixel tile order) of this launch
 
     __device__ __forceinline__ bool load(const SceneView&, uint32_t i, TravState& st) const {
         uint32_t px, py;
-        if (!tile_pixel(i, pd.frameSize[0], pd.frameSize[1], px, py) || py == 0u) return false;
+        if (!tile_pixel(item0 + i, pd.frameSize[0], pd.frameSize[1], px, py) || py == 0u) return false;
         st.slot = py * pd.frameSize[0] + px;
         camera_ray(pd, px, ngy16 - py, st.r.dx, st.r.dy, st.r.dz);
         st.r.ox = pd.cameraPos[0]; st.r.oy = pd.cameraPos[1]; st.r.oz = pd.cameraPos[2];
@@ -118,7 +119,7 @@ struct CameraPolicy {
     }
     __device__ __forceinline__ void skip(uint32_t i) const {
         uint32_t px, py;
-        if (!tile_pixel(i, pd.frameSize[0], pd.frameSize[1], px, py)) return;
+        if (!tile_pixel(item0 + i, pd.frameSize[0], pd.frameSize[1], px, py)) return;
         const uint32_t pix = py * pd.frameSize[0] + px;
         out[2u * pix] = make_uint4(0u, 0u, 0u, 0u);
         out[2u * pix + 1u] = make_uint4(0u, 0u, 0u, 0u);
@@ -298,6 +299,7 @@ struct GenParams {
     uint32_t* q_pixel;
     uint32_t* q_counts;     // kNumKinds counters
     uint32_t seg_cap;
+    uint32_t item0, item1;  // work items (8x4-pixel tile order) of this launch
 };
 
 __device__ __forceinline__ void lpf_position(const tim_rt_pass_data& pd, uint32_t cx, uint32_t cy, uint32_t cz,
@@ -343,9 +345,9 @@ __device__ __forceinline__ void emit(const GenParams& g, uint32_t kind, bool has
 __global__ void __launch_bounds__(256) k_gen_secondary(SceneView s, GenParams g) {
     const tim_rt_pass_data& pd = g.pd;
     const uint32_t W = pd.frameSize[0], H = pd.frameSize[1];
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t i = g.item0 + blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t px = 0, py = 0;
-    const bool valid = i < tiled_work_items(W, H) && tile_pixel(i, W, H, px, py);
+    const bool valid = i < g.item1 && tile_pixel(i, W, H, px, py);
     const uint32_t pix = py * W + px;
     uint4 rec = make_uint4(0, 0, 0, 0);
     if (valid) rec = reinterpret_cast<const uint4*>(g.out_words)[2u * pix];
@@ -602,14 +604,20 @@ cudaError_t launch_camera(const SceneView& s, const tim_rt_pass_data& pd, uint32
                           const uint32_t* tile_counts, const uint32_t* tile_lists, uint32_t* out, uint32_t* bounce_out,
                           uint32_t* leaf_nid, tim_rt_ray* q_rays, uint32_t* q_pixel, uint32_t seg_cap,
                           uint32_t* counters, uint32_t* err, uint64_t* d_ray_count, cudaStream_t stream,
-                          const LaunchConfig& cfg) {
+                          const LaunchConfig& cfg, uint32_t row_begin, uint32_t row_end) {
     const uint32_t W = pd.frameSize[0], H = pd.frameSize[1];
-    const uint32_t items = tiled_work_items(W, H);
+    // output rows [row_begin, row_end): whole rows of 8x4-pixel tiles (row_begin a multiple of 4)
+    row_end = min(row_end, H);
+    if (row_begin >= row_end) return cudaSuccess;
+    const uint32_t tiles_x = (W + 7u) >> 3;
+    const uint32_t item0 = (row_begin >> 2) * tiles_x * 32u;
+    const uint32_t item1 = min(tiled_work_items(W, H), ((row_end + 3u) >> 2) * tiles_x * 32u);
+    const uint32_t items = item1 - item0;
     const uint32_t ngy16 = 16u * ((H + 15u) / 16u);
     // counters: [0] pixel work, [1] secondary work, [2..27] kind counts, [28..54] kind prefix
     uint32_t* q_counts = counters + 2;
     uint32_t* prefix = counters + 2 + kNumKinds;
-    CameraPolicy CP{pd, ngy16, reinterpret_cast<uint4*>(out), leaf_nid};
+    CameraPolicy CP{pd, ngy16, reinterpret_cast<uint4*>(out), leaf_nid, item0};
     if (cfg.phase_ev) cudaEventRecord(cfg.phase_ev[0], stream);
     // primary rays: a warp refills only when all 32 lanes are idle, so it always
     // traces one whole 8x4-pixel tile together (measured fastest for these
@@ -636,6 +644,8 @@ cudaError_t launch_camera(const SceneView& s, const tim_rt_pass_data& pd, uint32
     g.q_pixel = q_pixel;
     g.q_counts = q_counts;
     g.seg_cap = seg_cap;
+    g.item0 = item0;
+    g.item1 = item1;
     k_gen_secondary<<<(items + 255u) / 256u, 256, 0, stream>>>(s, g);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     k_kind_prefix<<<1, 1, 0, stream>>>(q_counts, prefix, seg_cap);
@@ -647,7 +657,9 @@ cudaError_t launch_camera(const SceneView& s, const tim_rt_pass_data& pd, uint32
                  : launch_persistent<false>(s, SP, 0u, prefix + kNumKinds, counters + 1, err, stream, cfg2);
     if (cfg.phase_ev) cudaEventRecord(cfg.phase_ev[3], stream);
     if (e != cudaSuccess || !d_ray_count) return e;
-    k_add_ray_count<<<1, 1, 0, stream>>>(d_ray_count, (uint64_t)W * (H - 1u), prefix + kNumKinds);
+    // primary rays of the rows traced (output row 0 is never traced)
+    const uint64_t primary = (uint64_t)W * (row_end - max(row_begin, 1u));
+    k_add_ray_count<<<1, 1, 0, stream>>>(d_ray_count, primary, prefix + kNumKinds);
     return cudaGetLastError();
 }
 
