@@ -464,6 +464,17 @@ struct tim_rt_probe_desc {
 #define TIM_RT_PROBE_WIDE 0x100u
 #define TIM_RT_PROBE_PRIMARY_BINARY 0x400u /* with TIM_RT_PROBE_WIDE: the probe rays take the binary walk and
                                             only their shadow rays the 8-wide one (identical results) */
+/* Probe ray directions (4 floats each) and, when sh_basis is not NULL, their SH9
+ * basis weights (9 floats each, the constants and order of LightProbFieldPass::
+ * sampleRays, lightProbFieldPass.cpp:186-199) for count = side^2 rays (1..4096):
+ *   TIM_RT_DIRS_STRATIFIED: sampleRays' jittered stratified sphere directions
+ *     (lightProbFieldPass.cpp:151-185), drawn from a std::mt19937 seeded with
+ *     `seed` (the reference uses std::random_device, not reproducible);
+ *   TIM_RT_DIRS_OCTAHEDRAL: the cell centres of a side x side octahedral grid in the
+ *     order TIM_RT_PROBE_OCTA bins (index j * side + i). Host only. */
+#define TIM_RT_DIRS_STRATIFIED 0u
+#define TIM_RT_DIRS_OCTAHEDRAL 1u
+int tim_rt_probe_directions(uint32_t count, uint32_t kind, uint64_t seed, float *dirs, float *sh_basis);
 int tim_rt_update_probes(tim_rt_ctx *ctx, tim_rt_scene_id scene, const tim_rt_probe_desc *desc, const float *dirs,
                          const float *sh_basis, uint32_t probe_begin, uint32_t probe_end, uint32_t *trace_out,
                          float *irradiance, uint16_t *sh9_fp16, float *sh9_fp32, float *octa, tim_rt_stats *stats);

@@ -35,7 +35,7 @@ EXPORTED = [
     "tim_rt_server_submit", "tim_rt_server_wait", "tim_rt_server_drain", "tim_rt_server_stats_get",
     "tim_rt_server_destroy", "tim_rt_verify_hits", "tim_rt_server_submit_probes", "tim_rt_bvh_file_write",
     "tim_rt_bvh_file_read", "tim_rt_bvh_file_info", "tim_rt_bvh_file_free", "tim_rt_upload_bvh_file",
-    "tim_rt_shade_camera", "tim_rt_shade_camera_dev", "tim_rt_build_bvh_gpu",
+    "tim_rt_shade_camera", "tim_rt_shade_camera_dev", "tim_rt_build_bvh_gpu", "tim_rt_probe_directions",
 ]
 SORT_NONE, SORT_OCTANT, SORT_MORTON = 0, 1, 2
 BATCH_WIDE = 0x100
@@ -205,6 +205,7 @@ def lib() -> ctypes.CDLL:
     L.tim_rt_build_bvh_gpu.argtypes = [vp, vp, u32, vp, u32, vp, u32, vp, u32, ctypes.POINTER(BuildParams),
                                        ctypes.POINTER(vp)]
     L.tim_rt_shade_camera_dev.argtypes = [vp, u32, vp, u32, vp, vp, vp, vp, vp]
+    L.tim_rt_probe_directions.argtypes = [u32, u32, u64, vp, vp]
     for name in EXPORTED:
         if name not in ("tim_rt_version", "tim_rt_last_error", "tim_rt_build_params_default", "tim_rt_bvh_blob_free",
                         "tim_rt_bvh_file_free"):
@@ -305,6 +306,17 @@ def build_bvh(scene, ctx: "Context" = None, **params) -> BvhImage:
     finally:
         L.tim_rt_bvh_blob_free(out)
     return BvhImage(data, ranges, (pc.numTriangles, pc.numBlas, pc.numPrimitives, pc.numLights, pc.numNodes), aabb)
+
+
+DIRS_STRATIFIED, DIRS_OCTAHEDRAL = 0, 1
+
+
+def probe_directions(count: int, kind: int = DIRS_STRATIFIED, seed: int = 0):
+    """tim_rt_probe_directions: (dirs float32 [count, 4], SH9 basis float32 [count, 9])."""
+    dirs = np.zeros((count, 4), np.float32)
+    basis = np.zeros((count, 9), np.float32)
+    _check(lib().tim_rt_probe_directions(count, kind, seed, dirs.ctypes.data, basis.ctypes.data))
+    return dirs, basis
 
 
 def save_bvh_file(path, img: BvhImage, positions, normals=None, uvs=None) -> None:
