@@ -145,8 +145,25 @@ def cpu_baseline(scene, img, pd, threads, budget_s=12.0):
         elapsed += time.perf_counter() - t0
         rays += int(c.sum())
         rows += 1
-    return {"value": rays / elapsed / 1e6, "unit": METRIC, "cores": threads, "kind": "port",
-            "sample": f"{rows} of {H - 1} traced rows ({rays} rays) of the same frame, {elapsed:.1f} s"}
+    out = {"value": rays / elapsed / 1e6, "unit": METRIC, "cores": threads, "kind": "port",
+           "sample": f"{rows} of {H - 1} traced rows ({rays} rays) of the same frame, {elapsed:.1f} s"}
+    out.update(reference_builder(scene))
+    return out
+
+
+def reference_builder(scene, want_image=False):
+    """The reference's own CPU BVH builder (BVHBuilder::build with its worker
+    threads, compiled from its sources into oracle/_ref) on the frame's scene: the
+    other half of the reference's CPU path. Returns the report (and the image)."""
+    from oracle import oracle as O
+    if not O.have_refbuild():
+        rep = {"reference_builder": "not built (oracle/_ref/libtimref_build.so missing)"}
+        return (rep, None) if want_image else rep
+    t0 = time.perf_counter()
+    img = O.ref_build(scene, multithread=True)
+    rep = {"reference_builder": {"s": time.perf_counter() - t0, "triangles": int(scene.num_tris),
+                                 "nodes": int(img.pc[4]), "threads": "BVHBuilder::build(true) workers"}}
+    return (rep, img) if want_image else rep
 
 
 def run_reference(args, rank, world):
@@ -155,9 +172,17 @@ def run_reference(args, rank, world):
     if rank != 0:
         return 0
     from oracle import oracle as O
-    from tim_raytracing_b200 import _native as N, scenes
+    from tim_raytracing_b200 import scenes
     scene = make_workload()
-    img = N.build_bvh(scene)
+    # the reference's own builder (its CPU path end to end); its threaded build order
+    # varies run to run, which does not matter for a timing
+    builder, img = reference_builder(scene, want_image=True)
+    if img is not None:
+        bvh = "reference BVHBuilder (oracle/_ref)"
+    else:
+        from tim_raytracing_b200 import _native as N
+        img = N.build_bvh(scene)
+        bvh = "product builder (reference builder not built)"
     pd = scenes.pass_data(scene, W, H, aabb=(img.aabb[:3], img.aabb[3:]))
     threads = O.threads_available()
     sc = O.Scene(img, scene.positions, scene.normals)
@@ -184,9 +209,10 @@ def run_reference(args, rank, world):
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": config_dict(scene, {"sample": f"{rows_per_step} rows x {W} pixels per step, spread over the frame"}),
+            "config": config_dict(scene, {"sample": f"{rows_per_step} rows x {W} pixels per step, spread over the frame",
+                                          "bvh": bvh}),
             "cpu_baseline": {"value": v, "unit": METRIC, "cores": threads, "kind": "port",
-                             "sample": f"{rows_per_step} rows spread over the frame per step"},
+                             "sample": f"{rows_per_step} rows spread over the frame per step", **builder},
             "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
