@@ -174,11 +174,13 @@ def test_wide_near_ties_match_oracle(ctx, native, oracle_mod):
         ctx.free_scene(sid)
 
 
-def test_wide_form_matches_plain(ctx, native):
+@pytest.mark.parametrize("grid,spheres", [(64, 12), (128, 53)])
+def test_wide_form_matches_plain(ctx, native, grid, spheres):
     """8-wide quantised BVH: hit records, leaf ids and barycentrics identical to the
-    binary walk's for every ray, near-ties included; any-hit results identical."""
+    binary walk's for every ray, near-ties included; any-hit results identical. The
+    larger scene (61K binary nodes) is collapsed on worker threads, subtree by subtree."""
     from tim_raytracing_b200 import scenes
-    s = scenes.heightfield_scene(seed=4, grid=64, n_spheres=12)
+    s = scenes.heightfield_scene(seed=4, grid=grid, n_spheres=spheres)
     img = native.build_bvh(s)
     sid = ctx.upload(img, s, quant8=True)
     try:

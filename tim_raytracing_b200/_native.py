@@ -219,6 +219,13 @@ def _check(rc: int):
         raise TimRtError(rc, lib().tim_rt_last_error().decode())
 
 
+def _copy_bytes(ptr: int, n: int) -> np.ndarray:
+    """A uint8 copy of n bytes at a C pointer (one copy, no intermediate bytes object)."""
+    if n == 0:
+        return np.zeros(0, np.uint8)
+    return np.ctypeslib.as_array(ctypes.cast(ptr, ctypes.POINTER(ctypes.c_uint8)), shape=(n,)).copy()
+
+
 def _ptr(a):
     if a is None:
         return None
@@ -302,7 +309,7 @@ def build_bvh(scene, ctx: "Context" = None, **params) -> BvhImage:
         aabb = np.zeros(6, np.float32)
         _check(L.tim_rt_bvh_blob_info(out, ctypes.byref(bp), ctypes.byref(size), ranges.ctypes.data, ctypes.byref(pc),
                                       aabb.ctypes.data))
-        data = np.frombuffer(ctypes.string_at(bp.value, size.value), dtype=np.uint8).copy()
+        data = _copy_bytes(bp.value, size.value)
     finally:
         L.tim_rt_bvh_blob_free(out)
     return BvhImage(data, ranges, (pc.numTriangles, pc.numBlas, pc.numPrimitives, pc.numLights, pc.numNodes), aabb)
@@ -348,7 +355,7 @@ def load_bvh_file(path):
         _check(L.tim_rt_bvh_file_info(f, ctypes.byref(bp), ctypes.byref(size), ranges.ctypes.data, ctypes.byref(pc),
                                       aabb.ctypes.data, ctypes.byref(pp), ctypes.byref(pn), ctypes.byref(pu),
                                       ctypes.byref(mx), ctypes.byref(nv)))
-        data = np.frombuffer(ctypes.string_at(bp.value, size.value), dtype=np.uint8).copy()
+        data = _copy_bytes(bp.value, size.value)
         n = nv.value
 
         def arr(ptr, k):

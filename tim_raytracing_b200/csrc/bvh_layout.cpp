@@ -3,7 +3,9 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <atomic>
 #include <deque>
+#include <thread>
 #include "internal.h"
 
 namespace timrt {
@@ -207,18 +209,41 @@ bool quantise_axis(const float* lo, const float* hi, int n, float& origin, uint8
 
 }  // namespace
 
-bool build_wide(const uint8_t* blob, const uint32_t ranges[7][2], uint32_t num_nodes, const float* pos,
-                WideHost& out, std::string& err) {
-    const PNode* nodes = reinterpret_cast<const PNode*>(blob + ranges[TIM_RT_RANGE_NODE][0]);
-    const uint32_t* leaf = reinterpret_cast<const uint32_t*>(blob + ranges[TIM_RT_RANGE_LEAF][0]);
-    const uint64_t leaf_words = ranges[TIM_RT_RANGE_LEAF][1] / 4u;
-    out = WideHost();
-    auto leaf_tris = [&](uint32_t nid) -> uint32_t {
+namespace {
+
+// One wide node to fill: its index in the node array being written, the binary
+// subtrees that become its slots, and its depth.
+struct Job {
+    uint32_t w;
+    std::vector<Slot> slots;
+    uint32_t depth;
+};
+
+// Wide nodes, leaf-triangle records and their binary-leaf records of one part of
+// the collapse (the whole tree, or one subtree built on a worker thread).
+struct Part {
+    std::vector<uint32_t> nodes;     // 20 words per node
+    std::vector<float> tris;         // 12 floats per leaf triangle
+    std::vector<uint32_t> tri_leaf;  // 8 words per leaf triangle
+    uint32_t num_nodes = 0;
+    uint32_t max_depth = 0;
+    std::string err;
+};
+
+struct Collapse {
+    const PNode* nodes;
+    const uint32_t* leaf;
+    uint64_t leaf_words;
+    const float* pos;
+    bool root_is_leaf;
+
+    uint32_t leaf_tris(uint32_t nid) const {
         const uint32_t off = nodes[nid & kMask].nid[3];
         if (off == 0xFFFFFFFFu || off >= leaf_words) return 0u;
         return leaf[off] & 0xFFFu;
-    };
-    auto emit_tris = [&](uint32_t nid, const Slot& box, bool no_box_test) {
+    }
+
+    void emit_tris(Part& out, uint32_t nid, const Slot& box, bool no_box_test) const {
         const uint32_t nm = nid & kMask;
         uint32_t e[8];
         std::memcpy(&e[0], box.elo, 12);
@@ -246,13 +271,11 @@ bool build_wide(const uint8_t* blob, const uint32_t ranges[7][2], uint32_t num_n
             out.tris.insert(out.tris.end(), w, w + 12);
             out.tri_leaf.insert(out.tri_leaf.end(), e, e + 8);
         }
-    };
+    }
 
-    // Work queue of wide nodes to fill: (wide index, slots, depth).
-    struct Job { uint32_t w; std::vector<Slot> slots; uint32_t depth; };
-    std::deque<Job> q;
-    auto expand = [&](std::vector<Slot> fr) {
-        // greedily open the internal slot with the largest surface area until 8 slots
+    // Greedily opens the internal slot with the largest surface area until 8
+    // slots; leaves of no triangle are dropped (they never produce hits).
+    std::vector<Slot> expand(std::vector<Slot> fr) const {
         for (;;) {
             if (fr.size() >= 8) break;
             int best = -1;
@@ -266,35 +289,19 @@ bool build_wide(const uint8_t* blob, const uint32_t ranges[7][2], uint32_t num_n
             fr.push_back(a);
             fr.push_back(b);
         }
-        // empty leaves never produce hits
         std::vector<Slot> kept;
         for (const Slot& s : fr)
             if (!(s.id & kLeafBit) || leaf_tris(s.id) > 0u) kept.push_back(s);
         return kept;
-    };
-
-    out.nodes.reserve(20ull * (num_nodes / 4 + 4));
-    out.nodes.resize(20);
-    out.num_nodes = 1;
-    if (num_nodes == 1u) {
-        Slot s;
-        s.id = kLeafBit;
-        for (int a = 0; a < 3; ++a) { s.lo[a] = s.hi[a] = s.elo[a] = s.ehi[a] = 0.f; }
-        q.push_back({0u, {s}, 1u});
-        out.root_is_leaf = 1u;
-    } else {
-        Slot a, b;
-        child_slots(nodes[0], a, b, nullptr);
-        q.push_back({0u, expand({a, b}), 1u});
     }
-    while (!q.empty()) {
-        Job job = std::move(q.front());
-        q.pop_front();
+
+    // Writes wide node job.w of `out` and queues its internal children (numbered
+    // consecutively after the nodes `out` holds).
+    bool fill(const Job& job, Part& out, std::deque<Job>& q) const {
         out.max_depth = std::max(out.max_depth, job.depth);
-        // slot k of the node holds child slot_child[k] (-1 = empty)
         const std::vector<Slot>& fr = job.slots;
         int slot_child[8];
-        assign_octant_slots(fr, out.root_is_leaf != 0, slot_child);
+        assign_octant_slots(fr, root_is_leaf, slot_child);
         const int nf = (int)fr.size();
         float lo[3][8], hi[3][8];
         for (int i = 0; i < nf; ++i)
@@ -302,14 +309,12 @@ bool build_wide(const uint8_t* blob, const uint32_t ranges[7][2], uint32_t num_n
                 lo[a][i] = std::min(fr[i].lo[a], fr[i].hi[a]);   // the slab test orders each axis itself
                 hi[a][i] = std::max(fr[i].lo[a], fr[i].hi[a]);
             }
-        uint32_t* w = out.nodes.data() + 20ull * job.w;
-        std::memset(w, 0, 80);
         uint8_t e[3] = {1, 1, 1}, cq_lo[3][8] = {}, cq_hi[3][8] = {}, qlo[3][8] = {}, qhi[3][8] = {};
         float origin[3] = {0.f, 0.f, 0.f};
         if (nf > 0) {
             for (int a = 0; a < 3; ++a)
                 if (!quantise_axis(lo[a], hi[a], nf, origin[a], e[a], cq_lo[a], cq_hi[a])) {
-                    err = "box bounds cannot be quantised (non-finite coordinates)";
+                    out.err = "box bounds cannot be quantised (non-finite coordinates)";
                     return false;
                 }
         }
@@ -325,14 +330,14 @@ bool build_wide(const uint8_t* blob, const uint32_t ranges[7][2], uint32_t num_n
             sl[k] = fr[i];
             for (int a = 0; a < 3; ++a) { qlo[a][k] = cq_lo[a][i]; qhi[a][k] = cq_hi[a][i]; }
         }
-        const int n = 8;
         uint32_t imask = 0, n_internal = 0;
-        for (int k = 0; k < n; ++k)
+        for (int k = 0; k < 8; ++k)
             if (used[k] && !(sl[k].id & kLeafBit)) { imask |= 1u << k; ++n_internal; }
         const uint32_t child_base = out.num_nodes;
         out.num_nodes += n_internal;
         out.nodes.resize(20ull * out.num_nodes);
-        w = out.nodes.data() + 20ull * job.w;
+        uint32_t* w = out.nodes.data() + 20ull * job.w;
+        std::memset(w, 0, 80);
         std::memcpy(&w[0], &origin[0], 4);
         std::memcpy(&w[1], &origin[1], 4);
         std::memcpy(&w[2], &origin[2], 4);
@@ -340,12 +345,12 @@ bool build_wide(const uint8_t* blob, const uint32_t ranges[7][2], uint32_t num_n
         w[4] = child_base;
         w[5] = (uint32_t)(out.tris.size() / 12);
         uint8_t meta[8] = {};
-        for (int k = 0; k < n; ++k) {
+        for (int k = 0; k < 8; ++k) {
             if (used[k] && (sl[k].id & kLeafBit)) {
                 const uint32_t nt = leaf_tris(sl[k].id);
-                if (nt > 255u) { err = "a leaf holds more than 255 triangles (8-wide slot limit)"; return false; }
+                if (nt > 255u) { out.err = "a leaf holds more than 255 triangles (8-wide slot limit)"; return false; }
                 meta[k] = (uint8_t)nt;
-                emit_tris(sl[k].id, sl[k], out.root_is_leaf != 0);
+                emit_tris(out, sl[k].id, sl[k], root_is_leaf);
             }
         }
         std::memcpy(&w[6], meta, 8);
@@ -355,14 +360,127 @@ bool build_wide(const uint8_t* blob, const uint32_t ranges[7][2], uint32_t num_n
             qb[24 + k] = qhi[0][k]; qb[32 + k] = qhi[1][k]; qb[40 + k] = qhi[2][k];
         }
         uint32_t ci = child_base;
-        for (int k = 0; k < n; ++k) {
+        for (int k = 0; k < 8; ++k) {
             if (used[k] && !(sl[k].id & kLeafBit)) {
                 Slot a, b;
                 child_slots(nodes[sl[k].id], a, b, &sl[k]);
                 q.push_back({ci++, expand({a, b}), job.depth + 1u});
             }
         }
+        return true;
     }
+
+    // Every wide node below (and including) `job`, into a fresh part whose node 0
+    // is the job's own node.
+    void subtree(const Job& job, Part& out) const {
+        out.num_nodes = 1;
+        out.nodes.resize(20);
+        std::deque<Job> q;
+        q.push_back({0u, job.slots, job.depth});
+        while (!q.empty()) {
+            Job j = std::move(q.front());
+            q.pop_front();
+            if (!fill(j, out, q)) return;
+        }
+    }
+};
+
+}  // namespace
+
+bool build_wide(const uint8_t* blob, const uint32_t ranges[7][2], uint32_t num_nodes, const float* pos,
+                WideHost& out, std::string& err) {
+    Collapse C;
+    C.nodes = reinterpret_cast<const PNode*>(blob + ranges[TIM_RT_RANGE_NODE][0]);
+    C.leaf = reinterpret_cast<const uint32_t*>(blob + ranges[TIM_RT_RANGE_LEAF][0]);
+    C.leaf_words = ranges[TIM_RT_RANGE_LEAF][1] / 4u;
+    C.pos = pos;
+    C.root_is_leaf = num_nodes == 1u;
+    out = WideHost();
+    Part top;
+    top.nodes.reserve(20ull * (num_nodes / 4 + 4));
+    top.nodes.resize(20);
+    top.num_nodes = 1;
+    std::deque<Job> q;
+    if (C.root_is_leaf) {
+        Slot s;
+        s.id = kLeafBit;
+        for (int a = 0; a < 3; ++a) { s.lo[a] = s.hi[a] = s.elo[a] = s.ehi[a] = 0.f; }
+        q.push_back({0u, {s}, 1u});
+        out.root_is_leaf = 1u;
+    } else {
+        Slot a, b;
+        child_slots(C.nodes[0], a, b, nullptr);
+        q.push_back({0u, C.expand({a, b}), 1u});
+    }
+    // breadth first on this thread until there are enough independent subtrees ...
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const size_t enough = num_nodes > 16384u && hw > 1u ? 256u : (size_t)-1;
+    while (!q.empty() && q.size() < enough) {
+        Job j = std::move(q.front());
+        q.pop_front();
+        if (!C.fill(j, top, q)) { err = top.err; return false; }
+    }
+    // ... then each pending subtree on a worker thread, merged in queue order
+    // (the numbering does not depend on the number of threads)
+    std::vector<Job> pending(std::make_move_iterator(q.begin()), std::make_move_iterator(q.end()));
+    std::vector<Part> parts(pending.size());
+    std::atomic<size_t> next{0};
+    auto work = [&]() {
+        for (size_t k; (k = next.fetch_add(1)) < pending.size();) C.subtree(pending[k], parts[k]);
+    };
+    std::vector<std::thread> pool;
+    const size_t nthreads = pending.empty() ? 0 : std::min<size_t>(hw, pending.size());
+    for (size_t t = 1; t < nthreads; ++t) pool.emplace_back(work);
+    if (nthreads) work();
+    for (std::thread& t : pool) t.join();
+    uint32_t max_depth = top.max_depth;
+    // merge: the parts' nodes follow the top nodes in queue order, each part's node 0
+    // replaces its pending slot; sizes first, then copies and index fix-ups in parallel
+    std::vector<uint64_t> node_off(parts.size()), tri_off(parts.size());
+    uint64_t nn = top.num_nodes, nt = top.tris.size() / 12;
+    for (size_t k = 0; k < parts.size(); ++k) {
+        if (!parts[k].err.empty()) { err = parts[k].err; return false; }
+        max_depth = std::max(max_depth, parts[k].max_depth);
+        node_off[k] = nn;
+        tri_off[k] = nt;
+        nn += parts[k].num_nodes - 1u;
+        nt += parts[k].tris.size() / 12;
+    }
+    if (nn >= (1u << 24)) { err = "more than 2^24 8-wide nodes"; return false; }
+    top.nodes.resize(20ull * nn);
+    top.tris.resize(12ull * nt);
+    top.tri_leaf.resize(8ull * nt);
+    next = 0;
+    auto merge = [&]() {
+        for (size_t k; (k = next.fetch_add(1)) < parts.size();) {
+            Part& p = parts[k];
+            for (uint32_t i = 0; i < p.num_nodes; ++i) {
+                uint32_t* w = p.nodes.data() + 20ull * i;
+                w[4] = (uint32_t)node_off[k] + w[4] - 1u;   // children: local ids >= 1
+                w[5] += (uint32_t)tri_off[k];
+            }
+            std::memcpy(top.nodes.data() + 20ull * pending[k].w, p.nodes.data(), 80);
+            if (p.num_nodes > 1u)
+                std::memcpy(top.nodes.data() + 20ull * node_off[k], p.nodes.data() + 20, 80ull * (p.num_nodes - 1u));
+            if (!p.tris.empty()) {
+                std::memcpy(top.tris.data() + 12ull * tri_off[k], p.tris.data(), 4ull * p.tris.size());
+                std::memcpy(top.tri_leaf.data() + 8ull * tri_off[k], p.tri_leaf.data(), 4ull * p.tri_leaf.size());
+            }
+            std::vector<uint32_t>().swap(p.nodes);   // release the part's memory early
+            std::vector<float>().swap(p.tris);
+            std::vector<uint32_t>().swap(p.tri_leaf);
+        }
+    };
+    pool.clear();
+    for (size_t t = 1; t < nthreads; ++t) pool.emplace_back(merge);
+    if (nthreads) merge();
+    for (std::thread& t : pool) t.join();
+    top.num_nodes = (uint32_t)nn;
+    out.nodes = std::move(top.nodes);
+    out.tris = std::move(top.tris);
+    out.tri_leaf = std::move(top.tri_leaf);
+    out.num_nodes = top.num_nodes;
+    out.max_depth = max_depth;
     if (out.max_depth > 32u) { err = "8-wide tree deeper than 32 levels"; return false; }
     if (out.num_nodes >= (1u << 24)) { err = "more than 2^24 8-wide nodes"; return false; }
     return true;
