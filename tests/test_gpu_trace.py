@@ -81,7 +81,7 @@ def test_camera_heightfield_tile_lights_bounce(ctx, native, oracle_mod, wide):
         ctx.free_scene(sid)
 
 
-@pytest.mark.parametrize("H", [120, 257])
+@pytest.mark.parametrize("H", [257, 400])
 def test_camera_pipelined_bands_match_oracle(ctx, native, oracle_mod, H):
     """TIM_RT_CAM_PIPELINED (bands of rows, copies overlapped with tracing) gives the
     oracle's records, bounce records and ray count, frame heights with and without

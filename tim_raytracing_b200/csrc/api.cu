@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <cstdio>
+#include <cmath>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -819,8 +820,22 @@ int tim_rt_trace_camera(tim_rt_ctx* c, tim_rt_scene_id id, const tim_rt_pass_dat
     uint64_t* acc = static_cast<uint64_t*>(c->ray_acc.ptr);
     TIMRT_CUDA(cudaMemsetAsync(acc, 0, 8, c->stream));
     TIMRT_CUDA(cudaEventRecord(c->ev[1], c->stream));
+    // band sizes shrink geometrically (ratio 0.7, about the copy / trace time ratio per
+    // row) so each band's copy hides under the next band's trace and the last copy,
+    // which nothing hides, is small
+    uint32_t edge[kMaxBands + 1] = {};
+    {
+        double w[kMaxBands], sum = 0.0;
+        for (uint32_t b = 0; b < bands; ++b) sum += (w[b] = std::pow(0.7, (double)b));
+        double acc = 0.0;
+        for (uint32_t b = 0; b < bands; ++b) {
+            acc += w[b];
+            edge[b + 1] = b + 1u == bands ? tile_rows : std::min(tile_rows, (uint32_t)(tile_rows * (acc / sum) + 0.5));
+        }
+    }
     for (uint32_t b = 0; b < bands; ++b) {
-        const uint32_t r0 = 4u * (tile_rows * b / bands), r1 = std::min(H, 4u * (tile_rows * (b + 1u) / bands));
+        const uint32_t r0 = 4u * edge[b], r1 = std::min(H, 4u * edge[b + 1]);
+        if (r0 >= r1) continue;
         TIMRT_CUDA(cudaMemsetAsync(ctr, 0, 4 * kCamCounterWords, c->stream));
         TIMRT_CUDA(launch_camera(s->view, *pd, flags, seed, static_cast<const uint32_t*>(c->tiles_counts.ptr),
                                  static_cast<const uint32_t*>(c->tiles_lists.ptr), static_cast<uint32_t*>(c->cam_out.ptr),
