@@ -224,27 +224,43 @@ void fail_all(tim_rt_server* s, int code, const std::string& msg) {
     s->cv_done.notify_all();
 }
 
+// A request's rays are on the device (its upload has completed, or an earlier
+// step already traced part of it).
+bool uploaded(const Req* r) {
+    if (!r->first_chunk) return true;
+    return r->uploaded && cudaEventQuery(r->uploaded) == cudaSuccess;
+}
+
 // Plans the next step under the mutex: an equal share of max_rays_per_step for
-// every admitted request with rays left, then the rest in admission order.
+// every admitted request with rays left, then the rest in admission order. Only
+// requests whose rays are already on the device take part, so a step never waits
+// for uploads that later admissions queued; when none is ready, the oldest request
+// alone (its upload was queued first; the step waits for it on the device).
 void plan_step(tim_rt_server* s, Plan& P) {
     const uint32_t cap = s->p.max_rays_per_step;
-    const size_t k = std::min<size_t>(s->active.size(), s->p.max_jobs_per_step);
+    std::vector<Req*> cand;
+    for (Req* r : s->active) {
+        if (cand.size() >= s->p.max_jobs_per_step) break;
+        if (uploaded(r)) cand.push_back(r);
+    }
+    if (cand.empty()) cand.push_back(s->active.front());   // its upload was queued first
+    const size_t k = cand.size();
     std::vector<uint32_t> take(k, 0);
     const uint32_t share = std::max<uint32_t>(1u, cap / (uint32_t)k);
     uint64_t used = 0;
     for (size_t i = 0; i < k; ++i) {
-        Req* r = s->active[i];
+        Req* r = cand[i];
         take[i] = std::min<uint32_t>(r->r.n - r->issued, share);
         used += take[i];
     }
     for (size_t i = 0; i < k && used < cap; ++i) {
-        Req* r = s->active[i];
+        Req* r = cand[i];
         const uint32_t extra = (uint32_t)std::min<uint64_t>(r->r.n - r->issued - take[i], cap - used);
         take[i] += extra;
         used += extra;
     }
     for (size_t i = 0; i < k; ++i)
-        if (take[i]) P.chunks.push_back({s->active[i], take[i]});
+        if (take[i]) P.chunks.push_back({cand[i], take[i]});
 }
 
 int issue_step(tim_rt_server* s, Plan& P) {
