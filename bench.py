@@ -397,8 +397,8 @@ def bench_serving(N, ctx, dev, jobs_per_rate=1500):
     basis = scenes.sh9_basis(dirs)
     fields = [torch.zeros((7, 8, 16, 16, 4), dtype=torch.int16).pin_memory() for _ in range(8)]
     field_owner = [0] * len(fields)
-    pool = []
-    for e in range(64):
+    pool = []   # 256 reusable pinned ray / hit buffers: up to 256 requests in flight
+    for e in range(256):
         n = int(np.exp(rng.uniform(np.log(1e3), np.log(1e6))))
         r = torch.from_numpy(scenes.serving_rays(60_000 + e, n)).pin_memory()
         h = torch.empty((n, 4), dtype=torch.int32).pin_memory()
