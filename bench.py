@@ -490,6 +490,71 @@ def bench_build(N, ctx, frame_scene, pd, tx, ty):
     return out
 
 
+def bench_jobs_100k(N, ctx, dev, frame_scene, sid, steps=10):
+    """A stream of ray jobs on the ~100K-triangle benchmark scene: 512 jobs of
+    log-U [1K, 64K] mixed primary / shadow / probe-direction rays (the serving
+    generator), traced (a) in the plain form as one binary-BVH launch per job, the
+    way a caller without batching dispatches them (each launch then lasts at least
+    one ray's chain of dependent node loads), and (b) in the quantised batched form
+    as one 8-wide k_multi launch over all jobs in a CUDA graph; also the two mixed
+    cases. Device-resident rays; hit records must be identical. Most of the gain
+    of (b) over (a) is the batching, not the quantisation: the plain batched form
+    is reported beside it."""
+    import torch
+    from tim_raytracing_b200 import scenes
+    rng = np.random.default_rng(31)
+    nr = np.exp(rng.uniform(np.log(1e3), np.log(6.4e4), 512)).astype(np.int64)
+    d_rays = [torch.from_numpy(scenes.serving_rays(90_000 + k, int(n))).to(dev) for k, n in enumerate(nr)]
+    total = int(nr.sum())
+    stream = torch.cuda.Stream(device=dev)
+    res, hits = {}, {}
+
+    def time_it(fn):
+        with torch.cuda.stream(stream):   # graph replays go to the current stream
+            for _ in range(2):
+                fn()
+            torch.cuda.synchronize()
+            ms = []
+            for _ in range(steps):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                fn()
+                e1.record(stream)
+                torch.cuda.synchronize()
+                ms.append(e0.elapsed_time(e1))
+        return float(np.median(ms))
+
+    ctx.set_launch_config()
+    for form, wide in (("plain", False), ("wide", True)):
+        hits[form] = [torch.empty((int(n), 4), dtype=torch.int32, device=dev) for n in nr]
+        mode = N.MODE_PER_RAY | (N.TRACE_WIDE if wide else 0)
+
+        def per_job():
+            for k in range(len(nr)):
+                ctx.trace_dev(sid, d_rays[k], int(nr[k]), mode, hits[form][k], stream=stream.cuda_stream)
+
+        res[f"{form}_per_job_launches"] = time_it(per_job)
+        b = ctx.batch_create([(sid, N.MODE_PER_RAY, int(nr[k]), d_rays[k], hits[form][k], None, None)
+                              for k in range(len(nr))], wide=wide)
+        ctx.batch_launch(b, stream=stream.cuda_stream)
+        stream.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=stream):
+            ctx.batch_launch(b, stream=stream.cuda_stream)
+        res[f"{form}_batched_graph"] = time_it(lambda: g.replay())
+        del g
+        ctx.batch_destroy(b)
+    torch.cuda.synchronize()
+    differing = sum(int((hits["plain"][k] != hits["wide"][k]).any(dim=1).sum().item()) for k in range(len(nr)))
+    out = {"workload": "512 jobs of log-U 1K..64K mixed rays on the 100,608-triangle benchmark scene",
+           "rays": total, "hit_records_differing": differing}
+    for key, ms in res.items():
+        out[key] = {"ms": ms, "value": total / (ms / 1e3) / 1e6}
+    out["speedup_quantised_batched_over_plain_per_job"] = res["plain_per_job_launches"] / res["wide_batched_graph"]
+    out["speedup_quantised_batched_over_plain_batched"] = res["plain_batched_graph"] / res["wide_batched_graph"]
+    return out
+
+
 def profile_frames(form):
     """Two frames of the benchmark workload in one form (tim_rt_trace_camera)."""
     from tim_raytracing_b200 import _native as N, scenes
@@ -774,6 +839,7 @@ def main():
                          f"sun from the shadow masks, probe-masked SH9 sample of a {lres[0]}x{lres[1]}x{lres[2]} "
                          "FP16 probe field, RGBA16F out"}
     build = bench_build(N, ctx, scene, pd, tx, ty) if world == 1 and not args.no_build else None
+    jobs_100k = bench_jobs_100k(N, ctx, dev, scene, sid) if world == 1 and not args.no_batched else None
     # the batched multi-scene and serving workloads (one GPU; skipped in scaling runs)
     batched = serving = None
     if world == 1 and not args.no_batched:
@@ -826,6 +892,8 @@ def main():
         line["shade"] = shade
         if build:
             line["build"] = build
+        if jobs_100k:
+            line["jobs_100k"] = jobs_100k
         if serving:
             line["serving"] = serving
             r8 = serving["rates"][1]
