@@ -176,7 +176,7 @@ struct SecondaryPolicy {
 // lives in dynamic shared memory, entry k of thread t at [k * BLOCK + t]
 // (binary form) or [(2k, 2k+1) * BLOCK + t] (8-wide form).
 template <int BLOCK, bool WIDE, bool STATS, class Policy>
-__global__ void __launch_bounds__(BLOCK, WIDE ? 896 / BLOCK : 1) k_persistent(SceneView s, Policy P, uint32_t n_static,
+__global__ void __launch_bounds__(BLOCK, WIDE ? 896 / BLOCK : 1024 / BLOCK) k_persistent(SceneView s, Policy P, uint32_t n_static,
                                                       const uint32_t* n_dev, uint32_t* counter, uint32_t* err,
                                                       unsigned long long* stats, int sdepth, int knobs) {
     extern __shared__ uint32_t stack_mem[];

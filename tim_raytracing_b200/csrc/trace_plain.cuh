@@ -29,8 +29,9 @@ struct TravState {
     // work counters (dead code unless a counting kernel reads them)
     uint32_t c_node, c_leaf, c_tri, c_reload;
     uint32_t slot;      // policy scratch (pixel or queue slot of the ray)
+    float ix, iy, iz;   // 1 / direction (8-wide form: zero components replaced, see wide_inv)
+    float boxabs;       // binary walk: absolute margin of the filtered box test (+inf: exact test only)
     // 8-wide form only
-    float ix, iy, iz;   // 1 / direction
     uint32_t order;     // rank mask of the current wide node's hit slots still to visit
     uint32_t oct;       // ray octant: bit a set when the direction's component a is negative
     uint32_t first;     // rank of the nearest hit slot still to visit first (8 = none)
@@ -41,7 +42,20 @@ struct TravState {
     uint32_t leaf;      // pending leaf slot of the current wide node (8 = none)
 };
 
+// Direction components for which the binary walk's filtered box test is exact
+// (see box_filter): 0, or a magnitude within [2^-100, 2^100].
+__device__ __forceinline__ bool box_dir_ok(float d) {
+    const float a = fabsf(d);
+    return a == 0.0f || (a >= 7.888609052210118e-31f && a <= 1.2676506002282294e30f);   // 0 or [2^-100, 2^100]
+}
+
 __device__ __forceinline__ void trav_init(TravState& st, uint32_t root) {
+    st.ix = 1.0f / st.r.dx;
+    st.iy = 1.0f / st.r.dy;
+    st.iz = 1.0f / st.r.dz;
+    st.boxabs = (box_dir_ok(st.r.dx) && box_dir_ok(st.r.dy) && box_dir_ok(st.r.dz) && st.t <= 1.2676506002282294e30f)
+                    ? 7.888609052210118e-31f   // 2^-100
+                    : __int_as_float(0x7F800000);
     st.node = root;
     st.c_node = st.c_leaf = st.c_tri = st.c_reload = 0u;
     st.sp = 0;
@@ -50,6 +64,66 @@ __device__ __forceinline__ void trav_init(TravState& st, uint32_t root) {
     st.rec0 = st.rec1 = st.rec2 = 0u;
     st.nid = 0xFFFFFFFFu;
     st.u = st.v = 0.0f;
+}
+
+// The two child boxes of an inner node, with CollideBox's outcome: which children
+// are hit and whether child 1 is entered first (d1 < d0).
+//
+// Filtered test. CollideBox divides, t = RN(RN(p - o) / d); the filter multiplies
+// by inv = RN(1/d) instead, t' = RN(RN(p - o) * inv). For a ray whose direction
+// components are 0 or within [2^-100, 2^100] (box_dir_ok) and whose tmax is at
+// most 2^100 each slab value obeys
+// |t - t'| <= 3.05u |t'| + 2^-148 (u = 2^-24), or both are at least 2^126 in
+// magnitude with the same sign (overflow), and for d = 0 the two are identical
+// (x / +-0 and x * +-inf give the same infinities, 0 / 0 and 0 * inf both NaN).
+// min and max carry such bounds through to the aggregates M (largest slab entry)
+// and T = min(tmax, smallest slab exit), so with m = 2^-20 (|M| + |T|) + 2^-100
+// (four times the error plus the rounding of the tests themselves):
+//   tmin + m < T - m   -> CollideBox hits, with its tmin in [lo, hi];
+//   tmin - m >= T + m  -> CollideBox misses.
+// Anything else (a box grazed within the margin, a ray outside the safe range:
+// boxabs = +inf makes m infinite, every infinity or NaN in M or T does too), and
+// an order that the tmin intervals cannot settle, takes the reference's
+// divisions. The outcome is CollideBox's in every case; only the work differs.
+__device__ __forceinline__ bool box_filter(const TravState& st, float mnx, float mny, float mnz, float mxx, float mxy,
+                                           float mxz, bool& hit, float& lo, float& hi) {
+    const float t0x = (mnx - st.r.ox) * st.ix, t0y = (mny - st.r.oy) * st.iy, t0z = (mnz - st.r.oz) * st.iz;
+    const float t1x = (mxx - st.r.ox) * st.ix, t1y = (mxy - st.r.oy) * st.iy, t1z = (mxz - st.r.oz) * st.iz;
+    const float M = fmaxf(fminf(t0x, t1x), fmaxf(fminf(t0y, t1y), fminf(t0z, t1z)));
+    const float T = fminf(st.t, fminf(fmaxf(t0x, t1x), fminf(fmaxf(t0y, t1y), fmaxf(t0z, t1z))));
+    const float m = __fmaf_rn(fabsf(M) + fabsf(T), 9.5367431640625e-07f, st.boxabs);   // 2^-20
+    const float tmin = fmaxf(0.0f, M);
+    if (tmin + m < T - m) {
+        hit = true;
+        const bool zero = M + m <= 0.0f;   // the entry lies behind the origin: tmin is exactly 0
+        lo = zero ? 0.0f : fmaxf(0.0f, M - m);
+        hi = zero ? 0.0f : tmin + m;
+        return true;
+    }
+    hit = false;
+    lo = hi = 0.0f;
+    return tmin - m >= T + m;
+}
+
+// CollideBox of both children with the reference's divisions. Not inlined: the
+// filter settles nearly every node, and the division code stays out of the loop.
+static __device__ __noinline__ float2 exact_children(Ray r, float4 a, float4 b, float4 c, float tmax) {
+    return make_float2(collide_box(r, a.x, a.y, c.x, a.z, a.w, c.y, tmax), collide_box(r, b.x, b.y, c.z, b.z, b.w, c.w, tmax));
+}
+
+__device__ __forceinline__ void plain_children(const TravState& st, const float4& a, const float4& b, const float4& c,
+                                               bool& h0, bool& h1, bool& first1) {
+    float lo0, hi0, lo1, hi1;
+    bool ok = box_filter(st, a.x, a.y, c.x, a.z, a.w, c.y, h0, lo0, hi0);
+    ok = box_filter(st, b.x, b.y, c.z, b.z, b.w, c.w, h1, lo1, hi1) && ok;
+    first1 = hi1 < lo0;
+    if (ok && h0 && h1 && !first1 && !(lo1 >= hi0)) ok = false;
+    if (!ok) {
+        const float2 d = exact_children(st.r, a, b, c, st.t);
+        h0 = d.x >= 0.0f;
+        h1 = d.y >= 0.0f;
+        first1 = d.y < d.x;
+    }
 }
 
 // Leaf visit: bvh_collide (bvhCollision.glsl:177-239) for closest-hit rays,
@@ -117,14 +191,17 @@ __device__ __forceinline__ void plain_step(const SceneView& s, TravState& st, ui
         const float4 a = __ldg(np + 1);   // n0xy = (c0.min.x, c0.min.y, c0.max.x, c0.max.y)
         const float4 b = __ldg(np + 2);   // n1xy
         const float4 c = __ldg(np + 3);   // nz = (c0.min.z, c0.max.z, c1.min.z, c1.max.z)
+        // the reference's divisions: this walk only retraces the rare rays the 8-wide
+        // walk cannot settle, and the filter's code would only add registers there
         const float d0 = collide_box(st.r, a.x, a.y, c.x, a.z, a.w, c.y, st.t);
         const float d1 = collide_box(st.r, b.x, b.y, c.z, b.z, b.w, c.w, st.t);
+        const bool h0 = d0 >= 0.0f, h1 = d1 >= 0.0f, first1 = d1 < d0;
         const uint32_t packed = nid.z;
         uint32_t c0 = packed & kNidMask;
         uint32_t c1 = c0 + 1u;
         c0 |= (packed & kNidLeftLeafBit) ? kNidLeafBit : 0u;
         c1 |= (packed & kNidRightLeafBit) ? kNidLeafBit : 0u;
-        if (d0 < 0.0f && d1 < 0.0f) {
+        if (!h0 && !h1) {
             if (st.sp == 0) {
                 st.done = true;
                 return;
@@ -132,8 +209,7 @@ __device__ __forceinline__ void plain_step(const SceneView& s, TravState& st, ui
             node = stk[(--st.sp) * BLOCK];
             continue;
         }
-        if (d0 >= 0.0f && d1 >= 0.0f) {
-            const bool first1 = d1 < d0;
+        if (h0 && h1) {
             if (st.sp >= sdepth) {   // unreachable: the stack holds the tree depth
                 atomicOr(err, 1u);
                 st.done = true;
@@ -142,7 +218,7 @@ __device__ __forceinline__ void plain_step(const SceneView& s, TravState& st, ui
             stk[(st.sp++) * BLOCK] = first1 ? c0 : c1;
             node = first1 ? c1 : c0;
         } else {
-            node = (d0 >= 0.0f) ? c0 : c1;
+            node = h0 ? c0 : c1;
         }
     }
     plain_leaf(s, st, node);
@@ -168,14 +244,14 @@ __device__ __forceinline__ void plain_advance(const SceneView& s, TravState& st,
     const float4 a = __ldg(np + 1);
     const float4 b = __ldg(np + 2);
     const float4 c = __ldg(np + 3);
-    const float d0 = collide_box(st.r, a.x, a.y, c.x, a.z, a.w, c.y, st.t);
-    const float d1 = collide_box(st.r, b.x, b.y, c.z, b.z, b.w, c.w, st.t);
+    bool h0, h1, first1;
+    plain_children(st, a, b, c, h0, h1, first1);
     const uint32_t packed = nid.z;
     uint32_t c0 = packed & kNidMask;
     uint32_t c1 = c0 + 1u;
     c0 |= (packed & kNidLeftLeafBit) ? kNidLeafBit : 0u;
     c1 |= (packed & kNidRightLeafBit) ? kNidLeafBit : 0u;
-    if (d0 < 0.0f && d1 < 0.0f) {
+    if (!h0 && !h1) {
         if (st.sp == 0) {
             st.done = true;
             return;
@@ -183,8 +259,7 @@ __device__ __forceinline__ void plain_advance(const SceneView& s, TravState& st,
         st.node = stk[(--st.sp) * BLOCK];
         return;
     }
-    if (d0 >= 0.0f && d1 >= 0.0f) {
-        const bool first1 = d1 < d0;
+    if (h0 && h1) {
         if (st.sp >= sdepth) {   // unreachable: the stack holds the tree depth
             atomicOr(err, 1u);
             st.done = true;
@@ -193,7 +268,7 @@ __device__ __forceinline__ void plain_advance(const SceneView& s, TravState& st,
         stk[(st.sp++) * BLOCK] = first1 ? c0 : c1;
         st.node = first1 ? c1 : c0;
     } else {
-        st.node = (d0 >= 0.0f) ? c0 : c1;
+        st.node = h0 ? c0 : c1;
     }
 }
 

@@ -22,17 +22,19 @@
 // Box test, and why it never rejects a child the reference accepts. Per node
 // and axis the kernel forms A = RN(RN(o - r) * inv) and B = s * inv (exact: s is
 // a power of two), with inv = RN(1/d), and evaluates every plane as one fused
-// multiply-add t = RN(q * B + A). Against the exact distance T = (o + s*q - r)/d
-// the error is below 3u|A| + 2u|T| (u = 2^-24). The |A| part is absorbed by
-// moving A itself by |A| * 2^-18 (outward: down for near planes, up for far
-// planes), the |T| part by scaling the final near / far by (1 -+ 2^-18). Near
-// and far planes are picked from the sign of inv, which for d != 0 equals the
-// min / max of the two slab distances. A zero direction component is replaced
-// by +-2^-80 for this test only: the slab then holds every t the reference's
-// test (which divides by zero) accepts, and all values stay finite.
-// So tmin_here <= tmin_reference and tmax_here >= tmax_reference for every
-// child: the quantised traversal visits a superset of the binary traversal's
-// leaves and never loses a hit.
+// multiply-add t = RN(q * B' + A'), where A' and B' are A and B moved outward by
+// 2^-18 of their magnitude (down for near planes, up for far planes). Against
+// the exact distance T = (o + s*q - r)/d, A and q*B are within 3u|A| and u q|B|
+// (u = 2^-24), the moves shift the sum by 2^-18 (|A| + q|B|) and the roundings
+// of A', B' and the FMA add below 3u (|A| + q|B|); since |T| <= |A*| + q|B*| the
+// shift exceeds all of that plus the 2u|T| the reference's own two roundings
+// can take away. Near and far planes are picked from the sign of inv, which
+// for d != 0 equals the min / max of the two slab distances. A zero direction
+// component is replaced by +-2^-80 for this test only: the slab then holds
+// every t the reference's test (which divides by zero) accepts, and all values
+// stay finite. So tmin_here <= tmin_reference and tmax_here >= tmax_reference
+// for every child: the quantised traversal visits a superset of the binary
+// traversal's leaves and never loses a hit.
 //
 // Same hit as the binary walk, for every ray. The reference's closest-hit rule
 // is order-dependent: a hit at t is accepted iff t < c, and then c = t - 1e-5,
@@ -64,6 +66,19 @@ namespace timrt {
 
 constexpr float kWiden = 3.814697265625e-06f;   // 2^-18
 
+// Three-input max / min (PTX max.f32 / min.f32 with three sources, sm_100). Used
+// only where no operand can be NaN.
+__device__ __forceinline__ float max3f(float a, float b, float c) {
+    float r;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+__device__ __forceinline__ float min3f(float a, float b, float c) {
+    float r;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+
 // Byte k of `word` as a float (0x4B0000qq is 2^23 + q exactly).
 __device__ __forceinline__ float wbyte(uint32_t word, uint32_t k) {
     return __uint_as_float(__byte_perm(word, 0x4B000000u, 0x7650u | k)) - 8388608.0f;
@@ -94,6 +109,9 @@ __device__ __forceinline__ uint32_t wide_visit(const SceneView& s, const TravSta
     const float Anx = __fmaf_rn(-fabsf(Ax), kWiden, Ax), Afx = __fmaf_rn(fabsf(Ax), kWiden, Ax);
     const float Any = __fmaf_rn(-fabsf(Ay), kWiden, Ay), Afy = __fmaf_rn(fabsf(Ay), kWiden, Ay);
     const float Anz = __fmaf_rn(-fabsf(Az), kWiden, Az), Afz = __fmaf_rn(fabsf(Az), kWiden, Az);
+    const float Bnx = __fmaf_rn(-fabsf(Bx), kWiden, Bx), Bfx = __fmaf_rn(fabsf(Bx), kWiden, Bx);
+    const float Bny = __fmaf_rn(-fabsf(By), kWiden, By), Bfy = __fmaf_rn(fabsf(By), kWiden, By);
+    const float Bnz = __fmaf_rn(-fabsf(Bz), kWiden, Bz), Bfz = __fmaf_rn(fabsf(Bz), kWiden, Bz);
     // near / far plane words from the direction's sign
     const bool negx = __float_as_uint(ix) >> 31, negy = __float_as_uint(iy) >> 31, negz = __float_as_uint(iz) >> 31;
     const uint32_t nx0 = negx ? U3.z : U2.x, nx1 = negx ? U3.w : U2.y, fx0 = negx ? U2.x : U3.z, fx1 = negx ? U2.y : U3.w;
@@ -106,16 +124,14 @@ __device__ __forceinline__ uint32_t wide_visit(const SceneView& s, const TravSta
         const uint32_t wsel = k < 4u ? 0u : 1u, kk = k & 3u;
         // empty slots carry the inverted box qlo = 255, qhi = 0 and fail this test by
         // themselves (if rounding ever lets one through, it is a leaf of 0 triangles)
-        const float tnx = __fmaf_rn(wbyte(wsel ? nx1 : nx0, kk), Bx, Anx);
-        const float tny = __fmaf_rn(wbyte(wsel ? ny1 : ny0, kk), By, Any);
-        const float tnz = __fmaf_rn(wbyte(wsel ? nz1 : nz0, kk), Bz, Anz);
-        const float tfx = __fmaf_rn(wbyte(wsel ? fx1 : fx0, kk), Bx, Afx);
-        const float tfy = __fmaf_rn(wbyte(wsel ? fy1 : fy0, kk), By, Afy);
-        const float tfz = __fmaf_rn(wbyte(wsel ? fz1 : fz0, kk), Bz, Afz);
-        const float nearv = fmaxf(tnx, fmaxf(tny, tnz));
-        const float farv = fminf(tfx, fminf(tfy, tfz));
-        const float tmin = fmaxf(0.0f, __fmaf_rn(-fabsf(nearv), kWiden, nearv));
-        const float tm = fminf(tcur, __fmaf_rn(fabsf(farv), kWiden, farv));
+        const float tnx = __fmaf_rn(wbyte(wsel ? nx1 : nx0, kk), Bnx, Anx);
+        const float tny = __fmaf_rn(wbyte(wsel ? ny1 : ny0, kk), Bny, Any);
+        const float tnz = __fmaf_rn(wbyte(wsel ? nz1 : nz0, kk), Bnz, Anz);
+        const float tfx = __fmaf_rn(wbyte(wsel ? fx1 : fx0, kk), Bfx, Afx);
+        const float tfy = __fmaf_rn(wbyte(wsel ? fy1 : fy0, kk), Bfy, Afy);
+        const float tfz = __fmaf_rn(wbyte(wsel ? fz1 : fz0, kk), Bfz, Afz);
+        const float tmin = fmaxf(max3f(tnx, tny, tnz), 0.0f);
+        const float tm = fminf(min3f(tfx, tfy, tfz), tcur);
         const bool hit = tmin < tm;
         // slot k is visited at rank k ^ octant: children were placed by direction
         mask |= (hit ? 1u : 0u) << (k ^ st.oct);
