@@ -128,6 +128,103 @@ def test_random_scene_mixed_rays(ctx, native, oracle_mod, n_tris, seed):
         ctx.free_scene(sid)
 
 
+def _margin_rays(img, aabb, seed, n_per_kind):
+    """Rays whose child-box tests fall inside or near the error margin of the binary
+    walk's filtered box test (origins on box planes, rays grazing box corners and
+    edges, axis-parallel and near-axis-parallel directions, far origins, extreme
+    tmax), mixed closest / any-hit."""
+    rng = np.random.default_rng(seed)
+    f = img.nodes().view(np.float32)
+    lo = np.concatenate([f[:, [4, 5, 12]], f[:, [8, 9, 14]]])
+    hi = np.concatenate([f[:, [6, 7, 13]], f[:, [10, 11, 15]]])
+    keep = (hi > lo).any(axis=1)
+    lo, hi = lo[keep], hi[keep]
+    amin, amax = np.asarray(aabb[:3], np.float64), np.asarray(aabb[3:], np.float64)
+    span = amax - amin
+
+    def unit(k):
+        d = rng.normal(size=(k, 3))
+        return d / np.linalg.norm(d, axis=1, keepdims=True)
+
+    def boxes(k):
+        i = rng.integers(0, len(lo), k)
+        return lo[i].astype(np.float64), hi[i].astype(np.float64)
+
+    k = n_per_kind
+    out = []
+    # origin on a plane of a child box, inside the box on the other axes
+    bl, bh = boxes(k)
+    o = bl + rng.uniform(size=(k, 3)) * (bh - bl)
+    ax = rng.integers(0, 3, k)
+    side = rng.integers(0, 2, k).astype(bool)
+    o[np.arange(k), ax] = np.where(side, bh[np.arange(k), ax], bl[np.arange(k), ax])
+    out.append((o, unit(k)))
+    # aimed at a box corner or at a point on a box edge
+    bl, bh = boxes(k)
+    corner = np.where(rng.integers(0, 2, (k, 3)).astype(bool), bh, bl)
+    free = rng.integers(0, 4, k)
+    for a in range(3):
+        m = free == a
+        corner[m, a] = bl[m, a] + rng.uniform(size=m.sum()) * (bh[m, a] - bl[m, a])
+    o = amin - 0.2 * span + rng.uniform(size=(k, 3)) * 1.4 * span
+    out.append((o, corner - o))
+    # axis-parallel (one or two zero components, signed zeros) from box planes
+    bl, bh = boxes(k)
+    o = bl + rng.uniform(size=(k, 3)) * (bh - bl)
+    o[:, 0] = np.where(rng.integers(0, 2, k).astype(bool), bl[:, 0], o[:, 0])
+    d = unit(k)
+    z = rng.integers(0, 3, (k, 3)) == 0
+    z[z.all(axis=1), 0] = False
+    d[z] = 0.0
+    d[z & (rng.integers(0, 2, (k, 3)) == 0)] = -0.0
+    out.append((o, d))
+    # tiny (subnormal-range and 1e-20) components
+    o = amin + rng.uniform(size=(k, 3)) * span
+    d = unit(k)
+    t = rng.integers(0, 3, (k, 3)) == 0
+    d[t] = np.choose(rng.integers(0, 3, t.sum()), [1e-35, -1e-20, 1e-42])
+    out.append((o, d))
+    # far origins looking back at the scene
+    c = 0.5 * (amin + amax)
+    o = c + unit(k) * rng.choice([1e3, 1e5, 1e7], size=(k, 1))
+    out.append((o, c + (rng.uniform(size=(k, 3)) - 0.5) * span - o))
+    rays = []
+    for o, d in out:
+        r = np.zeros((len(o), 8), np.float32)
+        r[:, 0:3] = o
+        r[:, 4:7] = d
+        r[:, 3] = rng.choice(np.array([100.0, 1e-3, 7.5, 1e31, np.inf], np.float32), size=len(o))
+        r.view(np.uint32)[:, 7] = rng.integers(0, 2, len(o)).astype(np.uint32)
+        rays.append(r)
+    return np.concatenate(rays)
+
+
+@pytest.mark.parametrize("which", ["room", "heightfield"])
+def test_box_filter_margin_cases(ctx, native, oracle_mod, which):
+    """The binary walk's filtered child-box test decides only outside its error
+    margin and takes the reference's divisions inside it; rays built to sit on
+    that boundary must give the oracle's records bit for bit in both forms."""
+    from tim_raytracing_b200 import scenes
+    if which == "room":
+        s, img = load_room()
+    else:
+        s = scenes.heightfield_scene(5, grid=64, n_spheres=12)
+        img = native.build_bvh(s)
+    sid = ctx.upload(img, s, quant8=True)
+    try:
+        rays = _margin_rays(img, img.aabb, 11, 6000)
+        sc = oracle_mod.Scene(img, s.positions, s.normals)
+        oh, on, ob, _ = oracle_mod.trace(sc, rays, 2)
+        assert (oh[:, 3] != np.float32(100.0).view(np.uint32)).sum() > 1000   # plenty of hits
+        for form in (0, native.TRACE_WIDE):
+            hit, nid, bary, _ = ctx.trace(sid, rays, native.MODE_PER_RAY | form)
+            assert np.array_equal(hit, oh), form
+            assert np.array_equal(nid, on), form
+            assert np.array_equal(bary.view(np.uint32), ob.view(np.uint32)), form
+    finally:
+        ctx.free_scene(sid)
+
+
 def test_fp64_verification(ctx, native, oracle_mod):
     """tim_rt_verify_hits re-intersects every reported closest hit in FP64: all
     hits are counted, and the FP32 t of the reference arithmetic is close to FP64."""

@@ -30,11 +30,14 @@
 // shift exceeds all of that plus the 2u|T| the reference's own two roundings
 // can take away. Near and far planes are picked from the sign of inv, which
 // for d != 0 equals the min / max of the two slab distances. A zero direction
-// component is replaced by +-2^-80 for this test only: the slab then holds
-// every t the reference's test (which divides by zero) accepts, and all values
-// stay finite. So tmin_here <= tmin_reference and tmax_here >= tmax_reference
-// for every child: the quantised traversal visits a superset of the binary
-// traversal's leaves and never loses a hit.
+// component is replaced by +-2^-80 for this test only, which keeps all values
+// finite. So, for rays whose direction components are at least 2^-60 and whose
+// origin lies within 2^60, tmin_here <= tmin_reference and tmax_here >=
+// tmax_reference for every child: the quantised traversal visits a superset of
+// the binary traversal's leaves and never loses a hit. For other rays (a zero
+// component among them) the slab can come out narrower than the reference's, so
+// every hit they report is checked below and a miss is not trusted
+// (wide_miss_final): both go to the binary walk.
 //
 // Same hit as the binary walk, for every ray. The reference's closest-hit rule
 // is order-dependent: a hit at t is accepted iff t < c, and then c = t - 1e-5,
@@ -306,11 +309,28 @@ __device__ __forceinline__ void wide_step_warp(const SceneView& s, TravState& st
     }
 }
 
+// Whether an 8-wide walk that found no hit may report the miss. The slab
+// argument above needs finite plane distances that contain the reference's: a
+// zero direction component is replaced by +-2^-80, which turns the reference's
+// unbounded slab (origin strictly inside, 1/0 = inf) into a finite one that
+// can end short of a hit when the origin lies within about 2^-80 tmax of the
+// plane, and a component below 2^-126 overflows 1/d. So the miss is final only
+// when every component is at least 2^-60 in magnitude and the origin within
+// 2^60 (with scene coordinates below 2^60 every plane distance is then finite);
+// other rays that found nothing are traced again by the binary walk.
+__device__ __forceinline__ bool wide_miss_final(const Ray& r) {
+    constexpr float dlo = 8.673617379884035e-19f, ohi = 1.152921504606847e18f;   // 2^-60, 2^60
+    return fabsf(r.dx) >= dlo && fabsf(r.dy) >= dlo && fabsf(r.dz) >= dlo &&      // false for NaN too
+           fabsf(r.ox) <= ohi && fabsf(r.oy) <= ohi && fabsf(r.oz) <= ohi;
+}
+
 // Called when the 8-wide walk of a ray ends: keeps its answer (binary leaf nid,
 // closest t - 1e-5) when tests (a) and (b) above hold and returns true;
 // otherwise returns false and the caller has the ray traced by the binary walk.
 __device__ __forceinline__ bool wide_finish(const SceneView& s, TravState& st) {
-    if (!st.hit) return true;   // no hit below tmax anywhere: the binary walk finds none either
+    // no hit below tmax anywhere: the binary walk finds none either -- for rays whose
+    // box test stays finite and conservative (see wide_miss_final)
+    if (!st.hit) return wide_miss_final(st.r);
     const uint4 lo = __ldg(s.wtri_leaf + 2u * st.nid), hi = __ldg(s.wtri_leaf + 2u * st.nid + 1u);
     bool same = hi.w == 1u;     // a single-leaf tree is intersected without a box test
     // a zero direction component makes the reference divide by zero, and an empty
