@@ -161,6 +161,28 @@ int tim_rt_upload_bvh(tim_rt_ctx *ctx, const void *bvh_bytes, uint64_t n_bytes, 
  * New: the reference uploads without any check (BVHData.cpp:43-48). */
 int tim_rt_validate_bvh(const void *bvh_bytes, uint64_t n_bytes, const uint32_t ranges[7][2],
                         const tim_rt_push_constants *pc, uint32_t num_vertex, uint32_t *depth);
+/* Host-only check of the 8-wide quantised form that tim_rt_upload_bvh builds with
+ * TIM_RT_UPLOAD_QUANT8 (no GPU needed). New: the reference has no wide form. The
+ * call validates the image (as tim_rt_validate_bvh), builds the 8-wide form on the
+ * host exactly as the upload does, and checks it against the binary tree: every
+ * used slot's 8-bit box contains the box the reference stores for that subtree,
+ * empty slots are empty, internal slots reach every wide node once, and every
+ * binary leaf's triangles appear once, in order, with the reference's records,
+ * vertices and rounded edges bit for bit. Returns TIM_RT_EINVAL with the first
+ * violation in tim_rt_last_error(); fills the report either way as far as it got. */
+typedef struct {
+    uint32_t nodes;              /* 8-wide nodes */
+    uint32_t depth;              /* levels of 8-wide nodes */
+    uint32_t triangles;          /* leaf triangles (each binary leaf's triangles once) */
+    uint32_t leaf_slots;         /* slots holding a binary leaf */
+    uint32_t internal_slots;     /* slots pointing at a child node */
+    uint32_t slot_histogram[9];  /* nodes by number of used slots, 0..8 */
+    uint32_t reserved[2];
+    uint64_t device_bytes;       /* bytes of the 8-wide arrays on the device */
+} tim_rt_wide_report;
+int tim_rt_wide_check(const void *bvh_bytes, uint64_t n_bytes, const uint32_t ranges[7][2],
+                      const tim_rt_push_constants *pc, const float *pos, uint32_t num_vertex,
+                      tim_rt_wide_report *report);
 /* Replaces BVHData::~BVHData / BVHGeometry::~BVHGeometry (DestroyBuffer). */
 int tim_rt_free_scene(tim_rt_ctx *ctx, tim_rt_scene_id scene);
 /* Device bytes held by one scene. */

@@ -36,6 +36,7 @@ EXPORTED = [
     "tim_rt_server_destroy", "tim_rt_verify_hits", "tim_rt_server_submit_probes", "tim_rt_bvh_file_write",
     "tim_rt_bvh_file_read", "tim_rt_bvh_file_info", "tim_rt_bvh_file_free", "tim_rt_upload_bvh_file",
     "tim_rt_shade_camera", "tim_rt_shade_camera_dev", "tim_rt_build_bvh_gpu", "tim_rt_probe_directions",
+    "tim_rt_wide_check",
 ]
 SORT_NONE, SORT_OCTANT, SORT_MORTON = 0, 1, 2
 BATCH_WIDE = 0x100
@@ -206,6 +207,7 @@ def lib() -> ctypes.CDLL:
                                        ctypes.POINTER(vp)]
     L.tim_rt_shade_camera_dev.argtypes = [vp, u32, vp, u32, vp, vp, vp, vp, vp]
     L.tim_rt_probe_directions.argtypes = [u32, u32, u64, vp, vp]
+    L.tim_rt_wide_check.argtypes = [vp, u64, vp, ctypes.POINTER(PushConstants), vp, u32, ctypes.POINTER(WideReport)]
     for name in EXPORTED:
         if name not in ("tim_rt_version", "tim_rt_last_error", "tim_rt_build_params_default", "tim_rt_bvh_blob_free",
                         "tim_rt_bvh_file_free"):
@@ -268,6 +270,29 @@ def validate(img: BvhImage, num_vertex: int) -> int:
     _check(lib().tim_rt_validate_bvh(data.ctypes.data, data.nbytes, ranges.ctypes.data, ctypes.byref(pc), num_vertex,
                                      ctypes.byref(depth)))
     return depth.value
+
+
+class WideReport(ctypes.Structure):
+    _fields_ = [("nodes", ctypes.c_uint32), ("depth", ctypes.c_uint32), ("triangles", ctypes.c_uint32),
+                ("leaf_slots", ctypes.c_uint32), ("internal_slots", ctypes.c_uint32),
+                ("slot_histogram", ctypes.c_uint32 * 9), ("reserved", ctypes.c_uint32 * 2),
+                ("device_bytes", ctypes.c_uint64)]
+
+
+def wide_check(img: BvhImage, positions) -> dict:
+    """tim_rt_wide_check: builds the 8-wide quantised form on the host as the upload
+    does and checks it against the binary tree; raises TimRtError(EINVAL) on the
+    first violation, returns the report as a dict."""
+    pc = PushConstants(*[int(x) for x in img.pc])
+    ranges = np.ascontiguousarray(img.ranges, np.uint32)
+    data = np.ascontiguousarray(img.data, np.uint8)
+    pos = np.ascontiguousarray(positions, np.float32)
+    r = WideReport()
+    _check(lib().tim_rt_wide_check(data.ctypes.data, data.nbytes, ranges.ctypes.data, ctypes.byref(pc),
+                                   pos.ctypes.data, pos.size // 3, ctypes.byref(r)))
+    return {"nodes": r.nodes, "depth": r.depth, "triangles": r.triangles, "leaf_slots": r.leaf_slots,
+            "internal_slots": r.internal_slots, "slot_histogram": list(r.slot_histogram),
+            "device_bytes": int(r.device_bytes)}
 
 
 def measure_l2_gbs(device: int = 0, nbytes: int = 32 << 20, passes: int = 50) -> float:

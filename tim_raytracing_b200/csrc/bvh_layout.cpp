@@ -314,7 +314,7 @@ struct Collapse {
         if (nf > 0) {
             for (int a = 0; a < 3; ++a)
                 if (!quantise_axis(lo[a], hi[a], nf, origin[a], e[a], cq_lo[a], cq_hi[a])) {
-                    out.err = "box bounds cannot be quantised (non-finite coordinates)";
+                    out.err = "box bounds cannot be quantised (non-finite coordinates, or a node wider than 255 * 2^40)";
                     return false;
                 }
         }
@@ -486,4 +486,172 @@ bool build_wide(const uint8_t* blob, const uint32_t ranges[7][2], uint32_t num_n
     return true;
 }
 
+// ---------------------------------------------------------------------------------- 8-wide check
+
+namespace {
+
+bool same_bits(const float* a, const float* b, int n) { return std::memcmp(a, b, 4 * (size_t)n) == 0; }
+
+// One wide node of the check: its index and the binary subtrees that must be its slots.
+struct CheckJob {
+    uint32_t w;
+    std::vector<Slot> slots;
+    uint32_t depth;
+};
+
+}  // namespace
+
+// Checks an 8-wide form against the binary tree it was built from. It replays the
+// collapse's choice of slots (the same expand and octant placement) from the
+// root and verifies, node by node: each used slot's 8-bit box contains the box
+// the reference stores for that subtree (per plane, in extended precision);
+// empty slots hold the inverted box and no triangles; internal slots point at
+// distinct, in-range nodes; each leaf slot holds exactly its binary leaf's
+// triangles in the leaf's order, with the reference's records, p0 and the
+// rounded edges p1 - p0 and p2 - p0 bit for bit, and per triangle the leaf's id,
+// its ancestor-intersection box and its flag. Finally every wide node and every
+// wide triangle must have been reached exactly once.
+bool check_wide(const uint8_t* blob, const uint32_t ranges[7][2], uint32_t num_nodes, const float* pos,
+                const WideHost& w, tim_rt_wide_report& rep, std::string& err) {
+    Collapse C;
+    C.nodes = reinterpret_cast<const PNode*>(blob + ranges[TIM_RT_RANGE_NODE][0]);
+    C.leaf = reinterpret_cast<const uint32_t*>(blob + ranges[TIM_RT_RANGE_LEAF][0]);
+    C.leaf_words = ranges[TIM_RT_RANGE_LEAF][1] / 4u;
+    C.pos = pos;
+    C.root_is_leaf = num_nodes == 1u;
+    std::memset(&rep, 0, sizeof(rep));
+    const uint64_t nw = w.num_nodes, nt = w.tris.size() / 12;
+    if (nw == 0 || w.nodes.size() != 20ull * nw || w.tri_leaf.size() != 8ull * nt) { err = "8-wide arrays have inconsistent sizes"; return false; }
+    std::vector<uint8_t> node_seen(nw, 0), tri_seen(nt, 0);
+    std::vector<CheckJob> stack;
+    if (C.root_is_leaf) {
+        Slot s;
+        s.id = kLeafBit;
+        for (int a = 0; a < 3; ++a) { s.lo[a] = s.hi[a] = s.elo[a] = s.ehi[a] = 0.f; }
+        stack.push_back({0u, {s}, 1u});
+    } else {
+        Slot a, b;
+        child_slots(C.nodes[0], a, b, nullptr);
+        stack.push_back({0u, C.expand({a, b}), 1u});
+    }
+    auto fail = [&](uint32_t wi, const std::string& what) {
+        err = "8-wide node " + std::to_string(wi) + ": " + what;
+        return false;
+    };
+    while (!stack.empty()) {
+        CheckJob job = std::move(stack.back());
+        stack.pop_back();
+        const uint32_t wi = job.w;
+        if (wi >= nw) return fail(wi, "index out of range");
+        if (node_seen[wi]) return fail(wi, "reached twice");
+        node_seen[wi] = 1;
+        rep.depth = std::max(rep.depth, job.depth);
+        const uint32_t* W = w.nodes.data() + 20ull * wi;
+        float origin[3];
+        std::memcpy(origin, W, 12);
+        const uint32_t e[3] = {W[3] & 0xFFu, (W[3] >> 8) & 0xFFu, (W[3] >> 16) & 0xFFu};
+        const uint32_t imask = W[3] >> 24, child_base = W[4], tri_base = W[5];
+        uint8_t meta[8], qb[48];
+        std::memcpy(meta, &W[6], 8);
+        std::memcpy(qb, &W[8], 48);
+        int slot_child[8];
+        assign_octant_slots(job.slots, C.root_is_leaf, slot_child);
+        uint32_t used = 0, tri_cursor = tri_base;
+        for (int k = 0; k < 8; ++k) {
+            const int i = slot_child[k];
+            if (i < 0) {
+                for (int a = 0; a < 3; ++a)
+                    if (qb[8 * a + k] != 255u || qb[24 + 8 * a + k] != 0u) return fail(wi, "empty slot without the inverted box");
+                if (meta[k] || ((imask >> k) & 1u)) return fail(wi, "empty slot with content");
+                continue;
+            }
+            ++used;
+            const Slot& sl = job.slots[i];
+            for (int a = 0; a < 3; ++a) {
+                float sc;
+                const uint32_t bits = e[a] << 23;
+                std::memcpy(&sc, &bits, 4);
+                const float lo = std::min(sl.lo[a], sl.hi[a]), hi = std::max(sl.lo[a], sl.hi[a]);
+                if (!plane_le(origin[a], sc, qb[8 * a + k], lo) || !plane_ge(origin[a], sc, qb[24 + 8 * a + k], hi))
+                    return fail(wi, "slot " + std::to_string(k) + " box does not contain the reference box");
+            }
+            if (sl.id & kLeafBit) {
+                if ((imask >> k) & 1u) return fail(wi, "leaf slot marked internal");
+                const uint32_t n = C.leaf_tris(sl.id);
+                if (meta[k] != n) return fail(wi, "leaf slot triangle count differs from the binary leaf");
+                ++rep.leaf_slots;
+                const uint32_t nm = sl.id & kMask, off = C.nodes[nm].nid[3];
+                for (uint32_t t = 0; t < n; ++t, ++tri_cursor) {
+                    if (tri_cursor >= nt) return fail(wi, "leaf triangles out of range");
+                    if (tri_seen[tri_cursor]) return fail(wi, "wide triangle used twice");
+                    tri_seen[tri_cursor] = 1;
+                    const uint32_t* r = C.leaf + 1u + off + 3u * t;
+                    const float* T = w.tris.data() + 12ull * tri_cursor;
+                    uint32_t rec[3];
+                    std::memcpy(&rec[0], &T[3], 4);
+                    std::memcpy(&rec[1], &T[7], 4);
+                    std::memcpy(&rec[2], &T[11], 4);
+                    if (rec[0] != r[0] || rec[1] != r[1] || rec[2] != r[2]) return fail(wi, "triangle record differs");
+                    const float* P0 = pos + 3ull * (r[0] + (r[1] & 0xFFFFu));
+                    const float* P1 = pos + 3ull * (r[0] + (r[1] >> 16));
+                    const float* P2 = pos + 3ull * (r[0] + (r[2] & 0xFFFFu));
+                    const float e1[3] = {P1[0] - P0[0], P1[1] - P0[1], P1[2] - P0[2]};
+                    const float e2[3] = {P2[0] - P0[0], P2[1] - P0[1], P2[2] - P0[2]};
+                    if (!same_bits(T, P0, 3) || !same_bits(T + 4, e1, 3) || !same_bits(T + 8, e2, 3))
+                        return fail(wi, "triangle vertices or edges differ");
+                    const uint32_t* L = w.tri_leaf.data() + 8ull * tri_cursor;
+                    float elo[3], ehi[3];
+                    std::memcpy(elo, &L[0], 12);
+                    std::memcpy(ehi, &L[4], 12);
+                    const bool empty = sl.elo[0] > sl.ehi[0] || sl.elo[1] > sl.ehi[1] || sl.elo[2] > sl.ehi[2];
+                    const uint32_t flag = C.root_is_leaf ? 1u : (empty ? 2u : 0u);
+                    if (L[3] != nm || L[7] != flag || !same_bits(elo, sl.elo, 3) || !same_bits(ehi, sl.ehi, 3))
+                        return fail(wi, "binary-leaf record of a triangle differs");
+                }
+            } else {
+                if (!((imask >> k) & 1u)) return fail(wi, "internal slot not marked internal");
+                if (meta[k]) return fail(wi, "internal slot with triangles");
+                ++rep.internal_slots;
+                const uint32_t child = child_base + (uint32_t)__builtin_popcount(imask & ((1u << k) - 1u));
+                Slot a, b;
+                child_slots(C.nodes[sl.id], a, b, &sl);
+                stack.push_back({child, C.expand({a, b}), job.depth + 1u});
+            }
+        }
+        ++rep.slot_histogram[used];
+    }
+    for (uint64_t i = 0; i < nw; ++i)
+        if (!node_seen[i]) { err = "8-wide node " + std::to_string(i) + " is not reachable"; return false; }
+    for (uint64_t i = 0; i < nt; ++i)
+        if (!tri_seen[i]) { err = "8-wide triangle " + std::to_string(i) + " belongs to no leaf slot"; return false; }
+    rep.nodes = (uint32_t)nw;
+    rep.triangles = (uint32_t)nt;
+    rep.device_bytes = 80ull * nw + 48ull * nt + 32ull * nt;
+    if (rep.depth != w.max_depth) { err = "8-wide depth differs from the recorded depth"; return false; }
+    return true;
+}
+
 }  // namespace timrt
+
+extern "C" int tim_rt_wide_check(const void* bvh_bytes, uint64_t n_bytes, const uint32_t ranges[7][2],
+                                 const tim_rt_push_constants* pc, const float* pos, uint32_t num_vertex,
+                                 tim_rt_wide_report* report) {
+    if (!bvh_bytes || !ranges || !pc || !pos || !report) {
+        timrt::set_error("tim_rt_wide_check: null argument");
+        return TIM_RT_EINVAL;
+    }
+    std::string err;
+    const uint8_t* blob = static_cast<const uint8_t*>(bvh_bytes);
+    uint32_t depth = 0;
+    if (!timrt::validate_bvh(blob, n_bytes, ranges, pc->numNodes, num_vertex, pc->numLights, pc->numBlas, &depth, err)) {
+        timrt::set_error("tim_rt_wide_check: " + err);
+        return TIM_RT_EINVAL;
+    }
+    timrt::WideHost w;
+    if (!timrt::build_wide(blob, ranges, pc->numNodes, pos, w, err) ||
+        !timrt::check_wide(blob, ranges, pc->numNodes, pos, w, *report, err)) {
+        timrt::set_error("tim_rt_wide_check: " + err);
+        return TIM_RT_EINVAL;
+    }
+    return TIM_RT_OK;
+}
