@@ -1,0 +1,63 @@
+"""CPU property tests of the two margin arguments the traversal kernels rest on
+(no GPU needed). Each C program under tests/c restates a kernel's arithmetic and
+checks, on seeded cases built to sit on the decision boundary, the property the
+kernel's exactness depends on:
+
+* tests/c/box_filter_check.c -- the binary walk's filtered child-box test
+  (csrc/trace_plain.cuh: box_filter, plain_children) takes only decisions that
+  CollideBox (the reference's divisions) takes too;
+* tests/c/wide_slab_check.c -- the 8-wide walk's quantised slot test
+  (csrc/trace_wide.cuh: wide_visit) accepts every slot whose reference box
+  CollideBox accepts, for the rays the 8-wide walk trusts.
+
+The GPU parity tests check the kernels themselves against the oracle."""
+import shutil
+import subprocess
+from pathlib import Path
+
+import pytest
+
+HERE = Path(__file__).resolve().parent
+
+
+def _build(tmp_path_factory, name):
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    exe = tmp_path_factory.mktemp(name) / name
+    subprocess.run([cc, "-O2", "-ffp-contract=off", "-fno-fast-math", str(HERE / "c" / f"{name}.c"), "-o", str(exe),
+                    "-lm"], check=True)
+    return exe
+
+
+def _run(exe, cases, seed):
+    r = subprocess.run([str(exe), str(cases), str(seed)], capture_output=True, text=True)
+    words = r.stdout.split()
+    return r.returncode, dict(zip(words[0::2], map(int, words[1::2]))), r.stdout + r.stderr
+
+
+@pytest.fixture(scope="module")
+def box_filter_check(tmp_path_factory):
+    return _build(tmp_path_factory, "box_filter_check")
+
+
+@pytest.fixture(scope="module")
+def wide_slab_check(tmp_path_factory):
+    return _build(tmp_path_factory, "wide_slab_check")
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_filtered_box_test_never_decides_wrong(box_filter_check, seed):
+    rc, c, out = _run(box_filter_check, 1000000, seed)
+    assert rc == 0 and c["wrong"] == 0 and c["order_wrong"] == 0, out
+    # the boundary is really exercised: many undecided tests, many decided ones, many orders
+    assert c["undecided"] > 0.05 * c["tests"]
+    assert c["tests"] - c["undecided"] > 0.3 * c["tests"]
+    assert c["orders"] > 1000
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_quantised_slot_test_never_loses_a_hit(wide_slab_check, seed):
+    rc, c, out = _run(wide_slab_check, 1000000, seed)
+    assert rc == 0 and c["lost"] == 0 and c["nonfinite"] == 0, out
+    assert c["ref_hits"] > 0.2 * c["cases"]
