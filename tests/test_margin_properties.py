@@ -8,7 +8,10 @@ kernel's exactness depends on:
   CollideBox (the reference's divisions) takes too;
 * tests/c/wide_slab_check.c -- the 8-wide walk's quantised slot test
   (csrc/trace_wide.cuh: wide_visit) accepts every slot whose reference box
-  CollideBox accepts, for the rays the 8-wide walk trusts.
+  CollideBox accepts, for the rays the 8-wide walk trusts;
+* tests/c/ebox_check.c -- the 8-wide walk's cheap proof that the binary walk
+  reaches a hit's leaf (csrc/trace_wide.cuh: wide_finish) succeeds only where
+  CollideBox on the leaf's ancestor-intersection box agrees.
 
 The GPU parity tests check the kernels themselves against the oracle."""
 import shutil
@@ -46,6 +49,11 @@ def wide_slab_check(tmp_path_factory):
     return _build(tmp_path_factory, "wide_slab_check")
 
 
+@pytest.fixture(scope="module")
+def ebox_check(tmp_path_factory):
+    return _build(tmp_path_factory, "ebox_check")
+
+
 @pytest.mark.parametrize("seed", [1, 2, 3])
 def test_filtered_box_test_never_decides_wrong(box_filter_check, seed):
     rc, c, out = _run(box_filter_check, 1000000, seed)
@@ -61,3 +69,10 @@ def test_quantised_slot_test_never_loses_a_hit(wide_slab_check, seed):
     rc, c, out = _run(wide_slab_check, 1000000, seed)
     assert rc == 0 and c["lost"] == 0 and c["nonfinite"] == 0, out
     assert c["ref_hits"] > 0.2 * c["cases"]
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_reachability_proof_is_never_false(ebox_check, seed):
+    rc, c, out = _run(ebox_check, 1000000, seed)
+    assert rc == 0 and c["false_proofs"] == 0, out
+    assert c["proofs"] > 0.02 * c["cases"]
