@@ -11,7 +11,10 @@ kernel's exactness depends on:
   CollideBox accepts, for the rays the 8-wide walk trusts;
 * tests/c/ebox_check.c -- the 8-wide walk's cheap proof that the binary walk
   reaches a hit's leaf (csrc/trace_wide.cuh: wide_finish) succeeds only where
-  CollideBox on the leaf's ancestor-intersection box agrees.
+  CollideBox on the leaf's ancestor-intersection box agrees;
+* tests/c/tie_window_check.c -- the window in which the 8-wide walk keeps
+  testing triangles after its nearest hit t1 holds every t2 that could still
+  change the reference's answer (RN(t2 - 1e-5) <= t1).
 
 The GPU parity tests check the kernels themselves against the oracle."""
 import shutil
@@ -36,7 +39,7 @@ def _build(tmp_path_factory, name):
 def _run(exe, cases, seed):
     r = subprocess.run([str(exe), str(cases), str(seed)], capture_output=True, text=True)
     words = r.stdout.split()
-    return r.returncode, dict(zip(words[0::2], map(int, words[1::2]))), r.stdout + r.stderr
+    return r.returncode, dict(zip(words[0::2], map(float, words[1::2]))), r.stdout + r.stderr
 
 
 @pytest.fixture(scope="module")
@@ -52,6 +55,11 @@ def wide_slab_check(tmp_path_factory):
 @pytest.fixture(scope="module")
 def ebox_check(tmp_path_factory):
     return _build(tmp_path_factory, "ebox_check")
+
+
+@pytest.fixture(scope="module")
+def tie_window_check(tmp_path_factory):
+    return _build(tmp_path_factory, "tie_window_check")
 
 
 @pytest.mark.parametrize("seed", [1, 2, 3])
@@ -76,3 +84,10 @@ def test_reachability_proof_is_never_false(ebox_check, seed):
     rc, c, out = _run(ebox_check, 1000000, seed)
     assert rc == 0 and c["false_proofs"] == 0, out
     assert c["proofs"] > 0.02 * c["cases"]
+
+
+@pytest.mark.parametrize("seed", [1, 2])
+def test_near_tie_window_holds_every_blocking_hit(tie_window_check, seed):
+    rc, c, out = _run(tie_window_check, 300000, seed)
+    assert rc == 0 and c["missed"] == 0, out
+    assert c["min_gap_ulps"] >= 2
