@@ -91,3 +91,50 @@ def test_near_tie_window_holds_every_blocking_hit(tie_window_check, seed):
     rc, c, out = _run(tie_window_check, 300000, seed)
     assert rc == 0 and c["missed"] == 0, out
     assert c["min_gap_ulps"] >= 2
+
+
+def test_nearest_hit_is_order_independent_outside_the_window():
+    """Rule (a) of the 8-wide walk: if no other hit t2 has RN(t2 - 1e-5) <= t1
+    (t1 the smallest hit t), the reference's shrinking acceptance (accept t iff
+    t < c, then c = RN(t - 1e-5)) ends on t1 in every visit order; and when some
+    t2 is inside that window, some order gives another answer (so the walk must
+    hand such rays to the binary walk). Simulated in float32 over random hit sets
+    with many near-ties."""
+    import numpy as np
+    rng = np.random.default_rng(5)
+    off = np.float32(1e-5)
+    tmax = np.float32(100.0)
+
+    def final(order):
+        c, best = tmax, None
+        for i in order:
+            if ts[i] < c:
+                c, best = np.float32(ts[i] - off), i
+        return best
+
+    outside = inside = 0
+    for _ in range(20000):
+        n = int(rng.integers(2, 6))
+        base = np.float32(rng.uniform(0.01, 50.0))
+        ts = (base + rng.choice([0.0, 2e-6, 5e-6, 9.9e-6, 1e-5, 1.1e-5, 3e-5, 1.0], size=n)
+              * rng.choice([1.0, -1.0], size=n)).astype(np.float32)
+        ts = ts[ts > 0]
+        if len(ts) < 2:
+            continue
+        i1 = int(np.argmin(ts))
+        t1 = ts[i1]
+        others = np.delete(ts, i1)
+        window = bool(np.any((others - off).astype(np.float32) <= t1))
+        answers = {ts[final(rng.permutation(len(ts)))] for _ in range(12)}
+        answers.add(ts[final(range(len(ts)))])
+        if not window:
+            outside += 1
+            assert answers == {t1}, (ts, answers)
+        else:
+            inside += 1
+            # a hit j in the window visited before t1 lowers c to RN(t_j - 1e-5) <= t1,
+            # so t1 is rejected and the answer is another triangle: the rule is tight
+            j = next(i for i in range(len(ts)) if i != i1 and np.float32(ts[i] - off) <= t1)
+            order = [j, i1] + [i for i in range(len(ts)) if i not in (j, i1)]
+            assert final(order) != i1
+    assert outside > 1000 and inside > 1000
