@@ -15,7 +15,7 @@ The rewrites are mechanical and change no arithmetic or control flow:
      runtime-sized arrays `T name[];` become bounds-checked views
      (`GLSL_SSBO(T, name)`), other members static variables.
      `layout(...) uniform <image/sampler> name[...];` becomes a static variable and
-     `layout(local_size...) in;` is dropped (the driver dispatches invocations).
+     `layout(local_size...) in;` is dropped (the C++ host program dispatches the invocations).
   4. Parameter qualifiers: `in T x` -> `T x`, `out T x` / `inout T x` -> `T& x`.
   5. Unsuffixed floating-point literals get an `f` suffix: a GLSL literal such as
      `10e-6` is a float, a C++ one a double.

@@ -1,5 +1,5 @@
 // probe_bw.cu -- L2 read-bandwidth probe used as the roofline denominator for
-// kernels whose working set is L2-resident (the driver-measured peaks cover
+// kernels whose working set is L2-resident (the measured peaks in MEASURED_PEAKS.json cover
 // HBM and tensor throughput only).
 //
 // A buffer well below the L2 size is first touched, then read `passes` times
