@@ -169,7 +169,8 @@ int tim_rt_validate_bvh(const void *bvh_bytes, uint64_t n_bytes, const uint32_t 
  * empty slots are empty, internal slots reach every wide node once, and every
  * binary leaf's triangles appear once, in order, with the reference's records,
  * vertices and rounded edges bit for bit. Returns TIM_RT_EINVAL with the first
- * violation in tim_rt_last_error(); fills the report either way as far as it got. */
+ * violation in tim_rt_last_error(); the report is zeroed first and filled as far
+ * as the check got. */
 typedef struct {
     uint32_t nodes;              /* 8-wide nodes */
     uint32_t depth;              /* levels of 8-wide nodes */

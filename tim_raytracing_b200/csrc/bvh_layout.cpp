@@ -640,6 +640,7 @@ extern "C" int tim_rt_wide_check(const void* bvh_bytes, uint64_t n_bytes, const 
         timrt::set_error("tim_rt_wide_check: null argument");
         return TIM_RT_EINVAL;
     }
+    std::memset(report, 0, sizeof(*report));
     std::string err;
     const uint8_t* blob = static_cast<const uint8_t*>(bvh_bytes);
     uint32_t depth = 0;
