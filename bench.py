@@ -124,29 +124,41 @@ def profiled_traffic(name, form):
         return None
 
 
-def cpu_baseline(scene, img, pd, threads, budget_s=12.0):
+def cpu_baseline(scene, img, pd, threads, budget_s=15.0):
     """The oracle (C restatement of the reference's GLSL trace path, OpenMP over
-    pixels) on a bounded sample of the same frame: whole rows from the middle of
-    the image until about budget_s seconds of CPU work."""
+    pixels) on a bounded sample of the same frame: after a warm-up, whole rows
+    spread over the image until about a third of budget_s seconds of CPU work,
+    then the same rows twice more; the best of the three passes counts."""
     from oracle import oracle as O
     sc = O.Scene(img, scene.positions, scene.normals)
     tx, ty = (W + 15) // 16, (H + 15) // 16
     counts, lists = O.cull_lights(sc, pd, tx, ty, threads=threads)
     flags = 2 | 4
-    rays = 0
-    elapsed = 0.0
-    rows = 0
     stride = 37   # coprime with H - 1: visits rows spread over the whole frame
-    while elapsed < budget_s and rows < H - 1:
-        b = 1 + (rows * stride) % (H - 1)
-        t0 = time.perf_counter()
+
+    def row(k):
+        b = 1 + (k * stride) % (H - 1)
         _, _, c = O.camera(sc, pd, flags=flags, seed=1, tile_counts=counts, tile_lists=lists,
                            pix_range=(b * W, (b + 1) * W), threads=threads)
-        elapsed += time.perf_counter() - t0
-        rays += int(c.sum())
+        return int(c.sum())
+
+    for k in range(8):   # warm-up: page in the scene and the worker threads
+        row(k)
+    rays = rows = 0
+    t0 = time.perf_counter()
+    while time.perf_counter() - t0 < budget_s / 3 and rows < H - 1:
+        rays += row(rows)
         rows += 1
-    out = {"value": rays / elapsed / 1e6, "unit": METRIC, "cores": threads, "kind": "port",
-           "sample": f"{rows} of {H - 1} traced rows ({rays} rays) of the same frame, {elapsed:.1f} s"}
+    passes = [time.perf_counter() - t0]
+    for _ in range(2):
+        t0 = time.perf_counter()
+        for k in range(rows):
+            row(k)
+        passes.append(time.perf_counter() - t0)
+    best = min(passes)
+    out = {"value": rays / best / 1e6, "unit": METRIC, "cores": threads, "kind": "port",
+           "sample": f"{rows} of {H - 1} traced rows ({rays} rays) of the same frame, best of 3 passes "
+                     f"({', '.join(f'{t:.2f}' for t in passes)} s)"}
     out.update(reference_builder(scene))
     return out
 
