@@ -222,9 +222,9 @@ struct Job {
 // Wide nodes, leaf-triangle records and their binary-leaf records of one part of
 // the collapse (the whole tree, or one subtree built on a worker thread).
 struct Part {
-    std::vector<uint32_t> nodes;     // 20 words per node
-    std::vector<float> tris;         // 12 floats per leaf triangle
-    std::vector<uint32_t> tri_leaf;  // 8 words per leaf triangle
+    RawVec<uint32_t> nodes;          // 20 words per node (each written in full by its fill)
+    RawVec<float> tris;              // 12 floats per leaf triangle
+    RawVec<uint32_t> tri_leaf;       // 8 words per leaf triangle
     uint32_t num_nodes = 0;
     uint32_t max_depth = 0;
     std::string err;
@@ -466,9 +466,9 @@ bool build_wide(const uint8_t* blob, const uint32_t ranges[7][2], uint32_t num_n
                 std::memcpy(top.tris.data() + 12ull * tri_off[k], p.tris.data(), 4ull * p.tris.size());
                 std::memcpy(top.tri_leaf.data() + 8ull * tri_off[k], p.tri_leaf.data(), 4ull * p.tri_leaf.size());
             }
-            std::vector<uint32_t>().swap(p.nodes);   // release the part's memory early
-            std::vector<float>().swap(p.tris);
-            std::vector<uint32_t>().swap(p.tri_leaf);
+            RawVec<uint32_t>().swap(p.nodes);   // release the part's memory early
+            RawVec<float>().swap(p.tris);
+            RawVec<uint32_t>().swap(p.tri_leaf);
         }
     };
     pool.clear();

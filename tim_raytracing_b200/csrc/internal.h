@@ -1,7 +1,10 @@
 // internal.h -- host-side structures shared by the C-ABI implementation files.
 #pragma once
 #include <cstdint>
+#include <memory>
 #include <string>
+#include <type_traits>
+#include <utility>
 #include <vector>
 #include "../../include/tim_rt.h"
 
@@ -9,15 +12,32 @@ namespace timrt {
 
 void set_error(const std::string& msg);
 
+// Allocator whose value-initialisation leaves trivial elements uninitialised, so
+// that resize() of an array about to be overwritten in full does not zero it first.
+template <class T>
+struct NoInitAlloc : std::allocator<T> {
+    template <class U>
+    struct rebind { using other = NoInitAlloc<U>; };
+    NoInitAlloc() = default;
+    template <class U>
+    NoInitAlloc(const NoInitAlloc<U>&) noexcept {}
+    template <class U>
+    void construct(U* p) noexcept(std::is_nothrow_default_constructible<U>::value) { ::new (static_cast<void*>(p)) U; }
+    template <class U, class... A>
+    void construct(U* p, A&&... a) { ::new (static_cast<void*>(p)) U(std::forward<A>(a)...); }
+};
+template <class T>
+using RawVec = std::vector<T, NoInitAlloc<T>>;
+
 // Host image of the 8-wide quantised BVH built from the reference binary tree.
 struct WideHost {
-    std::vector<uint32_t> nodes;     // 20 words per node
-    std::vector<float> tris;         // 12 floats per leaf triangle
+    RawVec<uint32_t> nodes;          // 20 words per node
+    RawVec<float> tris;              // 12 floats per leaf triangle
     // per leaf triangle, 8 words about its binary leaf: lo.xyz of the intersection
     // of the leaf's box and all its ancestors' boxes, the leaf's nid, hi.xyz of
     // that intersection, and a flag: 1 when the reference tests the leaf without a
     // box (single-leaf tree), 2 when the intersection is empty
-    std::vector<uint32_t> tri_leaf;
+    RawVec<uint32_t> tri_leaf;
     uint32_t num_nodes = 0;
     uint32_t root_is_leaf = 0;
     uint32_t max_depth = 0;
