@@ -119,3 +119,40 @@ def test_malformed_images_are_rejected(native):
 
     for m in (child_loop, leaf_past_end, vertex_oob, range_oob):
         bad(m)
+
+
+def test_bad_builder_inputs_are_refused(native):
+    """tim_rt_build_bvh refuses inputs it cannot build from, with EINVAL and a
+    message, instead of building a tree that indexes out of range."""
+    import ctypes
+    from tim_raytracing_b200 import scenes
+    s = scenes.random_triangles(4, 200)
+    L = native.lib()
+    pos = np.ascontiguousarray(s.positions, np.float32)
+    rec = np.ascontiguousarray(s.tri_records())
+    mats = s.materials_bytes()
+    nmat = len(mats) // 48
+
+    def build(pos, rec, **params):
+        p = native.build_params(**params)
+        out = ctypes.c_void_p()
+        rc = L.tim_rt_build_bvh(pos.ctypes.data, pos.shape[0], rec.ctypes.data, rec.shape[0], mats, nmat, None, 0,
+                                ctypes.byref(p), ctypes.byref(out))
+        if rc == native.OK:
+            L.tim_rt_bvh_blob_free(out)
+        return rc, L.tim_rt_last_error().decode()
+
+    assert build(pos, rec)[0] == native.OK
+    bad = rec.copy()
+    bad[7, 0] = pos.shape[0]                      # vertex offset past the vertex array
+    rc, msg = build(pos, bad)
+    assert rc == native.EINVAL and "num_vertex" in msg
+    nanpos = pos.copy()
+    nanpos[5, 1] = np.nan
+    rc, msg = build(nanpos, rec)
+    assert rc == native.EINVAL and "non-finite" in msg
+    for params in ({"max_leaf_size": 0}, {"max_depth": 33}, {"max_depth": 0}):
+        rc, msg = build(pos, rec, **params)
+        assert rc == native.EINVAL and "max_leaf_size" in msg, params
+    rc, msg = build(pos, rec[:0])
+    assert rc == native.EINVAL

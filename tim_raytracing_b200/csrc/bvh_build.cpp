@@ -182,16 +182,17 @@ int tim_rt_build_bvh(const float* pos, uint32_t num_vertex, const uint32_t* tri,
             set_error("tim_rt_build_bvh: triangle " + std::to_string(t) + " indexes past num_vertex");
             return TIM_RT_EINVAL;
         }
+        // checked per coordinate: the box's min / max would step over a NaN
+        for (const uint64_t i : {i0, i1, i2})
+            for (int a = 0; a < 3; ++a)
+                if (!std::isfinite(pos[3 * i + a])) {
+                    set_error("tim_rt_build_bvh: non-finite vertex position");
+                    return TIM_RT_EINVAL;
+                }
         tb[t].grow(pos + 3 * i0);
         tb[t].grow(pos + 3 * i1);
         tb[t].grow(pos + 3 * i2);
-        for (int a = 0; a < 3; ++a) {
-            if (!std::isfinite(tb[t].lo[a]) || !std::isfinite(tb[t].hi[a])) {
-                set_error("tim_rt_build_bvh: non-finite vertex position");
-                return TIM_RT_EINVAL;
-            }
-            cen[3ull * t + a] = 0.5f * (tb[t].lo[a] + tb[t].hi[a]);
-        }
+        for (int a = 0; a < 3; ++a) cen[3ull * t + a] = 0.5f * (tb[t].lo[a] + tb[t].hi[a]);
     }
     std::vector<uint32_t> idx(num_tris);
     for (uint32_t t = 0; t < num_tris; ++t) idx[t] = t;
