@@ -148,3 +148,41 @@ def test_malformed_image_is_refused(native):
     with pytest.raises(native.TimRtError) as e:
         native.wide_check(bad, s.positions)
     assert e.value.code == native.EINVAL
+
+
+def test_corrupt_images_never_crash_the_host(native):
+    """Validation and the host-side 8-wide collapse on corrupted images: every
+    corruption is either refused (EINVAL) or yields a checked 8-wide form; none
+    may crash the process. A NaN or infinite child box once made the slot
+    assignment write outside its array."""
+    s, img = load_room()
+    rng = np.random.default_rng(17)
+    o, size = img.ranges[native.RANGE_NODE]
+    lo_, lsize = img.ranges[native.RANGE_LEAF]
+    # the regression: non-finite child boxes. A NaN plane cannot be quantised and is
+    # refused; an infinite one is refused or, where the collapse opens that child
+    # (its box is then not stored), checked like any other image.
+    for val in (np.nan, np.inf, -np.inf):
+        bad = native.BvhImage(img.data.copy(), img.ranges.copy(), img.pc, img.aabb)
+        bad.data[o + 16:o + 20] = np.frombuffer(np.float32(val).tobytes(), np.uint8)   # root's child 0 min.x
+        try:
+            native.wide_check(bad, s.positions)
+            assert not np.isnan(val)
+        except native.TimRtError as e:
+            assert e.code == native.EINVAL
+    refused = checked = 0
+    for _ in range(400):
+        data = img.data.copy()
+        words = data.view(np.uint32)
+        for _ in range(int(rng.integers(1, 5))):
+            base, n = (o, size) if rng.integers(0, 2) else (lo_, lsize)
+            i = (int(base) + 4 * int(rng.integers(0, int(n) // 4))) // 4
+            words[i] = rng.choice([0, 0xFFFFFFFF, 0x3FFFFFFF, 0x80000000, 0x7FC00000, int(rng.integers(0, 2**32)),
+                                   (int(words[i]) + 1) & 0xFFFFFFFF, int(words[i]) ^ (1 << int(rng.integers(0, 32)))])
+        try:
+            native.wide_check(native.BvhImage(data, img.ranges.copy(), img.pc, img.aabb), s.positions)
+            checked += 1
+        except native.TimRtError as e:
+            assert e.code == native.EINVAL
+            refused += 1
+    assert refused > 0 and checked > 0

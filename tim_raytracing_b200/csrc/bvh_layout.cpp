@@ -162,7 +162,9 @@ void assign_octant_slots(const std::vector<Slot>& fr, bool single_leaf_root, int
                 if (slot_child[s] >= 0) continue;
                 double cost = 0.0;
                 for (int a = 0; a < 3; ++a) cost -= (cen[i][a] - c[a]) * (((s >> a) & 1) ? 1.0 : -1.0);
-                if (cost < best) { best = cost; bi = i; bs = s; }
+                // the first candidate is taken whatever its cost, so that a NaN cost
+                // (a corrupt, non-finite box) cannot leave the child without a slot
+                if (bi < 0 || cost < best) { best = cost; bi = i; bs = s; }
             }
         }
         slot_child[bs] = bi;
