@@ -55,3 +55,19 @@ def test_struct_sizes(native):
     assert ctypes.sizeof(native.PushConstants) == 20
     assert scenes.PASS_DATA_DTYPE.itemsize == 240
     assert np.zeros((1, 8), np.float32).nbytes == 32   # tim_rt_ray
+
+
+def test_python_bindings_check_host_buffers(native):
+    """The bindings refuse host arrays the C call would read or write past,
+    before any call is made."""
+    r = native._ray_records(np.zeros((5, 8), np.float64))
+    assert r.dtype == np.float32 and r.shape == (5, 8)
+    for bad in (np.zeros((5, 7), np.float32), np.zeros(40, np.float32), np.zeros((2, 4, 8), np.float32)):
+        with pytest.raises(ValueError):
+            native._ray_records(bad)
+    ok = np.zeros((10, 4), np.uint32)
+    assert native._host_buf(ok, np.uint32, 40, "hit") is ok
+    for bad, count in ((np.zeros((10, 4), np.uint32), 41), (np.zeros((10, 4), np.int64), 40),
+                       (np.zeros((4, 10), np.uint32).T, 40), ([0] * 40, 40)):
+        with pytest.raises(ValueError):
+            native._host_buf(bad, np.uint32, count, "hit")

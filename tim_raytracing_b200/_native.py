@@ -221,6 +221,23 @@ def _check(rc: int):
         raise TimRtError(rc, lib().tim_rt_last_error().decode())
 
 
+def _host_buf(a, dtype, count: int, name: str):
+    """A caller-provided host array that the C call reads or writes `count` elements
+    of: checked (type, layout, size) and passed as it is, never copied."""
+    if not isinstance(a, np.ndarray) or a.dtype != np.dtype(dtype) or not a.flags["C_CONTIGUOUS"] or a.size < count:
+        raise ValueError(f"{name}: needs a C-contiguous {np.dtype(dtype).name} array of at least {count} elements")
+    return a
+
+
+def _ray_records(rays) -> np.ndarray:
+    """Rays as the C ABI reads them: 32-byte records, float32 [n, 8] (flags as raw
+    u32 bits in column 7)."""
+    r = np.ascontiguousarray(rays, np.float32)
+    if r.ndim != 2 or r.shape[1] != 8:
+        raise ValueError(f"rays: needs shape [n, 8] (32-byte tim_rt_ray records), got {r.shape}")
+    return r
+
+
 def _copy_bytes(ptr: int, n: int) -> np.ndarray:
     """A uint8 copy of n bytes at a C pointer (one copy, no intermediate bytes object)."""
     if n == 0:
@@ -505,11 +522,12 @@ class Context:
 
     def trace(self, sid: int, rays: np.ndarray, mode: int = MODE_CLOSEST, want_nid=True, want_bary=True,
               hit=None, nid=None, bary=None):
-        rays = np.ascontiguousarray(rays, np.float32)
+        rays = _ray_records(rays)
         n = rays.shape[0]
-        hit = np.empty((n, 4), np.uint32) if hit is None else hit
-        nid = (np.empty(n, np.uint32) if want_nid else None) if nid is None else nid
-        bary = (np.empty((n, 2), np.float32) if want_bary else None) if bary is None else bary
+        hit = np.empty((n, 4), np.uint32) if hit is None else _host_buf(hit, np.uint32, 4 * n, "hit")
+        nid = (np.empty(n, np.uint32) if want_nid else None) if nid is None else _host_buf(nid, np.uint32, n, "nid")
+        bary = ((np.empty((n, 2), np.float32) if want_bary else None) if bary is None
+                else _host_buf(bary, np.float32, 2 * n, "bary"))
         st = Stats()
         _check(self._L.tim_rt_trace(self._c, sid, rays.ctypes.data, n, mode, _ptr(hit), _ptr(nid), _ptr(bary),
                                     ctypes.byref(st)))
@@ -548,9 +566,11 @@ class Context:
         probe_end = total if probe_end is None else probe_end
         np_ = probe_end - probe_begin
         nd = int(desc.num_dirs)
-        assert sh16.dtype == np.uint16 and sh16.size == 7 * total * 4 and sh16.flags["C_CONTIGUOUS"]
+        _host_buf(sh16, np.uint16, 7 * total * 4, "sh16")
         dirs = np.ascontiguousarray(dirs, np.float32)
         basis = np.ascontiguousarray(sh_basis, np.float32)
+        if dirs.size < 4 * nd or basis.size < 9 * nd:
+            raise ValueError(f"dirs / sh_basis: need {nd} directions (float4) and {nd} x 9 basis weights")
         tr = np.empty((np_, nd, 8), np.uint32) if want_trace else None
         irr = np.empty((np_, nd, 3), np.float32) if want_irr else None
         s32 = np.empty((np_, 9, 3), np.float32) if want_sh32 else None
@@ -567,7 +587,12 @@ class Context:
         W, H = (int(x) for x in np.asarray(pd["frameSize"]).reshape(-1)[:2])
         pd = np.ascontiguousarray(pd)
         tr = np.ascontiguousarray(tracing, np.uint32)
+        if tr.size < 8 * W * H:
+            raise ValueError(f"tracing: needs the {W}x{H} frame's 32-byte records ({8 * W * H} words)")
         sh = np.ascontiguousarray(sh16, np.uint16) if sh16 is not None else None
+        if sh is not None:
+            lres = [int(x) for x in np.asarray(pd["lpfResolution"]).reshape(-1)[:3]]
+            _host_buf(sh, np.uint16, 7 * lres[0] * lres[1] * lres[2] * 4, "sh16")
         out = np.empty((W * H, 4), np.uint16)
         f32 = np.empty((W * H, 3), np.float32) if want_f32 else None
         st = Stats()
@@ -578,9 +603,16 @@ class Context:
     def trace_camera(self, sid: int, pd: np.ndarray, flags: int = 0, seed: int = 0, tile_counts=None, tile_lists=None,
                      out=None, bounce_out=None):
         W, H = (int(x) for x in np.asarray(pd["frameSize"]).reshape(-1)[:2])
-        out = np.empty((W * H, 8), np.uint32) if out is None else out
+        out = np.empty((W * H, 8), np.uint32) if out is None else _host_buf(out, np.uint32, 8 * W * H, "out")
         if (flags & CAM_BOUNCE) and bounce_out is None:
             bounce_out = np.empty((W * H, 4), np.uint32)
+        elif bounce_out is not None:
+            _host_buf(bounce_out, np.uint32, 4 * W * H, "bounce_out")
+        tiles = ((W + 15) // 16) * ((H + 15) // 16)
+        if tile_counts is not None:
+            _host_buf(tile_counts, np.uint32, tiles, "tile_counts")
+        if tile_lists is not None:
+            _host_buf(tile_lists, np.uint32, 16 * tiles, "tile_lists")
         st = Stats()
         pd = np.ascontiguousarray(pd)
         _check(self._L.tim_rt_trace_camera(self._c, sid, pd.ctypes.data, flags, seed, _ptr(tile_counts),
