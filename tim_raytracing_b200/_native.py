@@ -229,6 +229,17 @@ def _host_buf(a, dtype, count: int, name: str):
     return a
 
 
+def _need_bytes(a, nbytes: int, name: str) -> None:
+    """A caller-provided host buffer (numpy array or torch tensor, any element
+    type) that the request reads or writes `nbytes` of."""
+    if a is None:
+        return
+    have = a.nbytes if isinstance(a, np.ndarray) else (a.numel() * a.element_size() if hasattr(a, "numel") else None)
+    contiguous = a.flags["C_CONTIGUOUS"] if isinstance(a, np.ndarray) else (a.is_contiguous() if hasattr(a, "is_contiguous") else True)
+    if have is None or have < nbytes or not contiguous:
+        raise ValueError(f"{name}: needs a contiguous buffer of at least {nbytes} bytes")
+
+
 def _ray_records(rays) -> np.ndarray:
     """Rays as the C ABI reads them: 32-byte records, float32 [n, 8] (flags as raw
     u32 bits in column 7)."""
@@ -637,6 +648,8 @@ class Server:
 
     def submit(self, sid: int, rays, mode: int, hit, nid=None, bary=None) -> int:
         n = int(rays.shape[0])
+        for buf, per, name in ((rays, 32, "rays"), (hit, 16, "hit"), (nid, 4, "nid"), (bary, 8, "bary")):
+            _need_bytes(buf, per * n, name)
         r = Request(sid, mode, n, 0, _ptr(rays), _ptr(hit), _ptr(nid), _ptr(bary))
         t = ctypes.c_uint64()
         _check(self._L.tim_rt_server_submit(self._s, ctypes.byref(r), ctypes.byref(t)))
@@ -650,7 +663,14 @@ class Server:
         octa (float32 [probes][64][3]) is optional."""
         dirs = np.ascontiguousarray(dirs, np.float32)
         basis = np.ascontiguousarray(sh_basis, np.float32)
-        assert sh16.dtype == np.uint16 and sh16.flags.c_contiguous
+        res = [int(desc.resolution[i]) for i in range(3)]
+        if all(x > 0 and x % 4 == 0 for x in res):   # other grids the library refuses before reading sh16
+            _host_buf(sh16, np.uint16, 7 * res[0] * res[1] * res[2] * 4, "sh16")
+        nd = int(desc.num_dirs)
+        if dirs.size < 4 * nd or basis.size < 9 * nd:
+            raise ValueError(f"dirs / sh_basis: need {nd} directions (float4) and {nd} x 9 basis weights")
+        if octa is not None:
+            _host_buf(octa, np.float32, (probe_end - probe_begin) * 64 * 3, "octa")
         r = ProbeRequest(sid, probe_begin, probe_end, 0, ctypes.cast(ctypes.byref(desc), ctypes.c_void_p), _ptr(dirs),
                          _ptr(basis), _ptr(sh16), _ptr(octa))
         t = ctypes.c_uint64()
