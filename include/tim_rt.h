@@ -393,23 +393,46 @@ int tim_rt_trace_camera_dev(tim_rt_ctx *ctx, tim_rt_scene_id scene, const tim_rt
                             uint32_t seed, const uint32_t *d_tile_counts, const uint32_t *d_tile_lists,
                             uint32_t *d_out, uint32_t *d_bounce_out, uint64_t *d_ray_count, void *cuda_stream);
 
+/* tim_rt_trace_camera_dev restricted to the output rows [row_begin, row_end) of
+ * the frame (row_begin a multiple of 4, the height of the kernels' 8x4-pixel
+ * tiles; row_end <= H): the unit by which one frame is split across GPUs, each
+ * GPU tracing its contiguous band against its own copy of the scene. d_out and
+ * d_bounce_out are the whole frame's arrays (W*H*8 and W*H*4 u32, same pixel
+ * indexing as tim_rt_trace_camera_dev); only the band's pixels are written, so
+ * the band's records are the contiguous words [row_begin*W*8, row_end*W*8) of
+ * d_out. The results of all bands equal those of one whole-frame call. Same
+ * tile lists (of the whole frame), flags, scratch and stream rules as
+ * tim_rt_trace_camera_dev. No counterpart in the reference: its one renderer
+ * dispatches the whole frame on one device (RayTracingPass::tracePass,
+ * src/Renderer/raytracingPass.cpp:89-110). */
+int tim_rt_trace_camera_rows_dev(tim_rt_ctx *ctx, tim_rt_scene_id scene, const tim_rt_pass_data *pd, uint32_t flags,
+                                 uint32_t seed, uint32_t row_begin, uint32_t row_end,
+                                 const uint32_t *d_tile_counts, const uint32_t *d_tile_lists, uint32_t *d_out,
+                                 uint32_t *d_bounce_out, uint64_t *d_ray_count, void *cuda_stream);
+
 /* Camera trace that allocates nothing. It has no counterpart in the reference.
  * For callers that may not allocate device memory while they trace (a fixed
- * device budget owned by their engine, a CUDA graph being captured around the
- * call, or a frame loop that cannot take cudaMalloc's synchronisation): the
- * caller passes its own device copies of the BVH buffer (fillGpuBuffer image),
- * the vertex positions, the tile lists and the outputs; the scratch (counters,
- * hit-leaf ids, secondary-ray queue) is a static device array inside the
- * library, which holds it on every GPU that loads it until the process exits
- * (3.85 MB). Frames are limited to TIM_RT_NOALLOC_MAX_PIXELS pixels; larger
- * ones return TIM_RT_EINVAL. Same results as tim_rt_trace_camera_dev on the
- * binary form (flags PROB_MASK, TILE_LIGHTS, BOUNCE only). tree_depth is the
- * depth tim_rt_validate_bvh reports (0 = 32); the buffer must have passed that
- * check, since this call reads device memory it cannot validate. The first call
- * on a device looks up the scratch address (cudaGetSymbolAddress) and should
- * come before any stream capture. All calls share the one scratch array:
- * calls whose kernels overlap on the GPU (different streams, no ordering) race.
- * Stream-ordered, no synchronisation. */
+ * device budget owned by their engine, a plugin host that forbids allocation
+ * from its callbacks, or a frame loop that cannot take cudaMalloc's implicit
+ * synchronisation): the caller passes its own device copies of the BVH buffer
+ * (fillGpuBuffer image), the vertex positions, the tile lists and the outputs;
+ * the scratch (counters, hit-leaf ids, secondary-ray queue) is a static device
+ * array inside the library, which holds it on every GPU that loads it until the
+ * process exits (3.85 MB). Frames are limited to TIM_RT_NOALLOC_MAX_PIXELS
+ * pixels; larger ones return TIM_RT_EINVAL. Same results as
+ * tim_rt_trace_camera_dev on the binary form (flags PROB_MASK, TILE_LIGHTS,
+ * BOUNCE only). The buffer must have passed tim_rt_validate_bvh, since this call
+ * reads device memory it cannot check; every range offset must be a multiple of
+ * 4 bytes and the node range's of 16 (else TIM_RT_EINVAL). tree_depth is the
+ * depth tim_rt_validate_bvh reports, or 0 for the maximum (32): a value below
+ * the tree's real depth lets a ray's traversal stack run out, which ends that
+ * ray early with its hits so far, and the device error word that records it is
+ * not reported by this call -- pass 0 when unsure. The first call in each device
+ * context (again after a cudaDeviceReset) looks up the scratch array's address
+ * with cudaGetSymbolAddress, with that device current, and should come before
+ * any stream capture on the device. All calls share the one scratch array, and
+ * each call clears its counters before use: calls whose kernels overlap on the
+ * GPU (different streams, no ordering) race. Stream-ordered, no synchronisation. */
 #define TIM_RT_NOALLOC_MAX_PIXELS 4096u
 int tim_rt_trace_camera_noalloc(const void *d_bvh, const uint32_t ranges[7][2], const tim_rt_push_constants *pc,
                                 const float *d_pos, uint32_t num_vertex, uint32_t tree_depth,

@@ -25,9 +25,18 @@ REFBUILD_SO = HERE / "_ref" / "libtimref_build.so"
 Image = namedtuple("Image", "data ranges pc aabb")   # same fields as tim_raytracing_b200.BvhImage
 
 
+# Where this container keeps the reference's source tree (read-only). Only the
+# build recipe reads it; the GPU box has no such tree and uses the prebuilt _ref.
+REFERENCE_TREE = Path(os.environ.get("TIM_RT_REFERENCE_TREE", "/root/reference"))
+
+
 def build(quiet: bool = True) -> None:
-    """Compiles the restatement (and the reference builder when the reference tree is present)."""
-    r = subprocess.run(["make", "-C", str(HERE)], capture_output=True, text=True)
+    """Compiles the restatement, and the reference builder and shaders when the
+    reference tree is present."""
+    cmd = ["make", "-C", str(HERE)]
+    if (REFERENCE_TREE / "src" / "Renderer" / "BVHBuilder.cpp").exists():
+        cmd.append(f"REF={REFERENCE_TREE}")
+    r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"oracle build failed:\n{r.stdout}\n{r.stderr}")
     if not quiet:

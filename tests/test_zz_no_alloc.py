@@ -1,13 +1,15 @@
 """The allocation-free camera trace (tim_rt_trace_camera_noalloc).
 
 It exists for callers that may not allocate device memory while tracing -- an
-engine that owns a fixed device budget, a CUDA graph captured around the call,
-or a frame loop that cannot absorb cudaMalloc's synchronisation. Here the test
-plays that caller: it owns the device copies of the BVH buffer, positions, tile
-lists and outputs (torch tensors), calls the entry point through the C ABI twice
-in a row, and checks both calls against the context-based tim_rt_trace_camera on
-the same inputs (integer records: bit-identical). This file is collected last so
-that a failure here comes after every other test has run.
+engine that owns a fixed device budget, a plugin host that forbids allocation
+from its callbacks, or a frame loop that cannot absorb cudaMalloc's
+synchronisation. Here the test plays that caller: it owns the device copies of
+the BVH buffer, positions, tile lists and outputs (torch tensors), calls the
+entry point through the C ABI twice in a row, and checks both calls against the
+context-based tim_rt_trace_camera on the same inputs (integer records:
+bit-identical). Frames include one whose sides are not multiples of the 8x4
+tile (50x37), so partial tiles meet the fixed-stride scratch layout. This file is
+collected last so that a failure here comes after every other test has run.
 """
 import ctypes
 
@@ -38,6 +40,9 @@ def test_noalloc_camera_matches_context_path(native):
     himg = native.build_bvh(h)
     cases.append((h, himg, scenes.pass_data(h, 48, 40, aabb=(himg.aabb[:3], himg.aabb[3:])),
                   native.CAM_TILE_LIGHTS | native.CAM_BOUNCE | native.CAM_PROB_MASK, 7))
+    # 50 x 37 = 1850 pixels: partial 8x4 tiles on the right and bottom edges
+    cases.append((h, himg, scenes.pass_data(h, 50, 37, aabb=(himg.aabb[:3], himg.aabb[3:])),
+                  native.CAM_TILE_LIGHTS | native.CAM_BOUNCE, 3))
     with native.Context(0) as ctx:
         for scene, im, pd, flags, seed in cases:
             depth = native.validate(im, scene.num_vertex)
@@ -87,3 +92,12 @@ def test_noalloc_rejects_frames_above_the_limit(native):
                                        s.num_vertex, 0, pd.ctypes.data, 0, 0, None, None, d_out.data_ptr(), None, None)
     assert rc == native.EINVAL
     assert b"exceeds the allocation-free limit" in L.tim_rt_last_error()
+    # a materials range that is not 4-byte aligned is refused before any launch
+    bad = ranges.copy()
+    bad[3][0] += 2
+    pd_ok = np.ascontiguousarray(scenes.pass_data(s, 32, 32))
+    rc = L.tim_rt_trace_camera_noalloc(d_bvh.data_ptr(), bad.ctypes.data, ctypes.byref(pc), d_pos.data_ptr(),
+                                       s.num_vertex, 0, pd_ok.ctypes.data, 0, 0, None, None, d_out.data_ptr(), None,
+                                       None)
+    assert rc == native.EINVAL
+    assert b"misaligned" in L.tim_rt_last_error()

@@ -36,7 +36,7 @@ EXPORTED = [
     "tim_rt_server_destroy", "tim_rt_verify_hits", "tim_rt_server_submit_probes", "tim_rt_bvh_file_write",
     "tim_rt_bvh_file_read", "tim_rt_bvh_file_info", "tim_rt_bvh_file_free", "tim_rt_upload_bvh_file",
     "tim_rt_shade_camera", "tim_rt_shade_camera_dev", "tim_rt_build_bvh_gpu", "tim_rt_probe_directions",
-    "tim_rt_wide_check",
+    "tim_rt_wide_check", "tim_rt_trace_camera_rows_dev",
 ]
 SORT_NONE, SORT_OCTANT, SORT_MORTON = 0, 1, 2
 BATCH_WIDE = 0x100
@@ -172,6 +172,7 @@ def lib() -> ctypes.CDLL:
     L.tim_rt_bvh_blob_free.restype = None
     L.tim_rt_validate_bvh.argtypes = [vp, u64, vp, ctypes.POINTER(PushConstants), u32, ctypes.POINTER(u32)]
     L.tim_rt_trace_camera_dev.argtypes = [vp, u32, vp, u32, u32, vp, vp, vp, vp, vp, vp]
+    L.tim_rt_trace_camera_rows_dev.argtypes = [vp, u32, vp, u32, u32, u32, u32, vp, vp, vp, vp, vp, vp]
     L.tim_rt_cull_lights_dev.argtypes = [vp, u32, vp, u32, u32, vp, vp, vp]
     L.tim_rt_get_launch_config.argtypes = [vp, ctypes.POINTER(LaunchConfig)]
     L.tim_rt_measure_l2_bandwidth.argtypes = [i32, u64, i32, ctypes.POINTER(ctypes.c_float)]
@@ -567,6 +568,16 @@ class Context:
         _check(self._L.tim_rt_trace_camera_dev(self._c, sid, pd.ctypes.data, flags, seed, _ptr(d_tile_counts),
                                                _ptr(d_tile_lists), _ptr(d_out), _ptr(d_bounce), _ptr(d_ray_count),
                                                _ptr(stream) if stream is not None else None))
+
+    def trace_camera_rows_dev(self, sid: int, pd: np.ndarray, flags: int, seed: int, row_begin: int, row_end: int,
+                              d_tile_counts, d_tile_lists, d_out, d_bounce=None, d_ray_count=None, stream=None):
+        """tim_rt_trace_camera_rows_dev: output rows [row_begin, row_end) of the frame
+        into the whole frame's device arrays."""
+        pd = np.ascontiguousarray(pd)
+        _check(self._L.tim_rt_trace_camera_rows_dev(self._c, sid, pd.ctypes.data, flags, seed, row_begin, row_end,
+                                                    _ptr(d_tile_counts), _ptr(d_tile_lists), _ptr(d_out),
+                                                    _ptr(d_bounce), _ptr(d_ray_count),
+                                                    _ptr(stream) if stream is not None else None))
 
     def update_probes(self, sid: int, desc: ProbeDesc, dirs: np.ndarray, sh_basis: np.ndarray, sh16: np.ndarray,
                       probe_begin: int = 0, probe_end: int = None, want_trace=False, want_irr=False, want_sh32=False,

@@ -614,19 +614,26 @@ int tim_rt_cull_lights_dev(tim_rt_ctx* c, tim_rt_scene_id id, const tim_rt_pass_
     return TIM_RT_OK;
 }
 
-int tim_rt_trace_camera_dev(tim_rt_ctx* c, tim_rt_scene_id id, const tim_rt_pass_data* pd, uint32_t flags,
-                            uint32_t seed, const uint32_t* d_tile_counts, const uint32_t* d_tile_lists, uint32_t* d_out,
-                            uint32_t* d_bounce_out, uint64_t* d_ray_count, void* cuda_stream) {
+// tim_rt_trace_camera_dev over output rows [row_begin, row_end) (the whole frame: 0, H).
+static int camera_dev_rows(tim_rt_ctx* c, tim_rt_scene_id id, const tim_rt_pass_data* pd, uint32_t flags, uint32_t seed,
+                           uint32_t row_begin, uint32_t row_end, const uint32_t* d_tile_counts,
+                           const uint32_t* d_tile_lists, uint32_t* d_out, uint32_t* d_bounce_out, uint64_t* d_ray_count,
+                           void* cuda_stream, const char* who) {
     int rc = check_ctx(c);
     if (rc) return rc;
     Scene* s = find_scene(c, id);
     if (!s) return TIM_RT_ENOTFOUND;
     if (!d_out) {
-        set_error("tim_rt_trace_camera_dev: null output");
+        set_error(std::string(who) + ": null output");
         return TIM_RT_EINVAL;
     }
     uint64_t qcap = 0;
     if ((rc = camera_prepare(c, s, pd, flags, d_tile_counts && d_tile_lists, d_bounce_out != nullptr, &qcap))) return rc;
+    if (row_begin % 4u != 0u || row_begin >= row_end || row_end > pd->frameSize[1]) {
+        set_error(std::string(who) + ": rows [" + std::to_string(row_begin) + ", " + std::to_string(row_end) +
+                  ") must be a non-empty range inside the frame starting at a multiple of 4");
+        return TIM_RT_EINVAL;
+    }
     cudaStream_t st = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : c->stream;
     uint32_t* ctr = static_cast<uint32_t*>(c->counters.ptr);
     TIMRT_CUDA(cudaMemsetAsync(ctr, 0, 4 * kCamCounterWords, st));
@@ -634,8 +641,23 @@ int tim_rt_trace_camera_dev(tim_rt_ctx* c, tim_rt_scene_id id, const tim_rt_pass
                              (flags & TIM_RT_CAM_BOUNCE) ? d_bounce_out : nullptr, static_cast<uint32_t*>(c->cam_nid.ptr),
                              static_cast<tim_rt_ray*>(c->q_rays.ptr), static_cast<uint32_t*>(c->q_pixel.ptr),
                              (uint32_t)qcap, ctr, ctr + kErrWord, d_ray_count, st,
-                             cfg_for(c, s, (flags & TIM_RT_CAM_WIDE) != 0)));
+                             cfg_for(c, s, (flags & TIM_RT_CAM_WIDE) != 0), row_begin, row_end));
     return TIM_RT_OK;
+}
+
+int tim_rt_trace_camera_dev(tim_rt_ctx* c, tim_rt_scene_id id, const tim_rt_pass_data* pd, uint32_t flags,
+                            uint32_t seed, const uint32_t* d_tile_counts, const uint32_t* d_tile_lists, uint32_t* d_out,
+                            uint32_t* d_bounce_out, uint64_t* d_ray_count, void* cuda_stream) {
+    return camera_dev_rows(c, id, pd, flags, seed, 0u, pd ? pd->frameSize[1] : 0u, d_tile_counts, d_tile_lists, d_out,
+                           d_bounce_out, d_ray_count, cuda_stream, "tim_rt_trace_camera_dev");
+}
+
+int tim_rt_trace_camera_rows_dev(tim_rt_ctx* c, tim_rt_scene_id id, const tim_rt_pass_data* pd, uint32_t flags,
+                                 uint32_t seed, uint32_t row_begin, uint32_t row_end, const uint32_t* d_tile_counts,
+                                 const uint32_t* d_tile_lists, uint32_t* d_out, uint32_t* d_bounce_out,
+                                 uint64_t* d_ray_count, void* cuda_stream) {
+    return camera_dev_rows(c, id, pd, flags, seed, row_begin, row_end, d_tile_counts, d_tile_lists, d_out,
+                           d_bounce_out, d_ray_count, cuda_stream, "tim_rt_trace_camera_rows_dev");
 }
 
 // Checks of tim_rt_shade_camera(_dev): frame size, light-probe resolution, normals.

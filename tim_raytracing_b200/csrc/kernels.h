@@ -1,6 +1,7 @@
 // kernels.h -- host-side declarations of the kernel launchers (trace.cu, probes.cu).
 #pragma once
 #include <cstdint>
+#include <mutex>
 #include <cuda_runtime.h>
 #include "common.cuh"
 #include "../../include/tim_rt.h"
@@ -21,6 +22,28 @@ struct LaunchConfig {
     unsigned long long* stats = nullptr;
     // when set, the camera launcher records ev[0..3] around its three phases
     cudaEvent_t* phase_ev = nullptr;
+};
+
+// Grid sizes of one persistent kernel, per device ordinal and stack depth: the
+// occupancy calculator's resident blocks per SM times the device's SM count,
+// computed on first use with the device current (which also sets the kernel's
+// dynamic shared-memory limit in that device's context). Thread-safe.
+struct GridCache {
+    static constexpr int kDevices = 64;
+    std::mutex mu;
+    int blocks[kDevices][kStackSize + 1] = {};
+    template <class F>
+    int get(int depth, F compute) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kDevices) {
+            cudaGetLastError();
+            dev = -1;
+        }
+        std::lock_guard<std::mutex> lock(mu);
+        if (dev < 0) return compute(0);
+        if (!blocks[dev][depth]) blocks[dev][depth] = compute(dev);
+        return blocks[dev][depth];
+    }
 };
 
 // The kernels' packed knob word: refill threshold (1..32) | phase switch (0..31) << 8.

@@ -160,17 +160,15 @@ __global__ void __launch_bounds__(BLOCK, WIDE ? 768 / BLOCK : 1) k_multi(const S
 
 template <int BLOCK, bool WIDE>
 static int grid_multi(int depth) {
-    static int blocks[kStackSize + 1] = {};
-    if (!blocks[depth]) {
-        int dev = 0, sms = 0, per = 0;
-        cudaGetDevice(&dev);
+    static GridCache cache;
+    return cache.get(depth, [depth](int dev) {
+        int sms = 0, per = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         cudaFuncSetAttribute(k_multi<BLOCK, WIDE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)multi_stack_bytes<BLOCK, WIDE>(kStackSize));
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_multi<BLOCK, WIDE>, BLOCK, multi_stack_bytes<BLOCK, WIDE>(depth));
-        blocks[depth] = sms * (per > 0 ? per : 1);
-    }
-    return blocks[depth];
+        return (sms > 0 ? sms : 1) * (per > 0 ? per : 1);
+    });
 }
 
 template <int BLOCK, bool WIDE>

@@ -1,16 +1,16 @@
 // noalloc.cu -- camera trace that allocates no memory.
 //
 // Some callers cannot allocate device memory when they trace: an engine whose
-// allocator hands out every byte from a budget fixed at start-up, code that
-// runs while another component is capturing a CUDA graph (cudaMalloc is not a
-// capturable operation), or a frame loop that cannot afford cudaMalloc's
-// implicit device synchronisation. tim_rt_trace_camera_noalloc serves them:
-// the caller passes its own device copies of the BVH buffer, the vertex
-// positions, the tile lists and the outputs, and the scratch memory the camera
-// pipeline needs (work counters, the per-pixel hit-leaf ids and the
+// allocator hands out every byte from a budget fixed at start-up, a plugin host
+// that forbids allocation from its callbacks, or a frame loop that cannot afford
+// cudaMalloc's implicit device synchronisation. tim_rt_trace_camera_noalloc
+// serves them: the caller passes its own device copies of the BVH buffer, the
+// vertex positions, the tile lists and the outputs, and the scratch memory the
+// camera pipeline needs (work counters, the per-pixel hit-leaf ids and the
 // secondary-ray queue) lives in one file-scope device array sized for frames
 // of at most TIM_RT_NOALLOC_MAX_PIXELS pixels. The array exists on every GPU
 // that loads the library, from load until process exit.
+#include <cuda.h>   // driver types only: the entry points come from cudaGetDriverEntryPointByVersion
 #include <cuda_runtime.h>
 #include <mutex>
 #include <string>
@@ -35,9 +35,52 @@ static_assert((kHeaderWords + kNidWords + kPixelWords) % 4u == 0u, "ray records 
 static __device__ __align__(256) uint32_t g_noalloc_scratch[kScratchWords];
 
 std::mutex g_mu;
-void* g_addr[128] = {};   // device address of g_noalloc_scratch per device ordinal
 
-// Looks the array's device address up once per device, with that device current.
+// The array's device address is looked up once per device context: a context
+// torn down by cudaDeviceReset (or a primary-context reset) unloads the module,
+// and the next context may place the array elsewhere. Contexts are told apart by
+// cuCtxGetId, whose ids are never reused within a process; the two driver calls
+// are reached through the runtime's entry-point query, so the library does not
+// link libcuda itself.
+struct AddrCache {
+    unsigned long long ctx_id = 0;   // 0: nothing cached
+    void* addr = nullptr;
+};
+AddrCache g_cache[128];
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+CtxGetCurrentFn g_get_current = nullptr;
+CtxGetIdFn g_get_id = nullptr;
+bool g_fns_looked_up = false;
+
+// Id of the calling thread's current context, or 0 when the driver cannot say
+// (then the address is looked up on every call instead of cached).
+unsigned long long current_context_id() {
+    if (!g_fns_looked_up) {
+        g_fns_looked_up = true;
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            g_get_current = reinterpret_cast<CtxGetCurrentFn>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            g_get_id = reinterpret_cast<CtxGetIdFn>(f);
+        cudaGetLastError();
+    }
+    CUcontext c = nullptr;
+    unsigned long long id = 0;
+    if (!g_get_current || !g_get_id || g_get_current(&c) != CUDA_SUCCESS || !c || g_get_id(c, &id) != CUDA_SUCCESS)
+        return 0;
+    return id;
+}
+
+// Set-up of a call: the device address of g_noalloc_scratch in the current
+// device's context, looked up with that device current on the first call in
+// each context (cudaGetSymbolAddress loads the module there if needed). A
+// thread on which no runtime call has bound the context yet reports id 0 and
+// takes the lookup, which binds it.
 int scratch_address(uint32_t** out) {
     int dev = -1;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128) {
@@ -46,7 +89,9 @@ int scratch_address(uint32_t** out) {
         return TIM_RT_EDEVICE;
     }
     std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_addr[dev]) {
+    const unsigned long long id = current_context_id();
+    AddrCache& c = g_cache[dev];
+    if (id == 0 || c.ctx_id != id || !c.addr) {
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess || !p) {
@@ -54,9 +99,11 @@ int scratch_address(uint32_t** out) {
             set_error(std::string("tim_rt_trace_camera_noalloc: cudaGetSymbolAddress failed: ") + cudaGetErrorString(e));
             return TIM_RT_EDEVICE;
         }
-        g_addr[dev] = p;
+        // the lookup made the context current if it was not: read the id again
+        c.ctx_id = id ? id : current_context_id();
+        c.addr = p;
     }
-    *out = static_cast<uint32_t*>(g_addr[dev]);
+    *out = static_cast<uint32_t*>(c.addr);
     return TIM_RT_OK;
 }
 
@@ -95,8 +142,11 @@ extern "C" int tim_rt_trace_camera_noalloc(const void* d_bvh, const uint32_t ran
         set_error("tim_rt_trace_camera_noalloc: PROB_MASK needs lpfResolution >= 2 per axis");
         return TIM_RT_EINVAL;
     }
-    if (ranges[TIM_RT_RANGE_NODE][0] % 16u || ranges[TIM_RT_RANGE_LEAF][0] % 4u || ranges[TIM_RT_RANGE_LIGHT][0] % 4u ||
-        ranges[TIM_RT_RANGE_BLAS][0] % 4u || tree_depth > 32u) {
+    // every range is read as 4-byte words (materials and lights as floats), the
+    // nodes as 16-byte vectors
+    bool misaligned = ranges[TIM_RT_RANGE_NODE][0] % 16u != 0u;
+    for (int k = 0; k < 7; ++k) misaligned = misaligned || (ranges[k][0] % 4u != 0u);
+    if (misaligned || tree_depth > 32u) {
         set_error("tim_rt_trace_camera_noalloc: misaligned range or tree depth above 32");
         return TIM_RT_EINVAL;
     }

@@ -3,7 +3,7 @@
 // HBM and tensor throughput only).
 //
 // A buffer well below the L2 size is first touched, then read `passes` times
-// by a grid of 148 x 8 blocks with 16-byte loads; the reads go through L1 with
+// by a grid of 4 blocks of 512 threads per SM with 16-byte loads; the reads go through L1 with
 // the evict-first hint so each pass is served by L2. Bytes read / device time.
 #include <cuda_runtime.h>
 #include <cstdint>

@@ -543,21 +543,19 @@ constexpr size_t stack_bytes(int depth) {
 }
 
 // Grid of the persistent kernels: as many resident blocks as the occupancy
-// calculator allows on every SM for this stack depth (cached per depth).
+// calculator allows on every SM for this stack depth (cached per device and depth).
 template <int BLOCK, bool WIDE, bool STATS, class Policy>
 static int grid_for(int depth) {
-    static int blocks[kStackSize + 1] = {};
-    if (!blocks[depth]) {
-        int dev = 0, sms = 0, per = 0;
-        cudaGetDevice(&dev);
+    static GridCache cache;
+    return cache.get(depth, [depth](int dev) {
+        int sms = 0, per = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         cudaFuncSetAttribute(k_persistent<BLOCK, WIDE, STATS, Policy>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)stack_bytes<BLOCK, WIDE>(kStackSize));
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_persistent<BLOCK, WIDE, STATS, Policy>, BLOCK,
                                                       stack_bytes<BLOCK, WIDE>(depth));
-        blocks[depth] = sms * (per > 0 ? per : 1);
-    }
-    return blocks[depth];
+        return (sms > 0 ? sms : 1) * (per > 0 ? per : 1);
+    });
 }
 
 template <int BLOCK, bool WIDE, bool STATS, class Policy>
