@@ -44,6 +44,8 @@ extern "C" {
 #define TIM_RT_EDEVICE 4      /* CUDA error */
 #define TIM_RT_ENOTFOUND 5    /* unknown scene id */
 #define TIM_RT_EUNSUPPORTED 6 /* feature not available for this scene */
+#define TIM_RT_ECANCELLED 7   /* the serving request was cancelled (tim_rt_server_cancel) */
+#define TIM_RT_EBUSY 8        /* too late to cancel: the serving request completes normally */
 
 /* Sub-range indices of the BVH buffer, in fillGpuBuffer's memory order
  * (BVHBuilder.cpp:1326-1500): {offset bytes, size bytes}. */
@@ -324,6 +326,11 @@ typedef struct {
     float p50_ms, p99_ms, mean_ms, max_ms;   /* request latency, submit -> results on the host */
     float queue_p50_ms, queue_p99_ms;        /* submit -> admission */
     float wall_s;                            /* seconds since the first submit after the last reset */
+    uint64_t cancelled;                      /* requests completed by tim_rt_server_cancel */
+    uint64_t step_requests;                  /* sum over trace steps of the requests each step traced */
+    uint32_t max_step_requests;              /* most requests one trace step traced */
+    uint32_t max_inflight_steps;             /* most trace steps queued on the GPU at once */
+    float gpu_busy_ms;                       /* device time of the trace steps' kernels (CUDA events) */
 } tim_rt_server_stats;
 int tim_rt_server_create(tim_rt_ctx *ctx, const tim_rt_server_params *params, tim_rt_server **out);
 /* Queues a request; never blocks on the GPU. *ticket identifies it. */
@@ -350,9 +357,20 @@ typedef struct {
     float *octa;                    /* host, optional: [probes][64][3] */
 } tim_rt_probe_request;
 int tim_rt_server_submit_probes(tim_rt_server *srv, const tim_rt_probe_request *req, uint64_t *ticket);
-/* Waits until the request completes (timeout_ms 0 = no limit): TIM_RT_OK, or
- * TIM_RT_ETIMEOUT with the request still pending. */
+/* Waits until the request completes (timeout_ms 0 = no limit): TIM_RT_OK,
+ * TIM_RT_ECANCELLED for a cancelled request, or TIM_RT_ETIMEOUT with the request
+ * still pending. */
 int tim_rt_server_wait(tim_rt_server *srv, uint64_t ticket, uint32_t timeout_ms);
+/* Takes a request back. TIM_RT_OK: none of its remaining rays will be traced and
+ * its output buffers are not written; a request not yet admitted is gone at once,
+ * an admitted one completes once its upload and the steps already tracing part of
+ * it have finished -- tim_rt_server_wait then returns TIM_RT_ECANCELLED, after
+ * which its host buffers may be reused. TIM_RT_EBUSY: too late (its last rays
+ * are already in a queued step, or it is an admitted probe update); it completes
+ * normally. TIM_RT_ENOTFOUND: unknown or already completed ticket. Thread-safe.
+ * The reference has no request queue to cancel from: its passes run once per
+ * frame (src/Renderer/raytracingPass.cpp:89-110). */
+int tim_rt_server_cancel(tim_rt_server *srv, uint64_t ticket);
 /* Waits until every submitted request has completed. */
 int tim_rt_server_drain(tim_rt_server *srv, uint32_t timeout_ms);
 /* Statistics over the requests completed since the last reset (reset != 0 clears them afterwards). */

@@ -27,6 +27,10 @@ def test_reference_arm_json_line():
     assert d["metric"] == d["unit"] == "Mrays/s" and d["higher_is_better"] is True
     assert d["value"] > 0 and d["steps"] == 1 and d["warmup"] == 3 and d["n_gpus"] == 1
     assert d["config"]["workload"] == "heightfield_100k_frame_1080p"
+    # the same workload description as the GPU arm's line (same tree, frame and rays)
+    sys.path.insert(0, str(ROOT))
+    import bench
+    assert d["config"] == bench.config_dict(bench.make_workload(), 1)
     cb = d["cpu_baseline"]
     assert cb["kind"] in ("port", "reference") and cb["cores"] >= 1 and cb["value"] == d["value"] and cb["sample"]
     assert d["e2e"] == {"value": d["value"], "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}

@@ -88,6 +88,12 @@ def test_server_mix_matches_alone(ctx, native, served, wide):
         assert st["steps"] >= st["rays_completed"] // 16384
         assert 0 < st["p50_ms"] <= st["p99_ms"] <= st["max_ms"]
         assert 0 < st["arena_peak_bytes"] <= st["arena_bytes"]
+        # continuous batching: steps held several requests, and the worker queued the
+        # next step while the previous one still ran on the GPU
+        assert st["max_step_requests"] >= 2
+        assert st["step_requests"] > st["steps"]
+        assert st["max_inflight"] == 2
+        assert 0 < st["gpu_busy_ms"] < 1e3 * st["wall_s"]
     finally:
         srv.close()
     _check(ctx, native, reqs, wide)
@@ -194,3 +200,104 @@ def test_server_probe_request_errors(ctx, native, served):
         assert e.value.code == native.EINVAL
     finally:
         srv.close()
+
+
+def _sentinel_hits(n):
+    import torch
+    th, h = _pinned((n, 4), torch.int32)
+    h[:] = 0x7F7F7F7F
+    return th, h
+
+
+def test_server_cancel(ctx, native, served):
+    """tim_rt_server_cancel on a request still waiting for admission and on an
+    admitted one that many steps still have to trace: both complete as cancelled
+    (wait reports ECANCELLED) without writing their outputs, the other requests
+    are served as if alone, and tickets that are unknown or done are refused."""
+    import torch
+    from tim_raytracing_b200 import scenes
+    sid = served[2]
+    big_n, wait_n = 1_000_000, 200_000      # 48 B staged per ray: 48 MB and 9.6 MB
+    tb, big_rays = _pinned((big_n, 8), torch.float32)
+    big_rays[:] = scenes.random_rays(71, big_n)
+    tbh, big_hit = _sentinel_hits(big_n)
+    tw, wait_rays = _pinned((wait_n, 8), torch.float32)
+    wait_rays[:] = scenes.random_rays(72, wait_n)
+    twh, wait_hit = _sentinel_hits(wait_n)
+    reqs = _requests(served, 8, seed=43)
+    srv = native.Server(ctx, memory_budget_bytes=56 << 20, max_rays_per_step=4096, max_inflight_steps=2)
+    try:
+        t_big = srv.submit(sid, big_rays, native.MODE_PER_RAY, big_hit)
+        t_wait = srv.submit(sid, wait_rays, native.MODE_PER_RAY, wait_hit)   # cannot fit beside the big one
+        assert srv.cancel(t_wait) == native.OK        # still waiting: gone at once
+        assert srv.cancel(t_big) == native.OK         # admitted, most of its ~245 steps still to come
+        assert srv.cancel(t_big) in (native.OK, native.ENOTFOUND)   # again: still draining, or already done
+        for t in (t_wait, t_big):
+            with pytest.raises(native.TimRtError) as e:
+                srv.wait(t, timeout_ms=60000)
+            assert e.value.code == native.ECANCELLED
+        for q in reqs:
+            q["ticket"] = srv.submit(q["sid"], q["rays"], q["mode"], q["hit"], q["nid"], q["bary"])
+        srv.drain(timeout_ms=120000)
+        assert srv.cancel(reqs[0]["ticket"]) == native.ENOTFOUND    # completed
+        assert srv.cancel(10 ** 9) == native.ENOTFOUND             # never issued
+        st = srv.stats()
+        assert st["cancelled"] == 2
+        assert st["completed"] == len(reqs)
+    finally:
+        srv.close()
+    assert np.all(big_hit == 0x7F7F7F7F) and np.all(wait_hit == 0x7F7F7F7F)
+    _check(ctx, native, reqs, False)
+
+
+def test_server_stalled_submitter(ctx, native, served):
+    """Host-side fault injection: one client thread submits requests and then
+    stalls (blocks without ever waiting for them) while two other clients keep
+    submitting and waiting. The server does not depend on its clients: the other
+    clients' requests complete while the stalled one is blocked, so do the
+    stalled client's own requests (checked from the main thread), and every
+    result equals tracing alone."""
+    import time
+    stalled = _requests(served, 6, seed=51)
+    others = _requests(served, 24, seed=52)
+    srv = native.Server(ctx, memory_budget_bytes=8 << 20, max_rays_per_step=16384, max_inflight_steps=2)
+    release = threading.Event()
+    submitted = threading.Event()
+    errors = []
+
+    def stalled_client():
+        for q in stalled:
+            q["ticket"] = srv.submit(q["sid"], q["rays"], q["mode"], q["hit"], q["nid"], q["bary"])
+        submitted.set()
+        release.wait(120)       # the stall: no waits, no further calls
+
+    def client(part):
+        try:
+            for q in part:
+                t = srv.submit(q["sid"], q["rays"], q["mode"], q["hit"], q["nid"], q["bary"])
+                srv.wait(t, timeout_ms=60000)
+                q["done_while_stalled"] = not release.is_set()
+        except Exception as e:     # noqa: BLE001 -- reported below
+            errors.append(e)
+
+    ts = threading.Thread(target=stalled_client)
+    ts.start()
+    try:
+        assert submitted.wait(60)
+        workers = [threading.Thread(target=client, args=(others[k::2],)) for k in range(2)]
+        for w in workers:
+            w.start()
+        for w in workers:
+            w.join(120)
+        assert not errors, errors
+        assert all(q["done_while_stalled"] for q in others)
+        t0 = time.perf_counter()
+        for q in stalled:
+            srv.wait(q["ticket"], timeout_ms=60000)   # served without the stalled client's help
+        assert time.perf_counter() - t0 < 60
+        assert ts.is_alive()       # the stalled client is still blocked
+    finally:
+        release.set()
+        ts.join(60)
+        srv.close()
+    _check(ctx, native, stalled + others, False)

@@ -14,7 +14,7 @@ import numpy as np
 
 LIB_PATH = Path(__file__).resolve().parent / "libtim_rt.so"
 
-OK, EINVAL, ENOMEM, ETIMEOUT, EDEVICE, ENOTFOUND, EUNSUPPORTED = range(7)
+OK, EINVAL, ENOMEM, ETIMEOUT, EDEVICE, ENOTFOUND, EUNSUPPORTED, ECANCELLED, EBUSY = range(9)
 MODE_CLOSEST, MODE_ANY, MODE_PER_RAY = 0, 1, 2
 TRACE_WIDE = 0x100
 TRACE_COUNT = 0x400
@@ -36,7 +36,7 @@ EXPORTED = [
     "tim_rt_server_destroy", "tim_rt_verify_hits", "tim_rt_server_submit_probes", "tim_rt_bvh_file_write",
     "tim_rt_bvh_file_read", "tim_rt_bvh_file_info", "tim_rt_bvh_file_free", "tim_rt_upload_bvh_file",
     "tim_rt_shade_camera", "tim_rt_shade_camera_dev", "tim_rt_build_bvh_gpu", "tim_rt_probe_directions",
-    "tim_rt_wide_check", "tim_rt_trace_camera_rows_dev",
+    "tim_rt_wide_check", "tim_rt_trace_camera_rows_dev", "tim_rt_server_cancel",
 ]
 SORT_NONE, SORT_OCTANT, SORT_MORTON = 0, 1, 2
 BATCH_WIDE = 0x100
@@ -121,7 +121,9 @@ class ServerStats(ctypes.Structure):
                 ("steps", ctypes.c_uint64), ("arena_bytes", ctypes.c_uint64), ("arena_peak_bytes", ctypes.c_uint64),
                 ("p50_ms", ctypes.c_float), ("p99_ms", ctypes.c_float), ("mean_ms", ctypes.c_float),
                 ("max_ms", ctypes.c_float), ("queue_p50_ms", ctypes.c_float), ("queue_p99_ms", ctypes.c_float),
-                ("wall_s", ctypes.c_float)]
+                ("wall_s", ctypes.c_float), ("cancelled", ctypes.c_uint64), ("step_requests", ctypes.c_uint64),
+                ("max_step_requests", ctypes.c_uint32), ("max_inflight", ctypes.c_uint32),
+                ("gpu_busy_ms", ctypes.c_float)]
 
 
 class VerifyResult(ctypes.Structure):
@@ -190,6 +192,7 @@ def lib() -> ctypes.CDLL:
     L.tim_rt_server_submit.argtypes = [vp, ctypes.POINTER(Request), ctypes.POINTER(u64)]
     L.tim_rt_server_submit_probes.argtypes = [vp, ctypes.POINTER(ProbeRequest), ctypes.POINTER(u64)]
     L.tim_rt_server_wait.argtypes = [vp, u64, u32]
+    L.tim_rt_server_cancel.argtypes = [vp, u64]
     L.tim_rt_server_drain.argtypes = [vp, u32]
     L.tim_rt_server_stats_get.argtypes = [vp, ctypes.POINTER(ServerStats), i32]
     L.tim_rt_server_destroy.argtypes = [vp]
@@ -690,8 +693,19 @@ class Server:
         return t.value
 
     def wait(self, ticket: int, timeout_ms: int = 0):
-        _check(self._L.tim_rt_server_wait(self._s, ticket, timeout_ms))
-        self._keep.pop(ticket, None)
+        """tim_rt_server_wait; raises TimRtError (code ECANCELLED for a cancelled request)."""
+        rc = self._L.tim_rt_server_wait(self._s, ticket, timeout_ms)
+        if rc in (OK, ECANCELLED):
+            self._keep.pop(ticket, None)
+        _check(rc)
+
+    def cancel(self, ticket: int) -> int:
+        """tim_rt_server_cancel: OK (taken back; wait() then raises ECANCELLED), EBUSY
+        (too late, completes normally) or ENOTFOUND (unknown or completed)."""
+        rc = self._L.tim_rt_server_cancel(self._s, ticket)
+        if rc not in (OK, EBUSY, ENOTFOUND):
+            _check(rc)
+        return rc
 
     def drain(self, timeout_ms: int = 0):
         _check(self._L.tim_rt_server_drain(self._s, timeout_ms))

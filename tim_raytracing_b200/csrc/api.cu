@@ -259,7 +259,7 @@ int tim_rt_destroy(tim_rt_ctx* c) {
     c->batches.clear();
     for (auto& kv : c->scenes) {
         Scene* s = kv.second.get();
-        for (DevBuf* b : {&s->blob, &s->pos, &s->nrm, &s->uv, &s->wnodes, &s->wtris, &s->wnid}) dev_free(c, *b);
+        for (DevBuf* b : {&s->blob, &s->pos, &s->nrm, &s->uv, &s->wnodes, &s->wtris, &s->wnid, &s->ptris, &s->pleaf}) dev_free(c, *b);
     }
     c->scenes.clear();
     for (DevBuf* b : {&c->rays, &c->hits, &c->nid, &c->bary, &c->counters, &c->cam_out, &c->cam_bounce, &c->cam_nid,
@@ -359,14 +359,27 @@ int tim_rt_upload_bvh(tim_rt_ctx* c, const void* bvh_bytes, uint64_t n_bytes, co
             return TIM_RT_EUNSUPPORTED;
         }
     }
+    // the plain form's leaf-triangle copy (16-byte vector fetches instead of
+    // scalar gathers of the records and vertex positions)
+    RawVec<float> ptris;
+    RawVec<uint32_t> pleaf;
+    build_leaf_tris(blob, ranges, pc->numNodes, pos, ptris, pleaf);
     auto fail = [&](int code) {
-        for (DevBuf* b : {&s->blob, &s->pos, &s->nrm, &s->uv, &s->wnodes, &s->wtris, &s->wnid}) dev_free(c, *b);
+        for (DevBuf* b : {&s->blob, &s->pos, &s->nrm, &s->uv, &s->wnodes, &s->wtris, &s->wnid, &s->ptris, &s->pleaf}) dev_free(c, *b);
         return code;
     };
     if ((rc = dev_alloc(c, s->blob, n_bytes))) return fail(rc);
     if ((rc = dev_alloc(c, s->pos, 12ull * max_vertex))) return fail(rc);
     if (nrm && (rc = dev_alloc(c, s->nrm, 12ull * max_vertex))) return fail(rc);
     if (uv && (rc = dev_alloc(c, s->uv, 8ull * max_vertex))) return fail(rc);
+    if ((rc = dev_alloc(c, s->pleaf, 4ull * pleaf.size()))) return fail(rc);
+    if (!ptris.empty() && (rc = dev_alloc(c, s->ptris, 4ull * ptris.size()))) return fail(rc);
+    if (cudaMemcpyAsync(s->pleaf.ptr, pleaf.data(), 4ull * pleaf.size(), cudaMemcpyHostToDevice, c->stream) != cudaSuccess ||
+        (!ptris.empty() &&
+         cudaMemcpyAsync(s->ptris.ptr, ptris.data(), 4ull * ptris.size(), cudaMemcpyHostToDevice, c->stream) != cudaSuccess)) {
+        set_error("tim_rt_upload_bvh: host-to-device copy of the leaf triangles failed");
+        return fail(TIM_RT_EDEVICE);
+    }
     if (cudaMemcpyAsync(s->blob.ptr, blob, n_bytes, cudaMemcpyHostToDevice, c->stream) != cudaSuccess ||
         cudaMemcpyAsync(s->pos.ptr, pos, 12ull * num_vertex, cudaMemcpyHostToDevice, c->stream) != cudaSuccess ||
         (nrm && cudaMemcpyAsync(s->nrm.ptr, nrm, 12ull * num_vertex, cudaMemcpyHostToDevice, c->stream) != cudaSuccess) ||
@@ -410,7 +423,10 @@ int tim_rt_upload_bvh(tim_rt_ctx* c, const void* bvh_bytes, uint64_t n_bytes, co
     v.wtri_leaf = static_cast<const uint4*>(s->wnid.ptr);
     v.num_wnodes = s->has_wide ? wh.num_nodes : 0u;
     v.wide_root_is_leaf = wh.root_is_leaf;
-    s->bytes = s->blob.bytes + s->pos.bytes + s->nrm.bytes + s->uv.bytes + s->wnodes.bytes + s->wtris.bytes + s->wnid.bytes;
+    v.pleaf = static_cast<const uint4*>(s->pleaf.ptr);
+    v.ptris = static_cast<const float4*>(s->ptris.ptr);
+    s->bytes = s->blob.bytes + s->pos.bytes + s->nrm.bytes + s->uv.bytes + s->wnodes.bytes + s->wtris.bytes + s->wnid.bytes +
+               s->pleaf.bytes + s->ptris.bytes;
     const uint32_t id = c->next_id++;
     c->scenes[id] = std::move(s);
     *out = id;
@@ -443,7 +459,7 @@ int tim_rt_free_scene(tim_rt_ctx* c, tim_rt_scene_id id) {
         return TIM_RT_EINVAL;
     }
     cudaStreamSynchronize(c->stream);
-    for (DevBuf* b : {&s->blob, &s->pos, &s->nrm, &s->uv, &s->wnodes, &s->wtris, &s->wnid}) dev_free(c, *b);
+    for (DevBuf* b : {&s->blob, &s->pos, &s->nrm, &s->uv, &s->wnodes, &s->wtris, &s->wnid, &s->ptris, &s->pleaf}) dev_free(c, *b);
     c->scenes.erase(id);
     return TIM_RT_OK;
 }

@@ -76,6 +76,62 @@ bool validate_bvh(const uint8_t* blob, uint64_t n_bytes, const uint32_t ranges[7
     return true;
 }
 
+// ---------------------------------------------------------------------------------- leaf-triangle copy
+
+// Per node: (first triangle in `tris`, leaf header word, leaf-data offset, 0); a
+// node without leaf data (offset 0xFFFFFFFF) gets header 0, as the kernels read
+// it. Per leaf-data triangle record, in node order and, within a node, in the
+// leaf's stored order: (p0, vertexOffset) (p1 - p0, index01) (p2 - p0,
+// index2_matId) as 12 floats, the edges being the same rounded differences
+// CollideTriangle forms (collision.glsl:60-61). Runs after validate_bvh, so every
+// offset and vertex index is in range.
+void build_leaf_tris(const uint8_t* blob, const uint32_t ranges[7][2], uint32_t num_nodes, const float* pos,
+                     RawVec<float>& tris, RawVec<uint32_t>& info) {
+    const PNode* nodes = reinterpret_cast<const PNode*>(blob + ranges[TIM_RT_RANGE_NODE][0]);
+    const uint32_t* leaf = reinterpret_cast<const uint32_t*>(blob + ranges[TIM_RT_RANGE_LEAF][0]);
+    info.resize(4ull * num_nodes);
+    uint64_t total = 0;
+    for (uint32_t i = 0; i < num_nodes; ++i) {
+        const uint32_t off = nodes[i].nid[3];
+        const uint32_t hdr = off == 0xFFFFFFFFu ? 0u : leaf[off];
+        info[4ull * i + 0] = (uint32_t)total;
+        info[4ull * i + 1] = hdr;
+        info[4ull * i + 2] = off;
+        info[4ull * i + 3] = 0u;
+        total += hdr & 0xFFFu;
+    }
+    tris.resize(12ull * total);
+    const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    const uint32_t chunk = (num_nodes + hw - 1u) / hw;
+    auto fill = [&](uint32_t n0, uint32_t n1) {
+        for (uint32_t i = n0; i < n1; ++i) {
+            const uint32_t nt = info[4ull * i + 1] & 0xFFFu;
+            float* out = tris.data() + 12ull * info[4ull * i];
+            for (uint32_t t = 0; t < nt; ++t, out += 12) {
+                const uint32_t* r = leaf + 1u + info[4ull * i + 2] + 3u * t;
+                const float* P0 = pos + 3ull * (r[0] + (r[1] & 0xFFFFu));
+                const float* P1 = pos + 3ull * (r[0] + (r[1] >> 16));
+                const float* P2 = pos + 3ull * (r[0] + (r[2] & 0xFFFFu));
+                for (int a = 0; a < 3; ++a) {
+                    out[a] = P0[a];
+                    out[4 + a] = P1[a] - P0[a];
+                    out[8 + a] = P2[a] - P0[a];
+                }
+                std::memcpy(out + 3, &r[0], 4);
+                std::memcpy(out + 7, &r[1], 4);
+                std::memcpy(out + 11, &r[2], 4);
+            }
+        }
+    };
+    if (total < 65536u || hw == 1u) {
+        fill(0, num_nodes);
+        return;
+    }
+    std::vector<std::thread> pool;
+    for (uint32_t n0 = 0; n0 < num_nodes; n0 += chunk) pool.emplace_back(fill, n0, std::min(num_nodes, n0 + chunk));
+    for (std::thread& t : pool) t.join();
+}
+
 // ---------------------------------------------------------------------------------- 8-wide collapse
 
 namespace {
@@ -275,25 +331,107 @@ struct Collapse {
         }
     }
 
-    // Greedily opens the internal slot with the largest surface area until 8
-    // slots; leaves of no triangle are dropped (they never produce hits).
-    std::vector<Slot> expand(std::vector<Slot> fr) const {
-        for (;;) {
-            if (fr.size() >= 8) break;
-            int best = -1;
-            double ba = -1.0;
-            for (size_t k = 0; k < fr.size(); ++k)
-                if (!(fr[k].id & kLeafBit) && area(fr[k]) > ba) { ba = area(fr[k]); best = (int)k; }
-            if (best < 0) break;
+    // Choice of the slots of every wide node: a dynamic programme over the binary
+    // tree for the cut of at most 8 subtrees of least surface-area cost (the
+    // collapse of Ylitie, Karras & Laine 2017, section 3.1, restricted to cuts of
+    // the reference tree so that every slot stays one binary subtree and every
+    // binary leaf keeps its triangles and order). cost[x][k] is the least cost of
+    // covering the subtree of x with at most k slots: a leaf slot costs
+    // A * (c_leaf + c_tri * triangles), an internal slot A * c_node plus the best
+    // cover of its two children by at most 8 slots, A the surface area of the box
+    // the parent record stores; leaves without triangles take no slot. Filled
+    // bottom-up over node ids (children have larger ids than their parent).
+    static constexpr float kNodeCost = 1.0f, kLeafCost = 0.15f, kTriCost = 0.25f;
+    std::vector<float> cost;            // 9 per node (as a child of its parent)
+    std::vector<int8_t> choice;         // 9 per node: -1 = one slot, j = j slots on the left child's side
+    std::vector<int8_t> split;          // per left child id: slots on its side in its parent's wide node
+    bool boxes_finite = true;           // every child box of the tree is finite (else the collapse refuses it)
+
+    static float slot_area(const float lo[3], const float hi[3]) {
+        const float dx = std::fabs(hi[0] - lo[0]), dy = std::fabs(hi[1] - lo[1]), dz = std::fabs(hi[2] - lo[2]);
+        const float a = dx * dy + dy * dz + dz * dx;
+        return std::isfinite(a) ? a : 3.0e38f;
+    }
+
+    void plan(uint32_t num_nodes) {
+        const float inf = INFINITY;
+        cost.assign(9ull * num_nodes, inf);
+        choice.assign(9ull * num_nodes, (int8_t)-1);
+        split.assign(num_nodes, (int8_t)1);
+        // best cover of an internal node's two children by at most k slots
+        auto pair_best = [&](uint32_t l, int k, int& jbest) {
+            float best = inf;
+            jbest = -1;
+            for (int j = 0; j <= k; ++j) {
+                const float v = cost[9ull * l + j] + cost[9ull * (l + 1u) + (k - j)];
+                if (v < best) { best = v; jbest = j; }
+            }
+            return best;
+        };
+        for (uint32_t pi = num_nodes; pi-- > 0;) {
+            const PNode& p = nodes[pi];
+            const uint32_t left = p.nid[2] & kMask;
+            if (left == kInvalid) continue;
             Slot a, b;
-            child_slots(nodes[fr[best].id], a, b, &fr[best]);
-            fr.erase(fr.begin() + best);
-            fr.push_back(a);
-            fr.push_back(b);
+            child_slots(p, a, b, nullptr);
+            for (int ax = 0; ax < 3; ++ax)
+                boxes_finite = boxes_finite && std::isfinite(a.lo[ax]) && std::isfinite(a.hi[ax]) &&
+                               std::isfinite(b.lo[ax]) && std::isfinite(b.hi[ax]);
+            for (const Slot* c : {&a, &b}) {
+                const uint32_t ci = c->id & kMask;
+                float* f = cost.data() + 9ull * ci;
+                int8_t* ch = choice.data() + 9ull * ci;
+                const float area_c = slot_area(c->lo, c->hi);
+                if (c->id & kLeafBit) {
+                    const uint32_t nt = leaf_tris(c->id);
+                    for (int k = 0; k <= 8; ++k) f[k] = nt == 0u ? 0.0f : (k == 0 ? inf : area_c * (kLeafCost + kTriCost * (float)nt));
+                    continue;
+                }
+                const uint32_t cl = nodes[ci].nid[2] & kMask;   // validated: an inner node has children
+                int j8;
+                const float single = area_c * kNodeCost + pair_best(cl, 8, j8);
+                split[cl] = (int8_t)j8;
+                for (int k = 0; k <= 8; ++k) {
+                    int j;
+                    float best = pair_best(cl, k, j);   // several slots below this node
+                    int8_t c8 = (int8_t)j;
+                    if (k >= 1 && single <= best) { best = single; c8 = -1; }
+                    f[k] = best;
+                    ch[k] = c8;
+                }
+            }
         }
+        const uint32_t root_left = nodes[0].nid[2] & kMask;
+        if (root_left != kInvalid) {   // a single-leaf tree has no wide node to plan
+            int j0;
+            pair_best(root_left, 8, j0);
+            split[root_left] = (int8_t)j0;
+        }
+    }
+
+    // The slots of the cut of x's subtree by at most k slots (the plan's choice).
+    void cut(const Slot& x, int k, std::vector<Slot>& out) const {
+        if (x.id & kLeafBit) {
+            if (leaf_tris(x.id) > 0u) out.push_back(x);   // leaves of no triangle never produce hits
+            return;
+        }
+        const int8_t c = choice[9ull * (x.id & kMask) + k];
+        if (c < 0) {
+            out.push_back(x);
+            return;
+        }
+        Slot a, b;
+        child_slots(nodes[x.id & kMask], a, b, &x);
+        cut(a, c, out);
+        cut(b, k - c, out);
+    }
+
+    // The slots of the wide node of the binary node whose children are a and b.
+    std::vector<Slot> expand(const std::vector<Slot>& ab) const {
         std::vector<Slot> kept;
-        for (const Slot& s : fr)
-            if (!(s.id & kLeafBit) || leaf_tris(s.id) > 0u) kept.push_back(s);
+        const int j = split[ab[0].id & kMask];
+        cut(ab[0], j < 0 ? 1 : j, kept);
+        cut(ab[1], j < 0 ? 1 : 8 - j, kept);
         return kept;
     }
 
@@ -397,6 +535,12 @@ bool build_wide(const uint8_t* blob, const uint32_t ranges[7][2], uint32_t num_n
     C.leaf_words = ranges[TIM_RT_RANGE_LEAF][1] / 4u;
     C.pos = pos;
     C.root_is_leaf = num_nodes == 1u;
+    C.plan(num_nodes);
+    if (!C.boxes_finite) {
+        // a non-finite box can make the reference skip a subtree the 8-wide form would open
+        err = "box bounds cannot be quantised (non-finite coordinates)";
+        return false;
+    }
     out = WideHost();
     Part top;
     top.nodes.reserve(20ull * (num_nodes / 4 + 4));
@@ -521,7 +665,9 @@ bool check_wide(const uint8_t* blob, const uint32_t ranges[7][2], uint32_t num_n
     C.leaf_words = ranges[TIM_RT_RANGE_LEAF][1] / 4u;
     C.pos = pos;
     C.root_is_leaf = num_nodes == 1u;
+    C.plan(num_nodes);
     std::memset(&rep, 0, sizeof(rep));
+    if (!C.boxes_finite) { err = "box bounds cannot be quantised (non-finite coordinates)"; return false; }
     const uint64_t nw = w.num_nodes, nt = w.tris.size() / 12;
     if (nw == 0 || w.nodes.size() != 20ull * nw || w.tri_leaf.size() != 8ull * nt) { err = "8-wide arrays have inconsistent sizes"; return false; }
     std::vector<uint8_t> node_seen(nw, 0), tri_seen(nt, 0);

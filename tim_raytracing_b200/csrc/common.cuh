@@ -44,6 +44,10 @@ struct SceneView {
     const uint4* wtri_leaf;     // per wide triangle, its binary leaf: (E lo.xyz, nid), (E hi.xyz, flag)
     uint32_t num_wnodes;
     uint32_t wide_root_is_leaf; // scene is a single leaf
+    // the plain form's leaf-triangle copy (null: read the reference's leaf data and
+    // positions directly, as the allocation-free entry point does)
+    const uint4* pleaf;         // per node: (first triangle, leaf header, leaf-data offset, 0)
+    const float4* ptris;        // 3 x float4 per leaf triangle: (p0, vo) (e1, i01) (e2, i2m)
 };
 
 struct Ray {

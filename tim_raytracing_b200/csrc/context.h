@@ -20,6 +20,7 @@ struct DevBuf {
 
 struct Scene {
     DevBuf blob, pos, nrm, uv, wnodes, wtris, wnid;
+    DevBuf ptris, pleaf;   // the plain form's leaf-triangle copy (build_leaf_tris)
     SceneView view{};
     uint32_t ranges[7][2];
     tim_rt_push_constants pc{};

@@ -48,6 +48,13 @@ struct WideHost {
 bool validate_bvh(const uint8_t* blob, uint64_t n_bytes, const uint32_t ranges[7][2], uint32_t num_nodes,
                   uint32_t num_vertex, uint32_t num_lights, uint32_t num_blas, uint32_t* depth_out, std::string& err);
 
+// The plain form's copy of the leaf triangles: per node a 16-byte record (first
+// triangle, leaf header, leaf-data offset, 0) and per triangle 48 bytes
+// (p0, vertexOffset) (p1 - p0, index01) (p2 - p0, index2_matId), so that a leaf
+// visit reads one record and each triangle test three 16-byte vectors.
+void build_leaf_tris(const uint8_t* blob, const uint32_t ranges[7][2], uint32_t num_nodes, const float* pos,
+                     RawVec<float>& tris, RawVec<uint32_t>& info);
+
 // Collapses the binary tree into 8-wide nodes with 8-bit quantised child boxes.
 bool build_wide(const uint8_t* blob, const uint32_t ranges[7][2], uint32_t num_nodes, const float* pos,
                 WideHost& out, std::string& err);

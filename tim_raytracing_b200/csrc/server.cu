@@ -79,8 +79,11 @@ struct Req {
     uint4* d_hit = nullptr;
     uint32_t* d_nid = nullptr;
     float2* d_bary = nullptr;
-    uint32_t issued = 0;          // rays handed to steps so far
+    uint32_t issued = 0;          // rays handed to steps so far (worker only)
     bool first_chunk = true;      // the next step must wait for the upload
+    bool last_planned = false;    // a planned step traces its last rays (under the server mutex)
+    bool cancel = false;          // tim_rt_server_cancel took it back (under the server mutex)
+    uint32_t planned = 0;         // rays assigned to planned steps (under the server mutex)
     Clock::time_point t_submit, t_admit;
     cudaEvent_t uploaded = nullptr;
     // probe-field update requests
@@ -129,6 +132,8 @@ struct Slot {
     MultiJob* d_jobs = nullptr;
     uint32_t* d_counter = nullptr;
     cudaEvent_t done = nullptr;
+    cudaEvent_t t_begin = nullptr, t_end = nullptr;   // around the step's kernel, for the GPU-busy time
+    bool timing_pending = false;   // t_begin / t_end hold a step not yet added to gpu_busy_ms (under the mutex)
 };
 
 }  // namespace
@@ -159,6 +164,11 @@ struct tim_rt_server {
     // statistics (under m)
     std::vector<float> lat_ms, queue_ms;
     uint64_t submitted = 0, completed = 0, rays_completed = 0, steps = 0;
+    uint64_t cancelled = 0, step_requests = 0;
+    uint32_t max_step_requests = 0, max_inflight = 0;
+    double gpu_busy_ms = 0.0;
+    std::vector<Req*> cancel_q;        // admitted requests taken back, for the worker
+    std::set<uint64_t> cancelled_tickets;   // completed by cancellation (tim_rt_server_wait reports it)
     bool t0_set = false;
     Clock::time_point t0;
 
@@ -189,6 +199,25 @@ void CUDART_CB on_requests_done(void* p) {
             s->queue_ms.push_back(std::chrono::duration<float, std::milli>(r->t_admit - r->t_submit).count());
             s->completed++;
             s->rays_completed += r->rays;
+            s->pending.erase(r->ticket);
+            s->finished.push_back(r);
+        }
+    }
+    s->cv.notify_all();
+    s->cv_done.notify_all();
+    delete msg;
+}
+
+// Runs on the compute stream after every step that traced part of the cancelled
+// requests: they complete without results.
+void CUDART_CB on_requests_cancelled(void* p) {
+    DoneMsg* msg = static_cast<DoneMsg*>(p);
+    tim_rt_server* s = msg->s;
+    {
+        std::lock_guard<std::mutex> lk(s->m);
+        for (Req* r : msg->reqs) {
+            s->cancelled++;
+            s->cancelled_tickets.insert(r->ticket);
             s->pending.erase(r->ticket);
             s->finished.push_back(r);
         }
@@ -250,17 +279,21 @@ void plan_step(tim_rt_server* s, Plan& P) {
     uint64_t used = 0;
     for (size_t i = 0; i < k; ++i) {
         Req* r = cand[i];
-        take[i] = std::min<uint32_t>(r->r.n - r->issued, share);
+        take[i] = std::min<uint32_t>(r->r.n - r->planned, share);
         used += take[i];
     }
     for (size_t i = 0; i < k && used < cap; ++i) {
         Req* r = cand[i];
-        const uint32_t extra = (uint32_t)std::min<uint64_t>(r->r.n - r->issued - take[i], cap - used);
+        const uint32_t extra = (uint32_t)std::min<uint64_t>(r->r.n - r->planned - take[i], cap - used);
         take[i] += extra;
         used += extra;
     }
-    for (size_t i = 0; i < k; ++i)
-        if (take[i]) P.chunks.push_back({cand[i], take[i]});
+    for (size_t i = 0; i < k; ++i) {
+        if (!take[i]) continue;
+        P.chunks.push_back({cand[i], take[i]});
+        cand[i]->planned += take[i];
+        if (cand[i]->planned == cand[i]->r.n) cand[i]->last_planned = true;
+    }
 }
 
 int issue_step(tim_rt_server* s, Plan& P) {
@@ -307,9 +340,15 @@ int issue_step(tim_rt_server* s, Plan& P) {
     cfg.ray_sort = TIM_RT_SORT_NONE;
     if (cfg.stack_depth > depth) depth = cfg.stack_depth;
     uint32_t* err = static_cast<uint32_t*>(s->ctx->counters.ptr) + kErrWord;
-    if (launch_multi(sl.d_views, sl.d_jobs, nj, total, sl.d_counter, err, depth, s->wide, nullptr, s->comp, cfg) !=
-        cudaSuccess)
+    if (cudaEventRecord(sl.t_begin, s->comp) != cudaSuccess ||
+        launch_multi(sl.d_views, sl.d_jobs, nj, total, sl.d_counter, err, depth, s->wide, nullptr, s->comp, cfg) !=
+            cudaSuccess ||
+        cudaEventRecord(sl.t_end, s->comp) != cudaSuccess)
         return TIM_RT_EDEVICE;
+    {
+        std::lock_guard<std::mutex> lk(s->m);
+        sl.timing_pending = true;
+    }
     if (cudaLaunchHostFunc(s->comp, on_slot_free, new SlotMsg{s, P.slot}) != cudaSuccess) return TIM_RT_EDEVICE;
     if (!P.finishing.empty()) {
         if (cudaEventRecord(sl.done, s->comp) || cudaStreamWaitEvent(s->down, sl.done, 0)) return TIM_RT_EDEVICE;
@@ -391,16 +430,38 @@ void release_req(Req* r) {
     delete r;
 }
 
+// Adds a completed step's kernel time to gpu_busy_ms (caller holds the mutex; the
+// slot is free, so its end event has completed and the query does not wait).
+void account_slot(tim_rt_server* s, Slot& sl) {
+    if (!sl.timing_pending) return;
+    sl.timing_pending = false;
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, sl.t_begin, sl.t_end) == cudaSuccess) s->gpu_busy_ms += ms;
+    else cudaGetLastError();
+}
+
+// Cancelled requests that were admitted: after the upload and every step that
+// traced part of them, they complete without results (on_requests_cancelled).
+int issue_cancels(tim_rt_server* s, std::vector<Req*>& cancels) {
+    if (cancels.empty()) return TIM_RT_OK;
+    for (Req* r : cancels)
+        if (r->uploaded && cudaStreamWaitEvent(s->comp, r->uploaded, 0) != cudaSuccess) return TIM_RT_EDEVICE;
+    if (cudaLaunchHostFunc(s->comp, on_requests_cancelled, new DoneMsg{s, cancels}) != cudaSuccess)
+        return TIM_RT_EDEVICE;
+    return TIM_RT_OK;
+}
+
 void worker_main(tim_rt_server* s) {
     cudaSetDevice(s->ctx->device);
     for (;;) {
-        std::vector<Req*> release, admitted;
+        std::vector<Req*> release, admitted, cancels;
         Plan P;
         {
             std::unique_lock<std::mutex> lk(s->m);
             s->cv.wait(lk, [&] {
                 if (s->stop || !s->finished.empty()) return true;
                 if (s->error) return false;
+                if (!s->cancel_q.empty()) return true;
                 if (!s->waiting.empty()) {
                     // admissible once the head fits in the free arena
                     uint64_t off;
@@ -414,6 +475,11 @@ void worker_main(tim_rt_server* s) {
             if (s->stop && (s->error || (s->pending.empty() && s->finished.empty()))) break;
             release.swap(s->finished);
             for (Req* r : release) s->arena.release(r->off, r->bytes);
+            // admitted requests taken back leave the active list before planning
+            cancels.swap(s->cancel_q);
+            if (!cancels.empty())
+                s->active.erase(std::remove_if(s->active.begin(), s->active.end(), [](Req* r) { return r->cancel; }),
+                                s->active.end());
             if (!s->error) {
                 while (!s->waiting.empty()) {
                     Req* r = s->waiting.front();
@@ -428,8 +494,20 @@ void worker_main(tim_rt_server* s) {
                 if (!s->active.empty() && !s->free_slots.empty()) {
                     P.slot = s->free_slots.back();
                     s->free_slots.pop_back();
+                    account_slot(s, s->slots[P.slot]);
                     plan_step(s, P);
                     s->steps++;
+                    s->step_requests += P.chunks.size();
+                    s->max_step_requests = std::max<uint32_t>(s->max_step_requests, (uint32_t)P.chunks.size());
+                    // steps queued on the GPU and not yet completed, this one included
+                    s->max_inflight = std::max<uint32_t>(
+                        s->max_inflight, (uint32_t)(s->slots.size() - s->free_slots.size()));
+                    // requests whose last rays this step traces leave the active list
+                    for (auto& ch : P.chunks)
+                        if (ch.first->last_planned) P.finishing.push_back(ch.first);
+                    s->active.erase(std::remove_if(s->active.begin(), s->active.end(),
+                                                   [](Req* r) { return r->last_planned; }),
+                                    s->active.end());
                 }
             }
         }
@@ -460,16 +538,8 @@ void worker_main(tim_rt_server* s) {
         // admitted probe updates run on the compute stream ahead of the next trace step
         for (Req* r : admitted)
             if (r->probe && rc == TIM_RT_OK) rc = issue_probe(s, r);
-        if (P.slot >= 0 && rc == TIM_RT_OK) {
-            // requests whose last rays this step traces leave the active list
-            for (auto& ch : P.chunks)
-                if (ch.first->issued + ch.second == ch.first->r.n) P.finishing.push_back(ch.first);
-            rc = issue_step(s, P);
-            std::lock_guard<std::mutex> lk(s->m);
-            s->active.erase(std::remove_if(s->active.begin(), s->active.end(),
-                                           [](Req* r) { return r->issued == r->r.n; }),
-                            s->active.end());
-        }
+        if (P.slot >= 0 && rc == TIM_RT_OK) rc = issue_step(s, P);
+        if (rc == TIM_RT_OK) rc = issue_cancels(s, cancels);
         if (rc != TIM_RT_OK) fail_all(s, rc, std::string("serving step failed: ") + cudaGetErrorString(cudaGetLastError()));
     }
 }
@@ -495,6 +565,8 @@ int server_teardown(tim_rt_server* s) {
         dev_free(s->ctx, sl.dev);
         if (sl.host) cudaFreeHost(sl.host);
         if (sl.done) cudaEventDestroy(sl.done);
+        if (sl.t_begin) cudaEventDestroy(sl.t_begin);
+        if (sl.t_end) cudaEventDestroy(sl.t_end);
     }
     dev_free(s->ctx, s->arena_buf);
     for (cudaStream_t st : {s->up, s->comp, s->down})
@@ -547,7 +619,8 @@ int tim_rt_server_create(tim_rt_ctx* c, const tim_rt_server_params* params, tim_
     for (size_t i = 0; ok && i < s->slots.size(); ++i) {
         Slot& sl = s->slots[i];
         if (dev_alloc(c, sl.dev, vb + jb + 256) != TIM_RT_OK || cudaHostAlloc(&sl.host, vb + jb, 0) != cudaSuccess ||
-            cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming) != cudaSuccess) {
+            cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreate(&sl.t_begin) != cudaSuccess || cudaEventCreate(&sl.t_end) != cudaSuccess) {
             ok = false;
             break;
         }
@@ -693,6 +766,52 @@ int tim_rt_server_wait(tim_rt_server* s, uint64_t ticket, uint32_t timeout_ms) {
         set_error(s->error_msg);
         return s->error;
     }
+    if (s->cancelled_tickets.erase(ticket)) {
+        set_error("tim_rt_server_wait: the request was cancelled");
+        return TIM_RT_ECANCELLED;
+    }
+    return TIM_RT_OK;
+}
+
+int tim_rt_server_cancel(tim_rt_server* s, uint64_t ticket) {
+    if (!s) {
+        set_error("null server");
+        return TIM_RT_EINVAL;
+    }
+    std::unique_lock<std::mutex> lk(s->m);
+    if (s->error) {
+        set_error(s->error_msg);
+        return s->error;
+    }
+    auto it = s->pending.find(ticket);
+    if (it == s->pending.end()) {
+        set_error("tim_rt_server_cancel: unknown or completed request");
+        return TIM_RT_ENOTFOUND;
+    }
+    Req* r = it->second;
+    if (r->cancel) return TIM_RT_OK;
+    auto w = std::find(s->waiting.begin(), s->waiting.end(), r);
+    if (w != s->waiting.end()) {
+        // not admitted: nothing of it reached the device
+        s->waiting.erase(w);
+        s->pending.erase(it);
+        s->cancelled++;
+        s->cancelled_tickets.insert(ticket);
+        r->scene->batch_refs--;
+        delete r;
+        lk.unlock();
+        s->cv.notify_all();
+        s->cv_done.notify_all();
+        return TIM_RT_OK;
+    }
+    if (r->probe || r->last_planned) {
+        set_error("tim_rt_server_cancel: the request's work is already on the GPU; it completes normally");
+        return TIM_RT_EBUSY;
+    }
+    r->cancel = true;
+    s->cancel_q.push_back(r);
+    lk.unlock();
+    s->cv.notify_all();
     return TIM_RT_OK;
 }
 
@@ -742,10 +861,19 @@ int tim_rt_server_stats_get(tim_rt_server* s, tim_rt_server_stats* st, int reset
     st->queue_p50_ms = percentile(s->queue_ms, 0.50);
     st->queue_p99_ms = percentile(s->queue_ms, 0.99);
     st->wall_s = s->t0_set ? std::chrono::duration<float>(Clock::now() - s->t0).count() : 0.f;
+    for (int k : s->free_slots) account_slot(s, s->slots[k]);   // completed steps not yet counted
+    st->cancelled = s->cancelled;
+    st->step_requests = s->step_requests;
+    st->max_step_requests = s->max_step_requests;
+    st->max_inflight_steps = s->max_inflight;
+    st->gpu_busy_ms = (float)s->gpu_busy_ms;
     if (reset) {
         s->lat_ms.clear();
         s->queue_ms.clear();
         s->submitted = s->completed = s->rays_completed = s->steps = 0;
+        s->cancelled = s->step_requests = 0;
+        s->max_step_requests = s->max_inflight = 0;
+        s->gpu_busy_ms = 0.0;
         s->arena.peak = s->arena.used;
         s->t0_set = false;
     }

@@ -126,41 +126,72 @@ __device__ __forceinline__ void plain_children(const TravState& st, const float4
     }
 }
 
+// Acceptance of one triangle hit (bvh_collide / bvh_collide_fast): any-hit rays
+// end, closest-hit rays keep it and shrink their t by 1e-5. Returns true when
+// the ray ends.
+__device__ __forceinline__ bool plain_accept(TravState& st, float t, float u, float v, uint32_t r0, uint32_t r1,
+                                             uint32_t r2, uint32_t nidm) {
+    if (st.any) {
+        st.hit = true;
+        st.done = true;
+        return true;
+    }
+    st.t = t - kOffsetRayCollision;
+    st.rec0 = r0; st.rec1 = r1; st.rec2 = r2;
+    st.nid = nidm;
+    st.u = u; st.v = v;
+    st.hit = true;
+    return false;
+}
+
 // Leaf visit: bvh_collide (bvhCollision.glsl:177-239) for closest-hit rays,
-// bvh_collide_fast (bvhCollision.glsl:241-284) for any-hit rays.
+// bvh_collide_fast (bvhCollision.glsl:241-284) for any-hit rays. With the
+// scene's leaf-triangle copy the leaf's record is one 16-byte load and each
+// triangle three 16-byte loads of (p0, e1, e2) with the reference's record words
+// in .w; without it (the allocation-free entry point and the 8-wide kernels'
+// fallback walk) the record words and the vertex positions are gathered from the
+// reference's own buffers. Same triangles, same order, same arithmetic.
 __device__ __forceinline__ void plain_leaf(const SceneView& s, TravState& st, uint32_t node) {
     const uint32_t nidm = node & kNidMask;
-    const uint32_t off = __ldg(reinterpret_cast<const uint32_t*>(s.nodes + 4u * nidm) + 3);
-    const uint32_t hdr = leaf_header(s, off);
-    const uint32_t ntri = hdr & ((1u << kTriBits) - 1u);
-    const uint32_t* rec = s.leaf + off + 1u;
+    uint32_t hdr, off;
     st.c_leaf++;
-    for (uint32_t i = 0; i < ntri; ++i, rec += 3) {
-        st.c_tri++;
-        const uint32_t r0 = __ldg(rec), r1 = __ldg(rec + 1), r2 = __ldg(rec + 2);
-        const uint32_t i0 = r0 + (r1 & 0xFFFFu), i1 = r0 + (r1 >> 16), i2 = r0 + (r2 & 0xFFFFu);
-        const float* P0 = s.pos + 3u * i0;
-        const float* P1 = s.pos + 3u * i1;
-        const float* P2 = s.pos + 3u * i2;
-        const float p0x = __ldg(P0), p0y = __ldg(P0 + 1), p0z = __ldg(P0 + 2);
-        const float e1x = __ldg(P1) - p0x, e1y = __ldg(P1 + 1) - p0y, e1z = __ldg(P1 + 2) - p0z;
-        const float e2x = __ldg(P2) - p0x, e2y = __ldg(P2 + 1) - p0y, e2z = __ldg(P2 + 2) - p0z;
-        float u, v;
-        const float t = collide_triangle_e(st.r, p0x, p0y, p0z, e1x, e1y, e1z, e2x, e2y, e2z, st.t, u, v);
-        if (t > 0.0f) {
-            if (st.any) {
-                st.hit = true;
-                st.done = true;
+    if (s.ptris) {
+        const uint4 li = __ldg(s.pleaf + nidm);
+        hdr = li.y;
+        off = li.z;
+        const uint32_t ntri = hdr & ((1u << kTriBits) - 1u);
+        const float4* tp = s.ptris + 3u * li.x;
+        for (uint32_t i = 0; i < ntri; ++i, tp += 3) {
+            st.c_tri++;
+            const float4 A = __ldg(tp), B = __ldg(tp + 1), C = __ldg(tp + 2);
+            float u, v;
+            const float t = collide_triangle_e(st.r, A.x, A.y, A.z, B.x, B.y, B.z, C.x, C.y, C.z, st.t, u, v);
+            if (t > 0.0f && plain_accept(st, t, u, v, __float_as_uint(A.w), __float_as_uint(B.w), __float_as_uint(C.w),
+                                         nidm))
                 return;
-            }
-            st.t = t - kOffsetRayCollision;
-            st.rec0 = r0; st.rec1 = r1; st.rec2 = r2;
-            st.nid = nidm;
-            st.u = u; st.v = v;
-            st.hit = true;
+        }
+    } else {
+        off = __ldg(reinterpret_cast<const uint32_t*>(s.nodes + 4u * nidm) + 3);
+        hdr = leaf_header(s, off);
+        const uint32_t ntri = hdr & ((1u << kTriBits) - 1u);
+        const uint32_t* rec = s.leaf + off + 1u;
+        for (uint32_t i = 0; i < ntri; ++i, rec += 3) {
+            st.c_tri++;
+            const uint32_t r0 = __ldg(rec), r1 = __ldg(rec + 1), r2 = __ldg(rec + 2);
+            const uint32_t i0 = r0 + (r1 & 0xFFFFu), i1 = r0 + (r1 >> 16), i2 = r0 + (r2 & 0xFFFFu);
+            const float* P0 = s.pos + 3u * i0;
+            const float* P1 = s.pos + 3u * i1;
+            const float* P2 = s.pos + 3u * i2;
+            const float p0x = __ldg(P0), p0y = __ldg(P0 + 1), p0z = __ldg(P0 + 2);
+            const float e1x = __ldg(P1) - p0x, e1y = __ldg(P1 + 1) - p0y, e1z = __ldg(P1 + 2) - p0z;
+            const float e2x = __ldg(P2) - p0x, e2y = __ldg(P2 + 1) - p0y, e2z = __ldg(P2 + 2) - p0z;
+            float u, v;
+            const float t = collide_triangle_e(st.r, p0x, p0y, p0z, e1x, e1y, e1z, e2x, e2y, e2z, st.t, u, v);
+            if (t > 0.0f && plain_accept(st, t, u, v, r0, r1, r2, nidm)) return;
         }
     }
     if (st.any) {
+        const uint32_t ntri = hdr & ((1u << kTriBits) - 1u);
         const uint32_t nblas = (hdr >> kTriBits) & ((1u << kBlasBits) - 1u);
         for (uint32_t i = 0; i < nblas; ++i) {
             const uint32_t bi = __ldg(s.leaf + off + 1u + 3u * ntri + i);

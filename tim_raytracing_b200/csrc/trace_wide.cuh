@@ -35,9 +35,10 @@
 // origin lies within 2^60, tmin_here <= tmin_reference and tmax_here >=
 // tmax_reference for every child: the quantised traversal visits a superset of
 // the binary traversal's leaves and never loses a hit. For other rays (a zero
-// component among them) the slab can come out narrower than the reference's, so
-// every hit they report is checked below and a miss is not trusted
-// (wide_miss_final): both go to the binary walk.
+// or tiny component, a far origin) the slab can come out narrower than the
+// reference's, so their 8-wide answer, hit or miss, is not trusted
+// (wide_trusted): they are traced again by the binary walk (a single-leaf
+// tree, which both walks test without a box, excepted).
 //
 // Same hit as the binary walk, for every ray. The reference's closest-hit rule
 // is order-dependent: a hit at t is accepted iff t < c, and then c = t - 1e-5,
@@ -82,9 +83,32 @@ __device__ __forceinline__ float min3f(float a, float b, float c) {
     return r;
 }
 
-// Byte k of `word` as a float (0x4B0000qq is 2^23 + q exactly).
-__device__ __forceinline__ float wbyte(uint32_t word, uint32_t k) {
-    return __uint_as_float(__byte_perm(word, 0x4B000000u, 0x7650u | k)) - 8388608.0f;
+// Packed pairs of floats (sm_100 f32x2 arithmetic): lo in the low 32 bits.
+__device__ __forceinline__ uint64_t pack2f(float lo, float hi) {
+    uint64_t r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void unpack2f(uint64_t v, float& lo, float& hi) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ uint64_t fma2(uint64_t a, uint64_t b, uint64_t c) {
+    uint64_t r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+    return r;
+}
+__device__ __forceinline__ uint64_t sub2(uint64_t a, uint64_t b) {
+    uint64_t r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+// Byte k of w0 and of w1 as the floats 2^23 + q (0x4B0000qq is exact), packed;
+// sub2 with 2^23 then gives q.
+__device__ __forceinline__ uint64_t qbytes2(uint32_t w0, uint32_t w1, uint32_t k) {
+    uint64_t r;
+    const uint32_t lo = __byte_perm(w0, 0x4B000000u, 0x7650u | k), hi = __byte_perm(w1, 0x4B000000u, 0x7650u | k);
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "r"(lo), "r"(hi));
+    return r;
 }
 
 // Tests the 8 slots of wide node `ni` and returns the hit slots as a rank mask:
@@ -121,25 +145,46 @@ __device__ __forceinline__ uint32_t wide_visit(const SceneView& s, const TravSta
     const uint32_t ny0 = negy ? U4.x : U2.z, ny1 = negy ? U4.y : U2.w, fy0 = negy ? U2.z : U4.x, fy1 = negy ? U2.w : U4.y;
     const uint32_t nz0 = negz ? U4.z : U3.x, nz1 = negz ? U4.w : U3.y, fz0 = negz ? U3.x : U4.z, fz1 = negz ? U3.y : U4.w;
     const float tcur = st.t;
+    // Slots k and k + 4 in one packed pair, one axis at a time: each plane of both
+    // slots is one sub.f32x2 (byte to float) and one fma.f32x2, which round each
+    // half exactly as the scalar FADD and FFMA do (IEEE round to nearest per
+    // element), so every value is that of the scalar form of this test.
+    const uint64_t magic = pack2f(8388608.0f, 8388608.0f);
+    float tn[8], tf[8];   // running slab entry / exit per slot
+#pragma unroll
+    for (uint32_t kk = 0; kk < 4u; ++kk) {
+        unpack2f(fma2(sub2(qbytes2(nx0, nx1, kk), magic), pack2f(Bnx, Bnx), pack2f(Anx, Anx)), tn[kk], tn[kk + 4u]);
+        unpack2f(fma2(sub2(qbytes2(fx0, fx1, kk), magic), pack2f(Bfx, Bfx), pack2f(Afx, Afx)), tf[kk], tf[kk + 4u]);
+    }
+#pragma unroll
+    for (uint32_t kk = 0; kk < 4u; ++kk) {
+        float a, b, c, d;
+        unpack2f(fma2(sub2(qbytes2(ny0, ny1, kk), magic), pack2f(Bny, Bny), pack2f(Any, Any)), a, b);
+        unpack2f(fma2(sub2(qbytes2(fy0, fy1, kk), magic), pack2f(Bfy, Bfy), pack2f(Afy, Afy)), c, d);
+        tn[kk] = fmaxf(tn[kk], a);
+        tn[kk + 4u] = fmaxf(tn[kk + 4u], b);
+        tf[kk] = fminf(tf[kk], c);
+        tf[kk + 4u] = fminf(tf[kk + 4u], d);
+    }
     uint32_t mask = 0, nearest = 0xFFFFFFFFu;
 #pragma unroll
-    for (uint32_t k = 0; k < 8u; ++k) {
-        const uint32_t wsel = k < 4u ? 0u : 1u, kk = k & 3u;
-        // empty slots carry the inverted box qlo = 255, qhi = 0 and fail this test by
-        // themselves (if rounding ever lets one through, it is a leaf of 0 triangles)
-        const float tnx = __fmaf_rn(wbyte(wsel ? nx1 : nx0, kk), Bnx, Anx);
-        const float tny = __fmaf_rn(wbyte(wsel ? ny1 : ny0, kk), Bny, Any);
-        const float tnz = __fmaf_rn(wbyte(wsel ? nz1 : nz0, kk), Bnz, Anz);
-        const float tfx = __fmaf_rn(wbyte(wsel ? fx1 : fx0, kk), Bfx, Afx);
-        const float tfy = __fmaf_rn(wbyte(wsel ? fy1 : fy0, kk), Bfy, Afy);
-        const float tfz = __fmaf_rn(wbyte(wsel ? fz1 : fz0, kk), Bfz, Afz);
-        const float tmin = fmaxf(max3f(tnx, tny, tnz), 0.0f);
-        const float tm = fminf(min3f(tfx, tfy, tfz), tcur);
-        const bool hit = tmin < tm;
-        // slot k is visited at rank k ^ octant: children were placed by direction
-        mask |= (hit ? 1u : 0u) << (k ^ st.oct);
-        // the nearest hit slot goes first (non-negative floats order like their bits)
-        nearest = min(nearest, hit ? ((__float_as_uint(tmin) & ~7u) | (k ^ st.oct)) : 0xFFFFFFFFu);
+    for (uint32_t kk = 0; kk < 4u; ++kk) {
+        float a[2], c[2];
+        unpack2f(fma2(sub2(qbytes2(nz0, nz1, kk), magic), pack2f(Bnz, Bnz), pack2f(Anz, Anz)), a[0], a[1]);
+        unpack2f(fma2(sub2(qbytes2(fz0, fz1, kk), magic), pack2f(Bfz, Bfz), pack2f(Afz, Afz)), c[0], c[1]);
+#pragma unroll
+        for (uint32_t h2 = 0; h2 < 2u; ++h2) {
+            // empty slots carry the inverted box qlo = 255, qhi = 0 and fail this test
+            // by themselves (if rounding ever lets one through, it is a leaf of 0 triangles)
+            const uint32_t k = kk + 4u * h2;
+            const float tmin = max3f(tn[k], a[h2], 0.0f);
+            const float tm = min3f(tf[k], c[h2], tcur);
+            const bool hit = tmin < tm;
+            // slot k is visited at rank k ^ octant: children were placed by direction
+            mask |= (hit ? 1u : 0u) << (k ^ st.oct);
+            // the nearest hit slot goes first (non-negative floats order like their bits)
+            nearest = min(nearest, hit ? ((__float_as_uint(tmin) & ~7u) | (k ^ st.oct)) : 0xFFFFFFFFu);
+        }
     }
     first = nearest & 7u;
     return mask;
@@ -309,16 +354,17 @@ __device__ __forceinline__ void wide_step_warp(const SceneView& s, TravState& st
     }
 }
 
-// Whether an 8-wide walk that found no hit may report the miss. The slab
+// Whether the 8-wide walk's answer for this ray may stand at all. The slab
 // argument above needs finite plane distances that contain the reference's: a
 // zero direction component is replaced by +-2^-80, which turns the reference's
 // unbounded slab (origin strictly inside, 1/0 = inf) into a finite one that
 // can end short of a hit when the origin lies within about 2^-80 tmax of the
-// plane, and a component below 2^-126 overflows 1/d. So the miss is final only
-// when every component is at least 2^-60 in magnitude and the origin within
-// 2^60 (with scene coordinates below 2^60 every plane distance is then finite);
-// other rays that found nothing are traced again by the binary walk.
-__device__ __forceinline__ bool wide_miss_final(const Ray& r) {
+// plane, and a component below 2^-126 overflows 1/d. Such a narrower slab can
+// lose the nearest hit as well as every hit, so the walk's answer, a hit or a
+// miss, counts only when every component is at least 2^-60 in magnitude and the
+// origin within 2^60 (with scene coordinates below 2^60 every plane distance is
+// then finite); other rays are traced again by the binary walk.
+__device__ __forceinline__ bool wide_trusted(const Ray& r) {
     constexpr float dlo = 8.673617379884035e-19f, ohi = 1.152921504606847e18f;   // 2^-60, 2^60
     return fabsf(r.dx) >= dlo && fabsf(r.dy) >= dlo && fabsf(r.dz) >= dlo &&      // false for NaN too
            fabsf(r.ox) <= ohi && fabsf(r.oy) <= ohi && fabsf(r.oz) <= ohi;
@@ -328,14 +374,15 @@ __device__ __forceinline__ bool wide_miss_final(const Ray& r) {
 // closest t - 1e-5) when tests (a) and (b) above hold and returns true;
 // otherwise returns false and the caller has the ray traced by the binary walk.
 __device__ __forceinline__ bool wide_finish(const SceneView& s, TravState& st) {
-    // no hit below tmax anywhere: the binary walk finds none either -- for rays whose
-    // box test stays finite and conservative (see wide_miss_final)
-    if (!st.hit) return wide_miss_final(st.r);
+    // the box test is conservative only for trusted rays (see wide_trusted): for
+    // them, no hit below tmax anywhere means the binary walk finds none either
+    const bool trusted = wide_trusted(st.r);
+    if (!st.hit) return trusted;
     const uint4 lo = __ldg(s.wtri_leaf + 2u * st.nid), hi = __ldg(s.wtri_leaf + 2u * st.nid + 1u);
     bool same = hi.w == 1u;     // a single-leaf tree is intersected without a box test
-    // a zero direction component makes the reference divide by zero, and an empty
-    // E proves nothing: binary walk
-    if (hi.w == 0u && st.r.dx != 0.0f && st.r.dy != 0.0f && st.r.dz != 0.0f) {
+    // an untrusted ray may have lost a nearer hit, and an empty E proves nothing:
+    // binary walk (trusted rays have no zero direction component)
+    if (hi.w == 0u && trusted) {
         const float lx = __uint_as_float(lo.x), ly = __uint_as_float(lo.y), lz = __uint_as_float(lo.z);
         const float hx = __uint_as_float(hi.x), hy = __uint_as_float(hi.y), hz = __uint_as_float(hi.z);
         // Fast proof first: with inv = RN(1/d) (d != 0 here), RN((p - o) * inv) is

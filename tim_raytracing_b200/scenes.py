@@ -378,3 +378,44 @@ def sh9_basis(dirs: np.ndarray) -> np.ndarray:
     w[:, 7] = np.float32(0.315392) * (np.float32(3.0) * z * z - np.float32(1.0))
     w[:, 8] = np.float32(0.546274) * (x * x - y * y)
     return w
+
+
+def probe_coords(index, res):
+    """Probe indices -> (x, y, z) grid coordinates in the 4x4x4-tiled order of
+    getLightProbCoord (lightprobHelpers.glsl:33-61); vectorised over numpy arrays."""
+    index = np.asarray(index, np.int64)
+    trx, try_ = res[0] // 4, res[1] // 4
+    tile, inn = index // 64, index % 64
+    z = tile // (trx * try_)
+    tile = tile % (trx * try_)
+    y, x = tile // trx, tile % trx
+    return x * 4 + inn % 4, y * 4 + (inn // 4) % 4, z * 4 + (inn // 16) % 4
+
+
+def probe_positions(aabb_min, aabb_max, res, index) -> np.ndarray:
+    """Probe positions, getLightProbPosition (lightprobHelpers.glsl:63-69) in FP32
+    with the shader's operation order: min + (max - min) / res * (coord + 0.5)."""
+    x, y, z = probe_coords(index, res)
+    out = np.empty((len(np.atleast_1d(index)), 3), np.float32)
+    for a, c in enumerate((x, y, z)):
+        lo, hi = np.float32(aabb_min[a]), np.float32(aabb_max[a])
+        step = (hi - lo) / np.float32(res[a])
+        out[:, a] = lo + step * (c.astype(np.float32) + np.float32(0.5))
+    return out
+
+
+def sh9_from_images16(sh16, res, probes) -> np.ndarray:
+    """The SH9 of `probes` (FP32 [n, 27], coefficient-major: j * 3 + channel) as
+    fetchSH9 reads it from the 7 RGBA16F images (lightprob/fetchSH_inline.glsl:6-31,
+    layout of storeSH9, storeSH_inline.glsl:6-18)."""
+    rx, ry, rz = res
+    img = np.asarray(sh16, np.uint16).view(np.float16).astype(np.float32).reshape(7, rz, ry, rx, 4)
+    x, y, z = probe_coords(np.asarray(probes), res)
+    out = np.zeros((len(x), 27), np.float32)
+    out[:, 0:3] = img[0, z, y, x, 0:3]
+    for j in range(1, 9):
+        for ch in range(3):
+            image = 1 + 2 * ch if j <= 4 else 2 + 2 * ch
+            comp = j - 1 if j <= 4 else j - 5
+            out[:, 3 * j + ch] = img[image, z, y, x, comp]
+    return out
