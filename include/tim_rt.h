@@ -88,6 +88,11 @@ typedef struct { float o[3]; float tmax; float d[3]; uint32_t flags; } tim_rt_ra
 #define TIM_RT_MODE_PER_RAY 2u   /* ray.flags bit 0 selects any-hit */
 #define TIM_RT_TRACE_WIDE 0x100u /* trace the 8-wide quantised BVH (needs TIM_RT_UPLOAD_QUANT8) */
 #define TIM_RT_TRACE_COUNT 0x400u /* run the counting kernel variant and fill the work counters of tim_rt_stats */
+#define TIM_RT_TRACE_TLAS 0x800u  /* with TIM_RT_MODE_ANY: the two-level walk of USE_TRAVERSE_TLAS scenes
+                                     (traverseTlasFast + tlas_collide_fast, bvhCollision.glsl:321-348) over an
+                                     image from tim_rt_build_bvh_tlas; binary form only. The reference's
+                                     closest-hit two-level walk does not compile (HitBox and Hit exist only
+                                     commented out, collision.glsl:175-195): TIM_RT_EUNSUPPORTED */
 
 /* Upload flags. */
 #define TIM_RT_UPLOAD_QUANT8 0x2u /* also build the 8-wide BVH with 8-bit quantised child bounds */
@@ -576,6 +581,23 @@ int tim_rt_build_bvh(const float *pos, uint32_t num_vertex, const uint32_t *tri_
 int tim_rt_build_bvh_gpu(tim_rt_ctx *ctx, const float *pos, uint32_t num_vertex, const uint32_t *tri_records,
                          uint32_t num_tris, const void *materials, uint32_t num_materials, const void *lights,
                          uint32_t num_lights, const tim_rt_build_params *params, tim_rt_bvh_blob **out);
+/* A two-level image for the reference's TLAS/BLAS traversal (USE_TRAVERSE_TLAS,
+ * src/Shaders/bvh/bvhCollision.glsl:286-349), in the layout fillGpuBuffer gives a
+ * top-level builder holding BLAS instances (src/Renderer/BVHBuilder.cpp:1441-1457,
+ * 1521-1533; BVHBuilder::addBlas, :292-301): instance i is the BLAS over
+ * triangles [inst_first[i], inst_first[i] + inst_count[i]) of tri_records (at
+ * least 2; it is built with tim_rt_build_bvh, its root an inner node), the top
+ * level a binned-SAH tree over the instance boxes with at most tlas_max_leaf
+ * (1..255) instances per leaf; lights go into the top-level leaves' lists. The
+ * reference's own builder cannot write this image: with its inlined triangles
+ * (INLINE_TRIANGLES, BVHBuilder.cpp:13) fillGpuBuffer copies the BLAS leaves'
+ * triangles out of the top-level builder's own, empty, triangle array
+ * (BVHBuilder.cpp:1490-1495, under a TIM_ASSERT(!m_isTlas) that release builds
+ * drop). Trace it with TIM_RT_TRACE_TLAS. */
+int tim_rt_build_bvh_tlas(const float *pos, uint32_t num_vertex, const uint32_t *tri_records, uint32_t num_tris,
+                          const uint32_t *inst_first, const uint32_t *inst_count, uint32_t num_instances,
+                          const void *materials, uint32_t num_materials, const void *lights, uint32_t num_lights,
+                          const tim_rt_build_params *params, uint32_t tlas_max_leaf, tim_rt_bvh_blob **out);
 int tim_rt_bvh_blob_info(const tim_rt_bvh_blob *blob, const uint8_t **bytes, uint64_t *size,
                          uint32_t ranges[7][2], tim_rt_push_constants *pc, float aabb[6]);
 void tim_rt_bvh_blob_free(tim_rt_bvh_blob *blob);

@@ -25,6 +25,9 @@ REFBUILD_SO = HERE / "_ref" / "libtimref_build.so"
 Image = namedtuple("Image", "data ranges pc aabb")   # same fields as tim_raytracing_b200.BvhImage
 
 
+# orc_trace modes (oracle/reftrace.h); ORC_MODE_TLAS is or'ed into the mode
+ORC_MODE_CLOSEST, ORC_MODE_ANY, ORC_MODE_PER_RAY, ORC_MODE_TLAS = 0, 1, 2, 4
+
 # Where this container keeps the reference's source tree (read-only). Only the
 # build recipe reads it; the GPU box has no such tree and uses the prebuilt _ref.
 REFERENCE_TREE = Path(os.environ.get("TIM_RT_REFERENCE_TREE", "/root/reference"))
@@ -124,14 +127,15 @@ def refbuild_lib():
     return _ref
 
 
-def ref_build(scene, multithread: bool = False, **params) -> Image:
-    """Runs the reference's own BVHBuilder (single-threaded by default: its threaded
-    build numbers nodes in thread order, BVHBuilder.cpp:851-857,880-894)."""
-    L = refbuild_lib()
+def _ref_params(L, params):
     p = RefParams()
     L.timref_default_params(ctypes.byref(p))
     for k, v in params.items():
         setattr(p, k, v)
+    return p
+
+
+def _ref_call(L, scene, build):
     pos = np.ascontiguousarray(scene.positions, np.float32)
     nrm = np.ascontiguousarray(scene.normals, np.float32)
     chunks = np.ascontiguousarray(scene.chunks, np.uint32)
@@ -139,11 +143,10 @@ def ref_build(scene, multithread: bool = False, **params) -> Image:
     colors = np.ascontiguousarray(scene.colors, np.float32)
     lights = np.ascontiguousarray(scene.lights, np.float32)
     res = RefResult()
-    rc = L.timref_build(pos.ctypes.data, nrm.ctypes.data, pos.shape[0], chunks.ctypes.data, chunks.shape[0],
-                        idx.ctypes.data, colors.ctypes.data, lights.ctypes.data if len(lights) else None, len(lights),
-                        ctypes.byref(p), 1 if multithread else 0, ctypes.byref(res))
+    rc = build(pos.ctypes.data, nrm.ctypes.data, pos.shape[0], chunks.ctypes.data, chunks.shape[0], idx.ctypes.data,
+               colors.ctypes.data, lights.ctypes.data if len(lights) else None, len(lights), res)
     if rc != 0:
-        raise RuntimeError("timref_build failed")
+        raise RuntimeError("the reference builder failed")
     try:
         data = np.frombuffer(ctypes.string_at(res.blob, res.blob_size), np.uint8).copy()
         ranges = np.array([[res.ranges[i][0], res.ranges[i][1]] for i in range(7)], np.uint32)
@@ -154,6 +157,15 @@ def ref_build(scene, multithread: bool = False, **params) -> Image:
     finally:
         L.timref_free(ctypes.byref(res))
     return Image(data, ranges, pc, aabb)
+
+
+def ref_build(scene, multithread: bool = False, **params) -> Image:
+    """Runs the reference's own BVHBuilder (single-threaded by default: its threaded
+    build numbers nodes in thread order, BVHBuilder.cpp:851-857,880-894)."""
+    L = refbuild_lib()
+    p = _ref_params(L, params)
+    return _ref_call(L, scene, lambda *a: L.timref_build(*a[:9], ctypes.byref(p), 1 if multithread else 0,
+                                                         ctypes.byref(a[9])))
 
 
 class Scene:

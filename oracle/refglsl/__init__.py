@@ -39,8 +39,9 @@ def lib():
         L.refglsl_probe_light.argtypes = [vp, vp, vp, vp, vp]
         L.refglsl_probe_update.argtypes = [vp, vp, vp, vp]
         L.refglsl_shade.argtypes = [vp, vp, vp, vp, vp]
+        L.refglsl_trace_tlas.argtypes = [vp, vp, u64, vp]
         for f in (L.refglsl_trace, L.refglsl_camera, L.refglsl_probe_trace, L.refglsl_probe_light,
-                  L.refglsl_probe_update, L.refglsl_shade):
+                  L.refglsl_probe_update, L.refglsl_shade, L.refglsl_trace_tlas):
             f.restype = ctypes.c_int
         _lib = L
     return _lib
@@ -63,6 +64,16 @@ def trace(sc, rays: np.ndarray, mode: int = 0):
     nid = np.zeros(n, np.uint32)
     _check(lib().refglsl_trace(sc.ref, _ptr(rays), n, mode, _ptr(hit), _ptr(nid)), "trace")
     return hit, nid
+
+
+def trace_tlas(sc, rays: np.ndarray) -> np.ndarray:
+    """Any-hit rays through the USE_TRAVERSE_TLAS shader (traverseForShadow): hit
+    records [n,4] u32 = (occluded, 0, 0, bits(tmax)), as oracle.trace reports them."""
+    rays = np.ascontiguousarray(rays, np.float32)
+    n = rays.shape[0]
+    hit = np.zeros((n, 4), np.uint32)
+    _check(lib().refglsl_trace_tlas(sc.ref, _ptr(rays), n, _ptr(hit)), "trace_tlas")
+    return hit
 
 
 def camera(sc, pd: np.ndarray) -> np.ndarray:

@@ -24,6 +24,14 @@ The rewrites are mechanical and change no arithmetic or control flow:
      evalSphereLight when the light is out of range) returns a value-initialised
      (zero) result there; SPIR-V leaves that value undefined, and the restatement
      and the CUDA kernels use zero.
+  8. The body of bvh/bvhCollision.glsl's tlas_collide, the closest-hit half of the
+     two-level variant (USE_TRAVERSE_TLAS), becomes a call to
+     refglsl_unreachable() and a zero return: it names a ClosestHit member (nid)
+     and a type and function (Hit, HitBox) that the reference does not define
+     (HitBox and Hit exist only commented out, core/collision.glsl:175-195), so no
+     compiler accepts it. The any-hit half, tlas_collide_fast, is kept as is and
+     never calls it; a driver compiled with USE_TRAVERSE_TLAS defines
+     refglsl_unreachable to flag an error should it ever run.
 
 Usage: python make_refglsl.py --ref <reference>/src/Shaders --out <dir>/Shaders
 """
@@ -128,6 +136,32 @@ def _add_fallthrough_returns(src: str) -> str:
     return src
 
 
+# rewrite 8: functions whose bodies become a stub, per file
+STUBS = {"bvh/bvhCollision.glsl": {"tlas_collide": "{ refglsl_unreachable(); return 0u; }"}}
+
+
+def _stub_functions(src: str, stubs: dict) -> str:
+    mask = _code_mask(src)
+    for name, body in stubs.items():
+        m = re.search(rf"\b{name}\s*\([^()]*\)\s*\{{", src)
+        if not m or not mask[m.start()]:
+            raise SystemExit(f"make_refglsl: function {name} not found")
+        start = m.end() - 1
+        depth = 0
+        for i in range(start, len(src)):
+            if not mask[i]:
+                continue
+            if src[i] == "{":
+                depth += 1
+            elif src[i] == "}":
+                depth -= 1
+                if depth == 0:
+                    src = src[:start] + body + _lines(src[start:i + 1]) + src[i + 1:]
+                    break
+        mask = _code_mask(src)
+    return src
+
+
 def transform(src: str) -> str:
     src = re.sub(r"^[ \t]*#[ \t]*(version|extension)\b[^\n]*", "", src, flags=re.M)
     src = src.replace("__cplusplus", "TIM_REFGLSL_GLSL_ONLY_GUARD")
@@ -153,6 +187,9 @@ def main() -> None:
         dst = out / p.relative_to(ref)
         dst.parent.mkdir(parents=True, exist_ok=True)
         text = transform(p.read_text(encoding="utf-8", errors="replace"))
+        rel = p.relative_to(ref).as_posix()
+        if rel in STUBS:
+            text = _stub_functions(text, STUBS[rel])
         if not dst.exists() or dst.read_text() != text:
             dst.write_text(text)
         n += 1

@@ -299,6 +299,84 @@ static int traverse_any(const orc_scene *s, const ray_t *r, float tmax, orc_stat
     }
 }
 
+/* The two-level any-hit walk of USE_TRAVERSE_TLAS scenes:
+ * bvhTraversal_inline.glsl:83-151 compiled as traverseTlasFast (the same walk over
+ * the top-level nodes from the scene root) whose leaves call tlas_collide_fast
+ * (bvhCollision.glsl:321-348): only the leaf's BLAS instances are tested (its
+ * triangle records are skipped, and instances the builder lifted into inner
+ * nodes' lists are never looked at), each with CollideBox(..., tmax) > 0 -- so an
+ * origin inside the instance box (tmin = 0) skips it -- and on a pass the
+ * one-level any-hit walk traverseBvhFast from the instance's rootIndex (a node
+ * id without the leaf bit). */
+static int walk_any_from(const orc_scene *s, uint32_t root, const ray_t *r, float tmax, int tlas, orc_stats *st);
+
+static int tlas_collide_fast(const orc_scene *s, uint32_t nid, const ray_t *r, float tmax, orc_stats *st) {
+    nid &= NID_MASK;
+    uint32_t off = node_at(s, nid)->nid[3];
+    if (off == 0xFFFFFFFFu) return 0;
+    uint32_t hdr = leaf_header(s, off);
+    uint32_t ntri = hdr & ((1u << TRIANGLE_BITS) - 1u);
+    uint32_t nblas = (hdr >> TRIANGLE_BITS) & ((1u << BLAS_BITS) - 1u);
+    st->leaf_visit++;
+    const uint32_t *ld = leaf_data(s);
+    for (uint32_t i = 0; i < nblas; ++i) {
+        uint32_t bi = ld[1u + off + ntri * 3u + i];
+        const blas_header *bh = blas_at(s, bi);
+        box_t b; b.mn = ld3(bh->mn); b.mx = ld3(bh->mx);
+        if (collide_box(r, b, tmax) > 0.0f) {
+            if (bh->rootIndex >= s->num_nodes) continue;   /* not produced by the reference builder */
+            if (walk_any_from(s, bh->rootIndex, r, tmax, 0, st)) return 1;
+        }
+    }
+    return 0;
+}
+
+/* traverseBvhFast / traverseTlasFast from `root` (bvhTraversal_inline.glsl:83-151). */
+static int walk_any_from(const orc_scene *s, uint32_t root, const ray_t *r, float tmax, int tlas, orc_stats *st) {
+    uint32_t nodeId = root;
+    uint32_t bitstack = 0, parentId = 0, siblingId = 0;
+    for (;;) {
+        while (!(nodeId & NID_LEAF_BIT)) {
+            const packed_node *n = node_at(s, nodeId);
+            st->node_fetch++;
+            uint32_t packed = n->nid[2];
+            uint32_t c0 = packed & NID_MASK, c1 = c0 + 1u;
+            c0 |= (packed & NID_LEFT_LEAF_BIT) ? NID_LEAF_BIT : 0u;
+            c1 |= (packed & NID_RIGHT_LEAF_BIT) ? NID_LEAF_BIT : 0u;
+            box_t b0, b1;
+            node_boxes(n, &b0, &b1);
+            float d0 = collide_box(r, b0, tmax);
+            float d1 = collide_box(r, b1, tmax);
+            if (d0 < 0.0f && d1 < 0.0f) break;
+            bitstack <<= 1;
+            if (d0 >= 0.0f && d1 >= 0.0f) {
+                nodeId = (d1 < d0) ? c1 : c0;
+                bitstack |= 1u;
+            } else {
+                nodeId = (d0 >= 0.0f) ? c0 : c1;
+            }
+        }
+        if (nodeId & NID_LEAF_BIT) {
+            if (tlas ? tlas_collide_fast(s, nodeId, r, tmax, st) : bvh_collide_fast(s, nodeId, r, tmax, st)) return 1;
+        }
+        {
+            const packed_node *n = node_at(s, nodeId & NID_MASK);
+            st->backtrack_reload++;
+            parentId = n->nid[0]; siblingId = n->nid[1];
+        }
+        while ((bitstack & 1u) == 0u) {
+            if (bitstack == 0u) return 0;
+            nodeId = parentId;
+            const packed_node *n = node_at(s, nodeId & NID_MASK);
+            st->backtrack_reload++;
+            parentId = n->nid[0]; siblingId = n->nid[1];
+            bitstack >>= 1;
+        }
+        nodeId = siblingId;
+        bitstack ^= 1u;
+    }
+}
+
 /* baseRaytracingPass.glsl:16-27 rayTrace, with the ray's own tmax as the start t
  * (the reference always starts at TMAX = 100). */
 static inline void ray_trace(const orc_scene *s, const ray_t *r, float tmax, closest_t *c, orc_stats *st) {
@@ -319,14 +397,16 @@ void orc_trace(const orc_scene *s, const orc_ray *rays, uint64_t n, uint32_t mod
     int nt = nthreads(threads);
     (void)nt;
     int64_t nn = (int64_t)n;
+    const int tlas = (mode & ORC_MODE_TLAS) != 0u;
+    const uint32_t m = mode & ~ORC_MODE_TLAS;
 #pragma omp parallel for schedule(dynamic, 256) num_threads(nt)
     for (int64_t i = 0; i < nn; ++i) {
         const orc_ray *rr = rays + i;
         ray_t r; r.from = ld3(rr->o); r.dir = ld3(rr->d);
         orc_stats st = {0, 0, 0, 0};
-        int any = (mode == ORC_MODE_ANY) || (mode == ORC_MODE_PER_RAY && (rr->flags & 1u));
+        int any = (m == ORC_MODE_ANY) || (m == ORC_MODE_PER_RAY && (rr->flags & 1u));
         if (any) {
-            int occ = traverse_any(s, &r, rr->tmax, &st);
+            int occ = tlas ? walk_any_from(s, root_id(s), &r, rr->tmax, 1, &st) : traverse_any(s, &r, rr->tmax, &st);
             hit[4 * i + 0] = (uint32_t)occ; hit[4 * i + 1] = 0; hit[4 * i + 2] = 0; hit[4 * i + 3] = fbits(rr->tmax);
             if (nid) nid[i] = 0xFFFFFFFFu;
             if (bary) { bary[2 * i] = 0.f; bary[2 * i + 1] = 0.f; }

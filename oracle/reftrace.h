@@ -45,6 +45,9 @@ typedef struct { uint32_t node_fetch, backtrack_reload, leaf_visit, tri_test; } 
 #define ORC_MODE_CLOSEST 0u
 #define ORC_MODE_ANY 1u
 #define ORC_MODE_PER_RAY 2u
+/* or'ed into the mode: any-hit rays take the two-level walk of USE_TRAVERSE_TLAS
+ * scenes (traverseTlasFast); closest-hit rays keep the one-level walk */
+#define ORC_MODE_TLAS 4u
 
 int orc_version(void);
 

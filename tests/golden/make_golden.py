@@ -1,6 +1,6 @@
 """Generates the committed golden fixtures under tests/golden/.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [room|tlas|all]
 
 * room_refbvh.npz -- the reference's own BVHBuilder (compiled from the reference
   sources by oracle/Makefile, single-threaded so node numbering is stable) run
@@ -12,6 +12,12 @@
   reference's own compute shaders compiled as C++ (oracle/refglsl, built by
   oracle/Makefile from the reference tree); the tests check the two against each
   other and the CUDA kernels against them.
+* tlas_golden.npz -- a two-level scene (scenes.instanced_clusters(3, 12, 400):
+  12 BLAS instances) written by the product's tim_rt_build_bvh_tlas (the
+  reference's own builder cannot write a two-level image, see include/tim_rt.h),
+  8,000 any-hit rays aimed at the instances, and the occlusion results of the
+  reference's USE_TRAVERSE_TLAS shader compiled as C++ (glsl_hit) and of the C
+  restatement (hit).
 """
 from __future__ import annotations
 
@@ -44,8 +50,29 @@ def room_rays(seed=7, n=4096):
     return r
 
 
+def tlas_fixture():
+    from tim_raytracing_b200 import _native as N
+    s = scenes.instanced_clusters(3, 12, 400)
+    img = N.build_bvh_tlas(s)
+    sc = O.Scene(img, s.positions, s.normals)
+    rays = scenes.occlusion_rays(5, 8000, targets=s.meta["centres"])
+    hit, _, _, _ = O.trace(sc, rays, 1 | 4)
+    out = dict(data=img.data, ranges=img.ranges, pc=np.array(img.pc, np.uint32), aabb=img.aabb, rays=rays, hit=hit)
+    from oracle import refglsl
+    if not refglsl.available():
+        raise SystemExit("tlas_golden.npz needs oracle/_ref/librefglsl.so (make -C oracle REF=<reference tree>)")
+    out["glsl_hit"] = refglsl.trace_tlas(refglsl.Scene(img, s.positions, s.normals), rays)
+    np.savez_compressed(HERE / "tlas_golden.npz", **out)
+    print("wrote", HERE / "tlas_golden.npz", "occluded:", float(hit[:, 0].mean()))
+
+
 def main():
+    what = sys.argv[1] if len(sys.argv) > 1 else "all"
     O.build()
+    if what in ("tlas", "all"):
+        tlas_fixture()
+    if what == "tlas":
+        return
     s = scenes.room_scene(1)
     img = O.ref_build(s, multithread=False)
     np.savez_compressed(HERE / "room_refbvh.npz", data=img.data, ranges=img.ranges, pc=np.array(img.pc, np.uint32),

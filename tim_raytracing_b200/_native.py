@@ -18,6 +18,7 @@ OK, EINVAL, ENOMEM, ETIMEOUT, EDEVICE, ENOTFOUND, EUNSUPPORTED, ECANCELLED, EBUS
 MODE_CLOSEST, MODE_ANY, MODE_PER_RAY = 0, 1, 2
 TRACE_WIDE = 0x100
 TRACE_COUNT = 0x400
+TRACE_TLAS = 0x800
 UPLOAD_QUANT8 = 0x2
 CAM_PROB_MASK, CAM_TILE_LIGHTS, CAM_BOUNCE, CAM_WIDE, CAM_COUNT = 1, 2, 4, 0x100, 0x200
 CAM_PRIMARY_BINARY = 0x400
@@ -36,7 +37,7 @@ EXPORTED = [
     "tim_rt_server_destroy", "tim_rt_verify_hits", "tim_rt_server_submit_probes", "tim_rt_bvh_file_write",
     "tim_rt_bvh_file_read", "tim_rt_bvh_file_info", "tim_rt_bvh_file_free", "tim_rt_upload_bvh_file",
     "tim_rt_shade_camera", "tim_rt_shade_camera_dev", "tim_rt_build_bvh_gpu", "tim_rt_probe_directions",
-    "tim_rt_wide_check", "tim_rt_trace_camera_rows_dev", "tim_rt_server_cancel",
+    "tim_rt_wide_check", "tim_rt_trace_camera_rows_dev", "tim_rt_server_cancel", "tim_rt_build_bvh_tlas",
 ]
 SORT_NONE, SORT_OCTANT, SORT_MORTON = 0, 1, 2
 BATCH_WIDE = 0x100
@@ -169,6 +170,8 @@ def lib() -> ctypes.CDLL:
     L.tim_rt_build_params_default.argtypes = [ctypes.POINTER(BuildParams)]
     L.tim_rt_build_params_default.restype = None
     L.tim_rt_build_bvh.argtypes = [vp, u32, vp, u32, vp, u32, vp, u32, ctypes.POINTER(BuildParams), ctypes.POINTER(vp)]
+    L.tim_rt_build_bvh_tlas.argtypes = [vp, u32, vp, u32, vp, vp, u32, vp, u32, vp, u32, ctypes.POINTER(BuildParams), u32,
+                                        ctypes.POINTER(vp)]
     L.tim_rt_bvh_blob_info.argtypes = [vp, ctypes.POINTER(vp), ctypes.POINTER(u64), vp, ctypes.POINTER(PushConstants), vp]
     L.tim_rt_bvh_blob_free.argtypes = [vp]
     L.tim_rt_bvh_blob_free.restype = None
@@ -359,6 +362,30 @@ def build_bvh(scene, ctx: "Context" = None, **params) -> BvhImage:
     else:
         _check(L.tim_rt_build_bvh(pos.ctypes.data, pos.shape[0], rec.ctypes.data, rec.shape[0], mats, nmat,
                                   lights if nl else None, nl, ctypes.byref(p), ctypes.byref(out)))
+    return _take_blob(L, out)
+
+
+def build_bvh_tlas(scene, tlas_max_leaf: int = 2, **params) -> BvhImage:
+    """tim_rt_build_bvh_tlas over a scenes.Scene: one BLAS instance per chunk, a
+    top level over the instances (trace with MODE_ANY | TRACE_TLAS)."""
+    L = lib()
+    pos = np.ascontiguousarray(scene.positions, np.float32)
+    rec = np.ascontiguousarray(scene.tri_records())
+    first = np.ascontiguousarray(scene.chunks[:, 2], np.uint32)
+    count = np.ascontiguousarray(scene.chunks[:, 3], np.uint32)
+    mats = scene.materials_bytes()
+    lights = scene.packed_lights_bytes()
+    nl = len(lights) // 56
+    p = build_params(**params)
+    out = ctypes.c_void_p()
+    _check(L.tim_rt_build_bvh_tlas(pos.ctypes.data, pos.shape[0], rec.ctypes.data, rec.shape[0], first.ctypes.data,
+                                   count.ctypes.data, len(first), mats, len(mats) // 48, lights if nl else None, nl,
+                                   ctypes.byref(p), tlas_max_leaf, ctypes.byref(out)))
+    return _take_blob(L, out)
+
+
+def _take_blob(L, out) -> BvhImage:
+    """Copies a tim_rt_bvh_blob into a BvhImage and frees it."""
     try:
         bp, size = ctypes.c_void_p(), ctypes.c_uint64()
         ranges = np.zeros((7, 2), np.uint32)

@@ -339,6 +339,16 @@ int tim_rt_upload_bvh(tim_rt_ctx* c, const void* bvh_bytes, uint64_t n_bytes, co
     std::memcpy(s->ranges, ranges, sizeof(s->ranges));
     s->pc = *pc;
     s->depth = depth;
+    {   // whether a two-level walk may enter every BLAS root (validated: the header range holds numBlas records)
+        const uint32_t* bh = reinterpret_cast<const uint32_t*>(blob + ranges[TIM_RT_RANGE_BLAS][0]);
+        const uint32_t* nd = reinterpret_cast<const uint32_t*>(blob + ranges[TIM_RT_RANGE_NODE][0]);
+        bool ok = true;
+        for (uint32_t i = 0; i < pc->numBlas && ok; ++i) {
+            const uint32_t root = bh[8ull * i + 7];
+            ok = root < pc->numNodes && (nd[16ull * root + 2] & 0x3FFFFFFFu) != 0x3FFFFFFFu;
+        }
+        s->blas_roots_ok = ok;
+    }
     for (int a = 0; a < 3; ++a) {
         float lo = pos[a], hi = pos[a];
         for (uint32_t i = 1; i < num_vertex; ++i) {
@@ -475,16 +485,39 @@ int tim_rt_scene_bytes(tim_rt_ctx* c, tim_rt_scene_id id, uint64_t* bytes) {
     return TIM_RT_OK;
 }
 
+}  // extern "C"
+namespace {
+// TIM_RT_TRACE_TLAS: any-hit rays only (the reference's closest-hit two-level walk
+// does not compile), the binary form, and an image whose BLAS roots are inner nodes.
+int tlas_check(const Scene* s, uint32_t mode, const char* who) {
+    if (!(mode & TIM_RT_TRACE_TLAS)) return TIM_RT_OK;
+    if ((mode & 0xFFu) != TIM_RT_MODE_ANY || (mode & TIM_RT_TRACE_WIDE)) {
+        set_error(std::string(who) + ": TIM_RT_TRACE_TLAS traces any-hit rays (TIM_RT_MODE_ANY) in the binary form only");
+        return TIM_RT_EUNSUPPORTED;
+    }
+    if (!s->blas_roots_ok) {
+        set_error(std::string(who) + ": TIM_RT_TRACE_TLAS needs every BLAS rootIndex to name an inner node of the image");
+        return TIM_RT_EINVAL;
+    }
+    return TIM_RT_OK;
+}
+
+}  // namespace
+extern "C" {
+
 int tim_rt_trace_dev(tim_rt_ctx* c, tim_rt_scene_id id, const tim_rt_ray* d_rays, uint32_t n, uint32_t mode,
                      uint32_t* d_hit, uint32_t* d_nid, float* d_bary, void* cuda_stream) {
     int rc = check_ctx(c);
     if (rc) return rc;
     Scene* s = find_scene(c, id);
     if (!s) return TIM_RT_ENOTFOUND;
-    if ((mode & 0xFFu) > TIM_RT_MODE_PER_RAY || (mode & ~(0xFFu | TIM_RT_TRACE_WIDE | TIM_RT_TRACE_COUNT)) || n > 0x7FFFFFFFu || (n && (!d_rays || !d_hit))) {
+    if ((mode & 0xFFu) > TIM_RT_MODE_PER_RAY ||
+        (mode & ~(0xFFu | TIM_RT_TRACE_WIDE | TIM_RT_TRACE_COUNT | TIM_RT_TRACE_TLAS)) || n > 0x7FFFFFFFu ||
+        (n && (!d_rays || !d_hit))) {
         set_error("tim_rt_trace_dev: bad mode, size or null buffer");
         return TIM_RT_EINVAL;
     }
+    if ((rc = tlas_check(s, mode, "tim_rt_trace_dev"))) return rc;
     if ((mode & TIM_RT_TRACE_WIDE) && !s->has_wide) {
         set_error("tim_rt_trace_dev: scene was uploaded without TIM_RT_UPLOAD_QUANT8");
         return TIM_RT_EUNSUPPORTED;
@@ -505,10 +538,13 @@ int tim_rt_trace(tim_rt_ctx* c, tim_rt_scene_id id, const tim_rt_ray* rays, uint
     if (rc) return rc;
     Scene* s = find_scene(c, id);
     if (!s) return TIM_RT_ENOTFOUND;
-    if ((mode & 0xFFu) > TIM_RT_MODE_PER_RAY || (mode & ~(0xFFu | TIM_RT_TRACE_WIDE | TIM_RT_TRACE_COUNT)) || n > 0x7FFFFFFFu || (n && (!rays || !hit))) {
+    if ((mode & 0xFFu) > TIM_RT_MODE_PER_RAY ||
+        (mode & ~(0xFFu | TIM_RT_TRACE_WIDE | TIM_RT_TRACE_COUNT | TIM_RT_TRACE_TLAS)) || n > 0x7FFFFFFFu ||
+        (n && (!rays || !hit))) {
         set_error("tim_rt_trace: bad mode, size or null buffer");
         return TIM_RT_EINVAL;
     }
+    if ((rc = tlas_check(s, mode, "tim_rt_trace"))) return rc;
     if ((mode & TIM_RT_TRACE_WIDE) && !s->has_wide) {
         set_error("tim_rt_trace: scene was uploaded without TIM_RT_UPLOAD_QUANT8");
         return TIM_RT_EUNSUPPORTED;

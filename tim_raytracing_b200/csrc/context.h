@@ -26,6 +26,7 @@ struct Scene {
     tim_rt_push_constants pc{};
     uint32_t depth = 0;
     bool has_wide = false;
+    bool blas_roots_ok = true;              // every BLAS rootIndex is an inner node (TIM_RT_TRACE_TLAS)
     uint64_t bytes = 0;
     float bounds[6] = {0, 0, 0, 1, 1, 1};   // vertex bounds (ray-sort key)
     std::atomic<uint32_t> batch_refs{0};    // live batches and pending server requests on this scene

@@ -41,6 +41,12 @@ __host__ __device__ __forceinline__ uint32_t tiled_work_items(uint32_t W, uint32
 
 // -------------------------------------------------------------------- policies
 
+// The leaf kind a policy's rays take (kLeafOne unless the policy says otherwise).
+template <class P, class = void>
+struct leaf_kind { static constexpr int value = kLeafOne; };
+template <class P>
+struct leaf_kind<P, decltype((void)P::kLeaf)> { static constexpr int value = P::kLeaf; };
+
 struct BatchPolicy {
     const tim_rt_ray* rays;
     uint4* hit;
@@ -70,6 +76,12 @@ struct BatchPolicy {
         }
     }
     __device__ __forceinline__ void skip(uint32_t) const {}
+};
+
+// Any-hit rays of a two-level scene (TIM_RT_TRACE_TLAS): traverseTlasFast
+// (bvhTraversal_inline.glsl:83-151 with TLAS_COLLIDE) from the scene root.
+struct TlasBatchPolicy : BatchPolicy {
+    static constexpr int kLeaf = kLeafTlasTop;
 };
 
 // cameraPass.comp:44-76 pinhole ray of invocation (gx, gy) (cameraPass.comp:50-54).
@@ -227,6 +239,7 @@ __global__ void __launch_bounds__(BLOCK, WIDE ? 896 / BLOCK : 1024 / BLOCK) k_pe
                         idx = my;
                         if (P.load(s, idx, st)) {
                             st.t0 = st.t;
+                            st.err = err;
                             if (WIDE) wide_init(s, st, stk);
                             else trav_init(st, root);
                             active = true;
@@ -244,7 +257,7 @@ __global__ void __launch_bounds__(BLOCK, WIDE ? 896 / BLOCK : 1024 / BLOCK) k_pe
         if (WIDE) {
             wide_step_warp<BLOCK>(s, st, active, stk, err, sdepth, phase_sw);   // all lanes: warp-synchronous step
         } else {
-            plain_step_warp<BLOCK>(s, st, active, stk, err, sdepth, phase_sw);
+            plain_step_warp<BLOCK, leaf_kind<Policy>::value>(s, st, active, stk, err, sdepth, phase_sw);
         }
         if (active && st.done) {
             active = false;
@@ -591,6 +604,11 @@ cudaError_t launch_trace_batch(const SceneView& s, const tim_rt_ray* rays, uint3
                                uint32_t* nid, float* bary, uint32_t* counter, uint32_t* err, cudaStream_t stream,
                                const LaunchConfig& cfg) {
     BatchPolicy P{rays, reinterpret_cast<uint4*>(hit), nid, reinterpret_cast<float2*>(bary), mode & 0xFFu};
+    if (mode & TIM_RT_TRACE_TLAS) {   // any-hit only, binary form only (checked by the callers)
+        TlasBatchPolicy T;
+        static_cast<BatchPolicy&>(T) = P;
+        return launch_persistent<false>(s, T, n, nullptr, counter, err, stream, cfg);
+    }
     if (cfg.wide) return launch_persistent<true>(s, P, n, nullptr, counter, err, stream, cfg);
     return launch_persistent<false>(s, P, n, nullptr, counter, err, stream, cfg);
 }

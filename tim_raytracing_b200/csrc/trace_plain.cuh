@@ -40,6 +40,7 @@ struct TravState {
     float t1;           // closest: the smallest hit t; any: t of the hit
     bool near2;         // closest: another hit t2 has RN(t2 - 1e-5) <= t1
     uint32_t leaf;      // pending leaf slot of the current wide node (8 = none)
+    uint32_t* err;      // two-level walk: the device error word (a nested walk's stack guard)
 };
 
 // Direction components for which the binary walk's filtered box test is exact
@@ -126,6 +127,17 @@ __device__ __forceinline__ void plain_children(const TravState& st, const float4
     }
 }
 
+// What a leaf visit tests. kLeafOne: the one-level scene walk (bvh_collide /
+// bvh_collide_fast: triangles, then for any-hit rays the leaf's BLAS boxes).
+// kLeafTlasTop: the top level of a two-level walk (USE_TRAVERSE_TLAS, any-hit
+// only): the leaf's BLAS instances (tlas_collide_fast). kLeafInBlas: a leaf of a
+// BLAS entered from the top level (bvh_collide_fast compiled with
+// USE_TRAVERSE_TLAS: triangles only).
+constexpr int kLeafOne = 0, kLeafTlasTop = 1, kLeafInBlas = 2;
+
+template <int LEAF>
+__device__ __forceinline__ void plain_leaf(const SceneView& s, TravState& st, uint32_t node);
+
 // Acceptance of one triangle hit (bvh_collide / bvh_collide_fast): any-hit rays
 // end, closest-hit rays keep it and shrink their t by 1e-5. Returns true when
 // the ray ends.
@@ -151,10 +163,21 @@ __device__ __forceinline__ bool plain_accept(TravState& st, float t, float u, fl
 // in .w; without it (the allocation-free entry point and the 8-wide kernels'
 // fallback walk) the record words and the vertex positions are gathered from the
 // reference's own buffers. Same triangles, same order, same arithmetic.
+// The top-level leaf of a two-level any-hit walk; defined below.
+static __device__ __noinline__ bool tlas_leaf_any(SceneView s, uint32_t nidm, Ray r, float tmax, uint32_t* err);
+
+template <int LEAF>
 __device__ __forceinline__ void plain_leaf(const SceneView& s, TravState& st, uint32_t node) {
     const uint32_t nidm = node & kNidMask;
     uint32_t hdr, off;
     st.c_leaf++;
+    if (LEAF == kLeafTlasTop) {
+        if (tlas_leaf_any(s, nidm, st.r, st.t, st.err)) {
+            st.hit = true;
+            st.done = true;
+        }
+        return;
+    }
     if (s.ptris) {
         const uint4 li = __ldg(s.pleaf + nidm);
         hdr = li.y;
@@ -190,7 +213,7 @@ __device__ __forceinline__ void plain_leaf(const SceneView& s, TravState& st, ui
             if (t > 0.0f && plain_accept(st, t, u, v, r0, r1, r2, nidm)) return;
         }
     }
-    if (st.any) {
+    if (LEAF == kLeafOne && st.any) {
         const uint32_t ntri = hdr & ((1u << kTriBits) - 1u);
         const uint32_t nblas = (hdr >> kTriBits) & ((1u << kBlasBits) - 1u);
         for (uint32_t i = 0; i < nblas; ++i) {
@@ -211,7 +234,7 @@ __device__ __forceinline__ void plain_leaf(const SceneView& s, TravState& st, ui
 
 // One traversal step: descend to the next leaf (or exhaust the stack), test it,
 // and pop the next pending subtree. Returns with st.done set when the ray ends.
-template <int BLOCK>
+template <int BLOCK, int LEAF = kLeafOne>
 __device__ __forceinline__ void plain_step(const SceneView& s, TravState& st, uint32_t* stk, uint32_t* err,
                                            int sdepth) {
     uint32_t node = st.node;
@@ -252,7 +275,7 @@ __device__ __forceinline__ void plain_step(const SceneView& s, TravState& st, ui
             node = h0 ? c0 : c1;
         }
     }
-    plain_leaf(s, st, node);
+    plain_leaf<LEAF>(s, st, node);
     if (st.done) return;
     if (st.sp == 0) {
         st.done = true;
@@ -308,7 +331,7 @@ __device__ __forceinline__ void plain_advance(const SceneView& s, TravState& st,
 // has finished, or until only `sw` lanes still need nodes while some lane stands
 // on a leaf; then the leaves are tested together and each lane pops its next
 // pending subtree. Same per-ray visit order as plain_step.
-template <int BLOCK>
+template <int BLOCK, int LEAF = kLeafOne>
 __device__ __forceinline__ void plain_step_warp(const SceneView& s, TravState& st, bool active, uint32_t* stk,
                                                 uint32_t* err, int sdepth, uint32_t sw) {
     for (;;) {
@@ -320,12 +343,54 @@ __device__ __forceinline__ void plain_step_warp(const SceneView& s, TravState& s
         if (need) plain_advance<BLOCK>(s, st, stk, err, sdepth);
     }
     if (active && !st.done && (st.node & kNidLeafBit)) {
-        plain_leaf(s, st, st.node);
+        plain_leaf<LEAF>(s, st, st.node);
         if (!st.done) {
             if (st.sp == 0) st.done = true;
             else st.node = stk[(--st.sp) * BLOCK];
         }
     }
+}
+
+// tlas_collide_fast (bvhCollision.glsl:321-348) at top-level leaf nidm: for
+// each BLAS instance of the leaf, in order, CollideBox(ray, instance box, tmax)
+// > 0 -- an origin inside the box gives tmin = 0 and skips the instance -- then
+// traverseBvhFast from the instance's rootIndex, entered as an inner node
+// (bvhTraversal_inline.glsl:83-151; the image check makes every rootIndex an
+// inner node). The leaf's triangle records are not tested. Not inlined, with its
+// own stack in local memory: the nested walk runs while the top-level walk's
+// shared-memory stack is in use.
+static __device__ __noinline__ bool tlas_leaf_any(SceneView s, uint32_t nidm, Ray r, float tmax, uint32_t* err) {
+    uint32_t hdr, off;
+    if (s.ptris) {
+        const uint4 li = __ldg(s.pleaf + nidm);
+        hdr = li.y;
+        off = li.z;
+    } else {
+        off = __ldg(reinterpret_cast<const uint32_t*>(s.nodes + 4u * nidm) + 3);
+        hdr = leaf_header(s, off);
+    }
+    if (off == 0xFFFFFFFFu) return false;
+    const uint32_t ntri = hdr & ((1u << kTriBits) - 1u);
+    const uint32_t nblas = (hdr >> kTriBits) & ((1u << kBlasBits) - 1u);
+    uint32_t stk[kStackSize];
+    for (uint32_t i = 0; i < nblas; ++i) {
+        const uint32_t bi = __ldg(s.leaf + off + 1u + 3u * ntri + i);
+        const float* bh = s.blas + 8u * bi;
+        const float mnx = __ldg(bh), mny = __ldg(bh + 1), mnz = __ldg(bh + 2);
+        const float mxx = __ldg(bh + 4), mxy = __ldg(bh + 5), mxz = __ldg(bh + 6);
+        if (!(collide_box(r, mnx, mny, mnz, mxx, mxy, mxz, tmax) > 0.0f)) continue;
+        TravState st;
+        st.r = r;
+        st.t = tmax;
+        st.any = true;
+        st.err = err;
+        trav_init(st, __float_as_uint(__ldg(bh + 7)));   // rootIndex, an inner node id
+        do {
+            plain_step<1, kLeafInBlas>(s, st, stk, err, kStackSize);
+        } while (!st.done);
+        if (st.hit) return true;
+    }
+    return false;
 }
 
 }  // namespace timrt

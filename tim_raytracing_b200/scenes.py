@@ -419,3 +419,51 @@ def sh9_from_images16(sh16, res, probes) -> np.ndarray:
             comp = j - 1 if j <= 4 else j - 5
             out[:, 3 * j + ch] = img[image, z, y, x, comp]
     return out
+
+
+def instanced_clusters(seed: int, n_clusters: int = 12, tris_per_cluster: int = 600) -> Scene:
+    """A two-level scene for the reference's TLAS/BLAS traversal: n_clusters
+    objects, each one chunk (one BLAS instance when built with
+    BVHBuilder::addBlas): random triangles (edges log-uniform in [0.1, 0.6])
+    in a box of side 1..2.5 placed uniformly in [0, 10]^3, so instances overlap
+    now and then; a point light at the centre."""
+    rng = np.random.default_rng(seed)
+    b = _Builder()
+    centres = []
+    for c in range(n_clusters):
+        side = rng.uniform(1.0, 2.5)
+        lo = rng.uniform(0.0, 10.0 - side, size=3)
+        centres.append(lo + 0.5 * side)
+        n = tris_per_cluster
+        p0 = lo + rng.uniform(0.0, side, size=(n, 3))
+        e = rng.normal(size=(n, 2, 3))
+        e /= np.linalg.norm(e, axis=2, keepdims=True)
+        e *= np.exp(rng.uniform(math.log(0.1), math.log(0.6), size=(n, 2, 1)))
+        P = np.stack([p0, p0 + e[:, 0], p0 + e[:, 1]], 1)
+        Nf = np.cross(e[:, 0], e[:, 1])
+        Nf /= np.maximum(np.linalg.norm(Nf, axis=1, keepdims=True), 1e-30)
+        b.add(P.reshape(-1, 3), np.repeat(Nf, 3, 0), np.arange(3 * n, dtype=np.uint32).reshape(-1, 3),
+              tuple(rng.uniform(0.2, 0.9, 3)))
+    return b.scene(f"clusters{n_clusters}", [(5.0, 5.0, 5.0, 20.0, 1.0, 1.0, 1.0, 0.1)], seed=seed,
+                   centres=np.array(centres, np.float32))
+
+
+def occlusion_rays(seed: int, n: int, extent: float = 10.0, targets=None) -> np.ndarray:
+    """Any-hit rays for the two-level scene: origins uniform in [0, extent]^3
+    (some inside instance boxes), tmax log-uniform in [0.1, 20], directions
+    uniform -- or, with `targets`, two rays in three aimed at a random target
+    point (an instance centre) with a little jitter; every ray flagged any-hit."""
+    rng = np.random.default_rng(seed)
+    o = rng.uniform(0.0, extent, size=(n, 3))
+    d = rng.normal(size=(n, 3))
+    if targets is not None:
+        aim = rng.uniform(size=n) < 2.0 / 3.0
+        t = np.asarray(targets, np.float64)[rng.integers(len(targets), size=n)]
+        d = np.where(aim[:, None], t - o + rng.normal(scale=0.3, size=(n, 3)), d)
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    r = np.zeros((n, 8), np.float32)
+    r[:, 0:3] = o
+    r[:, 3] = np.exp(rng.uniform(math.log(0.1), math.log(20.0), n))
+    r[:, 4:7] = d
+    r.view(np.uint32)[:, 7] = 1
+    return r
