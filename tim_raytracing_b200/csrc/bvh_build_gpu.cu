@@ -8,7 +8,15 @@
 //      a key range split at its highest differing bit, equal keys split by index;
 //   4. subtrees of at most max_leaf_size triangles become leaves;
 //   5. bottom-up boxes and internal-node counts (the second child to arrive at a
-//      node merges), then per node its depth and pre-order rank among internal
+//      node merges);
+//   5b. treelet restructuring (Karras & Aila 2013, "Fast Parallel Construction of
+//      High-Quality Bounding Volume Hierarchies"): bottom-up again, each internal
+//      node, once both its subtrees are final, takes the treelet of up to 7 nodes
+//      below it (opening the largest-area inner node each time) and rebuilds the
+//      treelet's topology from the surface-area cost of every subset of its leaves
+//      (exact dynamic programme over the 127 subsets); two passes, then the
+//      internal-node counts again. Leaves keep their Morton-order triangle runs;
+//   5c. per node its depth and pre-order rank among internal
 //      nodes by walking to the root, which gives the host builder's numbering:
 //      root 0, the children of the internal node of rank r at 2r+1 and 2r+2;
 //   6. leaf sizes, exclusive scan in node order, leaf data (header, triangle
@@ -216,17 +224,184 @@ __global__ void k_bottom_up(uint32_t n, uint32_t max_leaf, const uint32_t* left,
     }
 }
 
+// Per handle: bit 0 = in the final tree (the root, or a child of a node of more
+// than max_leaf triangles), bit 1 = a leaf of the final tree. Fixed before the
+// treelet passes, which change only which internal node has which children.
+constexpr uint32_t kInTree = 1u, kIsLeaf = 2u;
+__global__ void k_mark(uint32_t n, uint32_t max_leaf, const uint32_t* first, const uint32_t* last,
+                       const uint32_t* parent, uint32_t* flags) {
+    const uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
+    if (h >= 2u * n - 1u) return;
+    const bool in_tree = h == 0u || hsize(parent[h], n, first, last) > max_leaf;
+    flags[h] = in_tree ? (kInTree | (hsize(h, n, first, last) <= max_leaf ? kIsLeaf : 0u)) : 0u;
+}
+
+__device__ __forceinline__ float half_area(const Aabb& b) {
+    const float dx = b.hi[0] - b.lo[0], dy = b.hi[1] - b.lo[1], dz = b.hi[2] - b.lo[2];
+    return dx * dy + dy * dz + dz * dx;
+}
+__device__ __forceinline__ Aabb merge_box(const Aabb& a, const Aabb& b) {
+    Aabb m;
+    for (int k = 0; k < 3; ++k) { m.lo[k] = fminf(a.lo[k], b.lo[k]); m.hi[k] = fmaxf(a.hi[k], b.hi[k]); }
+    return m;
+}
+
+// Surface-area costs of the treelet programme: an internal node costs kCi per
+// unit area, a leaf kCt per triangle per unit area (the leaves themselves are
+// fixed, so only their subtree costs enter).
+constexpr float kCi = 1.2f, kCt = 1.0f;
+constexpr int kTreeletLeaves = 7, kSubsets = 1 << kTreeletLeaves;
+constexpr uint32_t kTreeletBlock = 32;   // the programme's tables live in shared memory, [subset][thread]
+
+// SAH cost of every final-tree node, bottom-up with arrival counters (leaves: kCt
+// * triangles * area; internal: kCi * area + the children's costs).
+__global__ void k_sah_cost(uint32_t n, const uint32_t* left, const uint32_t* right, const uint32_t* first,
+                           const uint32_t* last, const uint32_t* parent, const uint32_t* flags, const Aabb* box,
+                           float* cost, uint32_t* arrive) {
+    const uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
+    if (h >= 2u * n - 1u || h == 0u || (flags[h] & (kInTree | kIsLeaf)) != (kInTree | kIsLeaf)) return;
+    cost[h] = kCt * (float)hsize(h, n, first, last) * half_area(box[h]);
+    uint32_t cur = h;
+    while (cur != 0u) {
+        const uint32_t p = parent[cur];
+        __threadfence();
+        if (atomicAdd(arrive + p, 1u) == 0u) return;
+        __threadfence();
+        cost[p] = kCi * half_area(load_box_cg(box + p)) + __ldcg(cost + left[p]) + __ldcg(cost + right[p]);
+        cur = p;
+    }
+}
+
+// One treelet pass: from every final leaf up to the root; the second child to
+// arrive at a node restructures the treelet rooted there. Every node below it is
+// final by then (its subtree's threads have all passed), so the thread owns the
+// treelet; writes are fenced before the next arrival, reads of other threads'
+// writes bypass L1.
+__global__ void __launch_bounds__(kTreeletBlock) k_treelet(uint32_t n, uint32_t* left, uint32_t* right,
+                                                           uint32_t* parent, const uint32_t* flags, Aabb* box,
+                                                           float* cost, uint32_t* arrive) {
+    __shared__ float s_area[kSubsets * kTreeletBlock];
+    __shared__ float s_cost[kSubsets * kTreeletBlock];
+    __shared__ uint8_t s_part[kSubsets * kTreeletBlock];
+    const uint32_t t = threadIdx.x;
+    const uint32_t h = blockIdx.x * blockDim.x + t;
+    if (h >= 2u * n - 1u || h == 0u || (flags[h] & (kInTree | kIsLeaf)) != (kInTree | kIsLeaf)) return;
+    uint32_t cur = h;
+    while (cur != 0u) {
+        const uint32_t p = parent[cur];
+        __threadfence();
+        if (atomicAdd(arrive + p, 1u) == 0u) return;
+        __threadfence();
+        // the treelet below p: open the largest-area inner node until 7 leaves
+        uint32_t leaf[kTreeletLeaves], inner[kTreeletLeaves - 2];
+        Aabb lb[kTreeletLeaves];
+        int nl = 2, ni = 0;
+        leaf[0] = __ldcg(left + p);
+        leaf[1] = __ldcg(right + p);
+        lb[0] = load_box_cg(box + leaf[0]);
+        lb[1] = load_box_cg(box + leaf[1]);
+        while (nl < kTreeletLeaves) {
+            int best = -1;
+            float ba = -1.0f;
+            for (int i = 0; i < nl; ++i) {
+                if (flags[leaf[i]] & kIsLeaf) continue;
+                const float a = half_area(lb[i]);
+                if (a > ba) { ba = a; best = i; }
+            }
+            if (best < 0) break;
+            const uint32_t x = leaf[best];
+            inner[ni++] = x;
+            leaf[best] = __ldcg(left + x);
+            leaf[nl] = __ldcg(right + x);
+            lb[best] = load_box_cg(box + leaf[best]);
+            lb[nl] = load_box_cg(box + leaf[nl]);
+            ++nl;
+        }
+        if (nl >= 3) {
+            // areas and best partitions of every subset of the treelet's leaves
+            const uint32_t full = (1u << nl) - 1u;
+            for (uint32_t sub = 1; sub <= full; ++sub) {
+                Aabb u = lb[__ffs(sub) - 1];
+                for (uint32_t r = sub & (sub - 1u); r; r &= r - 1u) u = merge_box(u, lb[__ffs(r) - 1]);
+                s_area[sub * kTreeletBlock + t] = half_area(u);
+                if ((sub & (sub - 1u)) == 0u) s_cost[sub * kTreeletBlock + t] = __ldcg(cost + leaf[__ffs(sub) - 1]);
+            }
+            for (uint32_t sub = 1; sub <= full; ++sub) {
+                if ((sub & (sub - 1u)) == 0u) continue;
+                // subsets are visited in increasing order, so every proper subset is done;
+                // a partition (P, sub \ P) is taken once, with P holding sub's lowest leaf
+                const uint32_t low = sub & (0u - sub), rest = sub ^ low;
+                float best = INFINITY;
+                uint32_t bp = low;
+                for (uint32_t q = rest;; q = (q - 1u) & rest) {
+                    const uint32_t P = q | low;
+                    if (P != sub) {
+                        const float c = s_cost[P * kTreeletBlock + t] + s_cost[(sub ^ P) * kTreeletBlock + t];
+                        if (c < best) { best = c; bp = P; }
+                    }
+                    if (q == 0u) break;
+                }
+                s_cost[sub * kTreeletBlock + t] = kCi * s_area[sub * kTreeletBlock + t] + best;
+                s_part[sub * kTreeletBlock + t] = (uint8_t)bp;
+            }
+            // rebuild: p keeps its place; the other internal nodes are reused in order
+            uint32_t stk_node[kTreeletLeaves], stk_set[kTreeletLeaves];
+            int sp = 0, next = 0;
+            stk_node[sp] = p;
+            stk_set[sp++] = full;
+            while (sp > 0) {
+                --sp;
+                const uint32_t node = stk_node[sp], set = stk_set[sp];
+                const uint32_t P = s_part[set * kTreeletBlock + t], Q = set ^ P;
+                uint32_t kid[2];
+                const uint32_t sides[2] = {P, Q};
+                for (int k = 0; k < 2; ++k) {
+                    if ((sides[k] & (sides[k] - 1u)) == 0u) {
+                        kid[k] = leaf[__ffs(sides[k]) - 1];
+                    } else {
+                        kid[k] = inner[next++];
+                        stk_node[sp] = kid[k];
+                        stk_set[sp++] = sides[k];
+                    }
+                    parent[kid[k]] = node;
+                }
+                left[node] = kid[0];
+                right[node] = kid[1];
+                Aabb u = lb[__ffs(set) - 1];
+                for (uint32_t r = set & (set - 1u); r; r &= r - 1u) u = merge_box(u, lb[__ffs(r) - 1]);
+                box[node] = u;
+                cost[node] = s_cost[set * kTreeletBlock + t];
+            }
+        }
+        cur = p;
+    }
+}
+
+// Internal-node counts again after the treelet passes (leaves 0).
+__global__ void k_recount(uint32_t n, const uint32_t* left, const uint32_t* right, const uint32_t* parent,
+                          const uint32_t* flags, uint32_t* icount, uint32_t* arrive) {
+    const uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
+    if (h >= 2u * n - 1u || h == 0u || (flags[h] & (kInTree | kIsLeaf)) != (kInTree | kIsLeaf)) return;
+    icount[h] = 0u;
+    uint32_t cur = h;
+    while (cur != 0u) {
+        const uint32_t p = parent[cur];
+        __threadfence();
+        if (atomicAdd(arrive + p, 1u) == 0u) return;
+        __threadfence();
+        icount[p] = 1u + __ldcg(icount + left[p]) + __ldcg(icount + right[p]);
+        cur = p;
+    }
+}
+
 // Per node of the final tree: depth, and output id from the pre-order rank of
 // internal nodes (rank(child) = rank(parent) + 1, plus the left sibling's internal
 // count for a right child); the root is 0, the children of rank r are 2r+1, 2r+2.
-__global__ void k_number(uint32_t n, uint32_t max_leaf, const uint32_t* left, const uint32_t* first,
-                         const uint32_t* last, const uint32_t* parent, const uint32_t* icount, uint32_t* out_id,
-                         uint32_t* rank_of, uint32_t* max_depth) {
+__global__ void k_number(uint32_t n, const uint32_t* left, const uint32_t* parent, const uint32_t* flags,
+                         const uint32_t* icount, uint32_t* out_id, uint32_t* rank_of, uint32_t* max_depth) {
     const uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
     if (h >= 2u * n - 1u) return;
-    const uint32_t sz = hsize(h, n, first, last);
-    const bool in_tree = h == 0u || hsize(parent[h], n, first, last) > max_leaf;
-    if (!in_tree) return;
+    if (!(flags[h] & kInTree)) return;
     // rank of h (meaningful for internal nodes) and depth
     uint32_t rank = 0, depth = 0, cur = h;
     while (cur != 0u) {
@@ -236,7 +411,7 @@ __global__ void k_number(uint32_t n, uint32_t max_leaf, const uint32_t* left, co
         ++depth;
         cur = p;
     }
-    if (sz > max_leaf) rank_of[h] = rank;
+    if (!(flags[h] & kIsLeaf)) rank_of[h] = rank;
     atomicMax(max_depth, depth);
     if (h == 0u) {
         out_id[0] = 0u;
@@ -259,13 +434,13 @@ __device__ __forceinline__ float widen_hi(float x) { return x + (1e-6f + fabsf(x
 // Leaf sizes (header + 3 words per triangle + light ids), indexed by output id;
 // internal nodes 0. Light ids: sphere (centre, radius) vs the widened leaf box,
 // at most 15 (BVHBuilder.cpp:36-42,749-756 with the 4-bit count kept below 16).
-__global__ void k_leaf_sizes(uint32_t n, uint32_t max_leaf, const uint32_t* first, const uint32_t* last,
-                             const uint32_t* parent, const uint32_t* out_id, const Aabb* box, const float* lights,
-                             uint32_t num_lights, uint32_t* leaf_size, uint32_t* leaf_nl) {
+__global__ void k_leaf_sizes(uint32_t n, const uint32_t* first, const uint32_t* last, const uint32_t* flags,
+                             const uint32_t* out_id, const Aabb* box, const float* lights, uint32_t num_lights,
+                             uint32_t* leaf_size, uint32_t* leaf_nl) {
     const uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
     if (h >= 2u * n - 1u || h == 0u) return;
+    if ((flags[h] & (kInTree | kIsLeaf)) != (kInTree | kIsLeaf)) return;
     const uint32_t sz = hsize(h, n, first, last);
-    if (sz > max_leaf || hsize(parent[h], n, first, last) <= max_leaf) return;
     const Aabb b = box[h];
     float lo[3], hi[3];
     for (int a = 0; a < 3; ++a) { lo[a] = widen_lo(b.lo[a]); hi[a] = widen_hi(b.hi[a]); }
@@ -286,17 +461,16 @@ __global__ void k_leaf_sizes(uint32_t n, uint32_t max_leaf, const uint32_t* firs
 }
 
 // Node records (packNodeData, BVHBuilder.cpp:1283-1317) and leaf data.
-__global__ void k_emit(uint32_t n, uint32_t max_leaf, const uint32_t* left, const uint32_t* right,
-                       const uint32_t* first, const uint32_t* last, const uint32_t* parent, const uint32_t* out_id,
+__global__ void k_emit(uint32_t n, const uint32_t* left, const uint32_t* right, const uint32_t* first,
+                       const uint32_t* last, const uint32_t* parent, const uint32_t* flags, const uint32_t* out_id,
                        const Aabb* box, const uint32_t* order, const uint32_t* tri, const float* lights,
                        uint32_t num_lights, const uint32_t* leaf_off, const uint32_t* leaf_nl, uint32_t* nodes,
                        uint32_t* leaf) {
     const uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
     if (h >= 2u * n - 1u) return;
+    if (!(flags[h] & kInTree)) return;
     const uint32_t sz = hsize(h, n, first, last);
-    const bool in_tree = h == 0u || hsize(parent[h], n, first, last) > max_leaf;
-    if (!in_tree) return;
-    const bool inner = sz > max_leaf;
+    const bool inner = !(flags[h] & kIsLeaf);
     const uint32_t id = out_id[h];
     uint32_t* w = nodes + 16ull * id;
     if (h == 0u) {
@@ -306,13 +480,12 @@ __global__ void k_emit(uint32_t n, uint32_t max_leaf, const uint32_t* left, cons
         const uint32_t p = parent[h];
         const uint32_t sib = left[p] == h ? right[p] : left[p];
         w[0] = out_id[p];
-        w[1] = out_id[sib] | (hsize(sib, n, first, last) <= max_leaf ? 0x80000000u : 0u);
+        w[1] = out_id[sib] | ((flags[sib] & kIsLeaf) ? 0x80000000u : 0u);
     }
     float f[12] = {};
     if (inner) {
         const uint32_t L = left[h], R = right[h];
-        w[2] = out_id[L] | (hsize(L, n, first, last) <= max_leaf ? 0x80000000u : 0u) |
-               (hsize(R, n, first, last) <= max_leaf ? 0x40000000u : 0u);
+        w[2] = out_id[L] | ((flags[L] & kIsLeaf) ? 0x80000000u : 0u) | ((flags[R] & kIsLeaf) ? 0x40000000u : 0u);
         w[3] = 0xFFFFFFFFu;
         const Aabb b0 = box[L], b1 = box[R];
         f[0] = widen_lo(b0.lo[0]); f[1] = widen_lo(b0.lo[1]); f[2] = widen_hi(b0.hi[0]); f[3] = widen_hi(b0.hi[1]);
@@ -425,6 +598,7 @@ int tim_rt_build_bvh_gpu(tim_rt_ctx* c, const float* pos, uint32_t num_vertex, c
         k.take<uint32_t>(nh); k.take<uint32_t>(1); k.take<float>(14ull * std::max(num_lights, 1u));
         k.take<uint8_t>(sort_bytes); k.take<uint32_t>(nh + 1ull); k.take<uint32_t>(nh); k.take<uint32_t>(nh + 1ull);
         k.take<uint8_t>(scan_bytes); k.take<uint32_t>(16ull * nh); k.take<uint32_t>(19ull * n);
+        k.take<uint32_t>(nh); k.take<float>(nh);
     };
     plan(K);
     if (c->bld.bytes < K.used) {
@@ -463,6 +637,8 @@ int tim_rt_build_bvh_gpu(tim_rt_ctx* c, const float* pos, uint32_t num_vertex, c
     uint8_t* d_scan = K.take<uint8_t>(scan_bytes);
     uint32_t* d_nodes = K.take<uint32_t>(16ull * nh);
     uint32_t* d_leaf = K.take<uint32_t>(19ull * n);
+    uint32_t* d_flags = K.take<uint32_t>(nh);
+    float* d_cost = K.take<float>(nh);
     if (K.used > c->bld.bytes) {   // the plan above and these takes list the same buffers
         set_error("tim_rt_build_bvh_gpu: scratch plan mismatch");
         return TIM_RT_EDEVICE;
@@ -486,8 +662,22 @@ int tim_rt_build_bvh_gpu(tim_rt_ctx* c, const float* pos, uint32_t num_vertex, c
     k_bottom_up<<<gh, B, 0, st>>>(n, p.max_leaf_size, d_left, d_right, d_first, d_last, d_parent, d_order, d_tbox,
                                   d_box, d_icount, d_arrive);
     GB_CUDA(cudaGetLastError());
-    k_number<<<gh, B, 0, st>>>(n, p.max_leaf_size, d_left, d_first, d_last, d_parent, d_icount, d_outid, d_rank,
-                               d_maxd);
+    // treelet restructuring: two passes, then the internal-node counts again
+    k_mark<<<gh, B, 0, st>>>(n, p.max_leaf_size, d_first, d_last, d_parent, d_flags);
+    GB_CUDA(cudaGetLastError());
+    GB_CUDA(cudaMemsetAsync(d_arrive, 0, 4ull * n, st));
+    k_sah_cost<<<gh, B, 0, st>>>(n, d_left, d_right, d_first, d_last, d_parent, d_flags, d_box, d_cost, d_arrive);
+    GB_CUDA(cudaGetLastError());
+    for (int pass = 0; pass < 2; ++pass) {
+        GB_CUDA(cudaMemsetAsync(d_arrive, 0, 4ull * n, st));
+        k_treelet<<<(nh + kTreeletBlock - 1) / kTreeletBlock, kTreeletBlock, 0, st>>>(n, d_left, d_right, d_parent,
+                                                                                      d_flags, d_box, d_cost, d_arrive);
+        GB_CUDA(cudaGetLastError());
+    }
+    GB_CUDA(cudaMemsetAsync(d_arrive, 0, 4ull * n, st));
+    k_recount<<<gh, B, 0, st>>>(n, d_left, d_right, d_parent, d_flags, d_icount, d_arrive);
+    GB_CUDA(cudaGetLastError());
+    k_number<<<gh, B, 0, st>>>(n, d_left, d_parent, d_flags, d_icount, d_outid, d_rank, d_maxd);
     GB_CUDA(cudaGetLastError());
     uint32_t h_err = 0, h_maxd = 0, h_root_icount = 0;
     GB_CUDA(cudaMemcpyAsync(&h_err, d_err, 4, cudaMemcpyDeviceToHost, st));
@@ -511,8 +701,7 @@ int tim_rt_build_bvh_gpu(tim_rt_ctx* c, const float* pos, uint32_t num_vertex, c
     const uint32_t num_nodes = 1u + 2u * h_root_icount;
     GB_CUDA(cudaMemsetAsync(d_lsize, 0, 4ull * (num_nodes + 1), st));
     GB_CUDA(cudaMemsetAsync(d_lnl, 0, 4ull * num_nodes, st));
-    k_leaf_sizes<<<gh, B, 0, st>>>(n, p.max_leaf_size, d_first, d_last, d_parent, d_outid, d_box, d_lights, num_lights,
-                                   d_lsize, d_lnl);
+    k_leaf_sizes<<<gh, B, 0, st>>>(n, d_first, d_last, d_flags, d_outid, d_box, d_lights, num_lights, d_lsize, d_lnl);
     GB_CUDA(cudaGetLastError());
     GB_CUDA(cub::DeviceScan::ExclusiveSum(d_scan, scan_bytes, d_lsize, d_loff, (int)num_nodes + 1, st));
     uint32_t leaf_words = 0;
@@ -522,8 +711,8 @@ int tim_rt_build_bvh_gpu(tim_rt_ctx* c, const float* pos, uint32_t num_vertex, c
         set_error("tim_rt_build_bvh_gpu: leaf data larger than its bound");
         return TIM_RT_EDEVICE;
     }
-    k_emit<<<gh, B, 0, st>>>(n, p.max_leaf_size, d_left, d_right, d_first, d_last, d_parent, d_outid, d_box, d_order,
-                             d_tri, d_lights, num_lights, d_loff, d_lnl, d_nodes, d_leaf);
+    k_emit<<<gh, B, 0, st>>>(n, d_left, d_right, d_first, d_last, d_parent, d_flags, d_outid, d_box, d_order, d_tri,
+                             d_lights, num_lights, d_loff, d_lnl, d_nodes, d_leaf);
     GB_CUDA(cudaGetLastError());
 
     // host image: fillGpuBuffer section order and 32-byte alignment
