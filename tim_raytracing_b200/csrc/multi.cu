@@ -84,7 +84,9 @@ __global__ void __launch_bounds__(BLOCK, WIDE ? 768 / BLOCK : 1) k_multi(const S
     const uint32_t lane = threadIdx.x & 31u;
     TravState st;
     st.done = true;
-    SceneView sv;
+    // the lane's scene: a pointer into the read-only view table, its fields loaded
+    // where they are used (through L1) rather than held in registers
+    const SceneView* svp = views;
     // active / pending as in k_persistent: lanes whose ray ended are finished
     // (8-wide proof, binary walk when it fails) and stored together when the warp
     // refills. The job's output pointers are read again at store time, so only
@@ -96,7 +98,7 @@ __global__ void __launch_bounds__(BLOCK, WIDE ? 768 / BLOCK : 1) k_multi(const S
         if (idle && (exhausted || __popc(idle) >= refill_min || idle == 0xFFFFFFFFu)) {
             if (pending) {
                 pending = false;
-                if (WIDE) wide_finish_or_walk(sv, st, err);
+                if (WIDE) wide_finish_or_walk(*svp, st, err);
                 const MultiJob& J = jobs[jidx];
                 uint4* hit = J.hit;
                 uint32_t* nid = J.nid;
@@ -124,7 +126,7 @@ __global__ void __launch_bounds__(BLOCK, WIDE ? 768 / BLOCK : 1) k_multi(const S
                         const uint32_t item = perm ? __ldg(perm + my) : my;
                         jidx = find_job(jobs, njobs, item);
                         const MultiJob& J = jobs[jidx];
-                        sv = views[J.scene_slot];
+                        svp = views + J.scene_slot;
                         idx = item - J.first;
                         const uint32_t mode = J.mode;
                         const float4* rp = reinterpret_cast<const float4*>(J.rays + idx);
@@ -135,8 +137,8 @@ __global__ void __launch_bounds__(BLOCK, WIDE ? 768 / BLOCK : 1) k_multi(const S
                         st.t0 = a.w;
                         st.any = (mode == TIM_RT_MODE_ANY) ||
                                  (mode == TIM_RT_MODE_PER_RAY && (__float_as_uint(b.w) & TIM_RT_RAY_ANY));
-                        if (WIDE) wide_init(sv, st, stk);
-                        else trav_init(st, sv.num_nodes == 1u ? kNidLeafBit : 0u);
+                        if (WIDE) wide_init(*svp, st, stk);
+                        else trav_init(st, svp->num_nodes == 1u ? kNidLeafBit : 0u);
                         active = true;
                     }
                 }
@@ -147,9 +149,9 @@ __global__ void __launch_bounds__(BLOCK, WIDE ? 768 / BLOCK : 1) k_multi(const S
             continue;
         }
         if (WIDE) {
-            wide_step_warp<BLOCK>(sv, st, active, stk, err, sdepth, phase_sw);   // all lanes: warp-synchronous step
+            wide_step_warp<BLOCK>(*svp, st, active, stk, err, sdepth, phase_sw);   // all lanes: warp-synchronous step
         } else {
-            plain_step_warp<BLOCK>(sv, st, active, stk, err, sdepth, phase_sw);
+            plain_step_warp<BLOCK>(*svp, st, active, stk, err, sdepth, phase_sw);
         }
         if (active && st.done) {
             active = false;
