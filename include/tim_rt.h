@@ -572,12 +572,14 @@ int tim_rt_build_bvh(const float *pos, uint32_t num_vertex, const uint32_t *tri_
 /* The same output (layout, node numbering scheme, leaf-data order, light lists)
  * built on the context's GPU: a linear BVH over 63-bit Morton codes of the
  * triangle centroids (radix tree split at the highest differing bit, Karras 2012),
- * subtrees of at most max_leaf_size triangles collapsed into leaves. Builds in
- * milliseconds where the binned-SAH host builder takes seconds; the tree is
- * usually slower to trace. traversal_cost, intersection_cost and num_threads are
- * not used. Returns TIM_RT_EUNSUPPORTED when the tree would be deeper than
- * max_depth (at most 32, the reference traversal's bitstack); scenes of at most
- * max_leaf_size triangles are built by tim_rt_build_bvh. */
+ * subtrees of at most max_leaf_size triangles collapsed into leaves, then two
+ * passes of treelet restructuring (7-leaf treelets rebuilt for the least
+ * surface-area cost, Karras & Aila 2013). Builds in milliseconds where the
+ * binned-SAH host builder takes tens to hundreds. traversal_cost,
+ * intersection_cost and num_threads are not used. A restructured tree deeper than
+ * max_depth falls back to the Morton-code tree; TIM_RT_EUNSUPPORTED when that is
+ * deeper too (max_depth at most 32, the reference traversal's bitstack); scenes
+ * of at most max_leaf_size triangles are built by tim_rt_build_bvh. */
 int tim_rt_build_bvh_gpu(tim_rt_ctx *ctx, const float *pos, uint32_t num_vertex, const uint32_t *tri_records,
                          uint32_t num_tris, const void *materials, uint32_t num_materials, const void *lights,
                          uint32_t num_lights, const tim_rt_build_params *params, tim_rt_bvh_blob **out);

@@ -598,7 +598,7 @@ int tim_rt_build_bvh_gpu(tim_rt_ctx* c, const float* pos, uint32_t num_vertex, c
         k.take<uint32_t>(nh); k.take<uint32_t>(1); k.take<float>(14ull * std::max(num_lights, 1u));
         k.take<uint8_t>(sort_bytes); k.take<uint32_t>(nh + 1ull); k.take<uint32_t>(nh); k.take<uint32_t>(nh + 1ull);
         k.take<uint8_t>(scan_bytes); k.take<uint32_t>(16ull * nh); k.take<uint32_t>(19ull * n);
-        k.take<uint32_t>(nh); k.take<float>(nh);
+        k.take<uint32_t>(nh); k.take<float>(nh); k.take<uint32_t>(n); k.take<uint32_t>(n); k.take<uint32_t>(nh);
     };
     plan(K);
     if (c->bld.bytes < K.used) {
@@ -639,6 +639,9 @@ int tim_rt_build_bvh_gpu(tim_rt_ctx* c, const float* pos, uint32_t num_vertex, c
     uint32_t* d_leaf = K.take<uint32_t>(19ull * n);
     uint32_t* d_flags = K.take<uint32_t>(nh);
     float* d_cost = K.take<float>(nh);
+    uint32_t* d_left0 = K.take<uint32_t>(n);
+    uint32_t* d_right0 = K.take<uint32_t>(n);
+    uint32_t* d_parent0 = K.take<uint32_t>(nh);
     if (K.used > c->bld.bytes) {   // the plan above and these takes list the same buffers
         set_error("tim_rt_build_bvh_gpu: scratch plan mismatch");
         return TIM_RT_EDEVICE;
@@ -662,9 +665,14 @@ int tim_rt_build_bvh_gpu(tim_rt_ctx* c, const float* pos, uint32_t num_vertex, c
     k_bottom_up<<<gh, B, 0, st>>>(n, p.max_leaf_size, d_left, d_right, d_first, d_last, d_parent, d_order, d_tbox,
                                   d_box, d_icount, d_arrive);
     GB_CUDA(cudaGetLastError());
-    // treelet restructuring: two passes, then the internal-node counts again
+    // treelet restructuring: two passes, then the internal-node counts again. The
+    // Morton-code tree's links are kept: a restructured tree deeper than max_depth
+    // (surface-area-optimal treelets can lean) falls back to it.
     k_mark<<<gh, B, 0, st>>>(n, p.max_leaf_size, d_first, d_last, d_parent, d_flags);
     GB_CUDA(cudaGetLastError());
+    GB_CUDA(cudaMemcpyAsync(d_left0, d_left, 4ull * n, cudaMemcpyDeviceToDevice, st));
+    GB_CUDA(cudaMemcpyAsync(d_right0, d_right, 4ull * n, cudaMemcpyDeviceToDevice, st));
+    GB_CUDA(cudaMemcpyAsync(d_parent0, d_parent, 4ull * nh, cudaMemcpyDeviceToDevice, st));
     GB_CUDA(cudaMemsetAsync(d_arrive, 0, 4ull * n, st));
     k_sah_cost<<<gh, B, 0, st>>>(n, d_left, d_right, d_first, d_last, d_parent, d_flags, d_box, d_cost, d_arrive);
     GB_CUDA(cudaGetLastError());
@@ -691,6 +699,22 @@ int tim_rt_build_bvh_gpu(tim_rt_ctx* c, const float* pos, uint32_t num_vertex, c
     if (h_err & 2u) {
         set_error("tim_rt_build_bvh_gpu: non-finite vertex position");
         return TIM_RT_EINVAL;
+    }
+    if (h_maxd > p.max_depth) {
+        // back to the Morton-code tree: its links, then boxes, counts and numbering again
+        GB_CUDA(cudaMemcpyAsync(d_left, d_left0, 4ull * n, cudaMemcpyDeviceToDevice, st));
+        GB_CUDA(cudaMemcpyAsync(d_right, d_right0, 4ull * n, cudaMemcpyDeviceToDevice, st));
+        GB_CUDA(cudaMemcpyAsync(d_parent, d_parent0, 4ull * nh, cudaMemcpyDeviceToDevice, st));
+        GB_CUDA(cudaMemsetAsync(d_arrive, 0, 4ull * n, st));
+        GB_CUDA(cudaMemsetAsync(d_maxd, 0, 4, st));
+        k_bottom_up<<<gh, B, 0, st>>>(n, p.max_leaf_size, d_left, d_right, d_first, d_last, d_parent, d_order, d_tbox,
+                                      d_box, d_icount, d_arrive);
+        GB_CUDA(cudaGetLastError());
+        k_number<<<gh, B, 0, st>>>(n, d_left, d_parent, d_flags, d_icount, d_outid, d_rank, d_maxd);
+        GB_CUDA(cudaGetLastError());
+        GB_CUDA(cudaMemcpyAsync(&h_maxd, d_maxd, 4, cudaMemcpyDeviceToHost, st));
+        GB_CUDA(cudaMemcpyAsync(&h_root_icount, d_icount, 4, cudaMemcpyDeviceToHost, st));
+        GB_CUDA(cudaStreamSynchronize(st));
     }
     if (h_maxd > p.max_depth) {
         set_error("tim_rt_build_bvh_gpu: the Morton-code tree is " + std::to_string(h_maxd) +
