@@ -271,6 +271,33 @@ def test_wide_near_ties_match_oracle(ctx, native, oracle_mod):
         ctx.free_scene(sid)
 
 
+@pytest.mark.parametrize("want_nid", [True, False])
+def test_wide_duplicated_triangles_match_oracle(ctx, native, oracle_mod, want_nid):
+    """The reference builder copies a triangle into every leaf it straddles. Without
+    a leaf-id output the 8-wide walk takes a second reference to its nearest
+    triangle as the same hit (only the leaf id could differ); with one it keeps
+    deciding such rays by the binary walk. Records, barycentrics and (when asked
+    for) leaf ids equal the oracle on a reference-built scene full of copies."""
+    from tim_raytracing_b200 import scenes
+    if not oracle_mod.have_refbuild():
+        pytest.skip("the reference builder is not built (oracle/_ref)")
+    s = scenes.random_triangles(41, 20000)
+    img = oracle_mod.ref_build(s)
+    sid = ctx.upload(img, s, quant8=True)
+    try:
+        rays = scenes.random_rays(42, 60000, any_fraction=0.25)
+        sc = oracle_mod.Scene(img, s.positions, s.normals)
+        oh, on, ob, _ = oracle_mod.trace(sc, rays, 2)
+        assert (oh[:, 3].view(np.float32) < 100).sum() > 5000
+        hw, nw, bw, _ = ctx.trace(sid, rays, native.MODE_PER_RAY | native.TRACE_WIDE, want_nid=want_nid)
+        assert np.array_equal(hw, oh)
+        assert np.array_equal(bw.view(np.uint32), ob.view(np.uint32))
+        if want_nid:
+            assert np.array_equal(nw, on)
+    finally:
+        ctx.free_scene(sid)
+
+
 @pytest.mark.parametrize("grid,spheres", [(64, 12), (128, 53)])
 def test_wide_form_matches_plain(ctx, native, grid, spheres):
     """8-wide quantised BVH: hit records, leaf ids and barycentrics identical to the

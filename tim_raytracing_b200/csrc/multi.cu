@@ -137,6 +137,7 @@ __global__ void __launch_bounds__(BLOCK, WIDE ? 768 / BLOCK : 1) k_multi(const S
                         st.t0 = a.w;
                         st.any = (mode == TIM_RT_MODE_ANY) ||
                                  (mode == TIM_RT_MODE_PER_RAY && (__float_as_uint(b.w) & TIM_RT_RAY_ANY));
+                        st.dup_ok = J.nid == nullptr;   // the leaf id is an output only with a nid buffer
                         if (WIDE) wide_init(*svp, st, stk);
                         else trav_init(st, svp->num_nodes == 1u ? kNidLeafBit : 0u);
                         active = true;

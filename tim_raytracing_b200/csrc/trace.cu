@@ -62,6 +62,7 @@ struct BatchPolicy {
         st.t = a.w;
         const uint32_t fl = __float_as_uint(b.w);
         st.any = (mode == TIM_RT_MODE_ANY) || (mode == TIM_RT_MODE_PER_RAY && (fl & TIM_RT_RAY_ANY));
+        st.dup_ok = nid == nullptr;
         return true;
     }
     __device__ __forceinline__ void store(const SceneView&, uint32_t i, const TravState& st, float tmax0) const {
@@ -121,6 +122,7 @@ struct CameraPolicy {
         st.r.ox = pd.cameraPos[0]; st.r.oy = pd.cameraPos[1]; st.r.oz = pd.cameraPos[2];
         st.t = kTMax;
         st.any = false;
+        st.dup_ok = false;   // the hit leaf's light list feeds the shadow rays
         return true;
     }
     __device__ __forceinline__ void store(const SceneView&, uint32_t, const TravState& st, float) const {
@@ -166,6 +168,7 @@ struct SecondaryPolicy {
         st.r.dx = b.x; st.r.dy = b.y; st.r.dz = b.z;
         st.t = a.w;
         st.any = (__float_as_uint(b.w) & 1u) != 0u;
+        st.dup_ok = true;   // bounce rays store the hit record only
         return true;
     }
     __device__ __forceinline__ void store(const SceneView&, uint32_t, const TravState& st, float) const {
@@ -737,6 +740,7 @@ struct ProbePolicy {
         st.r.dx = dir.x; st.r.dy = dir.y; st.r.dz = dir.z;
         st.t = kTMax;
         st.any = false;
+        st.dup_ok = false;   // the hit leaf's light list feeds the shadow rays
         return true;
     }
     __device__ __forceinline__ void store(const SceneView&, uint32_t, const TravState& st, float) const {

@@ -39,6 +39,7 @@ struct TravState {
     float t0;           // the ray's tmax
     float t1;           // closest: the smallest hit t; any: t of the hit
     bool near2;         // closest: another hit t2 has RN(t2 - 1e-5) <= t1
+    bool dup_ok;        // closest: the hit leaf's id is not an output (see wide_leaf)
     uint32_t leaf;      // pending leaf slot of the current wide node (8 = none)
     uint32_t* err;      // two-level walk: the device error word (a nested walk's stack guard)
 };

@@ -241,7 +241,14 @@ __device__ __forceinline__ void wide_leaf(const SceneView& s, TravState& st, con
                 st.v = v;
                 st.hit = true;
             } else {
-                st.near2 = st.near2 || (t - kOffsetRayCollision <= st.t1);
+                // A second reference to the nearest triangle itself -- the reference
+                // builder copies a triangle into every leaf it straddles -- gives the
+                // same record, t and barycentrics; whichever copy the binary walk meets
+                // first, the other then fails t < c. Only the leaf id would differ, so
+                // where the leaf id is not an output (dup_ok) it is no competing hit.
+                const bool same_tri = st.dup_ok && t == st.t1 && __float_as_uint(A.w) == st.rec0 &&
+                                      __float_as_uint(B.w) == st.rec1 && __float_as_uint(C.w) == st.rec2;
+                st.near2 = st.near2 || (!same_tri && t - kOffsetRayCollision <= st.t1);
             }
         }
     }
