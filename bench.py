@@ -746,8 +746,9 @@ def bench_serving(N, ctx, dev, keep_for_parity, jobs_per_rate=1500):
 
 def bench_build(N, ctx, frame_scene, pd, tx, ty):
     """Builders: the binned-SAH host builder (tim_rt_build_bvh, all host threads)
-    against the GPU builder (tim_rt_build_bvh_gpu: Morton-code tree plus treelet
-    restructuring, max_depth 32; wall time including the copies of the triangles in
+    against the GPU builder (tim_rt_build_bvh_gpu: Morton-code tree over single
+    triangles, four treelet-restructuring passes that also choose the leaves by
+    surface-area cost, max_depth 32; wall time including the copies of the triangles in
     and of the image out) on the benchmark frame's scene and on
     the 1M-triangle probe scene, and the frame's trace time on each tree (kernel
     time of tim_rt_trace_camera, median of 5, both forms)."""

@@ -106,8 +106,43 @@ def test_gpu_builder_errors(ctx, native):
     with pytest.raises(native.TimRtError) as e:
         native.build_bvh(s, ctx=ctx, max_depth=3)      # 100 triangles need more than 3 levels
     assert e.value.code == native.EUNSUPPORTED
+    for kw in ({"traversal_cost": 0.0}, {"intersection_cost": float("nan")}, {"intersection_cost": -1.0}):
+        with pytest.raises(native.TimRtError) as e:
+            native.build_bvh(s, ctx=ctx, **kw)
+        assert e.value.code == native.EINVAL
     bad = scenes.random_triangles(25, 100)
     bad.positions[7, 1] = np.nan
     with pytest.raises(native.TimRtError) as e:
         native.build_bvh(bad, ctx=ctx)
     assert e.value.code == native.EINVAL
+
+
+def test_gpu_builder_depth_fallback(ctx, native, oracle_mod):
+    """A max_depth below the restructured tree's depth but not below the
+    Morton-code tree's gives the Morton-code tree (its subtrees of at most
+    max_leaf_size triangles as leaves), still a valid image that traces like the
+    oracle on it."""
+    from tim_raytracing_b200 import scenes
+    s = scenes.random_triangles(21, 40000)
+    deep = native.validate(native.build_bvh(s, ctx=ctx, max_depth=32), s.num_vertex)
+    img = None
+    for md in range(deep - 1, 0, -1):
+        try:
+            img = native.build_bvh(s, ctx=ctx, max_depth=md)
+            break
+        except native.TimRtError as e:
+            assert e.code == native.EUNSUPPORTED
+    assert img is not None, "the Morton-code tree was never shallower than the restructured one"
+    assert native.validate(img, s.num_vertex) <= md
+    _check_image(native, s, img)
+    sid = ctx.upload(img, s)
+    try:
+        rays = scenes.random_rays(41, 20000, any_fraction=0.4)
+        lo, hi = img.aabb[:3], img.aabb[3:]
+        rays[:, 0:3] = lo + (hi - lo) * rays[:, 0:3]
+        sc = oracle_mod.Scene(img, s.positions, s.normals)
+        oh, on, _, _ = oracle_mod.trace(sc, rays, 2)
+        h, nid, _, _ = ctx.trace(sid, rays, 2)
+        assert np.array_equal(h, oh) and np.array_equal(nid, on)
+    finally:
+        ctx.free_scene(sid)

@@ -7,6 +7,7 @@ missing: there is no CPU fallback.
 from __future__ import annotations
 
 import ctypes
+import weakref
 from dataclasses import dataclass
 from pathlib import Path
 
@@ -385,7 +386,9 @@ def build_bvh_tlas(scene, tlas_max_leaf: int = 2, **params) -> BvhImage:
 
 
 def _take_blob(L, out) -> BvhImage:
-    """Copies a tim_rt_bvh_blob into a BvhImage and frees it."""
+    """Wraps a tim_rt_bvh_blob as a BvhImage without copying its bytes: the image's
+    data array reads the blob's memory, and the blob is freed when the last array
+    over it is collected (freed at once when there is nothing to wrap)."""
     try:
         bp, size = ctypes.c_void_p(), ctypes.c_uint64()
         ranges = np.zeros((7, 2), np.uint32)
@@ -393,9 +396,16 @@ def _take_blob(L, out) -> BvhImage:
         aabb = np.zeros(6, np.float32)
         _check(L.tim_rt_bvh_blob_info(out, ctypes.byref(bp), ctypes.byref(size), ranges.ctypes.data, ctypes.byref(pc),
                                       aabb.ctypes.data))
-        data = _copy_bytes(bp.value, size.value)
-    finally:
+    except BaseException:
         L.tim_rt_bvh_blob_free(out)
+        raise
+    if size.value == 0 or not bp.value:
+        L.tim_rt_bvh_blob_free(out)
+        data = np.zeros(0, np.uint8)
+    else:
+        buf = (ctypes.c_uint8 * size.value).from_address(bp.value)
+        weakref.finalize(buf, L.tim_rt_bvh_blob_free, ctypes.c_void_p(out.value))
+        data = np.frombuffer(buf, np.uint8)
     return BvhImage(data, ranges, (pc.numTriangles, pc.numBlas, pc.numPrimitives, pc.numLights, pc.numNodes), aabb)
 
 

@@ -165,7 +165,7 @@ void tim_rt_build_params_default(tim_rt_build_params* p) {
     p->max_leaf_size = 4;
     p->max_depth = 30;
     p->traversal_cost = 1.0f;
-    p->intersection_cost = 1.5f;
+    p->intersection_cost = 0.4f;
     p->num_threads = 0;
 }
 

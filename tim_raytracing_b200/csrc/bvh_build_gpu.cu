@@ -2,27 +2,30 @@
 // layout (BVHBuilder.cpp:1319-1534), with the node numbering and leaf-data order
 // of the host builder (bvh_build.cpp), for fast scene turnaround:
 //   1. triangle boxes and centroids, centroid bounds;
-//   2. 63-bit Morton codes of the centroids, radix sort (CUB, stable);
+//   2. 63-bit Morton codes of the centroids (one scale for all three axes: the
+//      largest centroid extent), radix sort (CUB, stable);
 //   3. radix tree over the sorted codes (Karras 2012, "Maximizing parallelism in
 //      the construction of BVHs, octrees, and k-d trees"): internal node i covers
 //      a key range split at its highest differing bit, equal keys split by index;
-//   4. subtrees of at most max_leaf_size triangles become leaves;
-//   5. bottom-up boxes and internal-node counts (the second child to arrive at a
-//      node merges);
-//   5b. treelet restructuring (Karras & Aila 2013, "Fast Parallel Construction of
+//      its leaves are single triangles;
+//   4. bottom-up boxes, triangle counts and surface-area costs (the second child
+//      to arrive at a node merges), each node choosing between staying internal
+//      and becoming one leaf of its (at most max_leaf_size) triangles;
+//   5. treelet restructuring (Karras & Aila 2013, "Fast Parallel Construction of
 //      High-Quality Bounding Volume Hierarchies"): bottom-up again, each internal
 //      node, once both its subtrees are final, takes the treelet of up to 7 nodes
 //      below it (opening the largest-area inner node each time) and rebuilds the
-//      treelet's topology from the surface-area cost of every subset of its leaves
-//      (exact dynamic programme over the 127 subsets); two passes, then the
-//      internal-node counts again. Leaves keep their Morton-order triangle runs;
-//   5c. per node its depth and pre-order rank among internal
+//      treelet's topology and leaf choices from the surface-area cost of every
+//      subset of its leaves (exact dynamic programme over the 127 subsets, a warp
+//      per treelet); four passes. The topmost nodes that chose to be leaves are
+//      the final tree's leaves, their triangles the radix leaves below them;
+//   5c. per node of the final tree its depth and pre-order rank among internal
 //      nodes by walking to the root, which gives the host builder's numbering:
 //      root 0, the children of the internal node of rank r at 2r+1 and 2r+2;
 //   6. leaf sizes, exclusive scan in node order, leaf data (header, triangle
-//      records in Morton order, light ids: sphere vs widened leaf box, at most
-//      15) and node records (parent, sibling, children, leaf offset, widened
-//      child boxes), copied back into the host image.
+//      records left to right below the leaf, light ids: sphere vs widened leaf
+//      box, at most 15) and node records (parent, sibling, children, leaf offset,
+//      widened child boxes), copied back into the host image.
 // Trees deeper than max_depth (the reference's traversal keeps a 32-bit
 // bitstack) are refused with TIM_RT_EUNSUPPORTED.
 #include <cuda_runtime.h>
@@ -119,9 +122,13 @@ __global__ void k_morton(const float4* cen, uint32_t n, const uint32_t* cbounds,
     const float4 c = cen[t];
     const float cv[3] = {c.x, c.y, c.z};
     uint64_t q[3];
+    // one scale for all three axes (the largest centroid extent): a flat scene's
+    // thin axis then enters the key only at the depth where its cells are as wide
+    // as the other axes', instead of being split as often as the wide axes
+    float ext = 0.f;
+    for (int a = 0; a < 3; ++a) ext = fmaxf(ext, ord2f(cbounds[3 + a]) - ord2f(cbounds[a]));
     for (int a = 0; a < 3; ++a) {
-        const float lo = ord2f(cbounds[a]), hi = ord2f(cbounds[3 + a]);
-        const float ext = hi - lo;
+        const float lo = ord2f(cbounds[a]);
         float u = ext > 0.f ? (cv[a] - lo) / ext : 0.f;
         u = fminf(fmaxf(u, 0.f), 1.f);
         q[a] = (uint64_t)(u * 2097151.0f);
@@ -224,16 +231,20 @@ __global__ void k_bottom_up(uint32_t n, uint32_t max_leaf, const uint32_t* left,
     }
 }
 
-// Per handle: bit 0 = in the final tree (the root, or a child of a node of more
-// than max_leaf triangles), bit 1 = a leaf of the final tree. Fixed before the
-// treelet passes, which change only which internal node has which children.
+// Per handle: bit 0 = in the final tree, bit 1 = a leaf of the final tree.
 constexpr uint32_t kInTree = 1u, kIsLeaf = 2u;
+
+// The Morton-code tree's own leaves (the fallback when the restructured tree is
+// too deep): every subtree of at most max_leaf triangles whose parent has more is
+// a leaf; size = triangles under the handle.
 __global__ void k_mark(uint32_t n, uint32_t max_leaf, const uint32_t* first, const uint32_t* last,
-                       const uint32_t* parent, uint32_t* flags) {
+                       const uint32_t* parent, uint32_t* flags, uint32_t* size) {
     const uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
     if (h >= 2u * n - 1u) return;
+    const uint32_t sz = hsize(h, n, first, last);
     const bool in_tree = h == 0u || hsize(parent[h], n, first, last) > max_leaf;
-    flags[h] = in_tree ? (kInTree | (hsize(h, n, first, last) <= max_leaf ? kIsLeaf : 0u)) : 0u;
+    flags[h] = in_tree ? (kInTree | (sz <= max_leaf ? kIsLeaf : 0u)) : 0u;
+    size[h] = sz;
 }
 
 __device__ __forceinline__ float half_area(const Aabb& b) {
@@ -246,135 +257,231 @@ __device__ __forceinline__ Aabb merge_box(const Aabb& a, const Aabb& b) {
     return m;
 }
 
-// Surface-area costs of the treelet programme: an internal node costs kCi per
-// unit area, a leaf kCt per triangle per unit area (the leaves themselves are
-// fixed, so only their subtree costs enter).
-constexpr float kCi = 1.2f, kCt = 1.0f;
+// Surface-area costs (Karras & Aila 2013, section 4): an internal node costs ci
+// per unit area, a leaf ct per triangle per unit area (the build parameters
+// traversal_cost and intersection_cost); a subtree of at most max_leaf triangles
+// may become one leaf, whichever costs less:
+//   C(x) = min(ci * A(x) + C(left) + C(right), ct * A(x) * N(x) if N(x) <= max_leaf).
 constexpr int kTreeletLeaves = 7, kSubsets = 1 << kTreeletLeaves;
-constexpr uint32_t kTreeletBlock = 32;   // the programme's tables live in shared memory, [subset][thread]
+constexpr uint32_t kTreeletWarps = 4;    // warps per block of the treelet pass
+constexpr int kTreeletPasses = 4;        // restructuring passes over the whole tree
+constexpr uint8_t kCollapse = 0x80u;     // s_part: the subset becomes one leaf (low 7 bits: its split)
 
-// SAH cost of every final-tree node, bottom-up with arrival counters (leaves: kCt
-// * triangles * area; internal: kCi * area + the children's costs).
-__global__ void k_sah_cost(uint32_t n, const uint32_t* left, const uint32_t* right, const uint32_t* first,
-                           const uint32_t* last, const uint32_t* parent, const uint32_t* flags, const Aabb* box,
-                           float* cost, uint32_t* arrive) {
+// Triangle counts, costs and leaf choices of every handle of the single-triangle
+// radix tree, bottom-up with arrival counters from its n leaves.
+__global__ void k_sah_cost(uint32_t n, uint32_t max_leaf, float ci_, float ct, const uint32_t* left, const uint32_t* right,
+                           const uint32_t* parent, const Aabb* box, float* cost, uint32_t* size, uint8_t* coll,
+                           uint32_t* arrive) {
     const uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
-    if (h >= 2u * n - 1u || h == 0u || (flags[h] & (kInTree | kIsLeaf)) != (kInTree | kIsLeaf)) return;
-    cost[h] = kCt * (float)hsize(h, n, first, last) * half_area(box[h]);
+    if (h >= 2u * n - 1u || h < n - 1u) return;
+    cost[h] = ct * half_area(box[h]);
+    size[h] = 1u;
+    coll[h] = 0u;
     uint32_t cur = h;
     while (cur != 0u) {
         const uint32_t p = parent[cur];
         __threadfence();
         if (atomicAdd(arrive + p, 1u) == 0u) return;
         __threadfence();
-        cost[p] = kCi * half_area(load_box_cg(box + p)) + __ldcg(cost + left[p]) + __ldcg(cost + right[p]);
+        const uint32_t L = left[p], R = right[p];
+        const float a = half_area(load_box_cg(box + p));
+        const uint32_t sz = __ldcg(size + L) + __ldcg(size + R);
+        const float ci = ci_ * a + __ldcg(cost + L) + __ldcg(cost + R);
+        const float cl = sz <= max_leaf ? ct * a * (float)sz : INFINITY;
+        size[p] = sz;
+        coll[p] = cl <= ci ? 1u : 0u;
+        cost[p] = fminf(cl, ci);
         cur = p;
     }
 }
 
-// One treelet pass: from every final leaf up to the root; the second child to
-// arrive at a node restructures the treelet rooted there. Every node below it is
-// final by then (its subtree's threads have all passed), so the thread owns the
-// treelet; writes are fenced before the next arrival, reads of other threads'
-// writes bypass L1.
-__global__ void __launch_bounds__(kTreeletBlock) k_treelet(uint32_t n, uint32_t* left, uint32_t* right,
-                                                           uint32_t* parent, const uint32_t* flags, Aabb* box,
-                                                           float* cost, uint32_t* arrive) {
-    __shared__ float s_area[kSubsets * kTreeletBlock];
-    __shared__ float s_cost[kSubsets * kTreeletBlock];
-    __shared__ uint8_t s_part[kSubsets * kTreeletBlock];
-    const uint32_t t = threadIdx.x;
-    const uint32_t h = blockIdx.x * blockDim.x + t;
-    if (h >= 2u * n - 1u || h == 0u || (flags[h] & (kInTree | kIsLeaf)) != (kInTree | kIsLeaf)) return;
-    uint32_t cur = h;
-    while (cur != 0u) {
-        const uint32_t p = parent[cur];
-        __threadfence();
-        if (atomicAdd(arrive + p, 1u) == 0u) return;
-        __threadfence();
-        // the treelet below p: open the largest-area inner node until 7 leaves
-        uint32_t leaf[kTreeletLeaves], inner[kTreeletLeaves - 2];
-        Aabb lb[kTreeletLeaves];
-        int nl = 2, ni = 0;
-        leaf[0] = __ldcg(left + p);
-        leaf[1] = __ldcg(right + p);
-        lb[0] = load_box_cg(box + leaf[0]);
-        lb[1] = load_box_cg(box + leaf[1]);
-        while (nl < kTreeletLeaves) {
-            int best = -1;
-            float ba = -1.0f;
-            for (int i = 0; i < nl; ++i) {
-                if (flags[leaf[i]] & kIsLeaf) continue;
-                const float a = half_area(lb[i]);
-                if (a > ba) { ba = a; best = i; }
+// One treelet pass, a warp per treelet: every lane walks from one radix leaf up
+// to the root; the lane that arrives second at a node has the treelet rooted
+// there to restructure, and the warp takes its lanes' treelets one after another,
+// the 127 subsets of a treelet spread over its 32 lanes. Every node below a
+// treelet root is final by then (its subtree's walks have all passed), so the
+// warp owns the treelet; writes are fenced before the next arrival, reads of
+// other warps' writes bypass L1.
+__global__ void __launch_bounds__(kTreeletWarps * 32) k_treelet(uint32_t n, uint32_t max_leaf, float ci_, float ct,
+                                                                uint32_t* left, uint32_t* right, uint32_t* parent,
+                                                                Aabb* box, float* cost, uint32_t* size, uint8_t* coll,
+                                                                uint32_t* arrive) {
+    __shared__ float s_area_all[kTreeletWarps][kSubsets];
+    __shared__ float s_cost_all[kTreeletWarps][kSubsets];
+    __shared__ uint8_t s_part_all[kTreeletWarps][kSubsets];
+    const uint32_t lane = threadIdx.x & 31u, w = threadIdx.x >> 5;
+    float* s_area = s_area_all[w];
+    float* s_cost = s_cost_all[w];
+    uint8_t* s_part = s_part_all[w];
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;   // radix leaf j: handle n - 1 + j
+    bool active = j < n;
+    uint32_t cur = n - 1u + j;
+    for (;;) {
+        // one step up for every walking lane
+        bool pending = false;
+        uint32_t p = 0;
+        if (active) {
+            if (cur == 0u) {
+                active = false;
+            } else {
+                p = parent[cur];
+                __threadfence();
+                if (atomicAdd(arrive + p, 1u) == 0u) {
+                    active = false;   // the sibling's walk finishes this node
+                } else {
+                    __threadfence();
+                    pending = true;
+                }
             }
-            if (best < 0) break;
-            const uint32_t x = leaf[best];
-            inner[ni++] = x;
-            leaf[best] = __ldcg(left + x);
-            leaf[nl] = __ldcg(right + x);
-            lb[best] = load_box_cg(box + leaf[best]);
-            lb[nl] = load_box_cg(box + leaf[nl]);
-            ++nl;
         }
-        if (nl >= 3) {
-            // areas and best partitions of every subset of the treelet's leaves
+        uint32_t todo = __ballot_sync(0xFFFFFFFFu, pending);
+        if (todo == 0u) break;   // walking lanes are exactly the pending ones
+        // A node whose parent holds at most 7 triangles is left alone: the parent's
+        // treelet opens every node below it, so its programme covers every
+        // topology and leaf choice of this subtree too.
+        const bool redundant = pending && p != 0u && __ldcg(size + parent[p]) <= (uint32_t)kTreeletLeaves;
+        todo &= ~__ballot_sync(0xFFFFFFFFu, redundant);
+        while (todo) {
+            const int src = __ffs(todo) - 1;
+            todo &= todo - 1u;
+            const uint32_t root = __shfl_sync(0xFFFFFFFFu, p, src);
+            // the treelet below root (every lane forms it, from the same loads):
+            // open the largest-area internal node until 7 leaves
+            uint32_t leaf[kTreeletLeaves], inner[kTreeletLeaves - 2];
+            Aabb lb[kTreeletLeaves];
+            int nl = 2, ni = 0;
+            leaf[0] = __ldcg(left + root);
+            leaf[1] = __ldcg(right + root);
+            lb[0] = load_box_cg(box + leaf[0]);
+            lb[1] = load_box_cg(box + leaf[1]);
+            while (nl < kTreeletLeaves) {
+                int best = -1;
+                float ba = -1.0f;
+                for (int i = 0; i < nl; ++i) {
+                    if (leaf[i] >= n - 1u) continue;   // a triangle
+                    const float a = half_area(lb[i]);
+                    if (a > ba) { ba = a; best = i; }
+                }
+                if (best < 0) break;
+                const uint32_t x = leaf[best];
+                inner[ni++] = x;
+                leaf[best] = __ldcg(left + x);
+                leaf[nl] = __ldcg(right + x);
+                lb[best] = load_box_cg(box + leaf[best]);
+                lb[nl] = load_box_cg(box + leaf[nl]);
+                ++nl;
+            }
+            if (nl < 3) continue;   // two triangles: nothing to rearrange
+            uint32_t lsz[kTreeletLeaves];
+            float lcost[kTreeletLeaves];
+#pragma unroll
+            for (int i = 0; i < kTreeletLeaves; ++i) {
+                lsz[i] = i < nl ? __ldcg(size + leaf[i]) : 0u;
+                lcost[i] = i < nl ? __ldcg(cost + leaf[i]) : 0.f;
+            }
+            // area of every subset of the treelet's leaves; a single leaf keeps its
+            // cost, a larger subset starts at its cost as one leaf (if small enough)
             const uint32_t full = (1u << nl) - 1u;
-            for (uint32_t sub = 1; sub <= full; ++sub) {
-                Aabb u = lb[__ffs(sub) - 1];
-                for (uint32_t r = sub & (sub - 1u); r; r &= r - 1u) u = merge_box(u, lb[__ffs(r) - 1]);
-                s_area[sub * kTreeletBlock + t] = half_area(u);
-                if ((sub & (sub - 1u)) == 0u) s_cost[sub * kTreeletBlock + t] = __ldcg(cost + leaf[__ffs(sub) - 1]);
-            }
-            for (uint32_t sub = 1; sub <= full; ++sub) {
-                if ((sub & (sub - 1u)) == 0u) continue;
-                // subsets are visited in increasing order, so every proper subset is done;
-                // a partition (P, sub \ P) is taken once, with P holding sub's lowest leaf
-                const uint32_t low = sub & (0u - sub), rest = sub ^ low;
-                float best = INFINITY;
-                uint32_t bp = low;
-                for (uint32_t q = rest;; q = (q - 1u) & rest) {
-                    const uint32_t P = q | low;
-                    if (P != sub) {
-                        const float c = s_cost[P * kTreeletBlock + t] + s_cost[(sub ^ P) * kTreeletBlock + t];
-                        if (c < best) { best = c; bp = P; }
+            for (uint32_t sub = lane + 1u; sub <= full; sub += 32u) {
+                Aabb u;
+                for (int k = 0; k < 3; ++k) { u.lo[k] = INFINITY; u.hi[k] = -INFINITY; }
+                uint32_t cnt = 0;
+                float single = 0.f;
+#pragma unroll
+                for (int i = 0; i < kTreeletLeaves; ++i)
+                    if (sub & (1u << i)) {
+                        u = merge_box(u, lb[i]);
+                        cnt += lsz[i];
+                        single = lcost[i];
                     }
-                    if (q == 0u) break;
-                }
-                s_cost[sub * kTreeletBlock + t] = kCi * s_area[sub * kTreeletBlock + t] + best;
-                s_part[sub * kTreeletBlock + t] = (uint8_t)bp;
+                const float a = half_area(u);
+                s_area[sub] = a;
+                s_cost[sub] = (sub & (sub - 1u)) == 0u ? single : (cnt <= max_leaf ? ct * a * (float)cnt : INFINITY);
             }
-            // rebuild: p keeps its place; the other internal nodes are reused in order
-            uint32_t stk_node[kTreeletLeaves], stk_set[kTreeletLeaves];
-            int sp = 0, next = 0;
-            stk_node[sp] = p;
-            stk_set[sp++] = full;
-            while (sp > 0) {
-                --sp;
-                const uint32_t node = stk_node[sp], set = stk_set[sp];
-                const uint32_t P = s_part[set * kTreeletBlock + t], Q = set ^ P;
-                uint32_t kid[2];
-                const uint32_t sides[2] = {P, Q};
-                for (int k = 0; k < 2; ++k) {
-                    if ((sides[k] & (sides[k] - 1u)) == 0u) {
-                        kid[k] = leaf[__ffs(sides[k]) - 1];
-                    } else {
-                        kid[k] = inner[next++];
-                        stk_node[sp] = kid[k];
-                        stk_set[sp++] = sides[k];
+            __syncwarp();
+            // best split of every subset, by size: all proper subsets are done first.
+            // A split (P, sub \ P) is taken once, with P holding sub's lowest leaf.
+            for (int k = 2; k <= nl; ++k) {
+                for (uint32_t sub = lane + 1u; sub <= full; sub += 32u) {
+                    if (__popc(sub) != k) continue;
+                    const uint32_t low = sub & (0u - sub), rest = sub ^ low;
+                    float best = INFINITY;
+                    uint32_t bp = low;
+                    for (uint32_t q = rest;; q = (q - 1u) & rest) {
+                        const uint32_t P = q | low;
+                        if (P != sub) {
+                            const float c = s_cost[P] + s_cost[sub ^ P];
+                            if (c < best) { best = c; bp = P; }
+                        }
+                        if (q == 0u) break;
                     }
-                    parent[kid[k]] = node;
+                    const float ci = ci_ * s_area[sub] + best;
+                    const float cl = s_cost[sub];
+                    s_cost[sub] = fminf(cl, ci);
+                    s_part[sub] = (uint8_t)bp | (cl <= ci ? kCollapse : 0u);
                 }
-                left[node] = kid[0];
-                right[node] = kid[1];
-                Aabb u = lb[__ffs(set) - 1];
-                for (uint32_t r = set & (set - 1u); r; r &= r - 1u) u = merge_box(u, lb[__ffs(r) - 1]);
-                box[node] = u;
-                cost[node] = s_cost[set * kTreeletBlock + t];
+                __syncwarp();
             }
+            // rebuild (lane 0): root keeps its place; the other internal nodes are
+            // reused in order. A subset that becomes one leaf still gets its best
+            // split below it, so its triangles stay reachable from it.
+            if (lane == 0u) {
+                uint32_t stk_node[kTreeletLeaves], stk_set[kTreeletLeaves];
+                int sp = 0, next = 0;
+                stk_node[sp] = root;
+                stk_set[sp++] = full;
+                while (sp > 0) {
+                    --sp;
+                    const uint32_t node = stk_node[sp], set = stk_set[sp];
+                    const uint8_t part = s_part[set];
+                    const uint32_t P = part & (kCollapse - 1u), Q = set ^ P;
+                    uint32_t kid[2];
+                    const uint32_t sides[2] = {P, Q};
+                    for (int k = 0; k < 2; ++k) {
+                        if ((sides[k] & (sides[k] - 1u)) == 0u) {
+                            kid[k] = leaf[__ffs(sides[k]) - 1];
+                        } else {
+                            kid[k] = inner[next++];
+                            stk_node[sp] = kid[k];
+                            stk_set[sp++] = sides[k];
+                        }
+                        parent[kid[k]] = node;
+                    }
+                    left[node] = kid[0];
+                    right[node] = kid[1];
+                    Aabb u;
+                    for (int k = 0; k < 3; ++k) { u.lo[k] = INFINITY; u.hi[k] = -INFINITY; }
+                    uint32_t cnt = 0;
+#pragma unroll
+                    for (int i = 0; i < kTreeletLeaves; ++i)
+                        if (set & (1u << i)) {
+                            u = merge_box(u, lb[i]);
+                            cnt += lsz[i];
+                        }
+                    box[node] = u;
+                    size[node] = cnt;
+                    coll[node] = (part & kCollapse) ? 1u : 0u;
+                    cost[node] = s_cost[set];
+                }
+                __threadfence();
+            }
+            __syncwarp();
         }
-        cur = p;
+        if (pending) cur = p;
     }
+}
+
+// Final tree: a handle is in it unless an ancestor became a leaf; it is a leaf if
+// it is a triangle or became a leaf itself.
+__global__ void k_final_flags(uint32_t n, const uint32_t* parent, const uint8_t* coll, uint32_t* flags) {
+    const uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
+    if (h >= 2u * n - 1u) return;
+    bool in_tree = true;
+    for (uint32_t a = h; a != 0u;) {
+        a = parent[a];
+        if (coll[a]) { in_tree = false; break; }
+    }
+    flags[h] = in_tree ? (kInTree | ((h >= n - 1u || coll[h]) ? kIsLeaf : 0u)) : 0u;
 }
 
 // Internal-node counts again after the treelet passes (leaves 0).
@@ -434,13 +541,13 @@ __device__ __forceinline__ float widen_hi(float x) { return x + (1e-6f + fabsf(x
 // Leaf sizes (header + 3 words per triangle + light ids), indexed by output id;
 // internal nodes 0. Light ids: sphere (centre, radius) vs the widened leaf box,
 // at most 15 (BVHBuilder.cpp:36-42,749-756 with the 4-bit count kept below 16).
-__global__ void k_leaf_sizes(uint32_t n, const uint32_t* first, const uint32_t* last, const uint32_t* flags,
-                             const uint32_t* out_id, const Aabb* box, const float* lights, uint32_t num_lights,
-                             uint32_t* leaf_size, uint32_t* leaf_nl) {
+__global__ void k_leaf_sizes(uint32_t n, const uint32_t* size, const uint32_t* flags, const uint32_t* out_id,
+                             const Aabb* box, const float* lights, uint32_t num_lights, uint32_t* leaf_size,
+                             uint32_t* leaf_nl) {
     const uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
     if (h >= 2u * n - 1u || h == 0u) return;
     if ((flags[h] & (kInTree | kIsLeaf)) != (kInTree | kIsLeaf)) return;
-    const uint32_t sz = hsize(h, n, first, last);
+    const uint32_t sz = size[h];
     const Aabb b = box[h];
     float lo[3], hi[3];
     for (int a = 0; a < 3; ++a) { lo[a] = widen_lo(b.lo[a]); hi[a] = widen_hi(b.hi[a]); }
@@ -460,16 +567,18 @@ __global__ void k_leaf_sizes(uint32_t n, const uint32_t* first, const uint32_t* 
     leaf_nl[id] = nl;
 }
 
-// Node records (packNodeData, BVHBuilder.cpp:1283-1317) and leaf data.
-__global__ void k_emit(uint32_t n, const uint32_t* left, const uint32_t* right, const uint32_t* first,
-                       const uint32_t* last, const uint32_t* parent, const uint32_t* flags, const uint32_t* out_id,
-                       const Aabb* box, const uint32_t* order, const uint32_t* tri, const float* lights,
-                       uint32_t num_lights, const uint32_t* leaf_off, const uint32_t* leaf_nl, uint32_t* nodes,
-                       uint32_t* leaf) {
+// Node records (packNodeData, BVHBuilder.cpp:1283-1317) and leaf data. A leaf's
+// triangles are the radix leaves below it, left to right (a walk over the links
+// without a stack: down the left edge, up past right children, over to the
+// sibling).
+__global__ void k_emit(uint32_t n, const uint32_t* left, const uint32_t* right, const uint32_t* size,
+                       const uint32_t* parent, const uint32_t* flags, const uint32_t* out_id, const Aabb* box,
+                       const uint32_t* order, const uint32_t* tri, const float* lights, uint32_t num_lights,
+                       const uint32_t* leaf_off, const uint32_t* leaf_nl, uint32_t* nodes, uint32_t* leaf) {
     const uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
     if (h >= 2u * n - 1u) return;
     if (!(flags[h] & kInTree)) return;
-    const uint32_t sz = hsize(h, n, first, last);
+    const uint32_t sz = size[h];
     const bool inner = !(flags[h] & kIsLeaf);
     const uint32_t id = out_id[h];
     uint32_t* w = nodes + 16ull * id;
@@ -497,12 +606,17 @@ __global__ void k_emit(uint32_t n, const uint32_t* left, const uint32_t* right, 
         w[3] = off;
         uint32_t* o = leaf + off;
         o[0] = sz | (nl << 28);
-        const uint32_t fs = hfirst(h, n, first);
-        for (uint32_t q = 0; q < sz; ++q) {
-            const uint32_t t = order[fs + q];
+        uint32_t cur = h, q = 0;
+        for (;;) {
+            while (cur < n - 1u) cur = left[cur];
+            const uint32_t t = order[cur - (n - 1u)];
             o[1 + 3 * q] = tri[3 * t];
             o[2 + 3 * q] = tri[3 * t + 1];
             o[3 + 3 * q] = tri[3 * t + 2];
+            ++q;
+            while (cur != h && left[parent[cur]] != cur) cur = parent[cur];
+            if (cur == h || q >= sz) break;
+            cur = right[parent[cur]];
         }
         // light ids, the same test as k_leaf_sizes
         const Aabb b = box[h];
@@ -572,6 +686,11 @@ int tim_rt_build_bvh_gpu(tim_rt_ctx* c, const float* pos, uint32_t num_vertex, c
         set_error("tim_rt_build_bvh_gpu: max_leaf_size must be 1..4095 and max_depth 1..32");
         return TIM_RT_EINVAL;
     }
+    if (!(p.traversal_cost > 0.f && p.traversal_cost < 1e30f && p.intersection_cost > 0.f &&
+          p.intersection_cost < 1e30f)) {
+        set_error("tim_rt_build_bvh_gpu: traversal_cost and intersection_cost must be positive and finite");
+        return TIM_RT_EINVAL;
+    }
     if (num_lights && !lights) {
         set_error("tim_rt_build_bvh_gpu: lights pointer is null");
         return TIM_RT_EINVAL;
@@ -599,6 +718,7 @@ int tim_rt_build_bvh_gpu(tim_rt_ctx* c, const float* pos, uint32_t num_vertex, c
         k.take<uint8_t>(sort_bytes); k.take<uint32_t>(nh + 1ull); k.take<uint32_t>(nh); k.take<uint32_t>(nh + 1ull);
         k.take<uint8_t>(scan_bytes); k.take<uint32_t>(16ull * nh); k.take<uint32_t>(19ull * n);
         k.take<uint32_t>(nh); k.take<float>(nh); k.take<uint32_t>(n); k.take<uint32_t>(n); k.take<uint32_t>(nh);
+        k.take<uint32_t>(nh); k.take<uint8_t>(nh);
     };
     plan(K);
     if (c->bld.bytes < K.used) {
@@ -642,6 +762,8 @@ int tim_rt_build_bvh_gpu(tim_rt_ctx* c, const float* pos, uint32_t num_vertex, c
     uint32_t* d_left0 = K.take<uint32_t>(n);
     uint32_t* d_right0 = K.take<uint32_t>(n);
     uint32_t* d_parent0 = K.take<uint32_t>(nh);
+    uint32_t* d_size = K.take<uint32_t>(nh);
+    uint8_t* d_coll = K.take<uint8_t>(nh);
     if (K.used > c->bld.bytes) {   // the plan above and these takes list the same buffers
         set_error("tim_rt_build_bvh_gpu: scratch plan mismatch");
         return TIM_RT_EDEVICE;
@@ -662,26 +784,30 @@ int tim_rt_build_bvh_gpu(tim_rt_ctx* c, const float* pos, uint32_t num_vertex, c
     GB_CUDA(cudaGetLastError());
     GB_CUDA(cudaMemsetAsync(d_arrive, 0, 4ull * n, st));
     GB_CUDA(cudaMemsetAsync(d_maxd, 0, 4, st));
-    k_bottom_up<<<gh, B, 0, st>>>(n, p.max_leaf_size, d_left, d_right, d_first, d_last, d_parent, d_order, d_tbox,
-                                  d_box, d_icount, d_arrive);
-    GB_CUDA(cudaGetLastError());
-    // treelet restructuring: two passes, then the internal-node counts again. The
-    // Morton-code tree's links are kept: a restructured tree deeper than max_depth
-    // (surface-area-optimal treelets can lean) falls back to it.
-    k_mark<<<gh, B, 0, st>>>(n, p.max_leaf_size, d_first, d_last, d_parent, d_flags);
+    // boxes of every handle of the single-triangle radix tree (its Morton-code
+    // links are kept: a restructured tree deeper than max_depth -- surface-area-
+    // optimal treelets can lean -- falls back to it)
+    k_bottom_up<<<gh, B, 0, st>>>(n, 1u, d_left, d_right, d_first, d_last, d_parent, d_order, d_tbox, d_box, d_icount,
+                                  d_arrive);
     GB_CUDA(cudaGetLastError());
     GB_CUDA(cudaMemcpyAsync(d_left0, d_left, 4ull * n, cudaMemcpyDeviceToDevice, st));
     GB_CUDA(cudaMemcpyAsync(d_right0, d_right, 4ull * n, cudaMemcpyDeviceToDevice, st));
     GB_CUDA(cudaMemcpyAsync(d_parent0, d_parent, 4ull * nh, cudaMemcpyDeviceToDevice, st));
+    // costs and leaf choices, two treelet passes, the final tree's leaves, then
+    // internal-node counts and numbering
     GB_CUDA(cudaMemsetAsync(d_arrive, 0, 4ull * n, st));
-    k_sah_cost<<<gh, B, 0, st>>>(n, d_left, d_right, d_first, d_last, d_parent, d_flags, d_box, d_cost, d_arrive);
+    k_sah_cost<<<gh, B, 0, st>>>(n, p.max_leaf_size, p.traversal_cost, p.intersection_cost, d_left, d_right, d_parent, d_box, d_cost, d_size, d_coll,
+                                 d_arrive);
     GB_CUDA(cudaGetLastError());
-    for (int pass = 0; pass < 2; ++pass) {
+    for (int pass = 0; pass < kTreeletPasses; ++pass) {
         GB_CUDA(cudaMemsetAsync(d_arrive, 0, 4ull * n, st));
-        k_treelet<<<(nh + kTreeletBlock - 1) / kTreeletBlock, kTreeletBlock, 0, st>>>(n, d_left, d_right, d_parent,
-                                                                                      d_flags, d_box, d_cost, d_arrive);
+        k_treelet<<<(n + kTreeletWarps * 32 - 1) / (kTreeletWarps * 32), kTreeletWarps * 32, 0, st>>>(
+            n, p.max_leaf_size, p.traversal_cost, p.intersection_cost, d_left, d_right, d_parent, d_box, d_cost, d_size,
+            d_coll, d_arrive);
         GB_CUDA(cudaGetLastError());
     }
+    k_final_flags<<<gh, B, 0, st>>>(n, d_parent, d_coll, d_flags);
+    GB_CUDA(cudaGetLastError());
     GB_CUDA(cudaMemsetAsync(d_arrive, 0, 4ull * n, st));
     k_recount<<<gh, B, 0, st>>>(n, d_left, d_right, d_parent, d_flags, d_icount, d_arrive);
     GB_CUDA(cudaGetLastError());
@@ -710,6 +836,8 @@ int tim_rt_build_bvh_gpu(tim_rt_ctx* c, const float* pos, uint32_t num_vertex, c
         k_bottom_up<<<gh, B, 0, st>>>(n, p.max_leaf_size, d_left, d_right, d_first, d_last, d_parent, d_order, d_tbox,
                                       d_box, d_icount, d_arrive);
         GB_CUDA(cudaGetLastError());
+        k_mark<<<gh, B, 0, st>>>(n, p.max_leaf_size, d_first, d_last, d_parent, d_flags, d_size);
+        GB_CUDA(cudaGetLastError());
         k_number<<<gh, B, 0, st>>>(n, d_left, d_parent, d_flags, d_icount, d_outid, d_rank, d_maxd);
         GB_CUDA(cudaGetLastError());
         GB_CUDA(cudaMemcpyAsync(&h_maxd, d_maxd, 4, cudaMemcpyDeviceToHost, st));
@@ -725,7 +853,7 @@ int tim_rt_build_bvh_gpu(tim_rt_ctx* c, const float* pos, uint32_t num_vertex, c
     const uint32_t num_nodes = 1u + 2u * h_root_icount;
     GB_CUDA(cudaMemsetAsync(d_lsize, 0, 4ull * (num_nodes + 1), st));
     GB_CUDA(cudaMemsetAsync(d_lnl, 0, 4ull * num_nodes, st));
-    k_leaf_sizes<<<gh, B, 0, st>>>(n, d_first, d_last, d_flags, d_outid, d_box, d_lights, num_lights, d_lsize, d_lnl);
+    k_leaf_sizes<<<gh, B, 0, st>>>(n, d_size, d_flags, d_outid, d_box, d_lights, num_lights, d_lsize, d_lnl);
     GB_CUDA(cudaGetLastError());
     GB_CUDA(cub::DeviceScan::ExclusiveSum(d_scan, scan_bytes, d_lsize, d_loff, (int)num_nodes + 1, st));
     uint32_t leaf_words = 0;
@@ -735,8 +863,8 @@ int tim_rt_build_bvh_gpu(tim_rt_ctx* c, const float* pos, uint32_t num_vertex, c
         set_error("tim_rt_build_bvh_gpu: leaf data larger than its bound");
         return TIM_RT_EDEVICE;
     }
-    k_emit<<<gh, B, 0, st>>>(n, d_left, d_right, d_first, d_last, d_parent, d_flags, d_outid, d_box, d_order, d_tri,
-                             d_lights, num_lights, d_loff, d_lnl, d_nodes, d_leaf);
+    k_emit<<<gh, B, 0, st>>>(n, d_left, d_right, d_size, d_parent, d_flags, d_outid, d_box, d_order, d_tri, d_lights,
+                             num_lights, d_loff, d_lnl, d_nodes, d_leaf);
     GB_CUDA(cudaGetLastError());
 
     // host image: fillGpuBuffer section order and 32-byte alignment
