@@ -932,6 +932,23 @@ def profile_shade():
     return 0
 
 
+def profile_build():
+    """Two GPU builds (tim_rt_build_bvh_gpu, max_depth 32) of the 1M-triangle
+    heightfield scene of the builder comparison: the first warms the context's
+    build scratch, the second is the one to read."""
+    from tim_raytracing_b200 import _native as N, scenes
+    ctx = N.Context(0)
+    scene = scenes.scaled_heightfield(77, 1_000_000)
+    out = []
+    for _ in range(2):
+        t0 = time.perf_counter()
+        img = N.build_bvh(scene, ctx=ctx, max_depth=32)
+        out.append(1e3 * (time.perf_counter() - t0))
+    print(json.dumps({"build_wall_ms": out, "nodes": int(img.num_nodes)}))
+    ctx.close()
+    return 0
+
+
 # ---------------------------------------------------------------- main
 
 def main():
@@ -947,13 +964,13 @@ def main():
     ap.add_argument("--no-probes", action="store_true", help="skip the light-probe field workload")
     ap.add_argument("--no-build", action="store_true", help="skip the BVH builder comparison")
     ap.add_argument("--profile", choices=["plain", "wide", "batched-plain", "batched-wide", "probes-plain",
-                                          "probes-wide", "shade"],
+                                          "probes-wide", "shade", "build"],
                     help="only run a small, fixed launch sequence for ncu and exit: plain / wide = two frames of "
                          "one form (per frame one primary and one secondary k_persistent launch); batched-* = two "
                          "launches of one k_multi batch over the first 16 scenes of the batched workload; "
                          "probes-* = two probe-field updates of one form (per update one probe-ray and one "
                          "shadow-ray k_persistent launch); shade = one quantised frame, then two k_shade_camera "
-                         "launches")
+                         "launches; build = two GPU builds of the 1M-triangle scene")
     args = ap.parse_args()
     if args.profile in ("plain", "wide"):
         return profile_frames(args.profile)
@@ -961,6 +978,8 @@ def main():
         return profile_batched(args.profile == "batched-wide")
     if args.profile == "shade":
         return profile_shade()
+    if args.profile == "build":
+        return profile_build()
     if args.profile:
         return profile_probes(args.profile == "probes-wide")
     args.warmup = max(args.warmup, 3)

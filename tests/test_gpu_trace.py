@@ -369,3 +369,33 @@ def test_errors(ctx, native, room):
         assert e.value.code == native.ENOMEM
     finally:
         small.close()
+
+
+@pytest.mark.parametrize("wide", [False, True])
+def test_camera_leaf_lights_and_counts(ctx, native, oracle_mod, wide):
+    """Leaf light lists (no tile culling) on a scene where about half the hit
+    pixels are shadowed, against the oracle, and the counting variant: the same
+    records, and work counts whose secondary rays are the traced rays less the
+    primary ones."""
+    from tim_raytracing_b200 import scenes
+    s = scenes.heightfield_scene(seed=4, grid=40, n_spheres=12, n_lights=24, light_radius=6.0)
+    img = native.build_bvh(s)
+    sid = ctx.upload(img, s, quant8=wide)
+    try:
+        W, H = 136, 90
+        pd = scenes.pass_data(s, W, H, aabb=(img.aabb[:3], img.aabb[3:]))
+        sc = oracle_mod.Scene(img, s.positions, s.normals)
+        flags = native.CAM_PROB_MASK | native.CAM_BOUNCE
+        o_out, o_bounce, o_counts = oracle_mod.camera(sc, pd, flags=flags, seed=3)
+        masked = (o_out[:, 4] != 0).mean()
+        assert 0.05 < masked < 0.95            # both outcomes occur
+        form = native.CAM_WIDE if wide else 0
+        for extra in (0, native.CAM_COUNT):
+            out, bounce, st = ctx.trace_camera(sid, pd, flags=flags | form | extra, seed=3)
+            assert np.array_equal(out, o_out)
+            assert np.array_equal(bounce, o_bounce)
+            assert st.rays == int(o_counts.sum())
+            if extra & native.CAM_COUNT:
+                assert st.secondary_rays_counted == st.rays - st.primary_rays
+    finally:
+        ctx.free_scene(sid)
