@@ -8,7 +8,8 @@ the BVH buffer, positions, tile lists and outputs (torch tensors), calls the
 entry point through the C ABI twice in a row, and checks both calls against the
 context-based tim_rt_trace_camera on the same inputs (integer records:
 bit-identical). Frames include one whose sides are not multiples of the 8x4
-tile (50x37), so partial tiles meet the fixed-stride scratch layout. This file is
+tile (50x37), so partial tiles meet the fixed-stride scratch layout, and each
+case is also captured in a CUDA graph on a side stream and replayed. This file is
 collected last so that a failure here comes after every other test has run.
 """
 import ctypes
@@ -72,6 +73,30 @@ def test_noalloc_camera_matches_context_path(native):
                 if flags & native.CAM_BOUNCE:
                     gb = d_bounce.cpu().numpy().view(np.uint32).reshape(-1, 4)
                     assert np.array_equal(gb, want_b), f"call {call}: bounce records differ"
+            # the same call captured in a CUDA graph on a side stream (after the warm
+            # calls above), then replayed twice
+            side = torch.cuda.Stream()
+            g_out = torch.full((W * H * 8,), -1, dtype=torch.int32, device="cuda")
+            g_bounce = torch.full((W * H * 4,), -1, dtype=torch.int32, device="cuda")
+            graph = torch.cuda.CUDAGraph()
+            torch.cuda.synchronize()
+            with torch.cuda.graph(graph, stream=side):
+                rc = L.tim_rt_trace_camera_noalloc(d_bvh.data_ptr(), ranges.ctypes.data, ctypes.byref(pc),
+                                                   d_pos.data_ptr(), scene.num_vertex, depth, pdc.ctypes.data, flags,
+                                                   seed, d_counts.data_ptr(), d_lists.data_ptr(), g_out.data_ptr(),
+                                                   g_bounce.data_ptr(), ctypes.c_void_p(side.cuda_stream))
+            assert rc == native.OK, L.tim_rt_last_error().decode()
+            for rep in range(2):
+                g_out.fill_(-1)
+                g_bounce.fill_(-1)
+                graph.replay()
+                torch.cuda.synchronize()
+                got = g_out.cpu().numpy().view(np.uint32).reshape(-1, 8)
+                assert np.array_equal(got, want), f"replay {rep}: {np.sum(np.any(got != want, axis=1))} pixels differ"
+                if flags & native.CAM_BOUNCE:
+                    gb = g_bounce.cpu().numpy().view(np.uint32).reshape(-1, 4)
+                    assert np.array_equal(gb, want_b), f"replay {rep}: bounce records differ"
+            del graph
             ctx.free_scene(sid)
 
 
