@@ -1166,6 +1166,10 @@ def main():
     e2e_s, e2e_rays = aggregate(e2e_s, e2e_rays, dist, dev)
     e2e_v = e2e_rays / e2e_s / 1e6
     band_rows = row_e - row_b
+    # the host-pointer path's records (pipelined bands on two streams) against the
+    # device path's records of the same frame, this rank's rows
+    e2e_diff = int((out_h.view(H, W, 8)[row_b:row_e] != outs[best].cpu().view(H, W, 8)[row_b:row_e]).any(-1).sum() +
+                   (bounce_h.view(H, W, 4)[row_b:row_e] != bounces[best].cpu().view(H, W, 4)[row_b:row_e]).any(-1).sum())
     e2e_h2d = int(tx * ty * 68 + 240)
     e2e_d2h = int(tx * ty * 68 + W * H * 48) if world == 1 else int(W * band_rows * 48)
 
@@ -1242,7 +1246,8 @@ def main():
             "hit_ids": {"primary_records_differing": prim_mismatch, "bounce_records_differing": bnc_mismatch,
                         "shadow_masks_differing": mask_mismatch, "pixels": W * (row_e - row_b),
                         "compared": "plain vs quantised records of the same frame (rank 0's rows)"},
-            "e2e": {"value": e2e_v, "unit": METRIC, "h2d_bytes_per_step": e2e_h2d, "d2h_bytes_per_step": e2e_d2h},
+            "e2e": {"value": e2e_v, "unit": METRIC, "h2d_bytes_per_step": e2e_h2d, "d2h_bytes_per_step": e2e_d2h,
+                    "records_differing_vs_device_path": e2e_diff},
             "gpu_launches": None, "clocks": clocks,
         }
         # our kernels per frame: cull, primary trace, secondary generation, kind prefix, secondary trace, ray count

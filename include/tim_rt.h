@@ -398,9 +398,9 @@ int tim_rt_server_destroy(tim_rt_server *srv);
 #define TIM_RT_CAM_BOUNCE 4u
 #define TIM_RT_CAM_WIDE 0x100u   /* use the quantised 8-wide BVH */
 #define TIM_RT_CAM_COUNT 0x200u  /* counting kernel variant; fills the work counters of tim_rt_stats */
-#define TIM_RT_CAM_PIPELINED 0x800u /* tim_rt_trace_camera only: trace the frame in up to 4 bands of rows and copy
-                                       each band's results to the host while the next band traces (same results;
-                                       the stats' phase split is then not reported) */
+#define TIM_RT_CAM_PIPELINED 0x800u /* tim_rt_trace_camera only: copy the results to the host in up to 8 bands of
+                                       rows while the frame traces: the secondary rays are traced band by band and
+                                       each band's copy starts as soon as its records are final (same results) */
 #define TIM_RT_CAM_PRIMARY_BINARY 0x400u /* with TIM_RT_CAM_WIDE: primary rays take the binary walk (faster for
                                           coherent camera rays here; both walks give identical results) */
 int tim_rt_trace_camera(tim_rt_ctx *ctx, tim_rt_scene_id scene, const tim_rt_pass_data *pd, uint32_t flags,

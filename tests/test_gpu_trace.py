@@ -399,3 +399,35 @@ def test_camera_leaf_lights_and_counts(ctx, native, oracle_mod, wide):
                 assert st.secondary_rays_counted == st.rays - st.primary_rays
     finally:
         ctx.free_scene(sid)
+
+
+def test_camera_pipelined_bands_without_secondary_rays(ctx, native, oracle_mod):
+    """TIM_RT_CAM_PIPELINED on a frame whose hits fall in a few of its 8 bands: the
+    bands without secondary rays are flagged final before the secondary trace and
+    copied at once, the others as they complete; records equal the oracle's."""
+    from tim_raytracing_b200 import scenes
+    s = scenes.random_triangles(31, 300)
+    img = native.build_bvh(s)
+    sid = ctx.upload(img, s)
+    try:
+        W, H = 96, 512
+        lo, hi = img.aabb[:3], img.aabb[3:]
+        c, e = (lo + hi) / 2, hi - lo
+        pd = scenes.pass_data(s, W, H, cam_pos=c + np.array([0.0, -4.0 * e[1], 0.0]), cam_target=c, aabb=(lo, hi))
+        sc = oracle_mod.Scene(img, s.positions, s.normals)
+        o_out, o_bounce, o_counts = oracle_mod.camera(sc, pd, flags=native.CAM_BOUNCE, seed=1)
+        hit_rows = (o_out[:, 3].view(np.float32).reshape(H, W) < 100.0).sum(1)
+        band_hits = hit_rows.reshape(8, 64).sum(1)
+        assert (band_hits == 0).sum() >= 3 and (band_hits > 0).sum() >= 2
+        for form in (0, native.CAM_WIDE):
+            if form:
+                ctx.free_scene(sid)
+                sid = ctx.upload(img, s, quant8=True)
+            for _ in range(2):
+                out, bounce, st = ctx.trace_camera(sid, pd, flags=native.CAM_BOUNCE | native.CAM_PIPELINED | form,
+                                                   seed=1)
+                assert np.array_equal(out, o_out)
+                assert np.array_equal(bounce, o_bounce)
+                assert st.rays == int(o_counts.sum())
+    finally:
+        ctx.free_scene(sid)

@@ -236,7 +236,9 @@ int tim_rt_create(int device, uint64_t mem_budget_bytes, tim_rt_ctx** out) {
     for (auto& e : c->ev) TIMRT_CUDA(cudaEventCreate(&e));
     for (auto& e : c->pev) TIMRT_CUDA(cudaEventCreate(&e));
     TIMRT_CUDA(cudaStreamCreateWithFlags(&c->cstream, cudaStreamNonBlocking));
-    for (auto& e : c->bev) TIMRT_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    TIMRT_CUDA(cudaEventCreateWithFlags(&c->copy_ev, cudaEventDisableTiming));
+    TIMRT_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&c->band_flags), 4ull * kMaxCamBands, cudaHostAllocMapped));
+    TIMRT_CUDA(cudaHostGetDevicePointer(reinterpret_cast<void**>(&c->band_flags_dev), c->band_flags, 0));
     int rc = dev_alloc(c.get(), c->counters, 4ull * kCounterWords);
     if (rc) return rc;
     if ((rc = dev_alloc(c.get(), c->dstats, 256))) return rc;   // 16 counter words + 16 verification words
@@ -264,14 +266,15 @@ int tim_rt_destroy(tim_rt_ctx* c) {
     c->scenes.clear();
     for (DevBuf* b : {&c->rays, &c->hits, &c->nid, &c->bary, &c->counters, &c->cam_out, &c->cam_bounce, &c->cam_nid,
                       &c->q_rays, &c->q_pixel, &c->tiles_counts, &c->tiles_lists, &c->dstats, &c->p_dirs, &c->p_basis,
-                      &c->p_out, &c->p_nid, &c->p_irr, &c->p_sh16, &c->p_sh32, &c->p_octa, &c->sh_out, &c->sh_f32, &c->bld, &c->ray_acc})
+                      &c->p_out, &c->p_nid, &c->p_irr, &c->p_sh16, &c->p_sh32, &c->p_octa, &c->sh_out, &c->sh_f32, &c->bld, &c->ray_acc,
+                      &c->band_ctr})
         dev_free(c, *b);
     for (auto& e : c->ev)
         if (e) cudaEventDestroy(e);
     for (auto& e : c->pev)
         if (e) cudaEventDestroy(e);
-    for (auto& e : c->bev)
-        if (e) cudaEventDestroy(e);
+    if (c->copy_ev) cudaEventDestroy(c->copy_ev);
+    if (c->band_flags) cudaFreeHost(c->band_flags);
     if (c->cstream) {
         cudaStreamSynchronize(c->cstream);
         cudaStreamDestroy(c->cstream);
@@ -884,58 +887,62 @@ int tim_rt_trace_camera(tim_rt_ctx* c, tim_rt_scene_id id, const tim_rt_pass_dat
     const bool count = (flags & TIM_RT_CAM_COUNT) != 0;
     if (count) TIMRT_CUDA(cudaMemsetAsync(c->dstats.ptr, 0, 128, c->stream));
     LaunchConfig cam_cfg = cfg_for(c, s, (flags & TIM_RT_CAM_WIDE) != 0, count);
-    // TIM_RT_CAM_PIPELINED: horizontal bands of output rows; each band's records go
-    // down on the copy stream while the next band traces
+    // TIM_RT_CAM_PIPELINED: bands of output rows (equal, at least 64 rows each, up to
+    // 8). The frame traces as one launch sequence whose secondary trace takes the
+    // bands in order and raises each band's host flag once its records are final;
+    // this thread starts each band's copy as soon as its flag is up, so the copies
+    // run while the later bands trace.
     const uint32_t tile_rows = (H + 3u) / 4u;
-    constexpr uint32_t kMaxBands = sizeof(c->bev) / sizeof(c->bev[0]);   // one band-end event each
-    const uint32_t bands = (flags & TIM_RT_CAM_PIPELINED) ? std::min<uint32_t>(kMaxBands, std::max<uint32_t>(1u, tile_rows / 16u))
+    const uint32_t bands = (flags & TIM_RT_CAM_PIPELINED) ? std::min<uint32_t>(kMaxCamBands, std::max<uint32_t>(1u, tile_rows / 16u))
                                                            : 1u;
-    cam_cfg.phase_ev = bands == 1u ? c->pev : nullptr;
+    CameraBands cb{};
+    cb.n = bands;
+    for (uint32_t b = 0; b < bands; ++b) cb.row[b] = 4u * (uint32_t)((uint64_t)tile_rows * b / bands);
+    cb.row[bands] = H;
+    uint32_t* cctr = ctr;
+    if (bands > 1u) {
+        if ((rc = ensure(c, c->band_ctr, 4ull * cam_counter_words(kMaxCamBands)))) return rc;
+        cctr = static_cast<uint32_t*>(c->band_ctr.ptr);
+        for (uint32_t b = 0; b < kMaxCamBands; ++b) c->band_flags[b] = 0u;   // no kernel of this context runs
+        cb.flags = c->band_flags_dev;
+    }
+    cam_cfg.phase_ev = c->pev;
     uint64_t* acc = static_cast<uint64_t*>(c->ray_acc.ptr);
     TIMRT_CUDA(cudaMemsetAsync(acc, 0, 8, c->stream));
+    TIMRT_CUDA(cudaMemsetAsync(cctr, 0, 4ull * cam_counter_words(bands), c->stream));
     TIMRT_CUDA(cudaEventRecord(c->ev[1], c->stream));
-    // band sizes shrink geometrically (ratio 0.7, about the copy / trace time ratio per
-    // row) so each band's copy hides under the next band's trace and the last copy,
-    // which nothing hides, is small
-    uint32_t edge[kMaxBands + 1] = {};
-    {
-        double w[kMaxBands], sum = 0.0;
-        for (uint32_t b = 0; b < bands; ++b) sum += (w[b] = std::pow(0.7, (double)b));
-        double acc = 0.0;
-        for (uint32_t b = 0; b < bands; ++b) {
-            acc += w[b];
-            edge[b + 1] = b + 1u == bands ? tile_rows : std::min(tile_rows, (uint32_t)(tile_rows * (acc / sum) + 0.5));
-        }
-    }
-    for (uint32_t b = 0; b < bands; ++b) {
-        const uint32_t r0 = 4u * edge[b], r1 = std::min(H, 4u * edge[b + 1]);
-        if (r0 >= r1) continue;
-        TIMRT_CUDA(cudaMemsetAsync(ctr, 0, 4 * kCamCounterWords, c->stream));
-        TIMRT_CUDA(launch_camera(s->view, *pd, flags, seed, static_cast<const uint32_t*>(c->tiles_counts.ptr),
-                                 static_cast<const uint32_t*>(c->tiles_lists.ptr), static_cast<uint32_t*>(c->cam_out.ptr),
-                                 (flags & TIM_RT_CAM_BOUNCE) ? static_cast<uint32_t*>(c->cam_bounce.ptr) : nullptr,
-                                 static_cast<uint32_t*>(c->cam_nid.ptr), static_cast<tim_rt_ray*>(c->q_rays.ptr),
-                                 static_cast<uint32_t*>(c->q_pixel.ptr), (uint32_t)qcap, ctr, ctr + kErrWord, acc,
-                                 c->stream, cam_cfg, r0, r1));
-        if (bands > 1u) {
-            const uint64_t p0 = (uint64_t)W * r0, np = (uint64_t)W * (r1 - r0);
-            TIMRT_CUDA(cudaEventRecord(c->bev[b], c->stream));
-            TIMRT_CUDA(cudaStreamWaitEvent(c->cstream, c->bev[b], 0));
-            TIMRT_CUDA(cudaMemcpyAsync(out + 8ull * p0, static_cast<uint32_t*>(c->cam_out.ptr) + 8ull * p0, 32ull * np,
-                                       cudaMemcpyDeviceToHost, c->cstream));
-            if (flags & TIM_RT_CAM_BOUNCE)
-                TIMRT_CUDA(cudaMemcpyAsync(bounce_out + 4ull * p0, static_cast<uint32_t*>(c->cam_bounce.ptr) + 4ull * p0,
-                                           16ull * np, cudaMemcpyDeviceToHost, c->cstream));
-        }
-    }
+    TIMRT_CUDA(launch_camera(s->view, *pd, flags, seed, static_cast<const uint32_t*>(c->tiles_counts.ptr),
+                             static_cast<const uint32_t*>(c->tiles_lists.ptr), static_cast<uint32_t*>(c->cam_out.ptr),
+                             (flags & TIM_RT_CAM_BOUNCE) ? static_cast<uint32_t*>(c->cam_bounce.ptr) : nullptr,
+                             static_cast<uint32_t*>(c->cam_nid.ptr), static_cast<tim_rt_ray*>(c->q_rays.ptr),
+                             static_cast<uint32_t*>(c->q_pixel.ptr), (uint32_t)qcap, cctr, ctr + kErrWord, acc,
+                             c->stream, cam_cfg, 0u, H, &cb));
     TIMRT_CUDA(cudaEventRecord(c->ev[2], c->stream));
     if (bands == 1u) {
         TIMRT_CUDA(cudaMemcpyAsync(out, c->cam_out.ptr, 32ull * npix, cudaMemcpyDeviceToHost, c->stream));
         if (flags & TIM_RT_CAM_BOUNCE)
             TIMRT_CUDA(cudaMemcpyAsync(bounce_out, c->cam_bounce.ptr, 16ull * npix, cudaMemcpyDeviceToHost, c->stream));
     } else {
-        TIMRT_CUDA(cudaEventRecord(c->bev[bands - 1u], c->cstream));
-        TIMRT_CUDA(cudaStreamWaitEvent(c->stream, c->bev[bands - 1u], 0));
+        // Band b's copy starts when its flag is up. Should the trace end without a
+        // flag (an error ended a kernel early), the remaining copies wait for its end.
+        bool ended = false;
+        for (uint32_t b = 0; b < bands;) {
+            if (!ended && !reinterpret_cast<volatile uint32_t*>(c->band_flags)[b]) {
+                const cudaError_t q = cudaEventQuery(c->ev[2]);
+                if (q == cudaErrorNotReady) continue;
+                ended = true;
+                TIMRT_CUDA(cudaStreamWaitEvent(c->cstream, c->ev[2], 0));
+            }
+            const uint64_t p0 = (uint64_t)W * cb.row[b], np = (uint64_t)W * (cb.row[b + 1] - cb.row[b]);
+            TIMRT_CUDA(cudaMemcpyAsync(out + 8ull * p0, static_cast<uint32_t*>(c->cam_out.ptr) + 8ull * p0, 32ull * np,
+                                       cudaMemcpyDeviceToHost, c->cstream));
+            if (flags & TIM_RT_CAM_BOUNCE)
+                TIMRT_CUDA(cudaMemcpyAsync(bounce_out + 4ull * p0, static_cast<uint32_t*>(c->cam_bounce.ptr) + 4ull * p0,
+                                           16ull * np, cudaMemcpyDeviceToHost, c->cstream));
+            ++b;
+        }
+        TIMRT_CUDA(cudaEventRecord(c->copy_ev, c->cstream));
+        TIMRT_CUDA(cudaStreamWaitEvent(c->stream, c->copy_ev, 0));
     }
     uint64_t traced = 0;
     TIMRT_CUDA(cudaMemcpyAsync(&traced, acc, 8, cudaMemcpyDeviceToHost, c->stream));
@@ -950,11 +957,9 @@ int tim_rt_trace_camera(tim_rt_ctx* c, tim_rt_scene_id id, const tim_rt_pass_dat
         stats->shadow_rays = traced - primary;   // all secondary rays (shadow, probe-visibility, bounce)
         cudaEventElapsedTime(&stats->kernel_ms, c->ev[1], c->ev[2]);
         cudaEventElapsedTime(&stats->total_ms, c->ev[0], c->ev[3]);
-        if (bands == 1u) {
-            cudaEventElapsedTime(&stats->primary_ms, c->pev[0], c->pev[1]);
-            cudaEventElapsedTime(&stats->gen_ms, c->pev[1], c->pev[2]);
-            cudaEventElapsedTime(&stats->secondary_ms, c->pev[2], c->pev[3]);
-        }
+        cudaEventElapsedTime(&stats->primary_ms, c->pev[0], c->pev[1]);
+        cudaEventElapsedTime(&stats->gen_ms, c->pev[1], c->pev[2]);
+        cudaEventElapsedTime(&stats->secondary_ms, c->pev[2], c->pev[3]);
         if (count) read_counts(c, stats);
     }
     return TIM_RT_OK;

@@ -55,7 +55,10 @@ struct tim_rt_ctx {
     cudaEvent_t ev[4] = {};
     cudaEvent_t pev[4] = {};   // camera phases
     cudaStream_t cstream = nullptr;   // result copies overlapped with tracing (TIM_RT_CAM_PIPELINED)
-    cudaEvent_t bev[4] = {};          // end of each band of a pipelined camera trace
+    cudaEvent_t copy_ev = nullptr;    // the copies of a pipelined camera trace are done
+    DevBuf band_ctr;                  // counters of a pipelined camera trace (cam_counter_words(kMaxCamBands))
+    uint32_t* band_flags = nullptr;   // per band: records final (pinned host memory the device writes)
+    uint32_t* band_flags_dev = nullptr;
     DevBuf ray_acc;                   // rays traced by a pipelined camera trace (u64)
     LaunchConfig cfg;
     std::set<tim_rt_batch*> batches;

@@ -57,18 +57,36 @@ cudaError_t launch_trace_batch(const SceneView& s, const tim_rt_ray* rays, uint3
                                uint32_t* nid, float* bary, uint32_t* counter, uint32_t* err, cudaStream_t stream,
                                const LaunchConfig& cfg);
 
-// Secondary rays are queued in camera_queue_kinds() segments of seg_cap = W*H slots.
-// row_begin / row_end restrict a launch to a band of output rows (row_begin a
-// multiple of 4); counters must be cleared before each launch.
-// counters: [0] pixel work, [1] secondary work, [2..27] per-kind counts,
-// [28..54] per-kind prefix ([54] = secondary rays traced).
+// A camera trace whose results go down in bands of output rows while it runs:
+// band b covers rows [row[b], row[b+1]) (row[0] = 0, row[n] = H, the others
+// multiples of 4). Primary rays and their secondary rays are generated for the
+// whole frame at once, each band's secondary rays in its own part of the queue,
+// and the one secondary launch takes the bands in order, counting finished rays
+// per band and setting flags[b] (host memory the device writes) once band b's
+// records are final, so a host thread can start that band's copy.
+constexpr uint32_t kMaxCamBands = 8;
+struct CameraBands {
+    uint32_t n;
+    uint32_t row[kMaxCamBands + 1];
+    volatile uint32_t* flags;   // device address of the host flags
+};
+
+// Secondary rays are queued in camera_queue_kinds() segments of seg_cap = W*H slots
+// (with bands, band b's segments hold the band's pixels each). row_begin / row_end
+// restrict a launch to a band of output rows (row_begin a multiple of 4; no bands);
+// counters must be cleared before each launch. counters (nb bands, 1 without):
+// [0] pixel work, [1] secondary work, [2, 2 + 26 nb) per-band per-kind counts,
+// [2 + 26 nb, 3 + 52 nb) their prefix (the last entry = secondary rays traced),
+// [3 + 52 nb, 3 + 53 nb) finished rays per band.
 uint32_t camera_queue_kinds();
-constexpr uint32_t kCamCounterWords = 55, kCamTotalWord = 54;
+constexpr uint32_t cam_counter_words(uint32_t nb) { return 3u + 53u * nb; }
+constexpr uint32_t kCamCounterWords = cam_counter_words(1), kCamTotalWord = 54;
 cudaError_t launch_camera(const SceneView& s, const tim_rt_pass_data& pd, uint32_t flags, uint32_t seed,
                           const uint32_t* tile_counts, const uint32_t* tile_lists, uint32_t* out, uint32_t* bounce_out,
                           uint32_t* leaf_nid, tim_rt_ray* q_rays, uint32_t* q_pixel, uint32_t seg_cap,
                           uint32_t* counters, uint32_t* err, uint64_t* d_ray_count, cudaStream_t stream,
-                          const LaunchConfig& cfg, uint32_t row_begin = 0, uint32_t row_end = 0xFFFFFFFFu);
+                          const LaunchConfig& cfg, uint32_t row_begin = 0, uint32_t row_end = 0xFFFFFFFFu,
+                          const CameraBands* bands = nullptr);
 
 // One job of a batched multi-scene trace (device table entry).
 struct MultiJob {

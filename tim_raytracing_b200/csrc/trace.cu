@@ -26,6 +26,22 @@ namespace timrt {
 // Secondary-ray kinds, one queue segment each.
 constexpr uint32_t kKindSun = 0, kKindLight0 = 1, kKindProbe0 = 17, kKindBounce = 25, kNumKinds = 26;
 
+// The secondary queue split into bands of output rows (one band unless a camera
+// trace is pipelined): band b's rays of kind k take cap[b] slots from
+// base[b] + k * cap[b]; its counts and prefix entries are b * kNumKinds + k.
+struct QueueBands {
+    uint32_t n;
+    uint32_t row[kMaxCamBands + 1];   // band b: output rows [row[b], row[b + 1])
+    uint32_t base[kMaxCamBands];
+    uint32_t cap[kMaxCamBands];
+};
+
+__device__ __forceinline__ uint32_t band_of_row(const QueueBands& q, uint32_t r) {
+    uint32_t b = 0;
+    for (uint32_t k = 1; k < q.n; ++k) b += r >= q.row[k] ? 1u : 0u;
+    return b;
+}
+
 // Work item -> pixel in 8x4 tiles (row-major tiles over the frame).
 __device__ __forceinline__ bool tile_pixel(uint32_t i, uint32_t W, uint32_t H, uint32_t& px, uint32_t& py) {
     const uint32_t tiles_x = (W + 7u) >> 3;
@@ -46,6 +62,12 @@ template <class P, class = void>
 struct leaf_kind { static constexpr int value = kLeafOne; };
 template <class P>
 struct leaf_kind<P, decltype((void)P::kLeaf)> { static constexpr int value = P::kLeaf; };
+// Whether a policy wants its finished() hook called by the whole warp after each
+// round of stores.
+template <class P, class = void>
+struct finishes { static constexpr bool value = false; };
+template <class P>
+struct finishes<P, decltype((void)P::kFinishes)> { static constexpr bool value = P::kFinishes; };
 
 struct BatchPolicy {
     const tim_rt_ray* rays;
@@ -141,26 +163,32 @@ struct CameraPolicy {
     }
 };
 
-// Secondary rays queued by kind: segment k holds seg_cap slots; prefix[k] is
-// the first work item of kind k and prefix[kNumKinds] the total.
-// ray.flags: bit 0 any-hit, bits 8..15 the mask bit, bits 16..17 the output
-// (0 shadow mask, 1 probe mask, 2 bounce record).
+// Secondary rays queued by band and kind (QueueBands); prefix[b * kNumKinds + k] is
+// the first work item of band b's kind k and prefix[n * kNumKinds] the total, so
+// work items run band by band. ray.flags: bit 0 any-hit, bits 8..15 the mask
+// bit, bits 16..17 the output (0 shadow mask, 1 probe mask, 2 bounce record).
+// With done / flags (a pipelined camera trace), finished rays are counted per
+// band and flags[b] is set once all of band b's rays are stored.
 struct SecondaryPolicy {
+    static constexpr bool kFinishes = true;
     const tim_rt_ray* rays;
     const uint32_t* pixel;
     const uint32_t* prefix;
-    uint32_t seg_cap;
+    QueueBands qb;
     uint32_t* out_words;    // tracingData as u32 words (8 per pixel)
     uint4* bounce_out;
+    uint32_t* done;         // finished rays per band, or null
+    volatile uint32_t* flags;
 
     __device__ __forceinline__ bool load(const SceneView&, uint32_t i, TravState& st) const {
-        uint32_t lo = 0, hi = kNumKinds;   // largest k with prefix[k] <= i
+        uint32_t lo = 0, hi = qb.n * kNumKinds;   // largest segment k with prefix[k] <= i
         while (hi - lo > 1u) {
             const uint32_t mid = (lo + hi) >> 1;
             if (__ldg(prefix + mid) <= i) lo = mid;
             else hi = mid;
         }
-        const uint32_t slot = lo * seg_cap + (i - __ldg(prefix + lo));
+        const uint32_t band = lo / kNumKinds, kind = lo - band * kNumKinds;
+        const uint32_t slot = qb.base[band] + kind * qb.cap[band] + (i - __ldg(prefix + lo));
         st.slot = slot;
         const float4* rp = reinterpret_cast<const float4*>(rays + slot);
         const float4 a = __ldg(rp), b = __ldg(rp + 1);
@@ -170,6 +198,30 @@ struct SecondaryPolicy {
         st.any = (__float_as_uint(b.w) & 1u) != 0u;
         st.dup_ok = true;   // bounce rays store the hit record only
         return true;
+    }
+    // Called by all 32 lanes after a round of stores (`stored`: this lane stored
+    // the ray in queue slot `slot`): one count per band and warp, after each
+    // storing lane has fenced its stores; the count that completes a band raises
+    // the band's flag.
+    __device__ __forceinline__ void finished(bool stored, uint32_t slot) const {
+        if (!done) return;
+        uint32_t band = 0xFFFFFFFFu;
+        if (stored) {
+            band = 0;
+            for (uint32_t k = 1; k < qb.n; ++k) band += slot >= qb.base[k] ? 1u : 0u;
+            __threadfence();
+        }
+        const uint32_t peers = __match_any_sync(0xFFFFFFFFu, band);
+        __syncwarp();
+        const uint32_t lane = threadIdx.x & 31u;
+        if (stored && lane == (uint32_t)(__ffs(peers) - 1)) {
+            const uint32_t total = __ldg(prefix + (band + 1u) * kNumKinds) - __ldg(prefix + band * kNumKinds);
+            const uint32_t cnt = (uint32_t)__popc(peers);
+            if (atomicAdd(done + band, cnt) + cnt == total) {
+                __threadfence_system();
+                flags[band] = 1u;
+            }
+        }
     }
     __device__ __forceinline__ void store(const SceneView&, uint32_t, const TravState& st, float) const {
         const uint32_t slot = st.slot;
@@ -217,6 +269,7 @@ __global__ void __launch_bounds__(BLOCK, WIDE ? 896 / BLOCK : 1024 / BLOCK) k_pe
         // batches, which keeps coherent rays of a batch in lockstep); after the
         // last ray was handed out, finish pending lanes as they come
         if (idle && (exhausted || __popc(idle) >= refill_min || idle == 0xFFFFFFFFu)) {
+            const bool stored = pending;
             if (pending) {
                 pending = false;
                 if (WIDE) wide_finish_or_walk(s, st, err);
@@ -229,6 +282,7 @@ __global__ void __launch_bounds__(BLOCK, WIDE ? 896 / BLOCK : 1024 / BLOCK) k_pe
                     atomicAdd(stats + 4, (unsigned long long)st.c_reload);
                 }
             }
+            if constexpr (finishes<Policy>::value) P.finished(stored, st.slot);
             if (!exhausted) {
                 const uint32_t need = __ballot_sync(0xFFFFFFFFu, !active);
                 const int leader = __ffs(need) - 1;
@@ -313,8 +367,8 @@ struct GenParams {
     uint4* bounce_out;
     tim_rt_ray* q_rays;
     uint32_t* q_pixel;
-    uint32_t* q_counts;     // kNumKinds counters
-    uint32_t seg_cap;
+    uint32_t* q_counts;     // counters [band][kind]
+    QueueBands qb;
     uint32_t item0, item1;  // work items (8x4-pixel tile order) of this launch
 };
 
@@ -329,21 +383,24 @@ __device__ __forceinline__ void lpf_position(const tim_rt_pass_data& pd, uint32_
     z = pd.sceneMinExtent[2] + stz * ((float)cz + 0.5f);
 }
 
-// Appends one ray of `kind` for the lanes with has == true: warp-aggregated
-// atomic on the kind's counter, lane order preserved inside the segment.
-__device__ __forceinline__ void emit(const GenParams& g, uint32_t kind, bool has, uint32_t pix, float ox, float oy,
-                                     float oz, float tmax, float dx, float dy, float dz, uint32_t flags) {
+// Appends one ray of `kind` to the warp's band (uniform across the warp) for the
+// lanes with has == true: warp-aggregated atomic on the band's kind counter,
+// lane order preserved inside the segment.
+__device__ __forceinline__ void emit(const GenParams& g, uint32_t band, uint32_t kind, bool has, uint32_t pix,
+                                     float ox, float oy, float oz, float tmax, float dx, float dy, float dz,
+                                     uint32_t flags) {
     const uint32_t m = __ballot_sync(0xFFFFFFFFu, has);
     if (!m) return;
     const uint32_t lane = threadIdx.x & 31u;
     const int leader = __ffs(m) - 1;
     uint32_t base = 0;
-    if ((int)lane == leader) base = atomicAdd(g.q_counts + kind, (uint32_t)__popc(m));
+    if ((int)lane == leader) base = atomicAdd(g.q_counts + band * kNumKinds + kind, (uint32_t)__popc(m));
     base = __shfl_sync(0xFFFFFFFFu, base, leader);
     if (has) {
         const uint32_t off = base + __popc(m & lanemask_lt());
-        if (off < g.seg_cap) {
-            const uint64_t slot = (uint64_t)kind * g.seg_cap + off;
+        const uint32_t cap = g.qb.cap[band];
+        if (off < cap) {
+            const uint64_t slot = (uint64_t)g.qb.base[band] + (uint64_t)kind * cap + off;
             float4* rp = reinterpret_cast<float4*>(g.q_rays + slot);
             rp[0] = make_float4(ox, oy, oz, tmax);
             rp[1] = make_float4(dx, dy, dz, __uint_as_float(flags));
@@ -365,6 +422,8 @@ __global__ void __launch_bounds__(256) k_gen_secondary(SceneView s, GenParams g)
     uint32_t px = 0, py = 0;
     const bool valid = i < g.item1 && tile_pixel(i, W, H, px, py);
     const uint32_t pix = py * W + px;
+    // the warp's band: all its pixels lie in one 8x4 tile, bands end on tile rows
+    const uint32_t band = band_of_row(g.qb, (i >> 5) / ((W + 7u) >> 3) * 4u);
     uint4 rec = make_uint4(0, 0, 0, 0);
     if (valid) rec = reinterpret_cast<const uint4*>(g.out_words)[2u * pix];
     const float t = __uint_as_float(rec.w);
@@ -379,7 +438,7 @@ __global__ void __launch_bounds__(256) k_gen_secondary(SceneView s, GenParams g)
         hz = pd.cameraPos[2] + dz * t;
     }
     // sun ray, tmax = TMAX (bvhLighting.glsl:148-149)
-    emit(g, kKindSun, hit, pix, hx, hy, hz, kTMax, -pd.sunDir[0], -pd.sunDir[1], -pd.sunDir[2], 1u);
+    emit(g, band, kKindSun, hit, pix, hx, hy, hz, kTMax, -pd.sunDir[0], -pd.sunDir[1], -pd.sunDir[2], 1u);
     // light list of the tile or of the hit leaf
     const uint32_t* list = nullptr;
     uint32_t count = 0;
@@ -417,7 +476,7 @@ __global__ void __launch_bounds__(256) k_gen_secondary(SceneView s, GenParams g)
                 else direct_bits |= 1u << bit;   // out of range counts as masked
             }
         }
-        emit(g, kKindLight0 + j, has, pix, hx, hy, hz, rl, lx / rl, ly / rl, lz / rl, 1u | (bit << 8));
+        emit(g, band, kKindLight0 + j, has, pix, hx, hy, hz, rl, lx / rl, ly / rl, lz / rl, 1u | (bit << 8));
     }
     if (g.flags & TIM_RT_CAM_PROB_MASK) {
         // lightprobHelpers.glsl:71-77 getLightProbCoordUVW and bvhLighting.glsl:170-180
@@ -441,7 +500,8 @@ __global__ void __launch_bounds__(256) k_gen_secondary(SceneView s, GenParams g)
         for (uint32_t k = 0; k < 8u; ++k) {
             float qx = 0.f, qy = 0.f, qz = 0.f;
             if (hit) lpf_position(pd, cx + (k & 1u), cy + ((k >> 1) & 1u), cz + ((k >> 2) & 1u), qx, qy, qz);
-            emit(g, kKindProbe0 + k, hit, pix, hx, hy, hz, 1.0f, qx - hx, qy - hy, qz - hz, 1u | (k << 8) | (1u << 16));
+            emit(g, band, kKindProbe0 + k, hit, pix, hx, hy, hz, 1.0f, qx - hx, qy - hy, qz - hz,
+                 1u | (k << 8) | (1u << 16));
         }
     }
     if (g.flags & TIM_RT_CAM_BOUNCE) {
@@ -458,7 +518,7 @@ __global__ void __launch_bounds__(256) k_gen_secondary(SceneView s, GenParams g)
             if (dot3(nx, ny, nz, dx, dy, dz) > 0.0f) { nx = -nx; ny = -ny; nz = -nz; }
             bounce_dir(nx, ny, nz, pix, g.seed, bx, by, bz);
         }
-        emit(g, kKindBounce, hit, pix, hx, hy, hz, kTMax, bx, by, bz, 2u << 16);
+        emit(g, band, kKindBounce, hit, pix, hx, hy, hz, kTMax, bx, by, bz, 2u << 16);
     }
     if (valid) {
         g.out_words[8u * pix + 4u] = direct_bits;
@@ -467,14 +527,23 @@ __global__ void __launch_bounds__(256) k_gen_secondary(SceneView s, GenParams g)
     }
 }
 
-// prefix[k] = first work item of kind k over the (capacity-clamped) segment counts.
-__global__ void k_kind_prefix(const uint32_t* q_counts, uint32_t* prefix, uint32_t cap) {
+// prefix[b * kNumKinds + k] = first work item of band b's kind k over the
+// (capacity-clamped) segment counts. A band without secondary rays is final
+// already: its flag (when there are flags) is raised here.
+__global__ void k_kind_prefix(const uint32_t* q_counts, uint32_t* prefix, QueueBands qb, volatile uint32_t* flags) {
     uint32_t acc = 0;
-    for (uint32_t k = 0; k < kNumKinds; ++k) {
-        prefix[k] = acc;
-        acc += min(q_counts[k], cap);
+    for (uint32_t b = 0; b < qb.n; ++b) {
+        const uint32_t first = acc;
+        for (uint32_t k = 0; k < kNumKinds; ++k) {
+            prefix[b * kNumKinds + k] = acc;
+            acc += min(q_counts[b * kNumKinds + k], qb.cap[b]);
+        }
+        if (flags && acc == first) {
+            __threadfence_system();
+            flags[b] = 1u;
+        }
     }
-    prefix[kNumKinds] = acc;
+    prefix[qb.n * kNumKinds] = acc;
 }
 
 // Adds the frame's ray count (primary rays of rows 1..H-1 plus the secondary queue).
@@ -623,19 +692,40 @@ cudaError_t launch_camera(const SceneView& s, const tim_rt_pass_data& pd, uint32
                           const uint32_t* tile_counts, const uint32_t* tile_lists, uint32_t* out, uint32_t* bounce_out,
                           uint32_t* leaf_nid, tim_rt_ray* q_rays, uint32_t* q_pixel, uint32_t seg_cap,
                           uint32_t* counters, uint32_t* err, uint64_t* d_ray_count, cudaStream_t stream,
-                          const LaunchConfig& cfg, uint32_t row_begin, uint32_t row_end) {
+                          const LaunchConfig& cfg, uint32_t row_begin, uint32_t row_end, const CameraBands* bands) {
     const uint32_t W = pd.frameSize[0], H = pd.frameSize[1];
     // output rows [row_begin, row_end): whole rows of 8x4-pixel tiles (row_begin a multiple of 4)
     row_end = min(row_end, H);
     if (row_begin >= row_end) return cudaSuccess;
+    // the queue's bands: one (the launch's rows, segments of seg_cap slots), or the
+    // caller's bands of the whole frame (segments of each band's pixels)
+    QueueBands qb{};
+    qb.n = 1;
+    qb.row[0] = row_begin;
+    qb.row[1] = row_end;
+    qb.cap[0] = seg_cap;
+    if (bands && bands->n > 1u) {
+        if (bands->n > kMaxCamBands || row_begin != 0u || row_end != H || seg_cap != W * H) return cudaErrorInvalidValue;
+        qb.n = bands->n;
+        for (uint32_t b = 0; b <= qb.n; ++b) qb.row[b] = bands->row[b];
+        if (qb.row[0] != 0u || qb.row[qb.n] != H) return cudaErrorInvalidValue;
+        for (uint32_t b = 0; b < qb.n; ++b) {
+            if (qb.row[b + 1] <= qb.row[b] || qb.row[b] % 4u != 0u) return cudaErrorInvalidValue;
+            qb.base[b] = kNumKinds * W * qb.row[b];
+            qb.cap[b] = W * (qb.row[b + 1] - qb.row[b]);
+        }
+    }
+    volatile uint32_t* flags_host = bands && bands->n > 1u ? bands->flags : nullptr;
     const uint32_t tiles_x = (W + 7u) >> 3;
     const uint32_t item0 = (row_begin >> 2) * tiles_x * 32u;
     const uint32_t item1 = min(tiled_work_items(W, H), ((row_end + 3u) >> 2) * tiles_x * 32u);
     const uint32_t items = item1 - item0;
     const uint32_t ngy16 = 16u * ((H + 15u) / 16u);
-    // counters: [0] pixel work, [1] secondary work, [2..27] kind counts, [28..54] kind prefix
+    // counters: [0] pixel work, [1] secondary work, then the bands' kind counts, their
+    // prefix and the bands' finished rays
     uint32_t* q_counts = counters + 2;
-    uint32_t* prefix = counters + 2 + kNumKinds;
+    uint32_t* prefix = counters + 2 + kNumKinds * qb.n;
+    uint32_t* done = prefix + kNumKinds * qb.n + 1u;
     CameraPolicy CP{pd, ngy16, reinterpret_cast<uint4*>(out), leaf_nid, item0};
     if (cfg.phase_ev) cudaEventRecord(cfg.phase_ev[0], stream);
     // primary rays: a warp refills only when all 32 lanes are idle, so it always
@@ -662,23 +752,25 @@ cudaError_t launch_camera(const SceneView& s, const tim_rt_pass_data& pd, uint32
     g.q_rays = q_rays;
     g.q_pixel = q_pixel;
     g.q_counts = q_counts;
-    g.seg_cap = seg_cap;
+    g.qb = qb;
     g.item0 = item0;
     g.item1 = item1;
     k_gen_secondary<<<(items + 255u) / 256u, 256, 0, stream>>>(s, g);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    k_kind_prefix<<<1, 1, 0, stream>>>(q_counts, prefix, seg_cap);
+    k_kind_prefix<<<1, 1, 0, stream>>>(q_counts, prefix, qb, flags_host);
     if (cfg.phase_ev) cudaEventRecord(cfg.phase_ev[2], stream);
-    SecondaryPolicy SP{q_rays, q_pixel, prefix, seg_cap, out, reinterpret_cast<uint4*>(bounce_out)};
+    SecondaryPolicy SP{q_rays, q_pixel, prefix, qb, out, reinterpret_cast<uint4*>(bounce_out),
+                       flags_host ? done : nullptr, flags_host};
     LaunchConfig cfg2 = cfg;   // the secondary kernel counts into stats[8..12]
     if (cfg.stats) cfg2.stats = cfg.stats + 8;
-    e = cfg.wide ? launch_persistent<true>(s, SP, 0u, prefix + kNumKinds, counters + 1, err, stream, cfg2)
-                 : launch_persistent<false>(s, SP, 0u, prefix + kNumKinds, counters + 1, err, stream, cfg2);
+    const uint32_t* total = prefix + kNumKinds * qb.n;
+    e = cfg.wide ? launch_persistent<true>(s, SP, 0u, total, counters + 1, err, stream, cfg2)
+                 : launch_persistent<false>(s, SP, 0u, total, counters + 1, err, stream, cfg2);
     if (cfg.phase_ev) cudaEventRecord(cfg.phase_ev[3], stream);
     if (e != cudaSuccess || !d_ray_count) return e;
     // primary rays of the rows traced (output row 0 is never traced)
     const uint64_t primary = (uint64_t)W * (row_end - max(row_begin, 1u));
-    k_add_ray_count<<<1, 1, 0, stream>>>(d_ray_count, primary, prefix + kNumKinds);
+    k_add_ray_count<<<1, 1, 0, stream>>>(d_ray_count, primary, total);
     return cudaGetLastError();
 }
 
@@ -772,7 +864,7 @@ __global__ void __launch_bounds__(256) k_probe_gen(SceneView s, ProbeArgs d, Gen
         hy = oy + dir.y * t;
         hz = oz + dir.z * t;
     }
-    emit(g, kKindSun, hit, sample, hx, hy, hz, kTMax, -d.sun[0], -d.sun[1], -d.sun[2], 1u);
+    emit(g, 0u, kKindSun, hit, sample, hx, hy, hz, kTMax, -d.sun[0], -d.sun[1], -d.sun[2], 1u);
     const uint32_t* list = nullptr;
     uint32_t count = 0;
     if (hit) {
@@ -803,7 +895,7 @@ __global__ void __launch_bounds__(256) k_probe_gen(SceneView s, ProbeArgs d, Gen
                 else direct_bits |= 1u << bit;
             }
         }
-        emit(g, kKindLight0 + j, has, sample, hx, hy, hz, rl, lx / rl, ly / rl, lz / rl, 1u | (bit << 8));
+        emit(g, 0u, kKindLight0 + j, has, sample, hx, hy, hz, rl, lx / rl, ly / rl, lz / rl, 1u | (bit << 8));
     }
     if (valid) {
         g.out_words[8u * sample + 4u] = direct_bits;
@@ -1180,12 +1272,13 @@ cudaError_t launch_probes(const SceneView& s, const ProbeArgs& d, uint32_t* out,
     g.q_rays = q_rays;
     g.q_pixel = q_pixel;
     g.q_counts = q_counts;
-    g.seg_cap = n;
+    g.qb.n = 1;
+    g.qb.cap[0] = n;
     k_probe_gen<<<(n + 255u) / 256u, 256, 0, stream>>>(s, d, g, leaf_nid);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    k_kind_prefix<<<1, 1, 0, stream>>>(q_counts, prefix, n);
+    k_kind_prefix<<<1, 1, 0, stream>>>(q_counts, prefix, g.qb, nullptr);
     if (cfg.phase_ev) cudaEventRecord(cfg.phase_ev[2], stream);
-    SecondaryPolicy SP{q_rays, q_pixel, prefix, n, out, nullptr};
+    SecondaryPolicy SP{q_rays, q_pixel, prefix, g.qb, out, nullptr, nullptr, nullptr};
     LaunchConfig cfg2 = cfg;
     if (cfg.stats) cfg2.stats = cfg.stats + 8;
     e = cfg.wide ? launch_persistent<true>(s, SP, 0u, prefix + kNumKinds, counters + 1, err, stream, cfg2)
