@@ -848,7 +848,8 @@ def bench_jobs_100k(N, ctx, dev, frame_scene, sid, steps=10):
 # ---------------------------------------------------------------- small fixed launch sequences for ncu
 
 def profile_frames(form):
-    """Two frames of the benchmark workload in one form (tim_rt_trace_camera)."""
+    """Two frames of the benchmark workload in one form (tim_rt_trace_camera;
+    pipelined: the binary form with TIM_RT_CAM_PIPELINED, results copied in bands)."""
     from tim_raytracing_b200 import _native as N, scenes
     scene = make_workload()
     img = N.build_bvh(scene)
@@ -857,7 +858,7 @@ def profile_frames(form):
     pd = scenes.pass_data(scene, W, H, aabb=(img.aabb[:3], img.aabb[3:]))
     tx, ty = (W + 15) // 16, (H + 15) // 16
     counts, lists = ctx.cull_lights(sid, pd, tx, ty)
-    flags = FRAME_FLAGS | (N.CAM_WIDE if form == "wide" else 0)
+    flags = FRAME_FLAGS | (N.CAM_WIDE if form == "wide" else 0) | (N.CAM_PIPELINED if form == "pipelined" else 0)
     for _ in range(2):
         _, _, st = ctx.trace_camera(sid, pd, flags, 1, counts, lists)
     print(json.dumps({"form": form, "kernel_ms": st.kernel_ms, "rays": int(st.rays)}))
@@ -963,16 +964,17 @@ def main():
     ap.add_argument("--no-serving", action="store_true", help="skip the serving workload")
     ap.add_argument("--no-probes", action="store_true", help="skip the light-probe field workload")
     ap.add_argument("--no-build", action="store_true", help="skip the BVH builder comparison")
-    ap.add_argument("--profile", choices=["plain", "wide", "batched-plain", "batched-wide", "probes-plain",
-                                          "probes-wide", "shade", "build"],
+    ap.add_argument("--profile", choices=["plain", "wide", "pipelined", "batched-plain", "batched-wide",
+                                          "probes-plain", "probes-wide", "shade", "build"],
                     help="only run a small, fixed launch sequence for ncu and exit: plain / wide = two frames of "
-                         "one form (per frame one primary and one secondary k_persistent launch); batched-* = two "
+                         "one form (per frame one primary and one secondary k_persistent launch); pipelined = two "
+                         "binary frames whose results are copied in bands while they trace; batched-* = two "
                          "launches of one k_multi batch over the first 16 scenes of the batched workload; "
                          "probes-* = two probe-field updates of one form (per update one probe-ray and one "
                          "shadow-ray k_persistent launch); shade = one quantised frame, then two k_shade_camera "
                          "launches; build = two GPU builds of the 1M-triangle scene")
     args = ap.parse_args()
-    if args.profile in ("plain", "wide"):
+    if args.profile in ("plain", "wide", "pipelined"):
         return profile_frames(args.profile)
     if args.profile in ("batched-plain", "batched-wide"):
         return profile_batched(args.profile == "batched-wide")

@@ -201,15 +201,16 @@ struct SecondaryPolicy {
     }
     // Called by all 32 lanes after a round of stores (`stored`: this lane stored
     // the ray in queue slot `slot`): one count per band and warp, after each
-    // storing lane has fenced its stores; the count that completes a band raises
-    // the band's flag.
+    // storing lane's release fence; the count that completes a band follows every
+    // other count of the band in the counter's order, and raises the band's flag
+    // after a system-scope fence.
     __device__ __forceinline__ void finished(bool stored, uint32_t slot) const {
         if (!done) return;
         uint32_t band = 0xFFFFFFFFu;
         if (stored) {
             band = 0;
             for (uint32_t k = 1; k < qb.n; ++k) band += slot >= qb.base[k] ? 1u : 0u;
-            __threadfence();
+            asm volatile("fence.acq_rel.gpu;" ::: "memory");   // this lane's stores before the warp's count
         }
         const uint32_t peers = __match_any_sync(0xFFFFFFFFu, band);
         __syncwarp();
