@@ -640,7 +640,7 @@ def bench_probes(N, ctx, l2_gbs, keep_for_parity, reps=5):
     return out, checks
 
 
-def bench_serving(N, ctx, dev, keep_for_parity, jobs_per_rate=1500):
+def bench_serving(N, ctx, dev, keep_for_parity, jobs_per_rate=1500, pool_size=256):
     """Serving workload: 16 resident heightfield + icosphere scenes (log-U [10K, 2M]
     tris), Poisson arrivals of jobs, a 40 GB device arena. A job is a ray batch of
     log-U [1K, 1M] mixed primary / shadow / probe-direction rays, or, one job in
@@ -666,10 +666,10 @@ def bench_serving(N, ctx, dev, keep_for_parity, jobs_per_rate=1500):
                                   0.03, N.PROBE_WIDE | N.PROBE_PRIMARY_BINARY))
     dirs = scenes.octahedral_dirs(16)
     basis = scenes.sh9_basis(dirs)
-    fields = [torch.zeros((7, 8, 16, 16, 4), dtype=torch.int16).pin_memory() for _ in range(8)]
+    fields = [torch.zeros((7, 8, 16, 16, 4), dtype=torch.int16).pin_memory() for _ in range(32)]
     field_owner = [0] * len(fields)
-    pool = []   # 256 reusable pinned ray / hit buffers: up to 256 requests in flight
-    for e in range(256):
+    pool = []   # reusable pinned ray / hit buffers: up to pool_size requests in flight
+    for e in range(pool_size):
         n = int(np.exp(rng.uniform(np.log(1e3), np.log(1e6))))
         r = torch.from_numpy(scenes.serving_rays(60_000 + e, n)).pin_memory()
         h = torch.empty((n, 4), dtype=torch.int32).pin_memory()
@@ -699,7 +699,7 @@ def bench_serving(N, ctx, dev, keep_for_parity, jobs_per_rate=1500):
                                                    fields[f].numpy().view(np.uint16), p0, p0 + 64)
                 probe_jobs += 1
                 continue
-            e = int(rg.integers(len(pool)))
+            e = j % len(pool)   # the entry least recently handed out: its job is long done at saturation
             if owner[e]:
                 srv.wait(owner[e])
             r, h = pool[e]

@@ -1,8 +1,8 @@
 // server.cu -- the serving loop of include/tim_rt.h (tim_rt_server_*): admission
 // of trace and probe-update requests against a device arena, continuous batching
 // of trace-request chunks into batched multi-scene launches (launch_multi),
-// probe updates (launch_probes) between those launches, asynchronous result
-// copies and latency statistics.
+// probe updates (launch_probes) on a stream of their own beside those launches,
+// asynchronous result copies and latency statistics.
 //
 // Threads: callers submit and wait; one worker thread per server issues every
 // CUDA call; CUDA host functions (cudaLaunchHostFunc) report step and request
@@ -127,7 +127,8 @@ inline ProbeStaging probe_staging(const ProbePlan& P, bool octa) {
 
 struct Slot {
     DevBuf dev;                   // SceneView[max_jobs], MultiJob[max_jobs], counter
-    void* host = nullptr;         // pinned staging of the two tables
+    void* host = nullptr;         // pinned staging of the two tables (mapped into the device's address space)
+    const void* host_dev = nullptr;   // its device address
     SceneView* d_views = nullptr;
     MultiJob* d_jobs = nullptr;
     uint32_t* d_counter = nullptr;
@@ -135,6 +136,18 @@ struct Slot {
     cudaEvent_t t_begin = nullptr, t_end = nullptr;   // around the step's kernel, for the GPU-busy time
     bool timing_pending = false;   // t_begin / t_end hold a step not yet added to gpu_busy_ms (under the mutex)
 };
+
+// Copies a step's tables from the mapped pinned staging into device memory. A
+// kernel, not a copy: host-to-device copies of all streams share the copy
+// engine's queue, so a table copy on the compute stream would wait behind every
+// ray upload queued before it.
+__global__ void k_stage_tables(uint32_t* dv, const uint32_t* sv, uint32_t nv, uint32_t* dj, const uint32_t* sj,
+                               uint32_t nj) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nv + nj; i += gridDim.x * blockDim.x) {
+        if (i < nv) dv[i] = sv[i];
+        else dj[i - nv] = sj[i - nv];
+    }
+}
 
 }  // namespace
 }  // namespace timrt
@@ -148,6 +161,7 @@ struct tim_rt_server {
     DevBuf arena_buf;
     Arena arena;                  // worker-only
     cudaStream_t up = nullptr, comp = nullptr, down = nullptr;
+    cudaStream_t probe = nullptr;      // probe updates, beside the trace steps
     std::vector<Slot> slots;
 
     std::mutex m;
@@ -173,6 +187,8 @@ struct tim_rt_server {
     Clock::time_point t0;
 
     std::deque<Req*> active;           // worker-only: admitted, rays left to issue
+    int last_slot = -1;                // worker-only: slot of the step issued last
+    bool last_started = true;          // worker-only: that step has begun on the GPU
     std::thread worker;
 };
 
@@ -330,10 +346,12 @@ int issue_step(tim_rt_server* s, Plan& P) {
         r->issued += ch.second;
     }
     const uint64_t vb = round256(sizeof(SceneView) * maxj);
-    if (cudaMemcpyAsync(sl.d_views, hv, sizeof(SceneView) * slot_of.size(), cudaMemcpyHostToDevice, s->comp) ||
-        cudaMemcpyAsync(sl.d_jobs, static_cast<uint8_t*>(sl.host) + vb, sizeof(MultiJob) * nj, cudaMemcpyHostToDevice,
-                        s->comp))
-        return TIM_RT_EDEVICE;
+    static_assert(sizeof(SceneView) % 4 == 0 && sizeof(MultiJob) % 4 == 0, "tables are copied in 4-byte words");
+    const uint32_t nvw = (uint32_t)(sizeof(SceneView) * slot_of.size() / 4), njw = (uint32_t)(sizeof(MultiJob) * nj / 4);
+    const uint32_t* hd = static_cast<const uint32_t*>(sl.host_dev);
+    k_stage_tables<<<4, 256, 0, s->comp>>>(reinterpret_cast<uint32_t*>(sl.d_views), hd, nvw,
+                                           reinterpret_cast<uint32_t*>(sl.d_jobs), hd + vb / 4, njw);
+    if (cudaGetLastError() != cudaSuccess) return TIM_RT_EDEVICE;
     LaunchConfig cfg = s->ctx->cfg;
     cfg.stats = nullptr;
     cfg.phase_ev = nullptr;
@@ -365,9 +383,10 @@ int issue_step(tim_rt_server* s, Plan& P) {
     return TIM_RT_OK;
 }
 
-// Uploads nothing: the request's inputs went up on the upload stream at
-// admission. Runs the probe update on the compute stream, then copies the FP16
-// field (and the texels) back and completes the request.
+// Uploads nothing: the request's inputs were queued on the probe stream at
+// admission. Runs the probe update on the probe stream, beside the trace steps
+// (its small launches fill the SMs a step's tail leaves idle), then copies the
+// FP16 field (and the texels) back and completes the request.
 int issue_probe(tim_rt_server* s, Req* r) {
     ProbeArgs d = r->plan.args;
     d.dirs = r->d_dirs;
@@ -378,11 +397,10 @@ int issue_probe(tim_rt_server* s, Req* r) {
     cfg.wide = (r->pdesc.flags & TIM_RT_PROBE_WIDE) != 0 && r->scene->has_wide;
     cfg.primary_binary = (r->pdesc.flags & TIM_RT_PROBE_PRIMARY_BINARY) != 0;
     uint32_t* err = static_cast<uint32_t*>(s->ctx->counters.ptr) + kErrWord;
-    if (cudaStreamWaitEvent(s->comp, r->uploaded, 0) ||
-        cudaMemsetAsync(r->d_ctr, 0, 4ull * kCamCounterWords, s->comp) ||
+    if (cudaMemsetAsync(r->d_ctr, 0, 4ull * kCamCounterWords, s->probe) ||
         launch_probes(r->scene->view, d, r->d_out, r->d_pnid, r->d_qrays, r->d_qpix, r->d_ctr, err, r->d_irr,
-                      r->d_sh16, nullptr, r->d_octa, r->d_octa ? r->plan.side : 0, s->comp, cfg) != cudaSuccess ||
-        cudaEventCreateWithFlags(&r->ran, cudaEventDisableTiming) || cudaEventRecord(r->ran, s->comp) ||
+                      r->d_sh16, nullptr, r->d_octa, r->d_octa ? r->plan.side : 0, s->probe, cfg) != cudaSuccess ||
+        cudaEventCreateWithFlags(&r->ran, cudaEventDisableTiming) || cudaEventRecord(r->ran, s->probe) ||
         cudaStreamWaitEvent(s->down, r->ran, 0) ||
         cudaMemcpyAsync(r->pr.sh9_fp16, r->d_sh16, 56ull * r->plan.total, cudaMemcpyDeviceToHost, s->down) ||
         (r->d_octa && cudaMemcpyAsync(r->pr.octa, r->d_octa, 768ull * r->plan.args.np, cudaMemcpyDeviceToHost, s->down)))
@@ -391,7 +409,10 @@ int issue_probe(tim_rt_server* s, Req* r) {
     return TIM_RT_OK;
 }
 
-// Points a probe request's staging into its arena block and queues its uploads.
+// Points a probe request's staging into its arena block and queues its uploads
+// (a few hundred KB) on the probe stream, right ahead of the update itself:
+// queued on the upload stream they would wait behind every ray upload admitted
+// before them.
 int stage_probe(tim_rt_server* s, Req* r, uint8_t* p) {
     const ProbeStaging b = probe_staging(r->plan, r->pr.octa != nullptr);
     r->d_dirs = reinterpret_cast<float4*>(p);
@@ -415,10 +436,10 @@ int stage_probe(tim_rt_server* s, Req* r, uint8_t* p) {
     r->d_octa = b.octa ? reinterpret_cast<float*>(p) : nullptr;
     const uint64_t nd = r->plan.args.nd;
     if (cudaEventCreateWithFlags(&r->uploaded, cudaEventDisableTiming) ||
-        cudaMemcpyAsync(r->d_dirs, r->pr.dirs, 16 * nd, cudaMemcpyHostToDevice, s->up) ||
-        cudaMemcpyAsync(r->d_basis, r->pr.sh_basis, 36 * nd, cudaMemcpyHostToDevice, s->up) ||
-        cudaMemcpyAsync(r->d_sh16, r->pr.sh9_fp16, 56ull * r->plan.total, cudaMemcpyHostToDevice, s->up) ||
-        cudaEventRecord(r->uploaded, s->up))
+        cudaMemcpyAsync(r->d_dirs, r->pr.dirs, 16 * nd, cudaMemcpyHostToDevice, s->probe) ||
+        cudaMemcpyAsync(r->d_basis, r->pr.sh_basis, 36 * nd, cudaMemcpyHostToDevice, s->probe) ||
+        cudaMemcpyAsync(r->d_sh16, r->pr.sh9_fp16, 56ull * r->plan.total, cudaMemcpyHostToDevice, s->probe) ||
+        cudaEventRecord(r->uploaded, s->probe))
         return TIM_RT_EDEVICE;
     return TIM_RT_OK;
 }
@@ -451,14 +472,27 @@ int issue_cancels(tim_rt_server* s, std::vector<Req*>& cancels) {
     return TIM_RT_OK;
 }
 
+// A step is planned when a slot is free and the step issued before it has begun
+// on the GPU, so that at most one step waits behind a running one and each plan
+// takes every request uploaded while the previous step ran (planning as soon as a
+// slot frees would leave the second slot with whatever little had arrived since).
+// Whether the last step has begun is polled (its begin event, outside the mutex)
+// every 20 us while the worker waits.
 void worker_main(tim_rt_server* s) {
     cudaSetDevice(s->ctx->device);
     for (;;) {
         std::vector<Req*> release, admitted, cancels;
         Plan P;
+        if (!s->last_started) {
+            const cudaError_t q = cudaEventQuery(s->slots[s->last_slot].t_begin);
+            if (q != cudaErrorNotReady) {
+                s->last_started = true;
+                if (q != cudaSuccess) cudaGetLastError();   // a failed step reports itself on the stream
+            }
+        }
         {
             std::unique_lock<std::mutex> lk(s->m);
-            s->cv.wait(lk, [&] {
+            auto ready = [&] {
                 if (s->stop || !s->finished.empty()) return true;
                 if (s->error) return false;
                 if (!s->cancel_q.empty()) return true;
@@ -468,8 +502,13 @@ void worker_main(tim_rt_server* s) {
                     Arena probe = s->arena;
                     if (probe.alloc(s->waiting.front()->bytes, off)) return true;
                 }
-                return !s->active.empty() && !s->free_slots.empty();
-            });
+                return !s->active.empty() && !s->free_slots.empty() && s->last_started;
+            };
+            if (s->last_started) {
+                s->cv.wait(lk, ready);
+            } else if (!s->cv.wait_for(lk, std::chrono::microseconds(20), ready)) {
+                continue;   // poll the last step's begin event again
+            }
             // stop once everything completed (or, after a device error, at once:
             // teardown waits for the streams and releases what is left)
             if (s->stop && (s->error || (s->pending.empty() && s->finished.empty()))) break;
@@ -491,7 +530,7 @@ void worker_main(tim_rt_server* s) {
                     admitted.push_back(r);
                     if (!r->probe) s->active.push_back(r);
                 }
-                if (!s->active.empty() && !s->free_slots.empty()) {
+                if (!s->active.empty() && !s->free_slots.empty() && s->last_started) {
                     P.slot = s->free_slots.back();
                     s->free_slots.pop_back();
                     account_slot(s, s->slots[P.slot]);
@@ -535,10 +574,14 @@ void worker_main(tim_rt_server* s) {
                 cudaEventRecord(r->uploaded, s->up))
                 rc = TIM_RT_EDEVICE;
         }
-        // admitted probe updates run on the compute stream ahead of the next trace step
+        // admitted probe updates run on the probe stream, beside the trace steps
         for (Req* r : admitted)
             if (r->probe && rc == TIM_RT_OK) rc = issue_probe(s, r);
-        if (P.slot >= 0 && rc == TIM_RT_OK) rc = issue_step(s, P);
+        if (P.slot >= 0 && rc == TIM_RT_OK) {
+            rc = issue_step(s, P);
+            s->last_slot = P.slot;
+            s->last_started = false;
+        }
         if (rc == TIM_RT_OK) rc = issue_cancels(s, cancels);
         if (rc != TIM_RT_OK) fail_all(s, rc, std::string("serving step failed: ") + cudaGetErrorString(cudaGetLastError()));
     }
@@ -552,7 +595,7 @@ int server_teardown(tim_rt_server* s) {
     s->cv.notify_all();
     if (s->worker.joinable()) s->worker.join();
     cudaSetDevice(s->ctx->device);
-    for (cudaStream_t st : {s->up, s->comp, s->down})
+    for (cudaStream_t st : {s->up, s->comp, s->down, s->probe})
         if (st) cudaStreamSynchronize(st);
     // requests left behind (only after a device error or a failed create)
     std::set<Req*> left(s->finished.begin(), s->finished.end());
@@ -569,7 +612,7 @@ int server_teardown(tim_rt_server* s) {
         if (sl.t_end) cudaEventDestroy(sl.t_end);
     }
     dev_free(s->ctx, s->arena_buf);
-    for (cudaStream_t st : {s->up, s->comp, s->down})
+    for (cudaStream_t st : {s->up, s->comp, s->down, s->probe})
         if (st) cudaStreamDestroy(st);
     s->ctx->servers.erase(s);
     delete s;
@@ -615,10 +658,13 @@ int tim_rt_server_create(tim_rt_ctx* c, const tim_rt_server_params* params, tim_
     s->slots.resize(s->p.max_inflight_steps);
     bool ok = cudaStreamCreateWithFlags(&s->up, cudaStreamNonBlocking) == cudaSuccess &&
               cudaStreamCreateWithFlags(&s->comp, cudaStreamNonBlocking) == cudaSuccess &&
-              cudaStreamCreateWithFlags(&s->down, cudaStreamNonBlocking) == cudaSuccess;
+              cudaStreamCreateWithFlags(&s->down, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&s->probe, cudaStreamNonBlocking) == cudaSuccess;
     for (size_t i = 0; ok && i < s->slots.size(); ++i) {
         Slot& sl = s->slots[i];
-        if (dev_alloc(c, sl.dev, vb + jb + 256) != TIM_RT_OK || cudaHostAlloc(&sl.host, vb + jb, 0) != cudaSuccess ||
+        if (dev_alloc(c, sl.dev, vb + jb + 256) != TIM_RT_OK ||
+            cudaHostAlloc(&sl.host, vb + jb, cudaHostAllocMapped) != cudaSuccess ||
+            cudaHostGetDevicePointer(const_cast<void**>(&sl.host_dev), sl.host, 0) != cudaSuccess ||
             cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming) != cudaSuccess ||
             cudaEventCreate(&sl.t_begin) != cudaSuccess || cudaEventCreate(&sl.t_end) != cudaSuccess) {
             ok = false;
