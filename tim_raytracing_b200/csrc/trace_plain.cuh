@@ -87,10 +87,10 @@ __device__ __forceinline__ void trav_init(TravState& st, uint32_t root) {
 // boxabs = +inf makes m infinite, every infinity or NaN in M or T does too), and
 // an order that the tmin intervals cannot settle, takes the reference's
 // divisions. The outcome is CollideBox's in every case; only the work differs.
-__device__ __forceinline__ bool box_filter(const TravState& st, float mnx, float mny, float mnz, float mxx, float mxy,
-                                           float mxz, bool& hit, float& lo, float& hi) {
-    const float t0x = (mnx - st.r.ox) * st.ix, t0y = (mny - st.r.oy) * st.iy, t0z = (mnz - st.r.oz) * st.iz;
-    const float t1x = (mxx - st.r.ox) * st.ix, t1y = (mxy - st.r.oy) * st.iy, t1z = (mxz - st.r.oz) * st.iz;
+// The slab values t = RN(RN(p - o) * inv) arrive computed (box_slabs); this
+// decides from them.
+__device__ __forceinline__ bool box_filter(const TravState& st, float t0x, float t0y, float t0z, float t1x, float t1y,
+                                           float t1z, bool& hit, float& lo, float& hi) {
     const float M = fmaxf(fminf(t0x, t1x), fmaxf(fminf(t0y, t1y), fminf(t0z, t1z)));
     const float T = fminf(st.t, fminf(fmaxf(t0x, t1x), fminf(fmaxf(t0y, t1y), fmaxf(t0z, t1z))));
     const float m = __fmaf_rn(fabsf(M) + fabsf(T), 9.5367431640625e-07f, st.boxabs);   // 2^-20
@@ -113,11 +113,29 @@ static __device__ __noinline__ float2 exact_children(Ray r, float4 a, float4 b, 
     return make_float2(collide_box(r, a.x, a.y, c.x, a.z, a.w, c.y, tmax), collide_box(r, b.x, b.y, c.z, b.z, b.w, c.w, tmax));
 }
 
+// The six slab values of one child box, (p - o) * inv per plane, two planes per
+// packed f32x2 subtract and multiply: the node record holds (min.x, min.y) and
+// (max.x, max.y) of a child in adjacent words, its (min.z, max.z) likewise, so
+// the pairs need no moves. Each element is rounded as the scalar operation
+// rounds it, so the values are the scalar form's.
+__device__ __forceinline__ void box_slabs(uint64_t oxy, uint64_t ixy, uint64_t ozz, uint64_t izz, float mnx, float mny,
+                                          float mxx, float mxy, float mnz, float mxz, float& t0x, float& t0y, float& t0z,
+                                          float& t1x, float& t1y, float& t1z) {
+    unpack2f(mul2(sub2(pack2f(mnx, mny), oxy), ixy), t0x, t0y);
+    unpack2f(mul2(sub2(pack2f(mxx, mxy), oxy), ixy), t1x, t1y);
+    unpack2f(mul2(sub2(pack2f(mnz, mxz), ozz), izz), t0z, t1z);
+}
+
 __device__ __forceinline__ void plain_children(const TravState& st, const float4& a, const float4& b, const float4& c,
                                                bool& h0, bool& h1, bool& first1) {
     float lo0, hi0, lo1, hi1;
-    bool ok = box_filter(st, a.x, a.y, c.x, a.z, a.w, c.y, h0, lo0, hi0);
-    ok = box_filter(st, b.x, b.y, c.z, b.z, b.w, c.w, h1, lo1, hi1) && ok;
+    const uint64_t oxy = pack2f(st.r.ox, st.r.oy), ixy = pack2f(st.ix, st.iy);
+    const uint64_t ozz = pack2f(st.r.oz, st.r.oz), izz = pack2f(st.iz, st.iz);
+    float t0x, t0y, t0z, t1x, t1y, t1z;
+    box_slabs(oxy, ixy, ozz, izz, a.x, a.y, a.z, a.w, c.x, c.y, t0x, t0y, t0z, t1x, t1y, t1z);
+    bool ok = box_filter(st, t0x, t0y, t0z, t1x, t1y, t1z, h0, lo0, hi0);
+    box_slabs(oxy, ixy, ozz, izz, b.x, b.y, b.z, b.w, c.z, c.w, t0x, t0y, t0z, t1x, t1y, t1z);
+    ok = box_filter(st, t0x, t0y, t0z, t1x, t1y, t1z, h1, lo1, hi1) && ok;
     first1 = hi1 < lo0;
     if (ok && h0 && h1 && !first1 && !(lo1 >= hi0)) ok = false;
     if (!ok) {
