@@ -460,24 +460,33 @@ __global__ void __launch_bounds__(256) k_gen_secondary(SceneView s, GenParams g)
         }
     }
     uint32_t direct_bits = 0;
-    for (uint32_t j = 0; j < 16u; ++j) {
+    // lights past every lane's count emit nothing: the loop ends at the warp's
+    // largest count (one 16x16 tile's list with tile lists, so usually uniform)
+    const uint32_t jmax = __reduce_max_sync(0xFFFFFFFFu, count);
+    for (uint32_t j = 0; j < jmax; ++j) {
         bool has = false;
-        float lx = 0.f, ly = 0.f, lz = 0.f, rl = 1.f;
+        float rl = 1.f, dlx = 0.f, dly = 0.f, dlz = 0.f;
         uint32_t bit = 0;
         if (j < count) {
             const uint32_t li = __ldg(list + j);
             const float* L = s.lights + 14u * li;
             bit = li + 1u;
             if (__float_as_uint(__ldg(L)) == kLightSphere && bit < 32u) {   // evalShadow: sphere lights only
-                lx = __ldg(L + 1) - hx;
-                ly = __ldg(L + 2) - hy;
-                lz = __ldg(L + 3) - hz;
+                const float lx = __ldg(L + 1) - hx;
+                const float ly = __ldg(L + 2) - hy;
+                const float lz = __ldg(L + 3) - hz;
                 rl = sqrtf(dot3(lx, ly, lz, lx, ly, lz));
-                if (rl < __ldg(L + 4)) has = true;
-                else direct_bits |= 1u << bit;   // out of range counts as masked
+                if (rl < __ldg(L + 4)) {
+                    has = true;
+                    dlx = lx / rl;
+                    dly = ly / rl;
+                    dlz = lz / rl;
+                } else {
+                    direct_bits |= 1u << bit;   // out of range counts as masked
+                }
             }
         }
-        emit(g, band, kKindLight0 + j, has, pix, hx, hy, hz, rl, lx / rl, ly / rl, lz / rl, 1u | (bit << 8));
+        emit(g, band, kKindLight0 + j, has, pix, hx, hy, hz, rl, dlx, dly, dlz, 1u | (bit << 8));
     }
     if (g.flags & TIM_RT_CAM_PROB_MASK) {
         // lightprobHelpers.glsl:71-77 getLightProbCoordUVW and bvhLighting.glsl:170-180
@@ -879,24 +888,31 @@ __global__ void __launch_bounds__(256) k_probe_gen(SceneView s, ProbeArgs d, Gen
         list = s.leaf + skip + 1u + off;
     }
     uint32_t direct_bits = 0;
-    for (uint32_t j = 0; j < 15u; ++j) {
+    const uint32_t jmax = min(__reduce_max_sync(0xFFFFFFFFu, count), 15u);   // lights past every lane's count emit nothing
+    for (uint32_t j = 0; j < jmax; ++j) {
         bool has = false;
-        float lx = 0.f, ly = 0.f, lz = 0.f, rl = 1.f;
+        float rl = 1.f, dlx = 0.f, dly = 0.f, dlz = 0.f;
         uint32_t bit = 0;
         if (j < count) {
             const uint32_t li = __ldg(list + j);
             const float* L = s.lights + 14u * li;
             bit = li + 1u;
             if (__float_as_uint(__ldg(L)) == kLightSphere && bit < 32u) {
-                lx = __ldg(L + 1) - hx;
-                ly = __ldg(L + 2) - hy;
-                lz = __ldg(L + 3) - hz;
+                const float lx = __ldg(L + 1) - hx;
+                const float ly = __ldg(L + 2) - hy;
+                const float lz = __ldg(L + 3) - hz;
                 rl = sqrtf(dot3(lx, ly, lz, lx, ly, lz));
-                if (rl < __ldg(L + 4)) has = true;
-                else direct_bits |= 1u << bit;
+                if (rl < __ldg(L + 4)) {
+                    has = true;
+                    dlx = lx / rl;
+                    dly = ly / rl;
+                    dlz = lz / rl;
+                } else {
+                    direct_bits |= 1u << bit;
+                }
             }
         }
-        emit(g, 0u, kKindLight0 + j, has, sample, hx, hy, hz, rl, lx / rl, ly / rl, lz / rl, 1u | (bit << 8));
+        emit(g, 0u, kKindLight0 + j, has, sample, hx, hy, hz, rl, dlx, dly, dlz, 1u | (bit << 8));
     }
     if (valid) {
         g.out_words[8u * sample + 4u] = direct_bits;
