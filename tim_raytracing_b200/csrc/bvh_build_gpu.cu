@@ -349,19 +349,19 @@ __global__ void __launch_bounds__(kTreeletWarps * 32) k_treelet(uint32_t n, uint
             // open the largest-area internal node until 7 leaves
             uint32_t leaf[kTreeletLeaves], inner[kTreeletLeaves - 2];
             Aabb lb[kTreeletLeaves];
+            float la[kTreeletLeaves];   // area of an internal leaf of the treelet, -1 for a triangle
             int nl = 2, ni = 0;
             leaf[0] = __ldcg(left + root);
             leaf[1] = __ldcg(right + root);
             lb[0] = load_box_cg(box + leaf[0]);
             lb[1] = load_box_cg(box + leaf[1]);
+            la[0] = leaf[0] >= n - 1u ? -1.0f : half_area(lb[0]);
+            la[1] = leaf[1] >= n - 1u ? -1.0f : half_area(lb[1]);
             while (nl < kTreeletLeaves) {
                 int best = -1;
                 float ba = -1.0f;
-                for (int i = 0; i < nl; ++i) {
-                    if (leaf[i] >= n - 1u) continue;   // a triangle
-                    const float a = half_area(lb[i]);
-                    if (a > ba) { ba = a; best = i; }
-                }
+                for (int i = 0; i < nl; ++i)
+                    if (la[i] > ba) { ba = la[i]; best = i; }
                 if (best < 0) break;
                 const uint32_t x = leaf[best];
                 inner[ni++] = x;
@@ -369,6 +369,8 @@ __global__ void __launch_bounds__(kTreeletWarps * 32) k_treelet(uint32_t n, uint
                 leaf[nl] = __ldcg(right + x);
                 lb[best] = load_box_cg(box + leaf[best]);
                 lb[nl] = load_box_cg(box + leaf[nl]);
+                la[best] = leaf[best] >= n - 1u ? -1.0f : half_area(lb[best]);
+                la[nl] = leaf[nl] >= n - 1u ? -1.0f : half_area(lb[nl]);
                 ++nl;
             }
             if (nl < 3) continue;   // two triangles: nothing to rearrange
@@ -401,7 +403,42 @@ __global__ void __launch_bounds__(kTreeletWarps * 32) k_treelet(uint32_t n, uint
             __syncwarp();
             // best split of every subset, by size: all proper subsets are done first.
             // A split (P, sub \ P) is taken once, with P holding sub's lowest leaf.
+            // The two largest sizes have few subsets with many splits each (7 leaves:
+            // one set of 63 splits, seven of 31): there the lanes of a group share one
+            // subset's splits and reduce; smaller sizes take a subset per lane.
             for (int k = 2; k <= nl; ++k) {
+                if (nl >= 5 && k >= nl - 1) {
+                    const uint32_t G = k == nl ? 32u : 4u;   // lanes per subset
+                    const uint32_t gi = lane / G, gl = lane % G;
+                    // subset gi of this size: the whole set, or the set without leaf gi
+                    const bool real = k == nl ? gi == 0u : gi < (uint32_t)nl;
+                    const uint32_t sub = k == nl ? full : (real ? full ^ (1u << gi) : full);
+                    const uint32_t low = sub & (0u - sub), rest = sub ^ low;
+                    const uint32_t nsplit = (1u << (k - 1)) - 1u;   // subsets q of rest but rest itself
+                    float best = INFINITY;
+                    uint32_t bp = 0xFFu;
+                    for (uint32_t j = gl; real && j < nsplit; j += G) {
+                        uint32_t q = 0, jj = j;   // the j-th subset of rest: j's bits on rest's bits
+                        for (uint32_t b = rest; b; b &= b - 1u, jj >>= 1)
+                            if (jj & 1u) q |= b & (0u - b);
+                        const uint32_t P = q | low;
+                        const float c = s_cost[P] + s_cost[sub ^ P];
+                        if (c < best || (c == best && P < bp)) { best = c; bp = P; }
+                    }
+                    for (uint32_t o = G >> 1; o; o >>= 1) {   // least cost in the group, ties to the lower split
+                        const float ob = __shfl_xor_sync(0xFFFFFFFFu, best, o);
+                        const uint32_t op = __shfl_xor_sync(0xFFFFFFFFu, bp, o);
+                        if (ob < best || (ob == best && op < bp)) { best = ob; bp = op; }
+                    }
+                    if (real && gl == 0u) {
+                        const float ci = ci_ * s_area[sub] + best;
+                        const float cl = s_cost[sub];
+                        s_cost[sub] = fminf(cl, ci);
+                        s_part[sub] = (uint8_t)(bp == 0xFFu ? low : bp) | (cl <= ci ? kCollapse : 0u);
+                    }
+                    __syncwarp();
+                    continue;
+                }
                 for (uint32_t sub = lane + 1u; sub <= full; sub += 32u) {
                     if (__popc(sub) != k) continue;
                     const uint32_t low = sub & (0u - sub), rest = sub ^ low;
