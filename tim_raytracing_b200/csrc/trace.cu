@@ -197,6 +197,7 @@ struct SecondaryPolicy {
         st.t = a.w;
         st.any = (__float_as_uint(b.w) & 1u) != 0u;
         st.dup_ok = true;   // bounce rays store the hit record only
+        st.slot2 = __ldg(pixel + slot);   // read now, used when the ray is stored
         return true;
     }
     // Called by all 32 lanes after a round of stores (`stored`: this lane stored
@@ -228,7 +229,7 @@ struct SecondaryPolicy {
         const uint32_t slot = st.slot;
         const uint32_t fl = __float_as_uint(__ldg(reinterpret_cast<const float*>(rays + slot) + 7));
         const uint32_t kind = (fl >> 16) & 3u, bit = (fl >> 8) & 0xFFu;
-        const uint32_t p = __ldg(pixel + slot);
+        const uint32_t p = st.slot2;
         if (kind == 2u) {
             bounce_out[p] = make_uint4(st.rec0, st.rec1, st.rec2, __float_as_uint(st.t));
         } else if (st.hit) {

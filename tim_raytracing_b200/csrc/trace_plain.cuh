@@ -29,6 +29,7 @@ struct TravState {
     // work counters (dead code unless a counting kernel reads them)
     uint32_t c_node, c_leaf, c_tri, c_reload;
     uint32_t slot;      // policy scratch (pixel or queue slot of the ray)
+    uint32_t slot2;     // policy scratch (secondary rays: the pixel)
     float ix, iy, iz;   // 1 / direction (8-wide form: zero components replaced, see wide_inv)
     float boxabs;       // binary walk: absolute margin of the filtered box test (+inf: exact test only)
     // 8-wide form only
