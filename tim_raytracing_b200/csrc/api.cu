@@ -925,9 +925,13 @@ int tim_rt_trace_camera(tim_rt_ctx* c, tim_rt_scene_id id, const tim_rt_pass_dat
     } else {
         // Band b's copy starts when its flag is up. Should the trace end without a
         // flag (an error ended a kernel early), the remaining copies wait for its end.
+        // The flag is polled in host memory; the trace's end event (a driver call)
+        // only every 64th poll.
         bool ended = false;
+        uint32_t polls = 0;
         for (uint32_t b = 0; b < bands;) {
             if (!ended && !reinterpret_cast<volatile uint32_t*>(c->band_flags)[b]) {
+                if (++polls % 64u != 0u) continue;
                 const cudaError_t q = cudaEventQuery(c->ev[2]);
                 if (q == cudaErrorNotReady) continue;
                 ended = true;
