@@ -183,6 +183,7 @@ int probe_plan(Scene* s, const tim_rt_probe_desc* desc, uint32_t probe_begin, ui
     d.nd = nd;
     d.p0 = probe_begin;
     d.np = np;
+    d.trace_dir_major = side != 0u;
     out->args = d;
     out->side = side;
     out->n = n;
