@@ -912,18 +912,24 @@ def profile_batched(wide, scenes_used=16):
     return 0
 
 
-def profile_probes(wide):
-    """Two updates of the probe-field workload in one walk (pure 8-wide or binary)."""
+def profile_probes(wide, stratified=False):
+    """Two updates of the probe-field workload in one walk (pure 8-wide or binary), with the
+    octahedral directions or (binary only) the stratified sampleRays set."""
     from tim_raytracing_b200 import _native as N, scenes
     scene = scenes.scaled_heightfield(77, 1_000_000)
     img = N.build_bvh(scene)
     ctx = N.Context(0)
     sid = ctx.upload(img, scene, quant8=True)
     res = (32, 32, 8)
-    dirs = scenes.octahedral_dirs(16)
-    basis = scenes.sh9_basis(dirs)
+    if stratified:
+        dirs, basis = N.probe_directions(256, N.DIRS_STRATIFIED, seed=9)
+        flags = 0
+    else:
+        dirs = scenes.octahedral_dirs(16)
+        basis = scenes.sh9_basis(dirs)
+        flags = N.PROBE_OCTA | (N.PROBE_WIDE if wide else 0)
     desc = N.probe_desc(img.aabb[:3], img.aabb[3:], res, (-0.4, 0.3, -1.0), (1.0, 0.95, 0.9), len(dirs), 0.03,
-                        N.PROBE_OCTA | (N.PROBE_WIDE if wide else 0))
+                        flags)
     sh16 = np.zeros((7, res[2], res[1], res[0], 4), np.uint16)
     for _ in range(2):
         _, _, _, _, st = ctx.update_probes(sid, desc, dirs, basis, sh16)
@@ -985,13 +991,13 @@ def main():
     ap.add_argument("--no-probes", action="store_true", help="skip the light-probe field workload")
     ap.add_argument("--no-build", action="store_true", help="skip the BVH builder comparison")
     ap.add_argument("--profile", choices=["plain", "wide", "pipelined", "batched-plain", "batched-wide",
-                                          "probes-plain", "probes-wide", "shade", "build"],
+                                          "probes-plain", "probes-wide", "probes-stratified", "shade", "build"],
                     help="only run a small, fixed launch sequence for ncu and exit: plain / wide = two frames of "
                          "one form (per frame one primary and one secondary k_persistent launch); pipelined = two "
                          "binary frames whose results are copied in bands while they trace; batched-* = two "
                          "launches of one k_multi batch over the first 16 scenes of the batched workload; "
                          "probes-* = two probe-field updates of one form (per update one probe-ray and one "
-                         "shadow-ray k_persistent launch); shade = one quantised frame, then two k_shade_camera "
+                         "shadow-ray k_persistent launch; probes-stratified: binary, stratified directions); shade = one quantised frame, then two k_shade_camera "
                          "launches; build = two GPU builds of the 1M-triangle scene")
     args = ap.parse_args()
     if args.profile in ("plain", "wide", "pipelined"):
@@ -1003,7 +1009,7 @@ def main():
     if args.profile == "build":
         return profile_build()
     if args.profile:
-        return profile_probes(args.profile == "probes-wide")
+        return profile_probes(args.profile == "probes-wide", args.profile == "probes-stratified")
     args.warmup = max(args.warmup, 3)
 
     rank = int(os.environ.get("RANK", "0"))

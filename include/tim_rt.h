@@ -347,9 +347,9 @@ int tim_rt_server_submit(tim_rt_server *srv, const tim_rt_request *req, uint64_t
  * optional (TIM_RT_PROBE_OCTA). Admission counts its whole device staging
  * (directions, basis, the FP16 field, per-ray records, lit values, the shadow-ray
  * queue and the optional texels) against the same arena as trace requests, in the
- * same FIFO. Once admitted it runs as one probe-update launch sequence on the
- * server's compute stream between batched trace steps; the outputs equal those
- * of tim_rt_update_probes on the same inputs. */
+ * same FIFO. Once admitted it runs as one probe-update launch sequence on a
+ * server stream of its own, beside the batched trace steps; the outputs equal
+ * those of tim_rt_update_probes on the same inputs. */
 typedef struct tim_rt_probe_desc tim_rt_probe_desc;
 typedef struct {
     tim_rt_scene_id scene;

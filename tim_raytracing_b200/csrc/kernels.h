@@ -123,7 +123,7 @@ struct ProbeArgs {
     float sun[3], sunc[3];
     float hyst;
     uint32_t nd, p0, np;
-    uint32_t trace_dir_major;  // probe rays traced direction-major (see probe_trace_item)
+    uint32_t trace_dir_major;  // probe rays traced direction-major (TIM_RT_PROBE_OCTA; probe_trace_item)
     const float4* dirs;     // nd
     const float* basis;     // nd x 9
 };

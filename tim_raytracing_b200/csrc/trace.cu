@@ -831,9 +831,10 @@ __device__ __forceinline__ uint32_t probe_sample(const ProbeArgs& d, uint32_t i,
     return pl * d.nd + r;
 }
 
-// Work item i of the probe-ray trace. With the stratified direction set it is
-// probe-major like the generator; with the octahedral set it is direction-major
-// (r = i / np: a warp traces one direction from 32 neighbouring probes). Measured
+// Work item i of the probe-ray trace. It is probe-major like the generator,
+// except under TIM_RT_PROBE_OCTA (the directions are the octahedral grid), where it
+// is direction-major (r = i / np: a warp traces one direction from 32
+// neighbouring probes; trace_dir_major is set from that flag). Measured
 // per update on the 1M-triangle scene, 32x32x8 probes x 256 directions: the
 // octahedral set takes 4.17 ms this way against 4.28 ms probe-major, the
 // stratified set 3.71 ms probe-major against 3.85 ms direction-major.
