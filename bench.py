@@ -610,18 +610,21 @@ def bench_probes(N, ctx, l2_gbs, keep_for_parity, reps=5):
         out[set_name] = row
         if keep_for_parity:
             checks[set_name] = (scene, img, lo, hi, res, dirs, basis, sun, sunc, gpu)
-    # roofline of the probe-ray launch (closest hit, binary walk in both forms): its
-    # rays traced once more by the counting kernel
-    dirs = sets["octahedral"][0]
+    # roofline of the probe-ray launch (closest hit, binary walk in both forms) of each
+    # direction set: its rays traced once more by the counting kernel
     origins = scenes.probe_positions(lo, hi, res, np.arange(total))
-    rays = np.zeros((total * len(dirs), 8), np.float32)
-    rays[:, 0:3] = np.repeat(origins, len(dirs), axis=0)
-    rays[:, 3] = np.float32(100.0)
-    rays[:, 4:7] = np.tile(dirs[:, :3], (total, 1))
-    _, _, _, stc = ctx.trace(sid, rays, N.MODE_CLOSEST | N.TRACE_COUNT, want_nid=False, want_bary=False)
-    out["octahedral"]["roofline_probe_rays"] = roofline(
-        plain_bytes(stc), out["octahedral"]["plain_binary"]["probe_ray_launch_ms"], l2_gbs, "probe_rays_plain",
-        "k_persistent<256, 0, 0, ProbePolicy> (probe rays, binary walk)", BYTES_PLAIN)
+    for set_name, key in (("octahedral", "probe_rays_plain"), ("stratified", "probe_rays_plain_stratified")):
+        dirs = sets[set_name][0]
+        rays = np.zeros((total * len(dirs), 8), np.float32)
+        rays[:, 0:3] = np.repeat(origins, len(dirs), axis=0)
+        rays[:, 3] = np.float32(100.0)
+        rays[:, 4:7] = np.tile(dirs[:, :3], (total, 1))
+        _, _, _, stc = ctx.trace(sid, rays, N.MODE_CLOSEST | N.TRACE_COUNT, want_nid=False, want_bary=False)
+        out[set_name]["roofline_probe_rays"] = roofline(
+            plain_bytes(stc), out[set_name]["plain_binary"]["probe_ray_launch_ms"], l2_gbs, key,
+            "k_persistent<256, 0, 0, ProbePolicy> (probe rays, binary walk)", BYTES_PLAIN)
+        del rays
+    dirs = sets["octahedral"][0]
     # FP16 texel storage error against FP64 averaging of the same radiance
     desc = N.probe_desc(lo, hi, res, sun, sunc, len(dirs), 0.03, N.PROBE_OCTA | N.PROBE_WIDE)
     sh16 = np.zeros((7, res[2], res[1], res[0], 4), np.uint16)
