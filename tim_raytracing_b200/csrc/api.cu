@@ -151,7 +151,7 @@ int probe_plan(Scene* s, const tim_rt_probe_desc* desc, uint32_t probe_begin, ui
     }
     const uint32_t nd = desc->num_dirs, np = probe_end - probe_begin;
     const uint64_t n = (uint64_t)np * nd;
-    if (n * camera_queue_kinds() > 0xFFFFFFFFull) {
+    if (n * probe_queue_kinds() > 0xFFFFFFFFull) {
         set_error(w + ": too many probe rays in one call");
         return TIM_RT_EINVAL;
     }
@@ -810,8 +810,8 @@ int tim_rt_update_probes(tim_rt_ctx* c, tim_rt_scene_id id, const tim_rt_probe_d
     if ((rc = ensure(c, c->p_dirs, 16ull * nd)) || (rc = ensure(c, c->p_basis, 36ull * nd)) ||
         (rc = ensure(c, c->p_out, 32ull * n)) || (rc = ensure(c, c->p_nid, 4ull * n)) ||
         (rc = ensure(c, c->p_irr, 12ull * n)) || (rc = ensure(c, c->p_sh16, 56ull * total)) ||
-        (rc = ensure(c, c->q_rays, 32ull * n * camera_queue_kinds())) ||
-        (rc = ensure(c, c->q_pixel, 4ull * n * camera_queue_kinds())))
+        (rc = ensure(c, c->q_rays, 32ull * n * probe_queue_kinds())) ||
+        (rc = ensure(c, c->q_pixel, 4ull * n * probe_queue_kinds())))
         return rc;
     if (sh9_fp32 && (rc = ensure(c, c->p_sh32, 108ull * np))) return rc;
     if (octa && side && (rc = ensure(c, c->p_octa, 768ull * np))) return rc;

@@ -79,6 +79,9 @@ struct CameraBands {
 // [2 + 26 nb, 3 + 52 nb) their prefix (the last entry = secondary rays traced),
 // [3 + 52 nb, 3 + 53 nb) finished rays per band.
 uint32_t camera_queue_kinds();
+// Queue segments of a probe update (np*nd slots each): the sun and the 16 light
+// slots, the only kinds its shadow-ray generator emits.
+uint32_t probe_queue_kinds();
 constexpr uint32_t cam_counter_words(uint32_t nb) { return 3u + 53u * nb; }
 constexpr uint32_t kCamCounterWords = cam_counter_words(1), kCamTotalWord = 54;
 cudaError_t launch_camera(const SceneView& s, const tim_rt_pass_data& pd, uint32_t flags, uint32_t seed,

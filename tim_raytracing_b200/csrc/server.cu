@@ -110,7 +110,7 @@ struct ProbeStaging {
     uint64_t total() const { return dirs + basis + out + nid + irr + sh16 + qrays + qpix + ctr + octa; }
 };
 inline ProbeStaging probe_staging(const ProbePlan& P, bool octa) {
-    const uint64_t n = P.n, nd = P.args.nd, kinds = camera_queue_kinds();
+    const uint64_t n = P.n, nd = P.args.nd, kinds = probe_queue_kinds();
     ProbeStaging b;
     b.dirs = round256(16 * nd);
     b.basis = round256(36 * nd);

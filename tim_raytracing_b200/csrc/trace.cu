@@ -698,6 +698,7 @@ cudaError_t launch_trace_batch(const SceneView& s, const tim_rt_ray* rays, uint3
 
 uint32_t camera_queue_segment(uint32_t W, uint32_t H) { return W * H; }
 uint32_t camera_queue_kinds() { return kNumKinds; }
+uint32_t probe_queue_kinds() { return kKindProbe0; }
 
 cudaError_t launch_camera(const SceneView& s, const tim_rt_pass_data& pd, uint32_t flags, uint32_t seed,
                           const uint32_t* tile_counts, const uint32_t* tile_lists, uint32_t* out, uint32_t* bounce_out,
