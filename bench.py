@@ -12,8 +12,10 @@ Both the plain form (reference 64-B binary nodes) and the quantised form (8-wide
 8-bit child bounds) are timed; `value` is the faster form's Mrays/s (their records
 are identical), device time of the frame's CUDA graph (tile culling + primary +
 secondary generation + secondary trace) with the BVH resident in HBM and L2 flushed
-before each step. `e2e` runs the same frame through the host-pointer C-ABI calls
-(tile culling and tim_rt_trace_camera with pinned host buffers), copies included.
+before each step. `e2e` runs the same frame through the host-pointer C-ABI call,
+one per frame (tim_rt_trace_camera with pinned host buffers, the lights culled on the
+device, TIM_RT_CAM_DEVICE_CULL, and the records copied back band by band while the
+frame traces, TIM_RT_CAM_PIPELINED), copies included.
 
 On N GPUs (torchrun, one process per GPU) the same frame is split into N
 contiguous bands of output rows, balanced by a per-row cost estimate from a
@@ -1168,12 +1170,12 @@ def main():
 
     def e2e_step():
         if world == 1:
-            N._check(L.tim_rt_cull_lights(ctx.handle, sid, pdc.ctypes.data, tx, ty, counts_h.data_ptr(),
-                                          lists_h.data_ptr()))
+            # one call per frame: the pass data goes in, the lights are culled on the
+            # device, and the records come back to the pinned host buffers band by band
             st = N.Stats()
-            N._check(L.tim_rt_trace_camera(ctx.handle, sid, pdc.ctypes.data, FRAME_FLAGS | best_flags | N.CAM_PIPELINED,
-                                           1, counts_h.data_ptr(), lists_h.data_ptr(), out_h.data_ptr(),
-                                           bounce_h.data_ptr(), ctypes.byref(st)))
+            N._check(L.tim_rt_trace_camera(ctx.handle, sid, pdc.ctypes.data,
+                                           FRAME_FLAGS | best_flags | N.CAM_PIPELINED | N.CAM_DEVICE_CULL, 1,
+                                           None, None, out_h.data_ptr(), bounce_h.data_ptr(), ctypes.byref(st)))
             return st.rays
         # one band per rank: tile lists up, the band traced, the band's records down
         r0 = int(d_rays.item())
@@ -1204,8 +1206,10 @@ def main():
     # device path's records of the same frame, this rank's rows
     e2e_diff = int((out_h.view(H, W, 8)[row_b:row_e] != outs[best].cpu().view(H, W, 8)[row_b:row_e]).any(-1).sum() +
                    (bounce_h.view(H, W, 4)[row_b:row_e] != bounces[best].cpu().view(H, W, 4)[row_b:row_e]).any(-1).sum())
-    e2e_h2d = int(tx * ty * 68 + 240)
-    e2e_d2h = int(tx * ty * 68 + W * H * 48) if world == 1 else int(W * band_rows * 48)
+    # world 1: the pass data (240 B, the call's by-value kernel arguments) in, the
+    # frame's records out; N ranks: each rank's tile lists in, its band's records out
+    e2e_h2d = 240 if world == 1 else int(tx * ty * 68 + 240)
+    e2e_d2h = int(W * H * 48) if world == 1 else int(W * band_rows * 48)
 
     # Dominant kernel (the secondary trace): its launch duration from CUDA events
     # recorded around each phase on the context stream, and its work from the

@@ -403,6 +403,11 @@ int tim_rt_server_destroy(tim_rt_server *srv);
                                        each band's copy starts as soon as its records are final (same results) */
 #define TIM_RT_CAM_PRIMARY_BINARY 0x400u /* with TIM_RT_CAM_WIDE: primary rays take the binary walk (faster for
                                           coherent camera rays here; both walks give identical results) */
+#define TIM_RT_CAM_DEVICE_CULL 0x1000u /* tim_rt_trace_camera only, with TIM_RT_CAM_TILE_LIGHTS: the call culls the
+                                         lights itself on the device (the lists tim_rt_cull_lights returns, over
+                                         ceil(W/16) x ceil(H/16) tiles) right before the trace, as the reference's
+                                         culling feeds its camera pass on the GPU; tile_counts / tile_lists are not
+                                         read and may be NULL (same results) */
 int tim_rt_trace_camera(tim_rt_ctx *ctx, tim_rt_scene_id scene, const tim_rt_pass_data *pd, uint32_t flags,
                         uint32_t seed, const uint32_t *tile_counts, const uint32_t *tile_lists,
                         uint32_t *out, uint32_t *bounce_out, tim_rt_stats *stats);

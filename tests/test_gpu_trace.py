@@ -431,3 +431,45 @@ def test_camera_pipelined_bands_without_secondary_rays(ctx, native, oracle_mod):
                 assert st.rays == int(o_counts.sum())
     finally:
         ctx.free_scene(sid)
+
+
+@pytest.mark.gpu
+def test_camera_device_cull(ctx, native, oracle_mod):
+    """TIM_RT_CAM_DEVICE_CULL: tim_rt_trace_camera culls the tile lights on the device
+    itself (no host tile lists) and gives the oracle's records with the oracle's
+    culling, pipelined or not; it needs TIM_RT_CAM_TILE_LIGHTS and is refused by the
+    device-pointer forms."""
+    from tim_raytracing_b200 import scenes
+    s = scenes.heightfield_scene(seed=12, grid=32, n_spheres=6, n_lights=16, light_radius=5.0)
+    img = native.build_bvh(s)
+    sid = ctx.upload(img, s, quant8=True)
+    try:
+        W, H = 184, 136
+        pd = scenes.pass_data(s, W, H, aabb=(img.aabb[:3], img.aabb[3:]))
+        tx, ty = (W + 15) // 16, (H + 15) // 16
+        sc = oracle_mod.Scene(img, s.positions, s.normals)
+        counts, lists = oracle_mod.cull_lights(sc, pd, tx, ty)
+        flags = native.CAM_TILE_LIGHTS | native.CAM_BOUNCE
+        o_out, o_bounce, o_counts = oracle_mod.camera(sc, pd, flags=flags, seed=3, tile_counts=counts,
+                                                      tile_lists=lists)
+        assert int(counts.max()) > 0
+        for form in (0, native.CAM_WIDE | native.CAM_PRIMARY_BINARY):
+            for extra in (0, native.CAM_PIPELINED):
+                out, bounce, st = ctx.trace_camera(sid, pd, flags=flags | form | extra | native.CAM_DEVICE_CULL,
+                                                   seed=3)
+                assert np.array_equal(out, o_out)
+                assert np.array_equal(bounce, o_bounce)
+                assert st.rays == int(o_counts.sum())
+        with pytest.raises(native.TimRtError) as e:
+            ctx.trace_camera(sid, pd, flags=native.CAM_BOUNCE | native.CAM_DEVICE_CULL, seed=3)
+        assert e.value.code == native.EINVAL
+        import torch
+        d_out = torch.zeros((W * H, 8), dtype=torch.int32, device="cuda")
+        d_b = torch.zeros((W * H, 4), dtype=torch.int32, device="cuda")
+        d_c = torch.zeros(tx * ty, dtype=torch.int32, device="cuda")
+        d_l = torch.zeros(tx * ty * 16, dtype=torch.int32, device="cuda")
+        with pytest.raises(native.TimRtError) as e:
+            ctx.trace_camera_dev(sid, pd, flags | native.CAM_DEVICE_CULL, 3, d_c, d_l, d_out, d_b)
+        assert e.value.code == native.EINVAL
+    finally:
+        ctx.free_scene(sid)

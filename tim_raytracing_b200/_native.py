@@ -24,6 +24,7 @@ UPLOAD_QUANT8 = 0x2
 CAM_PROB_MASK, CAM_TILE_LIGHTS, CAM_BOUNCE, CAM_WIDE, CAM_COUNT = 1, 2, 4, 0x100, 0x200
 CAM_PRIMARY_BINARY = 0x400
 CAM_PIPELINED = 0x800
+CAM_DEVICE_CULL = 0x1000
 RANGE_BLAS, RANGE_TRI, RANGE_PRIM, RANGE_MAT, RANGE_LIGHT, RANGE_NODE, RANGE_LEAF = range(7)
 
 EXPORTED = [

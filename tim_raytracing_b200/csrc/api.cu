@@ -683,6 +683,11 @@ static int camera_dev_rows(tim_rt_ctx* c, tim_rt_scene_id id, const tim_rt_pass_
         set_error(std::string(who) + ": null output");
         return TIM_RT_EINVAL;
     }
+    if (flags & TIM_RT_CAM_DEVICE_CULL) {
+        set_error(std::string(who) + ": TIM_RT_CAM_DEVICE_CULL is for tim_rt_trace_camera (cull with "
+                                     "tim_rt_cull_lights_dev on the same stream instead)");
+        return TIM_RT_EINVAL;
+    }
     uint64_t qcap = 0;
     if ((rc = camera_prepare(c, s, pd, flags, d_tile_counts && d_tile_lists, d_bounce_out != nullptr, &qcap))) return rc;
     if (row_begin % 4u != 0u || row_begin >= row_end || row_end > pd->frameSize[1]) {
@@ -869,8 +874,14 @@ int tim_rt_trace_camera(tim_rt_ctx* c, tim_rt_scene_id id, const tim_rt_pass_dat
         set_error("tim_rt_trace_camera: null output");
         return TIM_RT_EINVAL;
     }
+    const bool device_cull = (flags & TIM_RT_CAM_DEVICE_CULL) != 0;
+    if (device_cull && !(flags & TIM_RT_CAM_TILE_LIGHTS)) {
+        set_error("tim_rt_trace_camera: TIM_RT_CAM_DEVICE_CULL needs TIM_RT_CAM_TILE_LIGHTS");
+        return TIM_RT_EINVAL;
+    }
     uint64_t qcap = 0;
-    if ((rc = camera_prepare(c, s, pd, flags, tile_counts && tile_lists, bounce_out != nullptr, &qcap))) return rc;
+    if ((rc = camera_prepare(c, s, pd, flags, device_cull || (tile_counts && tile_lists), bounce_out != nullptr, &qcap)))
+        return rc;
     const uint32_t W = pd->frameSize[0], H = pd->frameSize[1];
     const uint64_t npix = (uint64_t)W * H;
     const uint64_t tiles = (uint64_t)((W + 15) / 16) * ((H + 15) / 16);
@@ -881,7 +892,11 @@ int tim_rt_trace_camera(tim_rt_ctx* c, tim_rt_scene_id id, const tim_rt_pass_dat
         return rc;
     uint32_t* ctr = static_cast<uint32_t*>(c->counters.ptr);
     TIMRT_CUDA(cudaEventRecord(c->ev[0], c->stream));
-    if (flags & TIM_RT_CAM_TILE_LIGHTS) {
+    if (device_cull) {
+        TIMRT_CUDA(launch_cull_lights(s->view, *pd, (W + 15u) / 16u, (H + 15u) / 16u,
+                                      static_cast<uint32_t*>(c->tiles_counts.ptr),
+                                      static_cast<uint32_t*>(c->tiles_lists.ptr), c->stream));
+    } else if (flags & TIM_RT_CAM_TILE_LIGHTS) {
         TIMRT_CUDA(cudaMemcpyAsync(c->tiles_counts.ptr, tile_counts, 4ull * tiles, cudaMemcpyHostToDevice, c->stream));
         TIMRT_CUDA(cudaMemcpyAsync(c->tiles_lists.ptr, tile_lists, 64ull * tiles, cudaMemcpyHostToDevice, c->stream));
     }
