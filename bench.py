@@ -1285,7 +1285,14 @@ def main():
                         "shadow_masks_differing": mask_mismatch, "pixels": W * (row_e - row_b),
                         "compared": "plain vs quantised records of the same frame (rank 0's rows)"},
             "e2e": {"value": e2e_v, "unit": METRIC, "h2d_bytes_per_step": e2e_h2d, "d2h_bytes_per_step": e2e_d2h,
-                    "records_differing_vs_device_path": e2e_diff},
+                    "records_differing_vs_device_path": e2e_diff,
+                    "inputs": ("per step the frame's pass data (camera and sun, 240 B) goes in with the call and "
+                               "the lights are culled on the device (TIM_RT_CAM_DEVICE_CULL); the scene's BVH "
+                               "stays resident, uploaded once as the reference uploads it once per scene"
+                               if world == 1 else
+                               "per step each rank's tile lists and pass data go in; the scene stays resident"),
+                    "outputs": "the hit records (32 B) and bounce records (16 B) of every pixel of the frame "
+                               "(of the rank's band for N > 1), copied into pinned host buffers"},
             "gpu_launches": None, "clocks": clocks,
         }
         # our kernels per frame: cull, primary trace, secondary generation, kind prefix, secondary trace, ray count
