@@ -36,6 +36,21 @@ def test_binding_list_matches_header(native):
     assert sorted(native.EXPORTED) == declared_symbols()
 
 
+def test_binding_constants_match_header(native):
+    """Every flag, mode and error code the bindings name has the header's value."""
+    text = "\n".join(h.read_text() for h in (ROOT / "include").glob("*.h"))
+    defines = {m.group(1): int(m.group(2), 0)
+               for m in re.finditer(r"^#define TIM_RT_(\w+)\s+(0x[0-9a-fA-F]+|\d+)u?\b", text, flags=re.M)}
+    checked = 0
+    for name, value in defines.items():
+        if isinstance(getattr(native, name, None), int):
+            assert getattr(native, name) == value, name
+            checked += 1
+    for name in ("CAM_DEVICE_CULL", "CAM_PIPELINED", "CAM_PRIMARY_BINARY", "TRACE_TLAS", "PROBE_OCTA", "EINVAL"):
+        assert name in defines and getattr(native, name) == defines[name], name
+    assert checked >= 20
+
+
 def test_version_and_no_error(native):
     L = native.lib()
     assert b"sm_100a" in L.tim_rt_version()
