@@ -86,3 +86,23 @@ def test_python_bindings_check_host_buffers(native):
                        (np.zeros((4, 10), np.uint32).T, 40), ([0] * 40, 40)):
         with pytest.raises(ValueError):
             native._host_buf(bad, np.uint32, count, "hit")
+
+
+def test_header_is_c99_and_host_calls_work_from_c(native, tmp_path):
+    """include/tim_rt.h compiles as strict C99 (what a cgo or FFI binding parses),
+    and a C program linked with libtim_rt.so builds, validates and wide-checks a
+    BVH and has a malformed image refused (tests/c/abi_c_check.c; no GPU)."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    exe = tmp_path / "abi_c_check"
+    lib_dir = str(Path(native.LIB_PATH).parent)
+    r = subprocess.run([cc, "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror", "-I", str(ROOT / "include"),
+                        str(ROOT / "tests" / "c" / "abi_c_check.c"), "-L", lib_dir, "-ltim_rt",
+                        f"-Wl,-rpath,{lib_dir}", "-o", str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, (r.returncode, r.stdout, r.stderr)
+    assert r.stdout.startswith("ok ")
